@@ -1,0 +1,173 @@
+/*
+ * jfemgpu.h -- C ABI of the B200 SOL101 linear-static library (libjfemgpu.so).
+ *
+ * The library replaces the device-side half of OpenJFEM's SOL101 parity path:
+ * element stiffness (CQUAD4 / CQUAD8 / CTETRA10), assembly of the global
+ * stiffness K, the sparse Cholesky factorisation of K_ff and the triangular
+ * solves, residual and SPC-force recovery.  Parsing, SPC/AUTOSPC reduction
+ * and result output stay with the caller (the Julia host in the reference).
+ *
+ * Conventions
+ *   - Every pointer argument is a caller-owned HOST array; it is read (or
+ *     written) during the call only.  No pointer is retained after return.
+ *   - Indices are 0-based.  Node index n is the position of the GRID in the
+ *     sorted list of GRID ids (reference: src/solver/assembly.jl:2653-2665).
+ *     Global DOF d = 6*n + c, c in 0..5 = (T1,T2,T3,R1,R2,R3).
+ *   - Dense matrices are column-major (Julia layout): A[r + nrow*c].
+ *   - K is stored exactly like Julia's SparseMatrixCSC built by
+ *     sparse(I,J,V,ndof,ndof): colptr (ndof+1), rowval (nnz), nzval (nnz),
+ *     duplicates summed in triplet order, explicit zeros kept
+ *     (reference: src/solver/assembly.jl:5942, 5963-5974).
+ *   - Every function returns a jfg_status; on failure jfg_last_error()
+ *     returns a thread-local message.
+ */
+#ifndef JFEMGPU_H
+#define JFEMGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  JFG_OK = 0,
+  JFG_NOT_SPD = 1,          /* non-positive pivot; detail = permuted DOF index     */
+  JFG_IR_STALLED = 2,       /* iterative refinement did not reach the tolerance   */
+  JFG_OOM_BUDGET = 3,       /* request exceeds the device-memory budget           */
+  JFG_TIMEOUT = 4,          /* a bounded device wait expired                      */
+  JFG_UNSUPPORTED = 5,      /* element flags/geometry outside the supported path  */
+  JFG_BAD_INPUT = 6,        /* malformed arguments (sizes, indices, NaN, ...)     */
+  JFG_CUDA_ERROR = 7,       /* CUDA runtime error                                 */
+  JFG_NOT_READY = 8         /* call order violated (e.g. solve before factor)     */
+} jfg_status;
+
+typedef enum {
+  JFG_PREC_FP64 = 0,        /* plain FP64 supernodal Cholesky                      */
+  JFG_PREC_MIXED = 1        /* FP32-storage factor, 3xTF32 tensor-core updates,
+                               FP64 iterative refinement on the FP64 CSR matrix   */
+} jfg_precision;
+
+typedef struct jfg_ctx jfg_ctx;
+typedef struct jfg_model jfg_model;
+
+typedef struct {
+  int32_t device;           /* CUDA device ordinal                                */
+  int32_t flags;            /* reserved, 0                                        */
+  int64_t hbm_budget_bytes; /* 0 = no budget                                      */
+} jfg_config;
+
+/* Per-element section records (doubles, column-major 3x3 / 2x2 blocks). */
+#define JFG_Q4_SECT_STRIDE 26 /* Cm[9] Cb[9] Cs[4] h Eref k6rot flags              */
+#define JFG_Q8_SECT_STRIDE 22 /* A[9] D[9] shear(=Gts, INF=rigid) Dref hasA hasD  */
+#define JFG_T10_MAT_STRIDE 2  /* E nu                                             */
+
+/* Q4 section flag bits (flags word): only 0 is the supported default path.   */
+#define JFG_Q4_FLAG_DEFAULT 0
+
+typedef struct {
+  double rel_residual;      /* max over RHS of |K_ff u - F_ff| / |F_ff|            */
+  double max_rel_update;    /* last IR correction |du|/|u|                         */
+  int32_t ir_iters;         /* refinement steps taken                              */
+  int32_t fallback_used;    /* 1 when the FP64 factor replaced the mixed factor   */
+  int32_t precision;        /* precision of the factor that produced U            */
+  int32_t reserved;
+} jfg_solve_report;
+
+typedef struct {
+  int64_t n_supernodes;
+  int64_t n_levels;
+  int64_t nnz_L;            /* stored factor entries (lower, incl. diagonal)       */
+  double flops;             /* sum_j c_j^2 over the symbolic factor                */
+  int64_t factor_bytes;     /* device bytes of the factor                          */
+  int64_t max_front;        /* largest front order                                */
+} jfg_symbolic_info;
+
+/* ---- context ------------------------------------------------------------ */
+/* Replaces: nothing on the reference side (CPU); owns the CUDA stream.       */
+jfg_status jfg_create(jfg_ctx** ctx, const jfg_config* cfg);
+jfg_status jfg_destroy(jfg_ctx* ctx);
+const char* jfg_last_error(void);
+int64_t jfg_last_error_detail(void);
+
+/* ---- model upload ------------------------------------------------------- */
+/* Replaces the input side of Solver.assemble_stiffness
+ * (src/solver/assembly.jl:2630-2675 node indexing / node_R,
+ *  :3223-3480 per-element section arrays, :5806-5921 solid / CQUAD8 lists).
+ * xyz: n_nodes*3 (row per node); node_R: n_nodes*9 (3x3 column-major, the
+ * CD-frame rotation node_R of assembly.jl:2667-2675).
+ * q4_nodes: n_q4*4, q8_nodes: n_q8*8, t10_nodes: n_t10*10 (0-based node idx). */
+jfg_status jfg_model_upload(jfg_ctx* ctx, int64_t n_nodes, const double* xyz,
+                            const double* node_R, int64_t n_q4,
+                            const int32_t* q4_nodes, const double* q4_sect,
+                            int64_t n_q8, const int32_t* q8_nodes,
+                            const double* q8_sect, int64_t n_t10,
+                            const int32_t* t10_nodes, const double* t10_mat,
+                            jfg_model** out);
+jfg_status jfg_model_free(jfg_model* model);
+
+/* ---- assembly ------------------------------------------------------------ */
+/* Replaces Solver.assemble_stiffness's element loops and sparse()
+ * (src/solver/assembly.jl:3603-5335 Q4, :5806-5890 solids, :5893-5921 Q8,
+ *  :5942 sparse).  The first call builds the CSC pattern and the
+ * triplet->nzval slot map on the host; every call recomputes the values on
+ * the device (element kernels + deterministic slot-map gather).          */
+jfg_status jfg_assemble(jfg_model* model);
+jfg_status jfg_get_sizes(jfg_model* model, int64_t* ndof, int64_t* nnz,
+                         int64_t* n_triplets);
+jfg_status jfg_get_pattern(jfg_model* model, int64_t* colptr, int32_t* rowval);
+jfg_status jfg_get_values(jfg_model* model, double* nzval);
+jfg_status jfg_get_slot_map(jfg_model* model, int64_t* slot);
+/* max_elem_stiff and orig_diag of assembly.jl:5923-5936; diag has ndof entries. */
+jfg_status jfg_get_diag(jfg_model* model, double* diag, double* max_elem_stiff);
+/* 3x3 translational and rotational node blocks (column-major, 18 per node)
+ * consumed by the host's grid-point-singularity AUTOSPC
+ * (src/solver/boundary_conditions.jl:745-845).                            */
+jfg_status jfg_get_node_blocks(jfg_model* model, double* blocks);
+/* Element stiffness in the global frame, as captured by element_capture
+ * (assembly.jl:5333, 5885, 5918).  kind: 0=Q4 (24x24), 1=Q8 (48x48),
+ * 2=T10 (30x30).                                                          */
+jfg_status jfg_get_element_matrix(jfg_model* model, int32_t kind, int64_t elem,
+                                  double* Ke);
+
+/* ---- partition + symbolic analysis ---------------------------------------- */
+/* Replaces K_ff = K[free,free] (src/solver/boundary_conditions.jl:1591-1610)
+ * and the symbolic half of cholesky(Symmetric(K_ff)) (:1660): nested-
+ * dissection ordering, elimination tree, supernodes, front maps.  free_dofs
+ * must be strictly ascending global DOF indices.                          */
+jfg_status jfg_set_free_dofs(jfg_model* model, int64_t n_free,
+                             const int32_t* free_dofs);
+jfg_status jfg_get_symbolic_info(jfg_model* model, jfg_symbolic_info* info);
+/* Fill-reducing permutation (F.p of the factor object, :1666): perm[k] = the
+ * position in free_dofs of the k-th eliminated unknown.                   */
+jfg_status jfg_get_perm(jfg_model* model, int32_t* perm);
+
+/* ---- numeric factorisation and solves ------------------------------------ */
+/* Replaces cholesky(Symmetric(K_ff)) numeric phase (:1656-1660).          */
+jfg_status jfg_factor(jfg_model* model, int32_t precision);
+/* diag(F) in permuted order (:1663): L_ii of the FP64 or mixed factor.     */
+jfg_status jfg_get_factor_diag(jfg_model* model, double* Ldiag);
+/* Replaces F \ F_ff (:1714, cached path :1442) for nrhs load cases at once.
+ * F and U are ndof x nrhs column-major GLOBAL vectors; U is zero at fixed
+ * DOFs.  tol is the relative residual target of iterative refinement
+ * (<= 0: 1e-10), max_ir the refinement-step cap (<0: 10).                  */
+jfg_status jfg_solve(jfg_model* model, int32_t nrhs, const double* F,
+                     double* U, double tol, int32_t max_ir,
+                     jfg_solve_report* report);
+/* R = K*U - F over all ndof (solve_case.jl:1200); SPC forces are R at the
+ * fixed DOFs (solve_case.jl:212-262).                                       */
+jfg_status jfg_residual(jfg_model* model, int32_t nrhs, const double* U,
+                        const double* F, double* R);
+
+/* ---- re-solve fast paths --------------------------------------------------- */
+/* New Q4 sections for a subset of elements (thickness change): element +
+ * assembly values are recomputed on the next jfg_assemble; the symbolic
+ * analysis is kept (warm_model_session.jl:39-99 re-solve without re-parse). */
+jfg_status jfg_update_q4_sections(jfg_model* model, int64_t n,
+                                  const int32_t* q4_elems,
+                                  const double* q4_sect);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* JFEMGPU_H */

@@ -1,0 +1,250 @@
+"""Python side of the CPU oracle (test infrastructure, not product code).
+
+Restates OpenJFEM's SOL101 host-side partition (SPC1 + AUTOSPC) in numpy and
+wraps the C++ element/assembly restatement in ``oracle_fem.cpp``.  Only the
+tests, the smoke check and the CPU-baseline leg of ``bench.py`` use this
+module, always as the checker of the CUDA library, never as a product path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import Optional, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile oracle_fem.cpp + oracle_chol.cpp into _build/liboracle.so."""
+    srcs = [os.path.join(HERE, f) for f in ("oracle_fem.cpp", "oracle_chol.cpp")]
+    os.makedirs(os.path.dirname(LIB_PATH), exist_ok=True)
+    if not force and os.path.exists(LIB_PATH):
+        lib_m = os.path.getmtime(LIB_PATH)
+        if all(os.path.getmtime(s) <= lib_m for s in srcs):
+            return LIB_PATH
+    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-o", LIB_PATH] + srcs + ["-ldl"]
+    subprocess.check_call(cmd)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(LIB_PATH)
+        d, i32, i64 = ctypes.c_double, ctypes.c_int32, ctypes.c_int64
+        P = ctypes.c_void_p
+        L.or_q4_local.argtypes = [P, P, P, P, d, d, d, P]
+        L.or_q4_element.argtypes = [P, P, P, P]
+        L.or_q8_element.argtypes = [P, P, P, P]
+        L.or_q8_parallelogram.argtypes = [P]
+        L.or_t10_element.argtypes = [P, P, d, d, P]
+        L.or_assemble_triplets.argtypes = [i64, P, P, i64, P, P, i64, P, P, i64, P, P, i64, P, P, P, P]
+        L.or_assemble_triplets.restype = i64
+        L.or_build_csc.argtypes = [i64, i64, P, P, P, P, P, P, P]
+        L.or_build_csc.restype = i64
+        L.or_csc_matvec.argtypes = [i64, P, P, P, i32, P, P]
+        for name in ("or_q4_local", "or_q4_element", "or_q8_element", "or_q8_parallelogram", "or_t10_element"):
+            getattr(L, name).restype = ctypes.c_int
+        L.or_chol_factor_solve.argtypes = [i64, P, P, P, P, i32, P, P, i32, P]
+        L.or_chol_factor_solve.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def q4_local(lc, Cm, Cb, Cs, h, k6rot, drill_scale=1.0):
+    lc = np.asfortranarray(lc, dtype=np.float64)
+    Ke = np.zeros((24, 24), order="F")
+    st = lib().or_q4_local(_p(lc), _p(np.asfortranarray(Cm, float)), _p(np.asfortranarray(Cb, float)),
+                           _p(np.asfortranarray(Cs, float)), float(h), float(k6rot), float(drill_scale), _p(Ke))
+    if st:
+        raise ValueError(f"or_q4_local status {st}")
+    return Ke
+
+
+def _ident_R(n):
+    R = np.zeros((n, 9)); R[:, 0] = R[:, 4] = R[:, 8] = 1.0
+    return R
+
+
+def q4_element(xyz, sect, nodeR=None):
+    xyz = np.ascontiguousarray(xyz, float)
+    R = np.ascontiguousarray(_ident_R(4) if nodeR is None else nodeR, float)
+    Ke = np.zeros((24, 24), order="F")
+    st = lib().or_q4_element(_p(xyz), _p(R), _p(np.ascontiguousarray(sect, float)), _p(Ke))
+    if st:
+        raise ValueError(f"or_q4_element status {st}")
+    return Ke
+
+
+def q8_element(xyz, sect, nodeR=None):
+    xyz = np.ascontiguousarray(xyz, float)
+    R = np.ascontiguousarray(_ident_R(8) if nodeR is None else nodeR, float)
+    Ke = np.zeros((48, 48), order="F")
+    st = lib().or_q8_element(_p(xyz), _p(R), _p(np.ascontiguousarray(sect, float)), _p(Ke))
+    if st:
+        raise ValueError(f"or_q8_element status {st}")
+    return Ke
+
+
+def t10_element(xyz, E, nu, nodeR=None):
+    xyz = np.ascontiguousarray(xyz, float)
+    R = np.ascontiguousarray(_ident_R(10) if nodeR is None else nodeR, float)
+    Ke = np.zeros((30, 30), order="F")
+    st = lib().or_t10_element(_p(xyz), _p(R), float(E), float(nu), _p(Ke))
+    if st:
+        raise ValueError(f"or_t10_element status {st}")
+    return Ke
+
+
+def assemble(model):
+    """Triplets in reference order and Julia's sparse() CSC + slot map."""
+    L = lib()
+    xyz = np.ascontiguousarray(model.xyz, float)
+    R = np.ascontiguousarray(model.node_R, float)
+    q4n = np.ascontiguousarray(model.q4_nodes, np.int32)
+    q4s = np.ascontiguousarray(model.q4_sections())
+    q8n = np.ascontiguousarray(model.q8_nodes, np.int32)
+    q8s = np.ascontiguousarray(model.q8_sections())
+    t10n = np.ascontiguousarray(model.t10_nodes, np.int32)
+    t10m = np.ascontiguousarray(model.t10_materials())
+    cap = 576 * len(q4n) + 900 * len(t10n) + 2304 * len(q8n)
+    I = np.empty(cap, np.int64); J = np.empty(cap, np.int64); V = np.empty(cap)
+    err = np.full(1, -1, np.int32)
+    nt = L.or_assemble_triplets(model.n_nodes, _p(xyz), _p(R), len(q4n), _p(q4n), _p(q4s),
+                                len(q8n), _p(q8n), _p(q8s), len(t10n), _p(t10n), _p(t10m),
+                                cap, _p(I), _p(J), _p(V), _p(err))
+    if nt < 0:
+        raise ValueError(f"element {err[0]} failed with status {-nt}")
+    I, J, V = I[:nt], J[:nt], V[:nt]
+    n = model.ndof
+    colptr = np.empty(n + 1, np.int64)
+    rowval = np.empty(nt, np.int32)
+    nzval = np.empty(nt)
+    slot = np.empty(nt, np.int64)
+    nnz = L.or_build_csc(n, nt, _p(I), _p(J), _p(V), _p(colptr), _p(rowval), _p(nzval), _p(slot))
+    return dict(colptr=colptr, rowval=rowval[:nnz].copy(), nzval=nzval[:nnz].copy(), slot=slot,
+                I=I, J=J, V=V, ndof=n)
+
+
+def csc_matrix(asm):
+    import scipy.sparse as sp
+    n = asm["ndof"]
+    return sp.csc_matrix((asm["nzval"], asm["rowval"], asm["colptr"]), shape=(n, n))
+
+
+# ----------------------------------------------------------------------------
+# Partition (boundary_conditions.jl:1028-1138 diagonal AUTOSPC, :745-845 GPST)
+# ----------------------------------------------------------------------------
+
+def partition(model, K, eps_zero: float = 1e-8) -> Tuple[np.ndarray, np.ndarray, dict]:
+    """Fixed set = SPC1 u zero-diagonal AUTOSPC u grid-point singularities.
+
+    With grid-point-singularity processing on (the reference default) the
+    diagonal pass fixes exact zeros only; GPST then eigen-decomposes every
+    node's free 3x3 translational / rotational block and fixes the DOF the
+    eigenvector of each eigenvalue below eps_zero * lambda_max lies closest to.
+    Returns (free_dofs ascending, fixed_dofs ascending, diagnostics).
+    """
+    n = model.ndof
+    fixed = np.zeros(n, bool)
+    fixed[model.spc_dofs()] = True
+    diag = np.asarray(K.diagonal()).copy()
+    zero = (~fixed) & (diag == 0.0)
+    fixed |= zero
+    n_gpst = 0
+    Kc = K.tocsc()
+    nn = n // 6
+    for node in range(nn):
+        base = 6 * node
+        for off in (0, 3):
+            loc = [a for a in range(3) if not fixed[base + off + a]]
+            if not loc:
+                continue
+            idx = [base + off + a for a in loc]
+            blk = Kc[idx][:, idx].toarray()
+            S = 0.5 * (blk + blk.T)
+            vals, vecs = np.linalg.eigh(S)
+            lam = np.max(np.abs(vals))
+            if not lam > 0:
+                continue
+            claimed = set()
+            for k in range(len(loc)):
+                ratio = abs(vals[k]) / lam
+                if not ratio < eps_zero:
+                    continue
+                best_a, best_w = -1, -1.0
+                for ii, a in enumerate(loc):
+                    w = abs(vecs[ii, k])
+                    if a in claimed:
+                        continue
+                    if w > best_w + 1e-12:
+                        best_w, best_a = w, a
+                if best_a < 0:
+                    continue
+                g = base + off + best_a
+                if fixed[g]:
+                    continue
+                claimed.add(best_a)
+                fixed[g] = True
+                n_gpst += 1
+    free = np.where(~fixed)[0].astype(np.int32)
+    return free, np.where(fixed)[0], {"autospc_zero": int(zero.sum()), "autospc_gpst": n_gpst}
+
+
+def solve_reference(model, asm=None, free=None):
+    """FP64 SOL101 on the CPU with SciPy's SuperLU (independent small-case checker).
+
+    Returns dict(u (ndof x nrhs), F, R = K u - F, free, rel_residual).
+    """
+    import scipy.sparse.linalg as spla
+    if asm is None:
+        asm = assemble(model)
+    K = csc_matrix(asm)
+    if free is None:
+        free, _, _ = partition(model, K)
+    F = model.load_matrix()
+    Kff = K[free][:, free].tocsc()
+    # Symmetric(K_ff) (upper triangle) is what the reference factorises
+    import scipy.sparse as sp
+    U = sp.triu(Kff, format="csc")
+    A = (U + sp.triu(U, k=1, format="csc").T).tocsc()
+    lu = spla.splu(A, permc_spec="MMD_AT_PLUS_A")
+    u_ff = lu.solve(np.asfortranarray(F[free]))
+    u = np.zeros_like(F)
+    u[free] = u_ff
+    R = K @ u - F
+    rel = np.linalg.norm(Kff @ u_ff - F[free], axis=0) / np.maximum(np.linalg.norm(F[free], axis=0), 1e-300)
+    return dict(u=u, F=F, R=R, free=free, rel_residual=rel, asm=asm)
+
+
+def chol_solve(n, colptr, rowval, nzval, perm, F, nthreads=0):
+    """Oracle supernodal multifrontal FP64 Cholesky (OpenBLAS dense kernels).
+
+    (colptr,rowval,nzval): CSC of K_ff; only the upper triangle (row <= col)
+    is read, as Symmetric(K_ff) does.  perm: elimination order (perm[k] =
+    unknown eliminated k-th).  F: n x nrhs.  Returns U (n x nrhs).
+    """
+    L = lib()
+    F = np.asfortranarray(F, dtype=np.float64)
+    if F.ndim == 1:
+        F = F[:, None]
+    U = np.zeros_like(F, order="F")
+    info = np.zeros(4)
+    st = L.or_chol_factor_solve(int(n), _p(np.ascontiguousarray(colptr, np.int64)),
+                                _p(np.ascontiguousarray(rowval, np.int32)),
+                                _p(np.ascontiguousarray(nzval, np.float64)),
+                                _p(np.ascontiguousarray(perm, np.int32)), int(F.shape[1]),
+                                _p(F), _p(U), int(nthreads), _p(info))
+    if st != 0:
+        raise RuntimeError(f"oracle cholesky failed: status {st}, info {info}")
+    return U, dict(factor_s=info[0], solve_s=info[1], nnz_L=info[2], flops=info[3])
