@@ -1,0 +1,356 @@
+"""SOL101 throughput benchmark (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision fp64|mixed] [--workload wing_panel|plate|solid_block]
+
+Workload (default): the stiffened wing-box panel -- 200x400 CQUAD4 skin plus 9
+blade stiffeners of 20x400 CQUAD4 (152,781 GRIDs, 916,686 DOF, 914,400 free),
+8 subcases.  One step = one SOL101 analysis of that model on the device:
+element kernels + slot-map assembly + numeric Cholesky + forward/backward
+solves of the 8 subcases with FP64 refinement to relative residual 1e-10.
+The symbolic analysis and the CSC pattern are built once per mesh, before the
+timed region (the device-resident model registry keeps them).
+
+value  = SOL101 solves/s with the model and the load matrix resident in HBM.
+e2e    = the same through the public C ABI with host buffers: every step
+         copies the 8 load cases host->device and the 8 displacement fields
+         device->host (jfg_solve with host arrays).
+Multi-GPU: replicas only -- every rank solves its own copy; value is the sum
+over ranks of solves divided by the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SOL101 solves/s & p50/p99 latency, mixed+IR vs FP64 Cholesky, resid<=1e-10"
+
+
+def make_workload(name: str):
+    from jf_2026_05_25_b200 import model as M
+    if name == "wing_panel":
+        return M.wing_panel(), {"workload": "wing_panel_200x400_9blades_20x400", "grids": 152781,
+                                "cquad4": 152000, "ndof": 916686, "free_dof": 914400, "subcases": 8}
+    if name == "plate":
+        return M.flat_plate(), {"workload": "flat_plate_20x20", "grids": 441, "ndof": 2646, "subcases": 1}
+    if name == "solid_block":
+        return M.solid_block(), {"workload": "solid_block_40cube_ctetra10", "grids": 531441, "ctetra10": 384000,
+                                 "ndof": 3188646, "subcases": 4}
+    raise ValueError(name)
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU arms
+def cpu_sol101(mdl, free, perm, nthreads):
+    """The CPU restatement of the reference path (oracle): element loop,
+    sparse() CSC, K_ff, supernodal Cholesky with OpenBLAS, one RHS at a time."""
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    asm = O.assemble(mdl)
+    K = O.csc_matrix(asm)
+    Kff = K[free][:, free].tocsc()
+    t1 = time.perf_counter()
+    F = mdl.load_matrix()[free]
+    U, info = O.chol_solve(len(free), Kff.indptr.astype(np.int64), Kff.indices, Kff.data, perm, F, nthreads=nthreads)
+    t2 = time.perf_counter()
+    return dict(assembly_s=t1 - t0, factor_s=info["factor_s"], solve_s=info["solve_s"], total_s=t2 - t0,
+                flops=info["flops"], nnz_L=info["nnz_L"])
+
+
+def free_and_perm_host(mdl):
+    """Free set and ordering computed by the host code (no device)."""
+    from jf_2026_05_25_b200 import lib
+    from jf_2026_05_25_b200 import backend as B
+    from oracle import oracle as O
+    asm = O.assemble(mdl)
+    K = O.csc_matrix(asm)
+    Kc = K.tocsc()
+    nn = mdl.n_nodes
+    blocks = np.zeros((nn, 18))
+    # node blocks from the CSC (vectorised over the 6x6 diagonal blocks)
+    for off in (0, 1):
+        for b in range(3):
+            for a in range(3):
+                rows = 6 * np.arange(nn) + 3 * off + a
+                cols = 6 * np.arange(nn) + 3 * off + b
+                blocks[:, 9 * off + a + 3 * b] = np.asarray(Kc[rows, cols]).ravel()
+    free, fixed, _ = B.compute_free_dofs(mdl, K.diagonal(), blocks)
+    _, perm = lib.symbolic_dry_run(asm["colptr"], asm["rowval"], free, mdl.xyz)
+    return free, perm
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    os.environ.setdefault("JFEM_ORACLE_OPENBLAS", _openblas())
+    mdl, cfg = make_workload(args.workload)
+    nthreads = os.cpu_count() or 1
+    free, perm = free_and_perm_host(mdl)
+    times = []
+    for k in range(args.warmup + args.steps):
+        r = cpu_sol101(mdl, free, perm, nthreads)
+        if k >= args.warmup:
+            times.append(r["total_s"])
+    ms = 1000.0 * float(np.mean(times))
+    value = 1000.0 / ms
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": dict(cfg, parallelism="cpu", precision="fp64",
+                           note="CPU restatement of the reference SOL101 path (Julia/CHOLMOD unavailable on this box)"),
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nthreads, "kind": "port",
+                             "sample": f"full {cfg['workload']} SOL101 per step (assembly, sparse(), K_ff, "
+                                       f"supernodal Cholesky, {cfg['subcases']} single-RHS solves)"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "stages_s": r}
+    print(json.dumps(line), flush=True)
+
+
+def _openblas():
+    import glob
+    import scipy
+    c = glob.glob(os.path.join(os.path.dirname(scipy.__file__), "..", "scipy.libs", "libscipy_openblas-*.so"))
+    return os.path.abspath(c[0]) if c else ""
+
+
+# ---------------------------------------------------------------- device arm
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from jf_2026_05_25_b200 import backend as B
+    from jf_2026_05_25_b200 import lib
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local_rank))
+    L = lib.load()
+    prec = lib.PREC_MIXED if args.precision == "mixed" else lib.PREC_FP64
+    mdl, cfg = make_workload(args.workload)
+    be = B.JFEMGPUBackend(device=local_rank, precision=prec, tol=1e-10)
+    st = B.prepare(be, mdl)
+    dm = st["dm"]
+    sym = dm.symbolic_info()
+    F = mdl.load_matrix()
+    nrhs = F.shape[1]
+    dF = torch.from_numpy(np.asarray(F, order="F").T.copy()).to("cuda")   # [nrhs, ndof] == column-major ndof x nrhs
+    dU = torch.zeros_like(dF)
+    hF = torch.from_numpy(np.ascontiguousarray(np.asarray(F, order="F").T)).pin_memory()
+    hU = torch.zeros_like(hF).pin_memory()
+    stream = torch.cuda.current_stream()
+
+    def step_device():
+        dm.assemble()
+        dm.factor(prec)
+        return dm.solve_device(dF.data_ptr(), dU.data_ptr(), nrhs, 1e-10, 10)
+
+    def step_e2e():
+        dm.assemble()
+        dm.factor(prec)
+        rep = lib.SolveReport()
+        lib._check(L.jfg_solve(dm.h, nrhs, lib.P(hF.data_ptr()), lib.P(hU.data_ptr()), 1e-10, 10,
+                               lib._c.byref(rep)))
+        return rep.as_dict()
+
+    for _ in range(args.warmup):
+        rep = step_device()
+    # ---- timed region (device-resident inputs)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    L.jfg_reset_kernel_stats()
+    L.jfg_set_profiling(1)
+    launches0 = L.jfg_launch_count()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    t_wall0 = time.perf_counter()
+    reps = []
+    for _ in range(args.steps):
+        reps.append(step_device())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter() - t_wall0
+    launches = L.jfg_launch_count() - launches0
+    L.jfg_set_profiling(0)
+    # The library runs on its own stream and synchronises before returning, so
+    # the host interval between two device synchronisations brackets exactly
+    # the device work of the K steps; the torch events on the current stream
+    # give the same interval on the device clock.
+    ms_dev = max(e0.elapsed_time(e1), 1000.0 * t_wall)
+    if world > 1:
+        tt = torch.tensor([ms_dev], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_dev = float(tt.item())
+        dist.barrier()
+    clk = clocks.stop()
+    stats = {}
+    for which, name in ((0, "schur_update"), (1, "q4_element"), (2, "assembly_gather"), (3, "solves"),
+                        (4, "t10_element")):
+        o = np.zeros(3)
+        L.jfg_get_kernel_stats(which, o.ctypes.data_as(lib.P))
+        if o[0] > 0:
+            stats[name] = {"launches": int(o[0]), "ms": float(o[1]), "units": float(o[2])}
+    ms_step = ms_dev / args.steps
+    value = world * args.steps / (ms_dev / 1000.0)
+    # ---- e2e through the public API with host buffers
+    for _ in range(1):
+        step_e2e()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step_e2e()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        tt = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e_value = world * args.steps / e2e_s
+    # ---- roofline of the dominant kernel
+    peaks = _peaks()
+    dom = max(stats.items(), key=lambda kv: kv[1]["ms"]) if stats else None
+    roof = None
+    if dom:
+        name, s = dom
+        if name == "schur_update":
+            achieved = s["units"] / (s["ms"] / 1000.0) / 1e12
+            if prec == lib.PREC_MIXED:
+                peak, src = peaks["tf32x3_tflops"], peaks["src"] + " bf16/2/3 (3xTF32)"
+            else:
+                peak, src = peaks["fp64_tflops"], "nominal B200 FP64 40 TFLOP/s (no measured FP64 peak)"
+            roof = {"kernel": name, "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved / peak, "traffic": None, "peak_source": src,
+                    "launches": s["launches"], "ms_total": s["ms"]}
+        else:
+            achieved = s["units"] / (s["ms"] / 1000.0) / 1e9
+            peak = peaks["hbm_gbs"]
+            roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "traffic": None, "peak_source": peaks["src"] + " hbm_gbs",
+                    "launches": s["launches"], "ms_total": s["ms"]}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        os.environ.setdefault("JFEM_ORACLE_OPENBLAS", _openblas())
+        nthreads = os.cpu_count() or 1
+        r = cpu_sol101(mdl, st["free"], dm.perm(), nthreads)
+        cpu = {"value": 1.0 / r["total_s"], "unit": "solves/s", "cores": nthreads, "kind": "port",
+               "sample": f"one full {cfg['workload']} SOL101 (assembly, sparse(), K_ff, supernodal Cholesky with "
+                         f"OpenBLAS, {cfg['subcases']} single-RHS solves); same ordering as the device",
+               "stages_s": r}
+    rep = reps[-1]
+    tflops_factor = sym["flops"] / 1e12
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if prec == lib.PREC_FP64 else "f32+f64",
+            "data": "synthetic",
+            "config": dict(cfg, parallelism=f"replicas{world}", precision=args.precision,
+                           l2="inputs larger than L2 (factor %.1f GB)" % (sym["nnz_L"] * (8 if prec == 0 else 4) / 1e9)),
+            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(F.nbytes),
+                    "d2h_bytes_per_step": int(F.nbytes)},
+            "gpu_launches": int(launches),
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+            "detail": {"rel_residual": rep["rel_residual"], "ir_iters": rep["ir_iters"],
+                       "fallback_used": rep["fallback_used"], "subcase_solves_per_s": value * nrhs,
+                       "factor_tflop": tflops_factor, "factor_tflops_per_s": tflops_factor / (ms_step / 1000.0),
+                       "dof_per_s_assembled": cfg["ndof"] * value, "symbolic": sym, "kernel_stats": stats,
+                       "phase_s_last_step": dm.timings()}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    dm.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": d["hbm_gbs"], "tf32x3_tflops": d["bf16_tflops"] / 2 / 3, "fp64_tflops": 40.0,
+                "src": "MEASURED_PEAKS.json (measured)"}
+    return {"hbm_gbs": 6650.0, "tf32x3_tflops": 1590.0 / 2 / 3, "fp64_tflops": 40.0, "src": "fallback"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--workload", default="wing_panel", choices=["wing_panel", "plate", "solid_block"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus if "RANK" in os.environ else 1)))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -159,6 +159,34 @@ jfg_status jfg_solve(jfg_model* model, int32_t nrhs, const double* F,
 jfg_status jfg_residual(jfg_model* model, int32_t nrhs, const double* U,
                         const double* F, double* R);
 
+/* Same as jfg_solve with F and U in DEVICE memory (ndof x nrhs, column-major). */
+jfg_status jfg_solve_device(jfg_model* model, int32_t nrhs, const double* F_dev,
+                            double* U_dev, double tol, int32_t max_ir,
+                            jfg_solve_report* report);
+/* Device time of the last element, assembly, factor and solve calls (s). */
+jfg_status jfg_get_timings(jfg_model* model, double* seconds4);
+
+/* ---- instrumentation ----------------------------------------------------- */
+/* Number of kernels this library has launched since load.                   */
+int64_t jfg_launch_count(void);
+/* When on, the library brackets the launches of its main kernels with CUDA
+ * events on its stream and accumulates, per kernel class, launches, device
+ * milliseconds and algorithmic work (which: 0 = Schur-complement update,
+ * flops; 1 = CQUAD4 element kernel, bytes; 2 = assembly gather, bytes;
+ * 3 = triangular solves, bytes; 4 = CTETRA10 element kernel, bytes).        */
+jfg_status jfg_set_profiling(int32_t on);
+jfg_status jfg_get_kernel_stats(int32_t which, double* out3);
+jfg_status jfg_reset_kernel_stats(void);
+
+/* ---- host-only analysis (no device needed) ----------------------------------- */
+/* Runs the symbolic analysis of jfg_set_free_dofs on a given pattern and
+ * returns its summary and permutation; used to check the ordering on hosts
+ * without a GPU.  colptr/rowval: CSC pattern of K (ndof = 6*n_nodes).       */
+jfg_status jfg_symbolic_dry_run(int64_t ndof, const int64_t* colptr,
+                                const int32_t* rowval, int64_t n_free,
+                                const int32_t* free_dofs, const double* xyz,
+                                jfg_symbolic_info* info, int32_t* perm);
+
 /* ---- re-solve fast paths --------------------------------------------------- */
 /* New Q4 sections for a subset of elements (thickness change): element +
  * assembly values are recomputed on the next jfg_assemble; the symbolic

@@ -1,0 +1,74 @@
+"""Build libjfemgpu.so (sm_100a) in-tree with nvcc.
+
+    python -m jf_2026_05_25_b200.build [--force] [--debug]
+
+The shared library lands next to this file so that it travels with the
+source tree; object files go to ``_build/`` (git-ignored).
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import glob
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(PKG, "csrc")
+BUILD = os.path.join(PKG, "_build")
+LIB = os.path.join(PKG, "libjfemgpu.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _sources():
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
+
+
+def _headers():
+    return sorted(glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) +
+                  [os.path.join(PKG, "..", "include", "jfemgpu.h")])
+
+
+def _needs_build(force: bool) -> bool:
+    if force or not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    return any(os.path.getmtime(f) > t for f in _sources() + _headers() + [__file__])
+
+
+def build(force: bool = False, debug: bool = False, verbose: bool = False) -> str:
+    if not _needs_build(force):
+        return LIB
+    os.makedirs(BUILD, exist_ok=True)
+    opt = ["-O0", "-g", "-G"] if debug else ["-O3", "-lineinfo"]
+    common = ARCH + opt + ["-std=c++17", "-Xcompiler", "-fPIC,-fopenmp", "-I", CSRC]
+    if verbose:
+        common += ["-Xptxas", "-v"]
+
+    def compile_one(src):
+        obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+        cmd = [NVCC] + common + ["-c", src, "-o", obj]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}\n{r.stderr}")
+        return obj, r.stderr
+
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
+        results = list(ex.map(compile_one, _sources()))
+    if verbose:
+        for _, err in results:
+            sys.stderr.write(err)
+    objs = [o for o, _ in results]
+    tmp = LIB + ".tmp"
+    cmd = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-Xcompiler", "-fopenmp", "-lgomp"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, debug="--debug" in sys.argv, verbose="-v" in sys.argv)
+    print(LIB)

@@ -1,0 +1,278 @@
+// assembly.cu -- global CSC pattern, triplet slot map and the device assembly.
+//
+// Semantics of K = sparse(I,J,V,ndof,ndof) (src/solver/assembly.jl:5942):
+// pattern = every (I,J) emitted by an element (explicit zeros kept); values =
+// duplicates combined left to right in triplet order (:5963-5974).  The
+// triplet order is the element order: all CQUAD4 (positional slots
+// (ei-1)*576, :3506-3508), then the CTETRA10 (900 each, :5882-5884).
+//
+// The pattern is built once per mesh on the host from the node-pair blocks of
+// the connectivity.  The device assembly is a gather: every CSC entry sums its
+// own contributions, in triplet order, from the element value buffer -- no
+// atomics, bitwise deterministic, and the same summation order as Julia.
+#include <omp.h>
+
+#include <algorithm>
+
+#include "jfg_internal.h"
+
+namespace jfg {
+namespace {
+
+constexpr uint64_t MASK_Q4 = (1ull << 36) - 1;   // all 6x6 component pairs
+uint64_t mask_t10() {
+  uint64_t m = 0;
+  for (int j = 0; j < 3; ++j)
+    for (int i = 0; i < 3; ++i) m |= 1ull << (i + 6 * j);
+  return m;
+}
+
+struct ElemRef {
+  int64_t e;        // global element order: Q4 first, then T10
+  int8_t local;     // local index of the column node in the element
+};
+
+__global__ void k_assemble(int64_t nnz, const int32_t* __restrict__ nzptr,
+                           const int32_t* __restrict__ trip, const double* __restrict__ ev,
+                           double* __restrict__ nzval) {
+  int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nnz) return;
+  int32_t a = nzptr[q], b = nzptr[q + 1];
+  double v = ev[trip[a]];
+  for (int32_t k = a + 1; k < b; ++k) v = v + ev[trip[k]];
+  nzval[q] = v;
+}
+
+// y = K x with K in CSC and a structurally symmetric pattern: row i of K is
+// gathered through the transpose positions (one warp per row).
+__global__ void k_spmv(int64_t n, const int64_t* __restrict__ colptr, const int32_t* __restrict__ rowval,
+                       const int64_t* __restrict__ tpos, const double* __restrict__ nzval, int nrhs,
+                       const double* __restrict__ x, int64_t ldx, double* __restrict__ y, int64_t ldy) {
+  int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  int64_t a = colptr[row], b = colptr[row + 1];
+  for (int r0 = 0; r0 < nrhs; r0 += 8) {
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int nr = min(8, nrhs - r0);
+    for (int64_t p = a + lane; p < b; p += 32) {
+      double kv = nzval[tpos[p]];
+      int64_t col = rowval[p];
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        if (k < nr) acc[k] += kv * x[col + ldx * (r0 + k)];
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      double v = acc[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0 && k < nr) y[row + ldy * (r0 + k)] = v;
+    }
+  }
+}
+
+}  // namespace
+
+jfg_status build_pattern(jfg_model* m) {
+  if (m->n_q8 > 0) {
+    set_error("CQUAD8 pattern requires the CQUAD8 device kernel");
+    return JFG_UNSUPPORTED;
+  }
+  const int64_t nn = m->n_nodes, ndof = m->ndof;
+  const int64_t nq4 = m->n_q4, nt10 = m->n_t10;
+  const uint64_t mt10 = mask_t10();
+  // node -> incident elements (ascending global order)
+  std::vector<int64_t> iptr(nn + 1, 0);
+  for (int64_t e = 0; e < nq4; ++e)
+    for (int k = 0; k < 4; ++k) iptr[m->h_q4n[4 * e + k] + 1]++;
+  for (int64_t e = 0; e < nt10; ++e)
+    for (int k = 0; k < 10; ++k) iptr[m->h_t10n[10 * e + k] + 1]++;
+  for (int64_t v = 0; v < nn; ++v) iptr[v + 1] += iptr[v];
+  std::vector<ElemRef> inc(iptr[nn]);
+  {
+    std::vector<int64_t> pos(iptr.begin(), iptr.end() - 1);
+    for (int64_t e = 0; e < nq4; ++e)
+      for (int k = 0; k < 4; ++k) inc[pos[m->h_q4n[4 * e + k]]++] = {e, (int8_t)k};
+    for (int64_t e = 0; e < nt10; ++e)
+      for (int k = 0; k < 10; ++k) inc[pos[m->h_t10n[10 * e + k]]++] = {nq4 + e, (int8_t)k};
+  }
+  auto enodes = [&](int64_t ge, int& nnd) -> const int32_t* {
+    if (ge < nq4) { nnd = 4; return m->h_q4n.data() + 4 * ge; }
+    nnd = 10;
+    return m->h_t10n.data() + 10 * (ge - nq4);
+  };
+  auto emask = [&](int64_t ge) { return ge < nq4 ? MASK_Q4 : mt10; };
+  // per column node: sorted (row node, mask)
+  struct Blk { int32_t a; uint64_t mask; };
+  auto node_blocks = [&](int64_t b, std::vector<Blk>& out) {
+    out.clear();
+    for (int64_t p = iptr[b]; p < iptr[b + 1]; ++p) {
+      int nnd;
+      const int32_t* en = enodes(inc[p].e, nnd);
+      uint64_t mk = emask(inc[p].e);
+      for (int k = 0; k < nnd; ++k) out.push_back({en[k], mk});
+    }
+    std::sort(out.begin(), out.end(), [](const Blk& x, const Blk& y) { return x.a < y.a; });
+    size_t w = 0;
+    for (size_t r = 0; r < out.size(); ++r) {
+      if (w > 0 && out[w - 1].a == out[r].a) out[w - 1].mask |= out[r].mask;
+      else out[w++] = out[r];
+    }
+    out.resize(w);
+  };
+  // pass 1: column counts
+  m->colptr.assign(ndof + 1, 0);
+#pragma omp parallel
+  {
+    std::vector<Blk> blk;
+#pragma omp for schedule(dynamic, 256)
+    for (int64_t b = 0; b < nn; ++b) {
+      node_blocks(b, blk);
+      for (int j = 0; j < 6; ++j) {
+        int64_t cnt = 0;
+        for (auto& x : blk)
+          for (int i = 0; i < 6; ++i) cnt += (x.mask >> (i + 6 * j)) & 1;
+        m->colptr[6 * b + j + 1] = cnt;
+      }
+    }
+  }
+  for (int64_t j = 0; j < ndof; ++j) m->colptr[j + 1] += m->colptr[j];
+  const int64_t nnz = m->colptr[ndof];
+  m->nnz = nnz;
+  m->rowval.resize(nnz);
+  m->diag_pos.assign(ndof, -1);
+  m->n_trip = 576 * nq4 + 900 * nt10;
+  if (m->n_trip >= (int64_t)INT32_MAX) {
+    set_error("triplet count exceeds the 32-bit slot-map range");
+    return JFG_UNSUPPORTED;
+  }
+  std::vector<int32_t> cnt(nnz + 1, 0);
+  // pass 2: rows and contribution counts
+#pragma omp parallel
+  {
+    std::vector<Blk> blk;
+#pragma omp for schedule(dynamic, 256)
+    for (int64_t b = 0; b < nn; ++b) {
+      node_blocks(b, blk);
+      for (int j = 0; j < 6; ++j) {
+        int64_t q = m->colptr[6 * b + j];
+        for (auto& x : blk)
+          for (int i = 0; i < 6; ++i) {
+            if (!((x.mask >> (i + 6 * j)) & 1)) continue;
+            m->rowval[q] = 6 * x.a + i;
+            if (x.a == b && i == j) m->diag_pos[6 * b + j] = q;
+            // contributions: incident elements of b that contain node a and
+            // cover the (i, j) component pair
+            int32_t c = 0;
+            for (int64_t p = iptr[b]; p < iptr[b + 1]; ++p) {
+              if (!((emask(inc[p].e) >> (i + 6 * j)) & 1)) continue;
+              int nnd;
+              const int32_t* en = enodes(inc[p].e, nnd);
+              for (int k = 0; k < nnd; ++k)
+                if (en[k] == x.a) { ++c; break; }
+            }
+            cnt[q + 1] = c;
+            ++q;
+          }
+      }
+    }
+  }
+  for (int64_t q = 0; q < nnz; ++q) cnt[q + 1] += cnt[q];
+  if (cnt[nnz] != m->n_trip) {
+    set_error("internal: slot-map contribution count mismatch");
+    return JFG_BAD_INPUT;
+  }
+  std::vector<int32_t> trip(m->n_trip);
+  m->slot.assign(m->n_trip, -1);
+  // pass 3: contributions in triplet (element) order, and the slot map
+#pragma omp parallel
+  {
+    std::vector<Blk> blk;
+#pragma omp for schedule(dynamic, 256)
+    for (int64_t b = 0; b < nn; ++b) {
+      node_blocks(b, blk);
+      for (int j = 0; j < 6; ++j) {
+        int64_t q = m->colptr[6 * b + j];
+        for (auto& x : blk)
+          for (int i = 0; i < 6; ++i) {
+            if (!((x.mask >> (i + 6 * j)) & 1)) continue;
+            int32_t w = cnt[q];
+            for (int64_t p = iptr[b]; p < iptr[b + 1]; ++p) {
+              int64_t ge = inc[p].e;
+              if (!((emask(ge) >> (i + 6 * j)) & 1)) continue;
+              int nnd;
+              const int32_t* en = enodes(ge, nnd);
+              int la = -1;
+              for (int k = 0; k < nnd; ++k)
+                if (en[k] == x.a) { la = k; break; }
+              if (la < 0) continue;
+              int lb = inc[p].local;
+              int64_t t;
+              if (ge < nq4) {
+                int rr = 6 * la + i, cc = 6 * lb + j;
+                t = 576 * ge + rr + 24 * cc;
+              } else {
+                int rr = 3 * la + i, cc = 3 * lb + j;
+                t = 576 * nq4 + 900 * (ge - nq4) + rr + 30 * cc;
+              }
+              trip[w++] = (int32_t)t;
+              m->slot[t] = q;
+            }
+            ++q;
+          }
+      }
+    }
+  }
+  // transpose positions (row i of the symmetric pattern through column i)
+  std::vector<int64_t> tpos(nnz);
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int64_t j = 0; j < ndof; ++j)
+    for (int64_t p = m->colptr[j]; p < m->colptr[j + 1]; ++p) {
+      int64_t i = m->rowval[p];
+      const int32_t* beg = m->rowval.data() + m->colptr[i];
+      const int32_t* end = m->rowval.data() + m->colptr[i + 1];
+      const int32_t* f = std::lower_bound(beg, end, (int32_t)j);
+      tpos[p] = (f != end && *f == j) ? m->colptr[i] + (f - beg) : -1;
+    }
+  for (int64_t p = 0; p < nnz; ++p)
+    if (tpos[p] < 0) {
+      set_error("pattern is not structurally symmetric");
+      return JFG_BAD_INPUT;
+    }
+  jfg_ctx* c = m->ctx;
+  JFG_TRY(dev_alloc(c, (void**)&m->d_colptr, sizeof(int64_t) * (ndof + 1)));
+  JFG_TRY(dev_alloc(c, (void**)&m->d_rowval, sizeof(int32_t) * nnz));
+  JFG_TRY(dev_alloc(c, (void**)&m->d_nzptr, sizeof(int32_t) * (nnz + 1)));
+  JFG_TRY(dev_alloc(c, (void**)&m->d_trip, sizeof(int32_t) * m->n_trip));
+  JFG_TRY(dev_alloc(c, (void**)&m->d_tpos, sizeof(int64_t) * nnz));
+  JFG_TRY(dev_alloc(c, (void**)&m->d_nzval, sizeof(double) * nnz));
+  JFG_CUDA(cudaMemcpy(m->d_colptr, m->colptr.data(), sizeof(int64_t) * (ndof + 1), cudaMemcpyHostToDevice));
+  JFG_CUDA(cudaMemcpy(m->d_rowval, m->rowval.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice));
+  JFG_CUDA(cudaMemcpy(m->d_nzptr, cnt.data(), sizeof(int32_t) * (nnz + 1), cudaMemcpyHostToDevice));
+  JFG_CUDA(cudaMemcpy(m->d_trip, trip.data(), sizeof(int32_t) * m->n_trip, cudaMemcpyHostToDevice));
+  JFG_CUDA(cudaMemcpy(m->d_tpos, tpos.data(), sizeof(int64_t) * nnz, cudaMemcpyHostToDevice));
+  m->pattern_built = true;
+  return JFG_OK;
+}
+
+jfg_status launch_assembly(jfg_model* m, cudaStream_t st) {
+  int64_t blocks = (m->nnz + 255) / 256;
+  int ps = prof_start(st);
+  { k_assemble<<<(unsigned)blocks, 256, 0, st>>>(m->nnz, m->d_nzptr, m->d_trip, m->d_ev, m->d_nzval); count_launch(); }
+  // algorithmic bytes: each triplet's index + value read once, each entry's
+  // pointer read and value written once
+  prof_end(ps, st, KS_ASSEMBLY, (double)m->n_trip * 12 + (double)m->nnz * 12);
+  JFG_CUDA(cudaGetLastError());
+  return JFG_OK;
+}
+
+void spmv_csc_sym(const jfg_model* m, int nrhs, const double* x, int64_t ldx, double* y, int64_t ldy,
+                  cudaStream_t st) {
+  int64_t threads = m->ndof * 32;
+  int64_t blocks = (threads + 255) / 256;
+  { k_spmv<<<(unsigned)blocks, 256, 0, st>>>(m->ndof, m->d_colptr, m->d_rowval, m->d_tpos, m->d_nzval, nrhs,
+                                           x, ldx, y, ldy); count_launch(); }
+}
+
+}  // namespace jfg

@@ -1,0 +1,146 @@
+// jfg_internal.h -- shared internals of libjfemgpu (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/jfemgpu.h"
+#include "symbolic.h"
+
+namespace jfg {
+
+void set_error(const std::string& msg, int64_t detail = 0);
+
+// Launch accounting (one increment per kernel launch of this library) and
+// per-kernel device-time statistics for the roofline report.
+void count_launch(int n = 1);
+int64_t launch_count();
+
+enum KernelStat : int { KS_SCHUR = 0, KS_Q4 = 1, KS_ASSEMBLY = 2, KS_SOLVE = 3, KS_T10 = 4, KS_COUNT = 5 };
+struct KernelStats {
+  int64_t launches[KS_COUNT] = {0};
+  double ms[KS_COUNT] = {0};
+  double units[KS_COUNT] = {0};   // algorithmic flops (SCHUR) or bytes (others)
+};
+KernelStats& kernel_stats();
+bool profiling_enabled();
+void set_profiling(bool on);
+// Event brackets around instrumented launches (no-ops when profiling is off).
+int prof_start(cudaStream_t st);
+void prof_end(int slot, cudaStream_t st, int kind, double units);
+void prof_flush();   // call after the stream has been synchronised
+
+#define JFG_CUDA(call)                                                          \
+  do {                                                                          \
+    cudaError_t e_ = (call);                                                    \
+    if (e_ != cudaSuccess) {                                                    \
+      ::jfg::set_error(std::string("CUDA error: ") + cudaGetErrorString(e_) +   \
+                       " at " __FILE__ ":" + std::to_string(__LINE__));         \
+      return JFG_CUDA_ERROR;                                                    \
+    }                                                                           \
+  } while (0)
+
+#define JFG_TRY(call)                 \
+  do {                                \
+    jfg_status s_ = (call);           \
+    if (s_ != JFG_OK) return s_;      \
+  } while (0)
+
+// Device buffer with byte accounting against the context budget.
+struct DevMem {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+// Error record written by device kernels (first failing element / pivot).
+struct DevError {
+  int32_t code;        // 0 = none
+  int32_t pad;
+  int64_t index;       // element index or permuted column
+};
+
+// Element-kernel status codes written to DevError::code.
+enum ElemErr : int32_t {
+  EE_NONE = 0,
+  EE_NOT_FLAT = 100,
+  EE_FLAGS = 101,
+  EE_JACOBIAN = 1,
+  EE_SHEAR = 11,
+  EE_ENRICH = 20,
+  EE_T10_JAC = 200,
+  EE_T10_MAT = 202,
+  EE_Q8_SHAPE = 300,
+  EE_Q8_SINGULAR = 302,
+  EE_PIVOT = 500,
+};
+
+}  // namespace jfg
+
+// ---- opaque ABI objects -----------------------------------------------------
+struct jfg_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int64_t budget = 0;
+  int64_t used = 0;
+};
+
+struct NumericFactor;   // defined in factor.cu
+
+struct jfg_model {
+  jfg_ctx* ctx = nullptr;
+  int64_t n_nodes = 0, n_q4 = 0, n_q8 = 0, n_t10 = 0, ndof = 0;
+  // host copies of the inputs (pattern build, element capture)
+  std::vector<double> h_xyz, h_R, h_q4s, h_q8s, h_t10m;
+  std::vector<int32_t> h_q4n, h_q8n, h_t10n;
+  // device inputs
+  double *d_xyz = nullptr, *d_R = nullptr, *d_q4s = nullptr, *d_q8s = nullptr, *d_t10m = nullptr;
+  int32_t *d_q4n = nullptr, *d_q8n = nullptr, *d_t10n = nullptr;
+  // element values: Q4 576 / T10 900 / Q8 2304 doubles per element
+  int64_t ev_t10_off = 0, ev_q8_off = 0, n_ev = 0;
+  double* d_ev = nullptr;
+  jfg::DevError* d_err = nullptr;
+  // pattern + slot map (built once)
+  bool pattern_built = false;
+  int64_t nnz = 0, n_trip = 0;
+  std::vector<int64_t> colptr;
+  std::vector<int32_t> rowval;
+  std::vector<int64_t> slot;        // triplet -> nz position
+  std::vector<int64_t> diag_pos;    // ndof, -1 when structurally absent
+  int64_t* d_diag_pos = nullptr;
+  int64_t* d_colptr = nullptr;
+  int32_t* d_rowval = nullptr;
+  int32_t* d_nzptr = nullptr;       // nnz+1, into d_trip
+  int32_t* d_trip = nullptr;        // element-value index of each triplet, triplet order
+  int64_t* d_tpos = nullptr;        // CSC position of the transposed entry
+  double* d_nzval = nullptr;
+  bool values_ready = false;
+  // symbolic
+  bool sym_ready = false;
+  jfg::Symbolic sym;
+  NumericFactor* num = nullptr;
+  // timings of the last calls (seconds, device events)
+  double t_elements = 0, t_assembly = 0, t_factor = 0, t_solve = 0;
+};
+
+namespace jfg {
+
+// elements.cu
+jfg_status launch_elements(jfg_model* m, cudaStream_t st);
+// assembly.cu
+jfg_status build_pattern(jfg_model* m);
+jfg_status launch_assembly(jfg_model* m, cudaStream_t st);
+void spmv_csc_sym(const jfg_model* m, int nrhs, const double* x, int64_t ldx, double* y,
+                  int64_t ldy, cudaStream_t st);
+// factor.cu
+jfg_status numeric_create(jfg_model* m);
+void numeric_destroy(jfg_model* m);
+jfg_status numeric_factor(jfg_model* m, int precision);
+jfg_status numeric_solve(jfg_model* m, int nrhs, const double* hF, double* hU, double tol,
+                         int max_ir, jfg_solve_report* rep, bool device_io);
+jfg_status numeric_factor_diag(jfg_model* m, double* out);
+// memory
+jfg_status dev_alloc(jfg_ctx* c, void** p, size_t bytes);
+void dev_free(jfg_ctx* c, void* p, size_t bytes);
+
+}  // namespace jfg

@@ -833,24 +833,40 @@ int64_t or_assemble_triplets(int64_t n_nodes, const double* xyz, const double* n
   *err_elem = -1;
   std::vector<double> Ke(48 * 48);
   double exyz[30], eR[90];
-  for (int64_t e = 0; e < n_q4; ++e) {
-    for (int k = 0; k < 4; ++k) {
-      int n = q4_nodes[4 * e + k];
-      for (int a = 0; a < 3; ++a) exyz[3 * k + a] = xyz[3 * n + a];
-      for (int a = 0; a < 9; ++a) eR[9 * k + a] = node_R[9 * n + a];
-    }
-    int st = or_q4_element(exyz, eR, q4_sect + 26 * e, Ke.data());
-    if (st) { *err_elem = (int32_t)e; return -st; }
-    for (int cc = 0; cc < 24; ++cc)
-      for (int rr = 0; rr < 24; ++rr) {
-        if (cnt < cap) {
-          I[cnt] = 6 * (int64_t)q4_nodes[4 * e + rr / 6] + rr % 6;
-          J[cnt] = 6 * (int64_t)q4_nodes[4 * e + cc / 6] + cc % 6;
-          V[cnt] = Ke[rr + 24 * cc];
-        }
-        ++cnt;
+  // positional slots (e*576): the element loop is parallel like the
+  // reference's Threads.@threads :static loop (assembly.jl:3603)
+  int64_t q4_err = -1;
+  int q4_st = 0;
+#pragma omp parallel
+  {
+    std::vector<double> Kt(576);
+    double xy[12], Rr[36];
+#pragma omp for schedule(static)
+    for (int64_t e = 0; e < n_q4; ++e) {
+      for (int k = 0; k < 4; ++k) {
+        int n = q4_nodes[4 * e + k];
+        for (int a = 0; a < 3; ++a) xy[3 * k + a] = xyz[3 * n + a];
+        for (int a = 0; a < 9; ++a) Rr[9 * k + a] = node_R[9 * n + a];
       }
+      int st = or_q4_element(xy, Rr, q4_sect + 26 * e, Kt.data());
+      if (st) {
+#pragma omp critical
+        { if (q4_err < 0 || e < q4_err) { q4_err = e; q4_st = st; } }
+        continue;
+      }
+      int64_t base = 576 * e;
+      if (base + 576 <= cap)
+        for (int cc = 0; cc < 24; ++cc)
+          for (int rr = 0; rr < 24; ++rr) {
+            int64_t t = base + rr + 24 * cc;
+            I[t] = 6 * (int64_t)q4_nodes[4 * e + rr / 6] + rr % 6;
+            J[t] = 6 * (int64_t)q4_nodes[4 * e + cc / 6] + cc % 6;
+            V[t] = Kt[rr + 24 * cc];
+          }
+    }
   }
+  if (q4_err >= 0) { *err_elem = (int32_t)q4_err; return -q4_st; }
+  cnt = 576 * n_q4;
   for (int64_t e = 0; e < n_t10; ++e) {
     for (int k = 0; k < 10; ++k) {
       int n = t10_nodes[10 * e + k];

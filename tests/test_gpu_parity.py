@@ -1,0 +1,185 @@
+"""Device parity against the CPU oracle (runs on a B200; marked gpu).
+
+Bars: element matrices to 1e-12 relative, CSC pattern
+and slot map bit-exact, displacements / SPC forces to 1e-8 relative for the
+FP64 path and relative residual <= 1e-10 for both paths after refinement.
+"""
+import numpy as np
+import pytest
+
+from jf_2026_05_25_b200 import backend as B
+from jf_2026_05_25_b200 import build as jbuild
+from jf_2026_05_25_b200 import lib
+from jf_2026_05_25_b200 import model as M
+
+pytestmark = pytest.mark.gpu
+
+ELEM_RTOL = 1e-12
+DISP_RTOL = 1e-8
+RESID_TOL = 1e-10
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    jbuild.build()
+    c = lib.Context(0)
+    yield c
+    c.close()
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def _rot(ax, deg):
+    t = np.radians(deg)
+    c, s = np.cos(t), np.sin(t)
+    if ax == 0:
+        return np.array([[1, 0, 0], [0, c, -s], [0, s, c]])
+    if ax == 1:
+        return np.array([[c, 0, s], [0, 1, 0], [-s, 0, c]])
+    return np.array([[c, -s, 0], [s, c, 0], [0, 0, 1]])
+
+
+def _random_quads(rng, n):
+    """Flat convex quads (rectangles, parallelograms, tapers) in random planes."""
+    out = []
+    for k in range(n):
+        a, b = rng.uniform(0.005, 0.05, 2)
+        sk = rng.uniform(-0.3, 0.3) * b if k % 3 else 0.0
+        tp = rng.uniform(-0.25, 0.25) * a if k % 4 == 1 else 0.0
+        P = np.array([[0, 0], [a, 0], [a + sk + tp, b], [sk, b]], float)
+        P3 = np.c_[P, np.zeros(4)]
+        R = _rot(0, rng.uniform(0, 180)) @ _rot(1, rng.uniform(0, 180)) @ _rot(2, rng.uniform(0, 360))
+        out.append(P3 @ R.T + rng.uniform(-1, 1, 3))
+    return out
+
+
+def test_quad4_element_matrices(ctx, oracle_mod):
+    rng = np.random.default_rng(7)
+    quads = _random_quads(rng, 48)
+    xyz = np.vstack(quads)
+    q4 = np.arange(4 * len(quads), dtype=np.int32).reshape(-1, 4)
+    pids = np.arange(len(quads)) % 3 + 1
+    m = M.Sol101Model(name="q4set", grid_ids=np.arange(1, len(xyz) + 1), xyz=xyz, q4_nodes=q4, q4_pid=pids,
+                      pshells={1: M.PShell(T=0.002, MID1=1, MID2=1, MID3=1), 2: M.PShell(T=0.004, MID1=1, MID2=1, MID3=1),
+                               3: M.PShell(T=0.0015, MID1=1, MID2=1, MID3=1, BEND_RATIO=0.8, TS_T=0.7)},
+                      mats={1: M.Mat1(E=70e9, NU=0.33)})
+    dm = lib.DeviceModel(ctx, m)
+    dm.assemble()
+    sect = m.q4_sections()
+    worst = 0.0
+    for e in range(len(quads)):
+        Kd = dm.element_matrix(0, e)
+        Ko = oracle_mod.q4_element(xyz[q4[e]], sect[e])
+        worst = max(worst, _rel(Kd, Ko))
+    assert worst <= ELEM_RTOL, worst
+
+
+def test_tetra10_element_matrices(ctx, oracle_mod):
+    m = M.solid_block(n=2, n_cases=1)
+    rng = np.random.default_rng(3)
+    m.xyz = m.xyz + rng.uniform(-0.01, 0.01, m.xyz.shape) * (0.3 / 4)   # curved, still valid
+    dm = lib.DeviceModel(ctx, m)
+    dm.assemble()
+    worst = 0.0
+    for e in range(0, len(m.t10_nodes), 5):
+        Kd = dm.element_matrix(2, e)
+        Ko = oracle_mod.t10_element(m.xyz[m.t10_nodes[e]], 210e9, 0.3)
+        worst = max(worst, _rel(Kd, Ko))
+    assert worst <= ELEM_RTOL, worst
+
+
+MODELS = {
+    "plate": lambda: M.flat_plate(),
+    "wing_small": lambda: M.wing_panel(nx=24, ny=36, n_blades=3, blade_nz=4, n_cases=3, seed=5),
+    "solid_small": lambda: M.solid_block(n=4, n_cases=2),
+}
+
+
+@pytest.mark.parametrize("name", sorted(MODELS))
+def test_pattern_slot_map_and_values(ctx, oracle_mod, name):
+    m = MODELS[name]()
+    asm = oracle_mod.assemble(m)
+    dm = lib.DeviceModel(ctx, m)
+    dm.assemble()
+    colptr, rowval = dm.pattern()
+    assert np.array_equal(colptr, asm["colptr"])
+    assert np.array_equal(rowval, asm["rowval"])
+    assert np.array_equal(dm.slot_map(), asm["slot"])
+    v = dm.values()
+    scale = np.abs(asm["nzval"]).max()
+    assert np.abs(v - asm["nzval"]).max() <= ELEM_RTOL * scale
+    # bitwise determinism of the gather assembly
+    dm.assemble()
+    assert np.array_equal(dm.values(), v)
+
+
+@pytest.mark.parametrize("name", sorted(MODELS))
+@pytest.mark.parametrize("prec", [lib.PREC_FP64, lib.PREC_MIXED])
+def test_sol101_against_oracle(ctx, oracle_mod, name, prec):
+    m = MODELS[name]()
+    ref = oracle_mod.solve_reference(m)
+    be = B.JFEMGPUBackend(precision=prec, tol=RESID_TOL)
+    be._ctx = ctx
+    res = B.solve_model(be, m)
+    free = res["state"]["free"]
+    assert np.array_equal(free, ref["free"])
+    U = np.stack([s["raw_displacement"] for s in res["subcases"]], axis=1)
+    for sc in res["subcases"]:
+        assert sc["solver_diagnostics"]["linear_solver"]["rel_residual"] <= RESID_TOL
+    # displacement error against the FP64 oracle, relative to the field maximum
+    assert _rel(U, ref["u"]) <= DISP_RTOL
+    # SPC forces (residual at the fixed DOFs)
+    fixed = res["state"]["fixed"]
+    R_dev = np.stack([np.asarray(list(sc["spc_forces"].values())).ravel() if sc["spc_forces"] else np.zeros(0)
+                      for sc in res["subcases"]][0:1])
+    Rref = ref["R"][fixed]
+    Rdev = res["state"]["dm"].residual(U, m.load_matrix())[fixed]
+    assert _rel(Rdev, Rref) <= DISP_RTOL
+    assert R_dev.size > 0
+
+
+def test_factor_is_deterministic(ctx):
+    m = MODELS["wing_small"]()
+    be = B.JFEMGPUBackend()
+    be._ctx = ctx
+    st = B.prepare(be, m)
+    dm = st["dm"]
+    d1 = dm.factor_diag()
+    F = m.load_matrix()
+    U1, _ = dm.solve(F)
+    dm.factor(lib.PREC_FP64)
+    d2 = dm.factor_diag()
+    U2, _ = dm.solve(F)
+    assert np.array_equal(d1, d2)
+    assert np.array_equal(U1, U2)
+
+
+def test_not_spd_reports_pivot(ctx):
+    """A free rigid-body mode (no SPC, GPST off by eps 0) must surface as NOT_SPD."""
+    m = M.flat_plate(nx=4, ny=4)
+    m.spc1 = []
+    dm = lib.DeviceModel(ctx, m)
+    dm.assemble()
+    free = np.arange(m.ndof, dtype=np.int32)
+    dm.set_free_dofs(free)
+    with pytest.raises(lib.JfgError) as e:
+        dm.factor(lib.PREC_FP64)
+    assert e.value.status_name == "NOT_SPD"
+
+
+def test_thickness_update_resolve(ctx, oracle_mod):
+    m = MODELS["plate"]()
+    be = B.JFEMGPUBackend()
+    be._ctx = ctx
+    st = B.prepare(be, m)
+    dm = st["dm"]
+    m.pshells[1] = M.PShell(T=0.0025, MID1=1, MID2=1, MID3=1)
+    sect = m.q4_sections()
+    dm.update_q4_sections(np.arange(len(sect)), sect)
+    dm.assemble()
+    dm.factor(lib.PREC_FP64)
+    U, rep = dm.solve(m.load_matrix())
+    ref = oracle_mod.solve_reference(m)
+    assert _rel(U, ref["u"]) <= DISP_RTOL
