@@ -16,6 +16,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "jfg_internal.h"
@@ -830,7 +832,8 @@ jfg_status numeric_solve(jfg_model* m, int nrhs, const double* hF, double* hU, d
     double fn[8], rn[8], prev[8];
     JFG_TRY(colnorm2(F, n, nr, F->dD, fn, st));
     bool use32 = prefer32;
-    int it = 0;
+    int it = 0, stall_count = 0;
+    double rn_max_prev = 1e300;
     double worst = 0;
     for (int q = 0; q < nr; ++q) prev[q] = 1e300;
     for (;;) {
@@ -853,21 +856,30 @@ jfg_status numeric_solve(jfg_model* m, int nrhs, const double* hF, double* hU, d
         rn[q] = rel;
         worst = std::max(worst, rel);
       }
+      if (std::getenv("JFG_IR_TRACE"))
+        std::fprintf(stderr, "[jfg] ir step %d (%s factor): max relative residual %.3e\n", it,
+                     use32 ? "mixed" : "fp64", worst);
       if (worst <= tol || it >= max_ir) break;
+      // stagnation: a step that does not reduce some unconverged residual by
+      // at least 10 % counts as stalled; two stalled steps in a row end the
+      // refinement (after a switch to the FP64 factor for the mixed path)
       bool stalled = false;
       for (int q = 0; q < nr; ++q)
-        if (rn[q] > tol && rn[q] > 0.5 * prev[q]) stalled = true;
-      if (stalled) {
+        if (rn[q] > tol && rn[q] > 0.9 * prev[q]) stalled = true;
+      stall_count = stalled ? stall_count + 1 : 0;
+      if (stall_count >= 2 || (stalled && use32 && rn_max_prev < worst)) {
         if (use32) {
           // refinement with the mixed factor stalls: FP64 factor fallback
           if (!F->have64) JFG_TRY(numeric_factor(m, JFG_PREC_FP64));
           use32 = false;
+          stall_count = 0;
           R.fallback_used = 1;
           R.precision = JFG_PREC_FP64;
         } else {
           break;
         }
       }
+      rn_max_prev = worst;
       for (int q = 0; q < nr; ++q) prev[q] = rn[q];
       ++it;
     }

@@ -96,6 +96,14 @@ def load():
         f = getattr(L, name)
         f.argtypes = args
         f.restype = _c.c_int
+    L.jfg_launch_count.restype = I64
+    L.jfg_launch_count.argtypes = []
+    L.jfg_set_profiling.argtypes = [I32]
+    L.jfg_set_profiling.restype = _c.c_int
+    L.jfg_get_kernel_stats.argtypes = [I32, P]
+    L.jfg_get_kernel_stats.restype = _c.c_int
+    L.jfg_reset_kernel_stats.argtypes = []
+    L.jfg_reset_kernel_stats.restype = _c.c_int
     L.jfg_last_error.restype = _c.c_char_p
     L.jfg_last_error.argtypes = []
     L.jfg_last_error_detail.restype = I64
@@ -262,9 +270,12 @@ class DeviceModel:
             _check(st)
         return U, rep.as_dict()
 
-    def solve_device(self, F_ptr: int, U_ptr: int, nrhs: int, tol: float = 1e-10, max_ir: int = 10):
+    def solve_device(self, F_ptr: int, U_ptr: int, nrhs: int, tol: float = 1e-10, max_ir: int = 10,
+                     raise_on_stall: bool = True):
         rep = SolveReport()
-        _check(load().jfg_solve_device(self.h, nrhs, P(F_ptr), P(U_ptr), tol, max_ir, _c.byref(rep)))
+        st = load().jfg_solve_device(self.h, nrhs, P(F_ptr), P(U_ptr), tol, max_ir, _c.byref(rep))
+        if st != JFG_OK and not (st == 2 and not raise_on_stall):
+            _check(st)
         return rep.as_dict()
 
     def residual(self, U: np.ndarray, F: np.ndarray) -> np.ndarray:
