@@ -72,7 +72,59 @@ __global__ void k_spmv(int64_t n, const int64_t* __restrict__ colptr, const int3
   }
 }
 
+// r = F - K x with error-free transformations (FMA product error + two-sum)
+// per row: the residual carries no rounding from the cancelling row sums of
+// the stiffness matrix, only the final rounding.
+__global__ void k_residual_dd(int64_t n, const int64_t* __restrict__ colptr, const int32_t* __restrict__ rowval,
+                              const int64_t* __restrict__ tpos, const double* __restrict__ nzval, int nrhs,
+                              const double* __restrict__ x, const double* __restrict__ f, int64_t ld,
+                              double* __restrict__ r) {
+  int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  int64_t a = colptr[row], b = colptr[row + 1];
+  for (int k = 0; k < nrhs; ++k) {
+    double hi = 0.0, lo = 0.0;
+    for (int64_t p = a + lane; p < b; p += 32) {
+      double kv = nzval[tpos[p]];
+      double xv = x[rowval[p] + ld * k];
+      double prod = kv * xv;
+      double perr = fma(kv, xv, -prod);
+      double s = hi + prod;
+      double bp = s - hi;
+      double serr = (hi - (s - bp)) + (prod - bp);
+      hi = s;
+      lo += serr + perr;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      double h2 = __shfl_down_sync(0xffffffffu, hi, o);
+      double l2 = __shfl_down_sync(0xffffffffu, lo, o);
+      double s = hi + h2;
+      double bp = s - hi;
+      double serr = (hi - (s - bp)) + (h2 - bp);
+      hi = s;
+      lo += l2 + serr;
+    }
+    if (lane == 0) {
+      // f - (hi + lo) in two-sum form
+      double fv = f[row + ld * k];
+      double s = fv - hi;
+      double bp = s - fv;
+      double serr = (fv - (s - bp)) + (-hi - bp);
+      r[row + ld * k] = s + (serr - lo);
+    }
+  }
+}
+
 }  // namespace
+
+void residual_dd(const jfg_model* m, int nrhs, const double* x, const double* f, double* r, cudaStream_t st) {
+  int64_t threads = m->ndof * 32;
+  int64_t blocks = (threads + 255) / 256;
+  { k_residual_dd<<<(unsigned)blocks, 256, 0, st>>>(m->ndof, m->d_colptr, m->d_rowval, m->d_tpos, m->d_nzval, nrhs, x,
+                                                   f, m->ndof, r); count_launch(); }
+}
 
 jfg_status build_pattern(jfg_model* m) {
   if (m->n_q8 > 0) {

@@ -45,21 +45,39 @@ struct NumericFactor {
   float* L32 = nullptr;
   float* U32 = nullptr;
   double* scale = nullptr;    // n, symmetric diagonal scaling of the mixed factor
+  // inverse diagonal blocks of the strip solve
+  int64_t n_strips = 0, dinv_len = 0, part_len = 0;
+  int32_t *strip_sn = nullptr, *strip_idx = nullptr;
+  int64_t *Dptr = nullptr, *part_off = nullptr;
+  double* Dinv64 = nullptr;
+  float* Dinv32 = nullptr;
+  double* part = nullptr;
   bool have64 = false, have32 = false;
   bool prefer_mixed = false;   // solve with the mixed factor when both exist
   // solve workspace
   int nrhs_cap = 0;
-  double *xp = nullptr, *V = nullptr, *dF = nullptr, *dU = nullptr, *dR = nullptr, *dD = nullptr;
+  double *xp = nullptr, *tt = nullptr, *V = nullptr, *dF = nullptr, *dU = nullptr, *dR = nullptr, *dD = nullptr;
+  double *dZ = nullptr, *dP = nullptr, *dQ = nullptr;
+  uint8_t* free_mask = nullptr;
   double *norms = nullptr;
   int64_t v_total = 0;
   jfg::DevError* err = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
+#define JFG_CUDA_VOID(x) (void)(x)
+
 namespace jfg {
 namespace {
 
-constexpr int NB = 32;       // panel block width
+// fine-grained per-kernel-class event brackets (JFG_FINE_PROFILE=1)
+inline bool fine_prof() {
+  static int v = -1;
+  if (v < 0) v = std::getenv("JFG_FINE_PROFILE") ? 1 : 0;
+  return v == 1 && profiling_enabled();
+}
+
+constexpr int NB = 64;       // panel block width
 constexpr int TILE = 64;     // Schur-update tile
 
 __device__ inline void rec_err(DevError* e, int32_t code, int64_t idx) {
@@ -86,18 +104,6 @@ __global__ void k_diag_scale(int64_t n, const int32_t* __restrict__ perm_dof, co
   scale[k] = d > 0.0 ? 1.0 / sqrt(d) : 1.0;
 }
 
-template <typename T>
-__global__ void k_zero_U(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
-                         const int32_t* __restrict__ mrows, const int64_t* __restrict__ Uptr, T* __restrict__ U) {
-  int s = list[blockIdx.y];
-  int64_t up = Uptr[s];
-  if (up < 0) return;
-  int64_t r = mrows[s] - (first[s + 1] - first[s]);
-  int64_t tot = r * r;
-  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += (int64_t)gridDim.x * blockDim.x)
-    U[up + q] = (T)0;
-}
-
 // Extend-add of child update matrices into their parents' fronts.  One launch
 // covers the children of one rank, so each parent receives one child.
 template <typename T>
@@ -105,7 +111,7 @@ __global__ void k_extend_add(const int32_t* __restrict__ child, const int32_t* _
                              const int32_t* __restrict__ mrows, const int32_t* __restrict__ parent,
                              const int64_t* __restrict__ Lptr, const int64_t* __restrict__ Uptr,
                              const int64_t* __restrict__ relptr, const int32_t* __restrict__ rel,
-                             T* __restrict__ L, T* __restrict__ U) {
+                             T* __restrict__ L, T* __restrict__ U, int pass) {
   int ch = child[blockIdx.y];
   int64_t uc = Uptr[ch];
   if (uc < 0) return;
@@ -119,6 +125,7 @@ __global__ void k_extend_add(const int32_t* __restrict__ child, const int32_t* _
   int rp = mp - cp;
   const int32_t* rl = rel + relptr[ch];
   int rb = rl[cb];
+  if ((pass == 0) != (rb < cp)) return;
   const T* src = U + uc + (int64_t)rc * cb;
   if (rb < cp) {
     T* dst = L + Lptr[p] + (int64_t)mp * rb;
@@ -129,73 +136,208 @@ __global__ void k_extend_add(const int32_t* __restrict__ child, const int32_t* _
   }
 }
 
+// 32 x 32 Cholesky of A[o..o+31][o..o+31] and its inverse into B, by one warp
+// (warp-synchronous, no block barrier).  Lane i holds row o+i in registers;
+// the factor runs on unscaled columns (a_ik -= a_ij a_kj / a_jj, the L D L^T
+// form) and scales column k by 1/sqrt(a_kk) at the end.  The inverse is
+// right-looking by rows with lane j holding column o+j of X = L^{-1}.
+// Pivots that are not positive and finite are replaced by 1 and the smallest
+// such column index is recorded in *bad_idx.
 template <typename T>
-__global__ void k_potrf_diag(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
-                             const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
-                             T* __restrict__ L, int k0, DevError* err) {
+__device__ __forceinline__ void chol32_inv(T (*A)[NB + 1], T (*B)[NB + 1], T* sv, T* pv, int o, int kn,
+                                           int* bad_idx) {
+  const int lane = threadIdx.x & 31;
+  const int gi = o + lane;
+  T a[32];
+#pragma unroll
+  for (int k = 0; k < 32; ++k) a[k] = (k <= lane) ? A[gi][o + k] : (T)0;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    T d = __shfl_sync(0xffffffffu, a[j], j);
+    T* s = sv + (j & 1) * 32;
+    s[lane] = a[j];
+    if (lane == 0) pv[j] = d;
+    bool bad = !(d > (T)0) || !isfinite((double)d);
+    T rd = bad ? (T)1 : (T)1 / d;
+    T lj = (lane > j) ? a[j] * rd : (T)0;
+    __syncwarp();
+#pragma unroll
+    for (int k = j + 1; k < 32; ++k) a[k] = fma(-lj, s[k], a[k]);
+  }
+  __syncwarp();
+  {
+    T p = pv[lane];
+    bool bad = !(p > (T)0) || !isfinite((double)p);
+    if (bad && gi < kn) atomicMin(bad_idx, gi);
+    T sq = bad ? (T)1 : sqrt(p);
+    sv[lane] = (T)1 / sq;
+    sv[32 + lane] = sq;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < 32; ++k) A[gi][o + k] = (k < lane) ? a[k] * sv[k] : (k == lane ? sv[32 + k] : (T)0);
+  __syncwarp();
+  T x[32];
+#pragma unroll
+  for (int i = 0; i < 32; ++i) x[i] = (i == lane) ? (T)1 : (T)0;
+#pragma unroll
+  for (int l = 0; l < 32; ++l) {
+    x[l] = x[l] * sv[l];
+#pragma unroll
+    for (int i = l + 1; i < 32; ++i) x[i] = fma(-A[o + i][o + l], x[l], x[i]);
+  }
+#pragma unroll
+  for (int i = 0; i < 32; ++i) B[o + i][gi] = (i >= lane) ? x[i] : (T)0;
+}
+
+template <typename T>
+constexpr int potrf_smem() { return (2 * NB * (NB + 1) + 2 * NB) * (int)sizeof(T); }
+
+// Cholesky of the NB x NB diagonal block at column k0 of every front of the
+// level, and the inverse of the factor block (kept for the panel triangular
+// solve and for the forward/backward solves).  The block is split 2 x 2 into
+// 32 x 32 tiles: L11 and X11 = L11^{-1} by one warp, L21 = A21 X11^T and
+// A22 -= L21 L21^T by the whole CTA, L22 and X22 by one warp, then
+// X21 = -X22 (L21 X11).  Rows and columns past the front's width are padded
+// with the identity so the tiles are always full.
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_potrf_diag(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
+             const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
+             const int64_t* __restrict__ Dptr, T* __restrict__ L, T* __restrict__ Dinv, int k0, DevError* err) {
   int s = list[blockIdx.x];
   int c = first[s + 1] - first[s];
   if (k0 >= c) return;
   int m = mrows[s];
   int kn = min(NB, c - k0);
-  __shared__ T A[NB][NB + 1];
-  int tx = threadIdx.x, ty = threadIdx.y;
+  extern __shared__ unsigned char smem_raw[];
+  T (*A)[NB + 1] = reinterpret_cast<T (*)[NB + 1]>(smem_raw);
+  T (*B)[NB + 1] = A + NB;
+  T* sv = reinterpret_cast<T*>(B + NB);  // 64 entries of broadcast scratch
+  T* pv = sv + 64;                       // 32 pivots
+  __shared__ int bad_idx;
   T* P = L + Lptr[s] + k0 + (int64_t)m * k0;
-  A[ty][tx] = (ty < kn && tx < kn && ty >= tx) ? P[ty + (int64_t)m * tx] : (T)0;
-  for (int j = 0; j < kn; ++j) {
-    __syncthreads();
-    if (tx == 0 && ty == 0) {
-      T d = A[j][j];
-      if (!(d > (T)0) || !isfinite((double)d)) {
-        rec_err(err, EE_PIVOT, (int64_t)first[s] + k0 + j);
-        d = (T)1;
-      }
-      A[j][j] = sqrt(d);
-    }
-    __syncthreads();
-    if (tx == j && ty > j && ty < kn) A[ty][j] /= A[j][j];
-    __syncthreads();
-    if (tx > j && ty >= tx && ty < kn) A[ty][tx] -= A[ty][j] * A[tx][j];
+  const int t = threadIdx.x, w = t >> 5, lane = t & 31;
+  if (t == 0) bad_idx = NB;
+  for (int e = t; e < NB * NB; e += blockDim.x) {
+    int i = e & (NB - 1), j = e >> 6;
+    A[i][j] = (i < kn && j < kn) ? (i >= j ? P[i + (int64_t)m * j] : (T)0) : (i == j ? (T)1 : (T)0);
   }
   __syncthreads();
-  if (ty < kn && tx < kn && ty >= tx) P[ty + (int64_t)m * tx] = A[ty][tx];
+  if (w == 0) chol32_inv<T>(A, B, sv, pv, 0, kn, &bad_idx);
+  __syncthreads();
+  if (kn > 32) {
+    const int i = 32 + lane;
+    T acc[4] = {0, 0, 0, 0};
+    // L21 = A21 X11^T  (thread: row i, columns w + 8q)
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k) {
+      T av = A[i][k];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] = fma(av, B[w + 8 * q][k], acc[q]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) A[i][w + 8 * q] = acc[q];
+    __syncthreads();
+    // A22 -= L21 L21^T, lower triangle
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] = 0;
+#pragma unroll 8
+    for (int j = 0; j < 32; ++j) {
+      T lv = A[i][j];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] = fma(lv, A[32 + w + 8 * q][j], acc[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int k = 32 + w + 8 * q;
+      if (k <= i) A[i][k] -= acc[q];
+    }
+    __syncthreads();
+    if (w == 0) chol32_inv<T>(A, B, sv, pv, 32, kn, &bad_idx);
+    __syncthreads();
+    // Tm = L21 X11 into the unused upper-right tile of B
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] = 0;
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k) {
+      T lv = A[i][k];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] = fma(lv, B[k][w + 8 * q], acc[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) B[lane][32 + w + 8 * q] = acc[q];
+    __syncthreads();
+    // X21 = -X22 Tm
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] = 0;
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k) {
+      T xv = B[i][32 + k];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] = fma(xv, B[k][32 + w + 8 * q], acc[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) B[i][w + 8 * q] = -acc[q];
+    __syncthreads();
+  }
+  if (t == 0 && bad_idx < kn) rec_err(err, EE_PIVOT, (int64_t)first[s] + k0 + bad_idx);
+  T* Dv = Dinv + Dptr[s] + (int64_t)(k0 / NB) * NB * NB;
+  for (int e = t; e < NB * NB; e += blockDim.x) {
+    int i = e & (NB - 1), j = e >> 6;
+    bool in = i < kn && j < kn && i >= j;
+    if (in) P[i + (int64_t)m * j] = A[i][j];
+    Dv[i + NB * j] = in ? B[i][j] : (T)0;
+  }
 }
 
-// rows [k1, m) of panel columns [k0, k1):  X := X * L_D^{-T}
+// rows [k1, m) of panel columns [k0, k1):  X := X * L_D^{-T} = X * Dinv^T,
+// 64 rows per CTA, both operands staged in shared memory.
 template <typename T>
-__global__ void k_trsm_panel(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
-                             const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
-                             T* __restrict__ L, int k0) {
+__global__ void __launch_bounds__(256)
+k_trsm_panel(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
+             const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr, const int64_t* __restrict__ Dptr,
+             T* __restrict__ L, const T* __restrict__ Dinv, int k0) {
   int s = list[blockIdx.y];
   int c = first[s + 1] - first[s];
   if (k0 >= c) return;
   int m = mrows[s];
   int k1 = min(k0 + NB, c), kn = k1 - k0;
-  __shared__ T D[NB][NB + 1];
+  int row0 = k1 + blockIdx.x * 64;
+  if (row0 >= m) return;
+  extern __shared__ unsigned char smem_raw[];
+  T (*Di)[NB + 1] = reinterpret_cast<T (*)[NB + 1]>(smem_raw);
+  T (*X)[NB + 1] = Di + NB;
+  const T* Dv = Dinv + Dptr[s] + (int64_t)(k0 / NB) * NB * NB;
   T* P = L + Lptr[s];
-  for (int q = threadIdx.x; q < NB * NB; q += blockDim.x) {
-    int i = q % NB, j = q / NB;
-    D[i][j] = (i < kn && j < kn && i >= j) ? P[(k0 + i) + (int64_t)m * (k0 + j)] : (T)0;
+  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+    int i = e % NB, j = e / NB;
+    Di[i][j] = Dv[i + NB * j];
+    int row = row0 + i;
+    X[i][j] = (row < m && j < kn) ? P[row + (int64_t)m * (k0 + j)] : (T)0;
   }
   __syncthreads();
-  int i = k1 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
-  T x[NB];
+  int r = threadIdx.x & 63, g = threadIdx.x >> 6;   // row, group of 16 output columns
+  int row = row0 + r;
+  T acc[16];
 #pragma unroll
-  for (int l = 0; l < NB; ++l) x[l] = l < kn ? P[i + (int64_t)m * (k0 + l)] : (T)0;
+  for (int t = 0; t < 16; ++t) acc[t] = (T)0;
+  for (int q = 0; q < kn; ++q) {
+    T xq = X[r][q];
 #pragma unroll
-  for (int l = 0; l < NB; ++l) {
-    if (l < kn) {
-      T v = x[l];
-#pragma unroll
-      for (int q = 0; q < NB; ++q)
-        if (q < l) v -= x[q] * D[l][q];
-      x[l] = v / D[l][l];
+    for (int t = 0; t < 16; ++t) {
+      int l = g * 16 + t;
+      acc[t] += (q <= l) ? xq * Di[l][q] : (T)0;
     }
   }
+  if (row < m) {
 #pragma unroll
-  for (int l = 0; l < NB; ++l)
-    if (l < kn) P[i + (int64_t)m * (k0 + l)] = x[l];
+    for (int t = 0; t < 16; ++t) {
+      int l = g * 16 + t;
+      if (l < kn) P[row + (int64_t)m * (k0 + l)] = acc[t];
+    }
+  }
 }
 
 // Tile update C -= A_rows * B_rows^T (lower part).  mode 0: trailing panel
@@ -269,7 +411,10 @@ k_front_update(const int32_t* __restrict__ list, const int32_t* __restrict__ fir
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
       int i = ti * TILE + ty + 16 * a, j = tj * TILE + tx + 16 * b;
-      if (i < nrow && j < ncol && row0 + i >= col0 + j) C[i + ldc * j] -= acc[a][b];
+      if (i < nrow && j < ncol && row0 + i >= col0 + j) {
+        if (mode == 0) C[i + ldc * j] -= acc[a][b];
+        else C[i + ldc * j] = -acc[a][b];      // U = -L21 L21^T; children are added after
+      }
     }
 }
 
@@ -307,98 +452,261 @@ __global__ void k_vec_extend_add(const int32_t* __restrict__ child, const int32_
   }
 }
 
+// ---------------------------------------------------------------- strip solves
+// The solve sweeps every front of a level in strips of SB columns.  The
+// inverse of each SB x SB diagonal block is formed once per factorisation,
+// so a strip costs one small matrix-vector product plus wide, coalesced
+// updates of the rows below the strip spread over many CTAs.
+constexpr int SB = 64;
+
+// Super-strips of SW = 4 x SB columns: the diagonal kernel chains the four
+// SB-blocks of a strip inside one CTA (inverse-block products plus the
+// couplings between them), the update and partial kernels spread the rows
+// below the strip over many CTAs.
+constexpr int SW = 256;
+
+// forward (a): y for the SB-blocks of strip kb (one CTA per front)
 template <typename T>
 __global__ void __launch_bounds__(256)
-k_fwd(const int32_t* __restrict__ list, const int32_t* __restrict__ first, const int32_t* __restrict__ mrows,
-      const int64_t* __restrict__ Lptr, const int64_t* __restrict__ relptr, const T* __restrict__ L, int nr,
-      int64_t n, double* __restrict__ xp, double* __restrict__ V) {
+k_fwd_sdiag(const int32_t* __restrict__ list, const int32_t* __restrict__ first, const int32_t* __restrict__ mrows,
+            const int64_t* __restrict__ Lptr, const int64_t* __restrict__ Dptr, const T* __restrict__ L,
+            const T* __restrict__ Dinv, int kb, int nr, int64_t n, double* __restrict__ xp) {
   int s = list[blockIdx.x];
-  int f = first[s], c = first[s + 1] - f, m = mrows[s], r = m - c;
+  int f = first[s], c = first[s + 1] - f, m = mrows[s];
+  int j0 = kb * SW;
+  if (j0 >= c) return;
   const T* P = L + Lptr[s];
-  double* v = V + relptr[s] * nr;
-  __shared__ double ys[NB][8];
-  for (int jb = 0; jb < c; jb += NB) {
-    int kn = min(NB, c - jb);
-    if (threadIdx.x < 32) {
-      int k = threadIdx.x;
-      if (k < nr) {
-        double y[NB];
+  __shared__ double ys[SW][8];
+  
+  int nsub = min(SW / SB, (c - j0 + SB - 1) / SB);
+  __shared__ double red[8][SB][8];
+  double (*bs)[8] = red[0];   // each (l, k) is reduced and rewritten by one thread
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int t = 0; t < nsub; ++t) {
+    int jt = j0 + t * SB, kt = min(SB, c - jt);
+    // couplings to the earlier sub-blocks: each warp takes a slice of the
+    // columns [j0, jt); lanes cover the SB rows (coalesced column loads)
+    double acc0[8] = {0, 0, 0, 0, 0, 0, 0, 0}, acc1[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int q = j0 + warp; q < jt; q += 8) {
+      const T* colp = P + (int64_t)m * q + jt;
+      double y8[8];
 #pragma unroll
-        for (int l = 0; l < NB; ++l) y[l] = l < kn ? xp[f + jb + l + n * k] : 0.0;
+      for (int k = 0; k < 8; ++k) y8[k] = ys[q - j0][k];
+      double l0v = lane < kt ? (double)colp[lane] : 0.0;
+      double l1v = lane + 32 < kt ? (double)colp[lane + 32] : 0.0;
 #pragma unroll
-        for (int l = 0; l < NB; ++l) {
-          if (l < kn) {
-            double t = y[l];
-            for (int q = 0; q < l; ++q) t -= (double)P[(jb + l) + (int64_t)m * (jb + q)] * y[q];
-            y[l] = t / (double)P[(jb + l) + (int64_t)m * (jb + l)];
-            ys[l][k] = y[l];
-            xp[f + jb + l + n * k] = y[l];
-          }
-        }
+      for (int k = 0; k < 8; ++k) { acc0[k] += l0v * y8[k]; acc1[k] += l1v * y8[k]; }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { red[warp][lane][k] = acc0[k]; red[warp][lane + 32][k] = acc1[k]; }
+    __syncthreads();
+    for (int e = threadIdx.x; e < SB * 8; e += blockDim.x) {
+      int l = e / 8, k = e % 8;
+      double v = 0.0;
+      if (l < kt && k < nr) {
+        v = xp[f + jt + l + n * k];
+        for (int w = 0; w < 8; ++w) v -= red[w][l][k];
       }
+      bs[l][k] = v;
     }
     __syncthreads();
-    for (int i = jb + kn + threadIdx.x; i < m; i += blockDim.x) {
-      double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      for (int l = 0; l < kn; ++l) {
-        double lv = (double)P[i + (int64_t)m * (jb + l)];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) acc[k] += lv * ys[l][k];
+    const T* Dv = Dinv + Dptr[s] + (int64_t)(jt / SB) * SB * SB;
+    for (int e = threadIdx.x; e < SB * 8; e += blockDim.x) {
+      int l = e % SB, k = e / SB;
+      double acc = 0.0;
+      if (l < kt && k < nr) {
+        for (int q = 0; q <= l; ++q) acc += (double)Dv[l + SB * q] * bs[q][k];
+        xp[f + jt + l + n * k] = acc;
       }
-      if (i < c) {
-        for (int k = 0; k < nr; ++k) xp[f + i + n * k] -= acc[k];
-      } else {
-        for (int k = 0; k < nr; ++k) v[(i - c) + (int64_t)r * k] -= acc[k];
-      }
+      ys[t * SB + l][k] = acc;
     }
     __syncthreads();
   }
 }
 
+// forward (b): rows below strip kb, 32 rows x SW columns per CTA
 template <typename T>
 __global__ void __launch_bounds__(256)
-k_bwd(const int32_t* __restrict__ list, const int32_t* __restrict__ first, const int32_t* __restrict__ mrows,
-      const int64_t* __restrict__ Lptr, const int64_t* __restrict__ rows_ptr, const int32_t* __restrict__ rows,
-      const T* __restrict__ L, int nr, int64_t n, double* __restrict__ xp) {
-  int s = list[blockIdx.x];
-  int f = first[s], c = first[s + 1] - f, m = mrows[s];
-  const T* P = L + Lptr[s];
+k_fwd_supdate(const int32_t* __restrict__ list, const int32_t* __restrict__ first, const int32_t* __restrict__ mrows,
+              const int64_t* __restrict__ Lptr, const int64_t* __restrict__ relptr, const T* __restrict__ L, int kb,
+              int nr, int64_t n, double* __restrict__ xp, double* __restrict__ V) {
+  int s = list[blockIdx.y];
+  int f = first[s], c = first[s + 1] - f, m = mrows[s], r = m - c;
+  int j0 = kb * SW;
+  if (j0 >= c) return;
+  int kw = min(SW, c - j0);
+  int row0 = j0 + kw + blockIdx.x * 32;
+  if (row0 >= m) return;
+  __shared__ double ys[SW][8];
+  __shared__ double red[8][32][9];
+  for (int e = threadIdx.x; e < SW * 8; e += blockDim.x) {
+    int l = e / 8, k = e % 8;
+    ys[l][k] = (l < kw && k < nr) ? xp[f + j0 + l + n * k] : 0.0;
+  }
+  __syncthreads();
+  int rr = threadIdx.x & 31, g = threadIdx.x >> 5;   // row, column group of SW/8
+  int i = row0 + rr;
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (i < m) {
+    const T* P = L + Lptr[s] + i;
+    int l0 = g * (SW / 8), l1 = min(l0 + SW / 8, kw);
+    for (int l = l0; l < l1; ++l) {
+      double lv = (double)P[(int64_t)m * (j0 + l)];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) acc[k] += lv * ys[l][k];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) red[g][rr][k] = acc[k];
+  __syncthreads();
+  if (threadIdx.x < 32 * 8) {
+    int row = threadIdx.x & 31, k = threadIdx.x >> 5;
+    int ii = row0 + row;
+    if (ii < m && k < nr) {
+      double t = 0.0;
+      for (int gg = 0; gg < 8; ++gg) t += red[gg][row][k];
+      if (ii < c) xp[f + ii + n * k] -= t;
+      else V[relptr[s] * nr + (ii - c) + (int64_t)r * k] -= t;
+    }
+  }
+}
+
+// Sums each of v[0..7] over the 32 lanes of a warp with 9 exchanges instead
+// of 8 separate 5-step reductions: every step hands half of the remaining
+// components to the partner lane.  Lane L ends with the total of component
+// (L >> 2) & 7 (all four lanes of a quad hold the same value).
+__device__ __forceinline__ double warp_sum8(const double (&v)[8], int lane) {
+  const unsigned full = 0xffffffffu;
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+  double a[4], b[2];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    double keep = b4 ? v[k + 4] : v[k], send = b4 ? v[k] : v[k + 4];
+    a[k] = keep + __shfl_xor_sync(full, send, 16);
+  }
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    double keep = b3 ? a[k + 2] : a[k], send = b3 ? a[k] : a[k + 2];
+    b[k] = keep + __shfl_xor_sync(full, send, 8);
+  }
+  double c = (b2 ? b[1] : b[0]) + __shfl_xor_sync(full, b2 ? b[0] : b[1], 4);
+  c += __shfl_xor_sync(full, c, 2);
+  c += __shfl_xor_sync(full, c, 1);
+  return c;
+}
+
+// backward (a): partial dots for the SW columns of strip kb over a tile of
+// 256 rows x 32 columns below the strip (8 warps x 4 columns)
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_bwd_spartial(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
+               const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
+               const int64_t* __restrict__ rows_ptr, const int32_t* __restrict__ rows,
+               const int64_t* __restrict__ part_off, const T* __restrict__ L, int kb, int nr, int64_t n,
+               const double* __restrict__ xp, double* __restrict__ part) {
+  int s = list[blockIdx.y];
+  int c = first[s + 1] - first[s], m = mrows[s];
+  int j0 = kb * SW;
+  if (j0 >= c) return;
+  int kw = min(SW, c - j0);
+  int nrb = (m - (j0 + kw) + 255) / 256;
+  int rb = blockIdx.x / (SW / 32), cg = blockIdx.x % (SW / 32);
+  if (rb >= nrb || cg * 32 >= kw) return;
+  int row0 = j0 + kw + rb * 256;
+  __shared__ double xs[256][8];
   const int32_t* R = rows + rows_ptr[s];
-  __shared__ double tsum[NB][8];
+  for (int e = threadIdx.x; e < 256 * 8; e += blockDim.x) {
+    int ii = e / 8, k = e % 8;
+    int i = row0 + ii;
+    xs[ii][k] = (i < m && k < nr) ? xp[(int64_t)R[i] + n * k] : 0.0;
+  }
+  __syncthreads();
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int nblk = (c + NB - 1) / NB;
-  for (int bi = nblk - 1; bi >= 0; --bi) {
-    int jb = bi * NB, kn = min(NB, c - jb);
-    // t_l = sum_{i >= jb+kn} L[i, jb+l] x_i
-    for (int l = warp; l < kn; l += 8) {
-      double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      const T* col = P + (int64_t)m * (jb + l);
-      for (int i = jb + kn + lane; i < m; i += 32) {
+  double* out = part + part_off[blockIdx.y] + (int64_t)rb * SW * 8;
+  for (int q = 0; q < 4; ++q) {
+    int jj = cg * 32 + warp * 4 + q;
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (jj < kw) {
+      const T* col = L + Lptr[s] + (int64_t)m * (j0 + jj);
+      for (int ii = lane; ii < 256; ii += 32) {
+        int i = row0 + ii;
+        if (i >= m) break;
         double lv = (double)col[i];
-        int64_t gi = R[i];
 #pragma unroll
-        for (int k = 0; k < 8; ++k)
-          if (k < nr) acc[k] += lv * xp[gi + n * k];
-      }
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        double v = acc[k];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if (lane == 0) tsum[l][k] = v;
+        for (int k = 0; k < 8; ++k) acc[k] += lv * xs[ii][k];
       }
     }
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      int k = threadIdx.x;
-      if (k < nr) {
-        double x[NB];
-        for (int l = kn - 1; l >= 0; --l) {
-          double t = xp[f + jb + l + n * k] - tsum[l][k];
-          for (int q = l + 1; q < kn; ++q) t -= (double)P[(jb + q) + (int64_t)m * (jb + l)] * x[q];
-          x[l] = t / (double)P[(jb + l) + (int64_t)m * (jb + l)];
-          xp[f + jb + l + n * k] = x[l];
+    double v = warp_sum8(acc, lane);
+    if ((lane & 3) == 0 && jj < SW) out[jj * 8 + (lane >> 2)] = v;
+  }
+}
+
+// backward (b): x for the SB-blocks of strip kb in reverse (one CTA per front)
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_bwd_sdiag(const int32_t* __restrict__ list, const int32_t* __restrict__ first, const int32_t* __restrict__ mrows,
+            const int64_t* __restrict__ Lptr, const int64_t* __restrict__ Dptr, const int64_t* __restrict__ part_off,
+            const T* __restrict__ L, const T* __restrict__ Dinv, int kb, int nr, int64_t n,
+            const double* __restrict__ part, double* __restrict__ xp) {
+  int s = list[blockIdx.x];
+  int f = first[s], c = first[s + 1] - f, m = mrows[s];
+  int j0 = kb * SW;
+  if (j0 >= c) return;
+  int kw = min(SW, c - j0);
+  int nrb = (m - (j0 + kw) + 255) / 256;
+  const T* P = L + Lptr[s];
+  const double* pp = part + part_off[blockIdx.x];
+  __shared__ double xs[SW][8];
+  __shared__ double bs[SB][8];
+  int nsub = (kw + SB - 1) / SB;
+  __shared__ double tsum[SB][8];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int t = nsub - 1; t >= 0; --t) {
+    int jt = j0 + t * SB, kt = min(SB, c - jt);
+    // couplings to the later sub-blocks: column l of this sub-block dotted
+    // with x over rows [jt+kt, j0+kw); one warp per column, lanes over rows
+    for (int l = warp; l < SB; l += 8) {
+      double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      if (l < kt) {
+        const T* colp = P + (int64_t)m * (jt + l);
+        for (int q = jt + kt + lane; q < j0 + kw; q += 32) {
+          double lv = (double)colp[q];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) acc[k] += lv * xs[q - j0][k];
         }
+      }
+      double v = warp_sum8(acc, lane);
+      if ((lane & 3) == 0) tsum[l][lane >> 2] = v;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < SB * 8; e += blockDim.x) {
+      int l = e / 8, k = e % 8;
+      double v = 0.0;
+      if (l < kt && k < nr) {
+        v = xp[f + jt + l + n * k] - tsum[l][k];
+        for (int rb = 0; rb < nrb; ++rb) v -= pp[(int64_t)rb * SW * 8 + (t * SB + l) * 8 + k];
+      }
+      bs[l][k] = v;
+    }
+    __syncthreads();
+    const T* Dv = Dinv + Dptr[s] + (int64_t)(jt / SB) * SB * SB;
+    // x_l = sum_{q >= l} Dinv[q][l] b_q: column l of Dinv is contiguous, so a
+    // warp takes one l and its lanes stride over q
+    for (int l = warp; l < SB; l += 8) {
+      double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      if (l < kt) {
+        const T* colD = Dv + SB * l;
+        for (int q = l + lane; q < kt; q += 32) {
+          double dv = (double)colD[q];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) acc[k] += dv * bs[q][k];
+        }
+      }
+      double v = warp_sum8(acc, lane);
+      if ((lane & 3) == 0) {
+        int k = lane >> 2;
+        if (l < kt && k < nr) xp[f + jt + l + n * k] = v;
+        xs[t * SB + l][k] = (l < kt && k < nr) ? v : 0.0;
       }
     }
     __syncthreads();
@@ -450,18 +758,38 @@ __global__ void k_colnorm2_final(int nb, int nr, const double* __restrict__ part
   out[q] = s;
 }
 
-__global__ void k_copy_scale(int64_t n, int nr, const double* __restrict__ src, const double* __restrict__ scale,
-                             double* __restrict__ dst) {
-  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  double sc = scale ? scale[k] : 1.0;
-  for (int q = 0; q < nr; ++q) dst[k + n * q] = src[k + n * q] * sc;
-}
+struct Coef8 { double v[8]; };
 
-__global__ void k_axpy_sub(int64_t len, const double* __restrict__ a, const double* __restrict__ b,
-                           double* __restrict__ out) {
-  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < len) out[k] = a[k] - b[k];
+__global__ void k_axpy_cols(int64_t len, int nr, Coef8 a, const double* __restrict__ x, double* __restrict__ y) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= len) return;
+  for (int k = 0; k < nr; ++k) y[i + len * k] += a.v[k] * x[i + len * k];
+}
+__global__ void k_xpby_cols(int64_t len, int nr, Coef8 b, const double* __restrict__ z, double* __restrict__ p) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= len) return;
+  for (int k = 0; k < nr; ++k) p[i + len * k] = z[i + len * k] + b.v[k] * p[i + len * k];
+}
+__global__ void k_mask_free(int64_t len, int nr, const uint8_t* __restrict__ free_mask, double* __restrict__ v) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= len || free_mask[i]) return;
+  for (int k = 0; k < nr; ++k) v[i + len * k] = 0.0;
+}
+// per-column dot products of two len x nr blocks (deterministic two-level tree)
+__global__ void k_coldot_partial(int64_t len, int nr, const double* __restrict__ a, const double* __restrict__ b,
+                                 double* __restrict__ part) {
+  __shared__ double sh[256];
+  int q = blockIdx.y;
+  double s = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
+    s += a[i + len * q] * b[i + len * q];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[q * gridDim.x + blockIdx.x] = sh[0];
 }
 
 __global__ void k_diag_of_factor64(int64_t ns, const int32_t* first, const int32_t* mrows, const int64_t* Lptr,
@@ -493,36 +821,44 @@ void upload(std::vector<T>& h, T** d, jfg_ctx* c, jfg_status& st) {
 }
 
 template <typename T>
-jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, cudaStream_t st) {
+jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, cudaStream_t st) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    int bytes = 2 * NB * (NB + 1) * (int)sizeof(T);
+    JFG_CUDA(cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, potrf_smem<T>()));
+    JFG_CUDA(cudaFuncSetAttribute(k_trsm_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    attr_set = true;
+  }
   const Symbolic& S = m->sym;
   for (const auto& lv : F->levels) {
     const int32_t* list = F->level_sn + lv.off;
-    // zero the update matrices of this level's fronts
-    if (lv.max_r > 0) {
-      int64_t mx = (int64_t)lv.max_r * lv.max_r;
-      unsigned gx = (unsigned)std::min<int64_t>((mx + 255) / 256, 4096);
-      { k_zero_U<T><<<dim3(gx, lv.count), 256, 0, st>>>(list, F->first, F->mrows, F->Uptr, Uf); count_launch(); }
-    }
-    // extend-add children, one launch per child rank
+    // extend-add, pass 0: children columns that land in this level's panels
     for (const auto& seg : lv.ea) {
       if (seg.second == 0) continue;
       unsigned gx = (unsigned)((lv.ea_max_r + 7) / 8);
       if (gx == 0) continue;
-      { k_extend_add<T><<<dim3(gx, seg.second), 256, 0, st>>>(F->ea_child + seg.first, F->first, F->mrows,
-                                                            F->parent, F->Lptr, F->Uptr, F->relptr, F->rel, Lf, Uf); count_launch(); }
+      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_extend_add<T><<<dim3(gx, seg.second), 256, 0, st>>>(F->ea_child + seg.first, F->first, F->mrows,
+                                                            F->parent, F->Lptr, F->Uptr, F->relptr, F->rel, Lf, Uf, 0);
+        count_launch(); } prof_end(ps_, st, KS_F_EA, 0.0); }
     }
     // blocked partial factorisation of every front of the level
     for (int k0 = 0; k0 < lv.max_c; k0 += NB) {
-      { k_potrf_diag<T><<<lv.count, dim3(NB, NB), 0, st>>>(list, F->first, F->mrows, F->Lptr, Lf, k0, F->err); count_launch(); }
+      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_potrf_diag<T><<<lv.count, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr,
+                                                                             F->Dptr, Lf, Dvf, k0, F->err);
+        count_launch(); } prof_end(ps_, st, KS_F_POTRF, 0.0); }
       int rows_max = lv.max_m - k0 - 1;
       if (rows_max > 0) {
-        unsigned gx = (unsigned)((rows_max + 127) / 128);
-        { k_trsm_panel<T><<<dim3(gx, lv.count), 128, 0, st>>>(list, F->first, F->mrows, F->Lptr, Lf, k0); count_launch(); }
+        unsigned gx = (unsigned)((rows_max + 63) / 64);
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_trsm_panel<T><<<dim3(gx, lv.count), 256, 2 * NB * (NB + 1) * sizeof(T), st>>>(list, F->first, F->mrows,
+                                                                                          F->Lptr, F->Dptr, Lf, Dvf, k0);
+          count_launch(); } prof_end(ps_, st, KS_F_TRSM, 0.0); }
         int nrow = lv.max_m - k0 - NB, ncol = lv.max_c - k0 - NB;
         if (nrow > 0 && ncol > 0) {
           int64_t tiles = (int64_t)((nrow + TILE - 1) / TILE) * ((ncol + TILE - 1) / TILE);
-          { k_front_update<T><<<dim3((unsigned)tiles, lv.count), 256, 0, st>>>(list, F->first, F->mrows, F->Lptr,
-                                                                          F->Uptr, Lf, Uf, 0, k0); count_launch(); }
+          { int ps_ = fine_prof() ? prof_start(st) : -1;
+            { k_front_update<T><<<dim3((unsigned)tiles, lv.count), 256, 0, st>>>(list, F->first, F->mrows, F->Lptr,
+                                                                            F->Uptr, Lf, Uf, 0, k0); count_launch(); }
+            prof_end(ps_, st, KS_F_PANEL, 0.0); }
         }
       }
     }
@@ -540,6 +876,15 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, cudaStrea
                                                                         F->Uptr, Lf, Uf, 1, 0); count_launch(); }
       prof_end(ps, st, KS_SCHUR, lv.schur_flops);
     }
+    // extend-add, pass 1: children columns that land in the U of this level
+    for (const auto& seg : lv.ea) {
+      if (seg.second == 0) continue;
+      unsigned gx = (unsigned)((lv.ea_max_r + 7) / 8);
+      if (gx == 0) continue;
+      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_extend_add<T><<<dim3(gx, seg.second), 256, 0, st>>>(F->ea_child + seg.first, F->first, F->mrows,
+                                                            F->parent, F->Lptr, F->Uptr, F->relptr, F->rel, Lf, Uf, 1);
+        count_launch(); } prof_end(ps_, st, KS_F_EA, 0.0); }
+    }
     JFG_CUDA(cudaGetLastError());
   }
   (void)S;
@@ -547,7 +892,7 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, cudaStrea
 }
 
 template <typename T>
-void solve_inner(jfg_model* m, NumericFactor* F, const T* Lf, int nr, cudaStream_t st) {
+void solve_inner(jfg_model* m, NumericFactor* F, const T* Lf, const T* Dv, int nr, cudaStream_t st) {
   const Symbolic& S = m->sym;
   int64_t n = S.n;
   int ps = prof_start(st);
@@ -555,19 +900,39 @@ void solve_inner(jfg_model* m, NumericFactor* F, const T* Lf, int nr, cudaStream
   for (size_t li = 0; li < F->levels.size(); ++li) {
     const auto& lv = F->levels[li];
     const int32_t* list = F->level_sn + lv.off;
-    { k_zero_V<<<lv.count, 256, 0, st>>>(list, F->first, F->mrows, F->relptr, nr, F->V); count_launch(); }
+    { int ps_ = fine_prof() ? prof_start(st) : -1; { k_zero_V<<<lv.count, 256, 0, st>>>(list, F->first, F->mrows, F->relptr, nr, F->V); count_launch(); } prof_end(ps_, st, KS_S_VEC, 0.0); }
     for (const auto& seg : lv.ea)
       if (seg.second > 0)
-        { k_vec_extend_add<<<seg.second, 256, 0, st>>>(F->ea_child + seg.first, F->first, F->mrows, F->parent,
-                                                     F->relptr, F->rel, nr, n, F->xp, F->V); count_launch(); }
-    { k_fwd<T><<<lv.count, 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->relptr, Lf, nr, n, F->xp, F->V); count_launch(); }
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_vec_extend_add<<<seg.second, 256, 0, st>>>(F->ea_child + seg.first, F->first, F->mrows, F->parent,
+                                                     F->relptr, F->rel, nr, n, F->xp, F->V); count_launch(); } prof_end(ps_, st, KS_S_VEC, 0.0); }
+    int nstrip = (lv.max_c + SW - 1) / SW;
+    for (int kb = 0; kb < nstrip; ++kb) {
+      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_fwd_sdiag<T><<<lv.count, 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->Dptr, Lf, Dv, kb, nr, n, F->xp);
+        count_launch(); } prof_end(ps_, st, KS_S_FDIAG, 0.0); }
+      int rows = lv.max_m - kb * SW;
+      if (rows > 0) {
+        unsigned gx = (unsigned)((rows + 31) / 32);
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_fwd_supdate<T><<<dim3(gx, lv.count), 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->relptr, Lf, kb,
+                                                              nr, n, F->xp, F->V); count_launch(); } prof_end(ps_, st, KS_S_FUPD, 0.0); }
+      }
+    }
   }
   // backward, root first
   for (size_t li = F->levels.size(); li-- > 0;) {
     const auto& lv = F->levels[li];
     const int32_t* list = F->level_sn + lv.off;
-    { k_bwd<T><<<lv.count, 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->rows_ptr, F->rows, Lf, nr, n,
-                                       F->xp); count_launch(); }
+    const int64_t* poff = F->part_off + lv.off;
+    int nstrip = (lv.max_c + SW - 1) / SW;
+    for (int kb = nstrip - 1; kb >= 0; --kb) {
+      int rows = lv.max_m - kb * SW;
+      if (rows > 0) {
+        unsigned gx = (unsigned)(((rows + 255) / 256) * (SW / 32));
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_bwd_spartial<T><<<dim3(gx, lv.count), 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->rows_ptr, F->rows,
+                                                               poff, Lf, kb, nr, n, F->xp, F->part); count_launch(); } prof_end(ps_, st, KS_S_BPART, 0.0); }
+      }
+      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_bwd_sdiag<T><<<lv.count, 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->Dptr, poff, Lf, Dv, kb, nr, n,
+                                                 F->part, F->xp); count_launch(); } prof_end(ps_, st, KS_S_BDIAG, 0.0); }
+    }
   }
   // algorithmic bytes: the factor read twice (forward and backward) plus the
   // permuted vectors read and written in each sweep
@@ -584,16 +949,20 @@ jfg_status ensure_workspace(jfg_model* m, NumericFactor* F, int nrhs) {
   int64_t n = m->sym.n, ndof = m->ndof;
   if (F->nrhs_cap > 0) {
     int oc = F->nrhs_cap;
-    fr(F->xp, n * oc); fr(F->V, F->v_total * oc); fr(F->dF, ndof * oc); fr(F->dU, ndof * oc);
-    fr(F->dR, ndof * oc); fr(F->dD, n * oc);
+    fr(F->xp, n * oc); fr(F->tt, n * oc); fr(F->V, F->v_total * oc); fr(F->dF, ndof * oc); fr(F->dU, ndof * oc);
+    fr(F->dR, ndof * oc); fr(F->dD, n * oc); fr(F->dZ, ndof * oc); fr(F->dP, ndof * oc); fr(F->dQ, ndof * oc);
   }
   int cap = std::max(nrhs, 8);
   JFG_TRY(dev_alloc(c, (void**)&F->xp, sizeof(double) * n * cap));
+  JFG_TRY(dev_alloc(c, (void**)&F->tt, sizeof(double) * n * cap));
   JFG_TRY(dev_alloc(c, (void**)&F->V, sizeof(double) * std::max<int64_t>(F->v_total, 1) * cap));
   JFG_TRY(dev_alloc(c, (void**)&F->dF, sizeof(double) * ndof * cap));
   JFG_TRY(dev_alloc(c, (void**)&F->dU, sizeof(double) * ndof * cap));
   JFG_TRY(dev_alloc(c, (void**)&F->dR, sizeof(double) * ndof * cap));
   JFG_TRY(dev_alloc(c, (void**)&F->dD, sizeof(double) * n * cap));
+  JFG_TRY(dev_alloc(c, (void**)&F->dZ, sizeof(double) * ndof * cap));
+  JFG_TRY(dev_alloc(c, (void**)&F->dP, sizeof(double) * ndof * cap));
+  JFG_TRY(dev_alloc(c, (void**)&F->dQ, sizeof(double) * ndof * cap));
   F->nrhs_cap = cap;
   return JFG_OK;
 }
@@ -606,6 +975,16 @@ jfg_status check_err(NumericFactor* F, const char* what) {
     JFG_CUDA(cudaMemset(F->err, 0, sizeof(DevError)));
     return JFG_NOT_SPD;
   }
+  return JFG_OK;
+}
+
+jfg_status coldot(NumericFactor* F, int64_t len, int nr, const double* a, const double* b, double* out_host,
+                  cudaStream_t st) {
+  const int nb = 256;
+  { k_coldot_partial<<<dim3(nb, nr), 256, 0, st>>>(len, nr, a, b, F->norms); count_launch(); }
+  { k_colnorm2_final<<<1, 64, 0, st>>>(nb, nr, F->norms, F->norms + nb * 64); count_launch(); }
+  JFG_CUDA(cudaMemcpyAsync(out_host, F->norms + nb * 64, sizeof(double) * nr, cudaMemcpyDeviceToHost, st));
+  JFG_CUDA(cudaStreamSynchronize(st));
   return JFG_OK;
 }
 
@@ -696,8 +1075,49 @@ jfg_status numeric_create(jfg_model* m) {
       }
     }
   }
+  // strip metadata: inverse-block offsets and per-level partial-sum offsets
+  {
+    std::vector<int32_t> ssn, sidx;
+    std::vector<int64_t> dptr(S.ns, 0), poff(S.ns, 0);
+    int64_t dl = 0;
+    for (int64_t sn = 0; sn < S.ns; ++sn) {
+      int64_t cc = S.sn_first[sn + 1] - S.sn_first[sn];
+      int64_t nb = (cc + 63) / 64;
+      dptr[sn] = dl;
+      dl += nb * 64 * 64;
+      for (int64_t b = 0; b < nb; ++b) { ssn.push_back((int32_t)sn); sidx.push_back((int32_t)b); }
+    }
+    int64_t pmax = 0;
+    for (int64_t l = 0; l < S.n_levels; ++l) {
+      int64_t acc = 0;
+      for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
+        int32_t sn = S.level_sn[q];
+        int64_t cc = S.sn_first[sn + 1] - S.sn_first[sn];
+        int64_t kw0 = std::min<int64_t>(256, cc);
+        int64_t nrb0 = (S.sn_m[sn] - kw0 + 255) / 256;
+        poff[q] = acc;
+        acc += nrb0 * 256 * 8;
+      }
+      pmax = std::max(pmax, acc);
+    }
+    F->n_strips = (int64_t)ssn.size();
+    F->dinv_len = std::max<int64_t>(dl, 1);
+    F->part_len = std::max<int64_t>(pmax, 1);
+    upload(ssn, &F->strip_sn, c, st);
+    upload(sidx, &F->strip_idx, c, st);
+    upload(dptr, &F->Dptr, c, st);
+    upload(poff, &F->part_off, c, st);
+    if (st != JFG_OK) return st;
+    JFG_TRY(dev_alloc(c, (void**)&F->part, sizeof(double) * F->part_len));
+  }
   JFG_TRY(dev_alloc(c, (void**)&F->err, sizeof(DevError)));
   JFG_CUDA(cudaMemset(F->err, 0, sizeof(DevError)));
+  {
+    std::vector<uint8_t> mask(m->ndof);
+    for (int64_t d = 0; d < m->ndof; ++d) mask[d] = S.gdof_to_perm[d] >= 0 ? 1 : 0;
+    upload(mask, &F->free_mask, c, st);
+    if (st != JFG_OK) return st;
+  }
   JFG_TRY(dev_alloc(c, (void**)&F->norms, sizeof(double) * (256 * 64 + 64)));
   JFG_CUDA(cudaEventCreate(&F->ev0));
   JFG_CUDA(cudaEventCreate(&F->ev1));
@@ -721,10 +1141,14 @@ void numeric_destroy(jfg_model* m) {
   fr(F->scale, 8 * S.n);
   int oc = F->nrhs_cap;
   if (oc > 0) {
-    fr(F->xp, 8 * S.n * oc); fr(F->V, 8 * std::max<int64_t>(F->v_total, 1) * oc);
+    fr(F->xp, 8 * S.n * oc); fr(F->tt, 8 * S.n * oc); fr(F->V, 8 * std::max<int64_t>(F->v_total, 1) * oc);
     fr(F->dF, 8 * m->ndof * oc); fr(F->dU, 8 * m->ndof * oc); fr(F->dR, 8 * m->ndof * oc);
-    fr(F->dD, 8 * S.n * oc);
+    fr(F->dD, 8 * S.n * oc); fr(F->dZ, 8 * m->ndof * oc); fr(F->dP, 8 * m->ndof * oc); fr(F->dQ, 8 * m->ndof * oc);
   }
+  fr(F->free_mask, m->ndof);
+  fr(F->strip_sn, 4 * std::max<int64_t>(F->n_strips, 1)); fr(F->strip_idx, 4 * std::max<int64_t>(F->n_strips, 1));
+  fr(F->Dptr, 8 * S.ns); fr(F->part_off, 8 * S.ns);
+  fr(F->Dinv64, 8 * F->dinv_len); fr(F->Dinv32, 4 * F->dinv_len); fr(F->part, 8 * F->part_len);
   fr(F->err, sizeof(DevError));
   fr(F->norms, 8 * (256 * 64 + 64));
   if (F->ev0) cudaEventDestroy(F->ev0);
@@ -753,7 +1177,8 @@ jfg_status numeric_factor(jfg_model* m, int precision) {
       { k_scatter_A<double><<<ga, 256, 0, st>>>(F->n_amap, F->amap_src, F->amap_dst, F->amap_pr, F->amap_pc,
                                               m->d_nzval, nullptr, F->L64); count_launch(); }
     F->have64 = false;
-    JFG_TRY(factor_levels<double>(m, F, F->L64, F->U64, st));
+    if (!F->Dinv64) JFG_TRY(dev_alloc(c, (void**)&F->Dinv64, sizeof(double) * F->dinv_len));
+    JFG_TRY(factor_levels<double>(m, F, F->L64, F->U64, F->Dinv64, st));
   } else if (precision == JFG_PREC_MIXED) {
     if (!F->L32) {
       JFG_TRY(dev_alloc(c, (void**)&F->L32, sizeof(float) * S.nnz_L));
@@ -768,7 +1193,8 @@ jfg_status numeric_factor(jfg_model* m, int precision) {
       { k_scatter_A<float><<<ga, 256, 0, st>>>(F->n_amap, F->amap_src, F->amap_dst, F->amap_pr, F->amap_pc,
                                              m->d_nzval, F->scale, F->L32); count_launch(); }
     F->have32 = false;
-    JFG_TRY(factor_levels<float>(m, F, F->L32, F->U32, st));
+    if (!F->Dinv32) JFG_TRY(dev_alloc(c, (void**)&F->Dinv32, sizeof(float) * F->dinv_len));
+    JFG_TRY(factor_levels<float>(m, F, F->L32, F->U32, F->Dinv32, st));
   } else {
     set_error("unknown precision");
     return JFG_BAD_INPUT;
@@ -802,91 +1228,123 @@ jfg_status numeric_factor_diag(jfg_model* m, double* out) {
   return JFG_OK;
 }
 
+// Preconditioned conjugate gradients on K_ff in FP64 with the Cholesky factor
+// (FP64, or the scaled mixed factor) as the preconditioner.  With the FP64
+// factor the first iterate is the direct solution and one or two further
+// steps polish it; with the mixed factor CG recovers FP64 accuracy.  Vectors
+// live in the global DOF space with fixed DOFs held at zero; the matrix-vector
+// product uses the FP64 CSC matrix.  Stagnation of the mixed preconditioner
+// switches to the FP64 factor (restart from the current iterate).
 jfg_status numeric_solve(jfg_model* m, int nrhs, const double* hF, double* hU, double tol, int max_ir,
                          jfg_solve_report* rep, bool device_io) {
   NumericFactor* F = m->num;
   if (!F || !(F->have64 || F->have32)) { set_error("solve before factor"); return JFG_NOT_READY; }
   if (nrhs <= 0) { set_error("nrhs must be positive"); return JFG_BAD_INPUT; }
   if (tol <= 0) tol = 1e-10;
-  if (max_ir < 0) max_ir = 10;
+  if (max_ir < 0) max_ir = 30;
   const Symbolic& S = m->sym;
   jfg_ctx* c = m->ctx;
   cudaStream_t st = c->stream;
-  int64_t n = S.n, ndof = m->ndof;
+  const int64_t n = S.n, ndof = m->ndof;
+  const bool trace = std::getenv("JFG_IR_TRACE") != nullptr;
   JFG_CUDA(cudaEventRecord(F->ev0, st));
-  int done_rhs = 0;
   jfg_solve_report R{};
-  R.precision = F->have32 && !F->have64 ? JFG_PREC_MIXED : JFG_PREC_FP64;
   bool prefer32 = F->have32 && (!F->have64 || F->prefer_mixed);
-  if (prefer32) R.precision = JFG_PREC_MIXED;
+  R.precision = prefer32 ? JFG_PREC_MIXED : JFG_PREC_FP64;
+  const unsigned gn = (unsigned)((n + 255) / 256), gd = (unsigned)((ndof + 255) / 256);
+  int done_rhs = 0;
   while (done_rhs < nrhs) {
     int nr = std::min(8, nrhs - done_rhs);
     JFG_TRY(ensure_workspace(m, F, nr));
+    double *X = F->dU, *Rv = F->dR, *Z = F->dZ, *Pv = F->dP, *Q = F->dQ;
     const double* srcF = hF + ndof * done_rhs;
     JFG_CUDA(cudaMemcpyAsync(F->dF, srcF, sizeof(double) * ndof * nr,
                              device_io ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
-    JFG_CUDA(cudaMemsetAsync(F->dU, 0, sizeof(double) * ndof * nr, st));
-    unsigned gn = (unsigned)((n + 255) / 256);
-    // r = F_ff (u = 0), permuted, and ||F_ff||
-    { k_gather_perm<<<gn, 256, 0, st>>>(n, nr, F->perm_dof, nullptr, F->dF, ndof, F->dD, 1.0); count_launch(); }
-    double fn[8], rn[8], prev[8];
-    JFG_TRY(colnorm2(F, n, nr, F->dD, fn, st));
     bool use32 = prefer32;
-    int it = 0, stall_count = 0;
-    double rn_max_prev = 1e300;
-    double worst = 0;
-    for (int q = 0; q < nr; ++q) prev[q] = 1e300;
-    for (;;) {
+    auto precond = [&](const double* rin, double* zout) -> jfg_status {
       const double* sc = use32 ? F->scale : nullptr;
-      int64_t len = n * nr;
-      { k_copy_scale<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, nr, F->dD, sc, F->xp); count_launch(); }
-      if (use32) solve_inner<float>(m, F, F->L32, nr, st);
-      else solve_inner<double>(m, F, F->L64, nr, st);
-      { k_scatter_add_perm<<<gn, 256, 0, st>>>(n, nr, F->perm_dof, sc, F->xp, F->dU, ndof); count_launch(); }
-      // R = F - K u over all DOFs; its free part is the next right-hand side
-      spmv_csc_sym(m, nr, F->dU, ndof, F->dR, ndof, st);
-      int64_t lg = ndof * nr;
-      { k_axpy_sub<<<(unsigned)((lg + 255) / 256), 256, 0, st>>>(lg, F->dF, F->dR, F->dR); count_launch(); }
-      { k_gather_perm<<<gn, 256, 0, st>>>(n, nr, F->perm_dof, nullptr, F->dR, ndof, F->dD, 1.0); count_launch(); }
-      (void)len;
-      JFG_TRY(colnorm2(F, n, nr, F->dD, rn, st));
-      worst = 0;
-      for (int q = 0; q < nr; ++q) {
-        double rel = fn[q] > 0 ? sqrt(rn[q] / fn[q]) : sqrt(rn[q]);
-        rn[q] = rel;
-        worst = std::max(worst, rel);
+      { k_gather_perm<<<gn, 256, 0, st>>>(n, nr, F->perm_dof, sc, rin, ndof, F->xp, 1.0); count_launch(); }
+      if (use32) solve_inner<float>(m, F, F->L32, F->Dinv32, nr, st);
+      else solve_inner<double>(m, F, F->L64, F->Dinv64, nr, st);
+      JFG_CUDA(cudaMemsetAsync(zout, 0, sizeof(double) * ndof * nr, st));
+      { k_scatter_add_perm<<<gn, 256, 0, st>>>(n, nr, F->perm_dof, sc, F->xp, zout, ndof); count_launch(); }
+      return JFG_OK;
+    };
+    auto matvec = [&](const double* x, double* y) {
+      spmv_csc_sym(m, nr, x, ndof, y, ndof, st);
+      { k_mask_free<<<gd, 256, 0, st>>>(ndof, nr, F->free_mask, y); count_launch(); }
+    };
+    // b = F restricted to the free DOFs
+    JFG_CUDA(cudaMemcpyAsync(Rv, F->dF, sizeof(double) * ndof * nr, cudaMemcpyDeviceToDevice, st));
+    { k_mask_free<<<gd, 256, 0, st>>>(ndof, nr, F->free_mask, Rv); count_launch(); }
+    double bn[8], rz[8], pq[8], rr[8], rzn[8];
+    JFG_TRY(coldot(F, ndof, nr, Rv, Rv, bn, st));
+    JFG_CUDA(cudaMemsetAsync(X, 0, sizeof(double) * ndof * nr, st));
+    int it = 0, restarts = 0, stall = 0;
+    double last_true = 1e300;
+    double worst = 1.0, best = 1e300;
+    bool fresh = true;
+    for (;;) {
+      if (fresh) {
+        JFG_TRY(precond(Rv, Z));
+        JFG_CUDA(cudaMemcpyAsync(Pv, Z, sizeof(double) * ndof * nr, cudaMemcpyDeviceToDevice, st));
+        JFG_TRY(coldot(F, ndof, nr, Rv, Z, rz, st));
+        fresh = false;
       }
-      if (std::getenv("JFG_IR_TRACE"))
-        std::fprintf(stderr, "[jfg] ir step %d (%s factor): max relative residual %.3e\n", it,
+      matvec(Pv, Q);
+      JFG_TRY(coldot(F, ndof, nr, Pv, Q, pq, st));
+      Coef8 al{}, nal{};
+      for (int k = 0; k < nr; ++k) {
+        al.v[k] = (pq[k] > 0.0 && rz[k] > 0.0) ? rz[k] / pq[k] : 0.0;
+        nal.v[k] = -al.v[k];
+      }
+      { k_axpy_cols<<<gd, 256, 0, st>>>(ndof, nr, al, Pv, X); count_launch(); }
+      { k_axpy_cols<<<gd, 256, 0, st>>>(ndof, nr, nal, Q, Rv); count_launch(); }
+      ++it;
+      JFG_TRY(coldot(F, ndof, nr, Rv, Rv, rr, st));
+      worst = 0.0;
+      for (int k = 0; k < nr; ++k) worst = std::max(worst, bn[k] > 0 ? std::sqrt(rr[k] / bn[k]) : std::sqrt(rr[k]));
+      if (trace)
+        std::fprintf(stderr, "[jfg] pcg step %d (%s preconditioner): max recursive relative residual %.3e\n", it,
                      use32 ? "mixed" : "fp64", worst);
-      if (worst <= tol || it >= max_ir) break;
-      // stagnation: a step that does not reduce some unconverged residual by
-      // at least 10 % counts as stalled; two stalled steps in a row end the
-      // refinement (after a switch to the FP64 factor for the mixed path)
-      bool stalled = false;
-      for (int q = 0; q < nr; ++q)
-        if (rn[q] > tol && rn[q] > 0.9 * prev[q]) stalled = true;
-      stall_count = stalled ? stall_count + 1 : 0;
-      if (stall_count >= 2 || (stalled && use32 && rn_max_prev < worst)) {
-        if (use32) {
-          // refinement with the mixed factor stalls: FP64 factor fallback
+      bool conv = worst <= 0.5 * tol;
+      stall = worst > 0.7 * best ? stall + 1 : 0;
+      best = std::min(best, worst);
+      if (conv || it >= max_ir || stall >= 3) {
+        // true residual F - K x on the free DOFs (compensated)
+        residual_dd(m, nr, X, F->dF, Rv, st);
+        { k_mask_free<<<gd, 256, 0, st>>>(ndof, nr, F->free_mask, Rv); count_launch(); }
+        JFG_TRY(coldot(F, ndof, nr, Rv, Rv, rr, st));
+        worst = 0.0;
+        for (int k = 0; k < nr; ++k) worst = std::max(worst, bn[k] > 0 ? std::sqrt(rr[k] / bn[k]) : std::sqrt(rr[k]));
+        if (trace) std::fprintf(stderr, "[jfg] pcg true relative residual %.3e after %d steps\n", worst, it);
+        if (worst <= tol || it >= max_ir || restarts >= 3 || worst > 0.9 * last_true) break;
+        last_true = worst;
+        // restart from the current iterate; a stalled mixed preconditioner is
+        // replaced by the FP64 factor
+        if (stall >= 3 && use32) {
           if (!F->have64) JFG_TRY(numeric_factor(m, JFG_PREC_FP64));
           use32 = false;
-          stall_count = 0;
           R.fallback_used = 1;
           R.precision = JFG_PREC_FP64;
-        } else {
-          break;
         }
+        ++restarts;
+        stall = 0;
+        best = 1e300;
+        fresh = true;
+        continue;
       }
-      rn_max_prev = worst;
-      for (int q = 0; q < nr; ++q) prev[q] = rn[q];
-      ++it;
+      JFG_TRY(precond(Rv, Z));
+      JFG_TRY(coldot(F, ndof, nr, Rv, Z, rzn, st));
+      Coef8 be{};
+      for (int k = 0; k < nr; ++k) be.v[k] = rz[k] > 0.0 ? rzn[k] / rz[k] : 0.0;
+      { k_xpby_cols<<<gd, 256, 0, st>>>(ndof, nr, be, Z, Pv); count_launch(); }
+      for (int k = 0; k < nr; ++k) rz[k] = rzn[k];
     }
     R.ir_iters = std::max(R.ir_iters, it);
     R.rel_residual = std::max(R.rel_residual, worst);
     double* dstU = hU + ndof * done_rhs;
-    JFG_CUDA(cudaMemcpyAsync(dstU, F->dU, sizeof(double) * ndof * nr,
+    JFG_CUDA(cudaMemcpyAsync(dstU, X, sizeof(double) * ndof * nr,
                              device_io ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
     done_rhs += nr;
   }
@@ -898,7 +1356,7 @@ jfg_status numeric_solve(jfg_model* m, int nrhs, const double* hF, double* hU, d
   prof_flush();
   if (rep) *rep = R;
   if (R.rel_residual > tol) {
-    set_error("iterative refinement did not reach the tolerance", 0);
+    set_error("refinement did not reach the tolerance", 0);
     return JFG_IR_STALLED;
   }
   return JFG_OK;

@@ -17,7 +17,9 @@ void set_error(const std::string& msg, int64_t detail = 0);
 void count_launch(int n = 1);
 int64_t launch_count();
 
-enum KernelStat : int { KS_SCHUR = 0, KS_Q4 = 1, KS_ASSEMBLY = 2, KS_SOLVE = 3, KS_T10 = 4, KS_COUNT = 5 };
+enum KernelStat : int { KS_SCHUR = 0, KS_Q4 = 1, KS_ASSEMBLY = 2, KS_SOLVE = 3, KS_T10 = 4,
+                        KS_F_EA = 5, KS_F_POTRF = 6, KS_F_TRSM = 7, KS_F_PANEL = 8, KS_S_VEC = 9,
+                        KS_S_FDIAG = 10, KS_S_FUPD = 11, KS_S_BPART = 12, KS_S_BDIAG = 13, KS_COUNT = 14 };
 struct KernelStats {
   int64_t launches[KS_COUNT] = {0};
   double ms[KS_COUNT] = {0};
@@ -132,6 +134,7 @@ jfg_status build_pattern(jfg_model* m);
 jfg_status launch_assembly(jfg_model* m, cudaStream_t st);
 void spmv_csc_sym(const jfg_model* m, int nrhs, const double* x, int64_t ldx, double* y,
                   int64_t ldy, cudaStream_t st);
+void residual_dd(const jfg_model* m, int nrhs, const double* x, const double* f, double* r, cudaStream_t st);
 // factor.cu
 jfg_status numeric_create(jfg_model* m);
 void numeric_destroy(jfg_model* m);
