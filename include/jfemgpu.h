@@ -166,6 +166,22 @@ jfg_status jfg_solve_device(jfg_model* model, int32_t nrhs, const double* F_dev,
 /* Device time of the last element, assembly, factor and solve calls (s). */
 jfg_status jfg_get_timings(jfg_model* model, double* seconds4);
 
+/* No counterpart in the reference.  Re-runs the element kernels and the
+ * slot-map gather of jfg_assemble and writes K's nnz values (the order of
+ * jfg_get_pattern) to nzval_dev, a DEVICE buffer the caller owns, without
+ * allocating any device memory: for callers that cannot call cudaMalloc
+ * between solves (device memory held by another framework's caching pool,
+ * or other streams that a device-wide cudaMalloc/cudaFree would stall).
+ * The element matrices live in one fixed 16 MiB device array of the
+ * library, so models needing more element storage (about 3,600 CQUAD4 or
+ * 2,300 CTETRA10) get JFG_BAD_INPUT.  jfg_assemble must have been called
+ * once on the model (it builds the pattern).  All calls on a device share
+ * that array: calls that overlap on the GPU race and must be serialised.
+ * The first call on each device looks the array's address up; make it
+ * before starting any stream capture on that device.  Returns after the
+ * values are written (synchronises the model's stream).                  */
+jfg_status jfg_assemble_values_noalloc(jfg_model* model, double* nzval_dev);
+
 /* ---- instrumentation ----------------------------------------------------- */
 /* Number of kernels this library has launched since load.                   */
 int64_t jfg_launch_count(void);

@@ -327,4 +327,13 @@ void spmv_csc_sym(const jfg_model* m, int nrhs, const double* x, int64_t ldx, do
                                            x, ldx, y, ldy); count_launch(); }
 }
 
+// The slot-map gather of launch_assembly reading element values from `ev`
+// and writing the nnz values to `nzval`; no profiling events.
+jfg_status launch_gather_into(const jfg_model* m, cudaStream_t st, const double* ev, double* nzval) {
+  int64_t blocks = (m->nnz + 255) / 256;
+  { k_assemble<<<(unsigned)blocks, 256, 0, st>>>(m->nnz, m->d_nzptr, m->d_trip, ev, nzval); count_launch(); }
+  JFG_CUDA(cudaGetLastError());
+  return JFG_OK;
+}
+
 }  // namespace jfg

@@ -762,4 +762,34 @@ jfg_status launch_elements(jfg_model* m, cudaStream_t st) {
   return JFG_OK;
 }
 
+// Same element kernels as launch_elements, writing the element matrices to
+// `ev` (n_ev doubles) and the first element error to `err` instead of the
+// model's own buffers; no profiling events.
+jfg_status launch_elements_into(const jfg_model* m, cudaStream_t st, double* ev, DevError* err) {
+  if (m->n_q8 > 0) {
+    set_error("CQUAD8 device kernel not built into this library version");
+    return JFG_UNSUPPORTED;
+  }
+  if (m->n_q4 > 0) {
+    int64_t blocks = (m->n_q4 + WARPS - 1) / WARPS;
+    { k_q4<<<(unsigned)blocks, WARPS * 32, 0, st>>>(m->n_q4, m->d_q4n, m->d_q4s, m->d_xyz, m->d_R, ev, err);
+      count_launch(); }
+    JFG_CUDA(cudaGetLastError());
+  }
+  if (m->n_t10 > 0) {
+    bool ident = true;
+    for (int64_t i = 0; i < m->n_nodes && ident; ++i) {
+      const double* R = m->h_R.data() + 9 * i;
+      ident = R[0] == 1 && R[4] == 1 && R[8] == 1 && R[1] == 0 && R[2] == 0 && R[3] == 0 &&
+              R[5] == 0 && R[6] == 0 && R[7] == 0;
+    }
+    int64_t blocks = (m->n_t10 + WARPS - 1) / WARPS;
+    { k_t10<<<(unsigned)blocks, WARPS * 32, 0, st>>>(m->n_t10, m->d_t10n, m->d_t10m, m->d_xyz, m->d_R,
+                                                  ident ? 1 : 0, ev + m->ev_t10_off, err);
+      count_launch(); }
+    JFG_CUDA(cudaGetLastError());
+  }
+  return JFG_OK;
+}
+
 }  // namespace jfg

@@ -129,9 +129,11 @@ namespace jfg {
 
 // elements.cu
 jfg_status launch_elements(jfg_model* m, cudaStream_t st);
+jfg_status launch_elements_into(const jfg_model* m, cudaStream_t st, double* ev, DevError* err);
 // assembly.cu
 jfg_status build_pattern(jfg_model* m);
 jfg_status launch_assembly(jfg_model* m, cudaStream_t st);
+jfg_status launch_gather_into(const jfg_model* m, cudaStream_t st, const double* ev, double* nzval);
 void spmv_csc_sym(const jfg_model* m, int nrhs, const double* x, int64_t ldx, double* y,
                   int64_t ldy, cudaStream_t st);
 void residual_dd(const jfg_model* m, int nrhs, const double* x, const double* f, double* r, cudaStream_t st);

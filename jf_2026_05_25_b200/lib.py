@@ -91,6 +91,7 @@ def load():
         "jfg_update_q4_sections": [P, I64, P, P],
         "jfg_get_timings": [P, P],
         "jfg_symbolic_dry_run": [I64, P, P, I64, P, P, P, P],
+        "jfg_assemble_values_noalloc": [P, P],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -290,6 +291,11 @@ class DeviceModel:
         elems = np.ascontiguousarray(elems, np.int32)
         sect = np.ascontiguousarray(sect, np.float64)
         _check(load().jfg_update_q4_sections(self.h, len(elems), _p(elems), _p(sect)))
+
+    def assemble_values_noalloc(self, nzval_dev_ptr: int):
+        """K's values into a caller-owned device buffer (nnz doubles) with no
+        device allocation inside the library; see jfg_assemble_values_noalloc."""
+        _check(load().jfg_assemble_values_noalloc(self.h, P(nzval_dev_ptr)))
 
     def timings(self) -> dict:
         t = np.zeros(4)
