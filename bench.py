@@ -43,6 +43,10 @@ def make_workload(name: str):
     if name == "wing_panel":
         return M.wing_panel(), {"workload": "wing_panel_200x400_9blades_20x400", "grids": 152781,
                                 "cquad4": 152000, "ndof": 916686, "free_dof": 914400, "subcases": 8}
+    if name == "wing_panel_small":
+        m = M.wing_panel(nx=100, ny=200, blade_nz=10)
+        return m, {"workload": "wing_panel_100x200_9blades_10x200", "grids": m.n_nodes,
+                   "cquad4": len(m.q4_nodes), "ndof": m.ndof, "subcases": len(m.load_cases)}
     if name == "plate":
         return M.flat_plate(), {"workload": "flat_plate_20x20", "grids": 441, "ndof": 2646, "subcases": 1}
     if name == "solid_block":
@@ -346,7 +350,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--workload", default="wing_panel", choices=["wing_panel", "plate", "solid_block"])
+    ap.add_argument("--workload", default="wing_panel", choices=["wing_panel", "wing_panel_small", "plate", "solid_block"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
     args = ap.parse_args()

@@ -46,11 +46,16 @@ struct NumericFactor {
   float* U32 = nullptr;
   double* scale = nullptr;    // n, symmetric diagonal scaling of the mixed factor
   // inverse diagonal blocks of the strip solve
-  int64_t n_strips = 0, dinv_len = 0, part_len = 0;
-  int32_t *strip_sn = nullptr, *strip_idx = nullptr;
+  int64_t dinv_len = 0, part_len = 0;
   int64_t *Dptr = nullptr, *part_off = nullptr;
   double* Dinv64 = nullptr;
   float* Dinv32 = nullptr;
+  // inverses of the 256-column strip diagonal blocks (solve only)
+  int64_t sinv_len = 0, n_inv_items = 0;
+  int64_t* Sptr = nullptr;
+  int32_t *inv_sn = nullptr, *inv_kb = nullptr, *inv_jb = nullptr;
+  double* Sinv64 = nullptr;
+  float* Sinv32 = nullptr;
   double* part = nullptr;
   bool have64 = false, have32 = false;
   bool prefer_mixed = false;   // solve with the mixed factor when both exist
@@ -443,9 +448,12 @@ __global__ void k_vec_extend_add(const int32_t* __restrict__ child, const int32_
   const int32_t* rl = rel + relptr[ch];
   const double* src = V + relptr[ch] * nr;
   double* vp = V + relptr[p] * nr;
-  for (int q = threadIdx.x; q < rc * nr; q += blockDim.x) {
-    int a = q % rc, k = q / rc;
-    int ra = rl[a];
+  // blockIdx.y takes a chunk of 256 update rows; children of one launch have
+  // distinct parents, and distinct rows of a child map to distinct targets
+  int a = blockIdx.y * 256 + threadIdx.x;
+  if (a >= rc) return;
+  int ra = rl[a];
+  for (int k = 0; k < nr; ++k) {
     double v = src[a + (int64_t)rc * k];
     if (ra < cp) xp[first[p] + ra + n * k] += v;
     else vp[(ra - cp) + (int64_t)rp * k] += v;
@@ -453,74 +461,159 @@ __global__ void k_vec_extend_add(const int32_t* __restrict__ child, const int32_
 }
 
 // ---------------------------------------------------------------- strip solves
-// The solve sweeps every front of a level in strips of SB columns.  The
-// inverse of each SB x SB diagonal block is formed once per factorisation,
-// so a strip costs one small matrix-vector product plus wide, coalesced
-// updates of the rows below the strip spread over many CTAs.
+// The solve sweeps every front of a level in strips of SW = 256 columns.  The
+// inverse X of each strip's diagonal block (kw x kw, kw = min(256, width
+// left)) is formed once per factorisation (k_strip_inverse), so the diagonal
+// part of a strip is one dense matrix-vector product per CTA; the rows below
+// the strip are updated (forward) or dotted (backward) by wide, coalesced
+// kernels over many CTAs.
 constexpr int SB = 64;
-
-// Super-strips of SW = 4 x SB columns: the diagonal kernel chains the four
-// SB-blocks of a strip inside one CTA (inverse-block products plus the
-// couplings between them), the update and partial kernels spread the rows
-// below the strip over many CTAs.
 constexpr int SW = 256;
 
-// forward (a): y for the SB-blocks of strip kb (one CTA per front)
+// Strip inverses from the 64 x 64 inverse blocks D_i of the factor: block
+// column jb of X = L_strip^{-1} is X_jj = D_jb and, for i > jb,
+// X_ij = -D_i * sum_{jb <= k < i} L_ik X_kj  (block forward substitution).
+// One CTA per (front, strip, block column); X is column-major with ld kw.
 template <typename T>
 __global__ void __launch_bounds__(256)
-k_fwd_sdiag(const int32_t* __restrict__ list, const int32_t* __restrict__ first, const int32_t* __restrict__ mrows,
-            const int64_t* __restrict__ Lptr, const int64_t* __restrict__ Dptr, const T* __restrict__ L,
-            const T* __restrict__ Dinv, int kb, int nr, int64_t n, double* __restrict__ xp) {
-  int s = list[blockIdx.x];
-  int f = first[s], c = first[s + 1] - f, m = mrows[s];
+k_strip_inverse(const int32_t* __restrict__ it_sn, const int32_t* __restrict__ it_kb,
+                const int32_t* __restrict__ it_jb, const int32_t* __restrict__ first,
+                const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
+                const int64_t* __restrict__ Dptr, const int64_t* __restrict__ Sptr, const T* __restrict__ L,
+                const T* __restrict__ Dinv, T* __restrict__ Sinv) {
+  const int s = it_sn[blockIdx.x], kb = it_kb[blockIdx.x], jb = it_jb[blockIdx.x];
+  const int c = first[s + 1] - first[s], m = mrows[s];
+  const int j0 = kb * SW, kw = min(SW, c - j0), nblk = (kw + SB - 1) / SB;
+  const T* P = L + Lptr[s];
+  const T* Dv = Dinv + Dptr[s] + (int64_t)(kb * (SW / SB)) * SB * SB;
+  T* X = Sinv + Sptr[s] + (int64_t)kb * SW * SW;
+  extern __shared__ unsigned char smem_raw[];
+  T (*As)[SB + 1] = reinterpret_cast<T (*)[SB + 1]>(smem_raw);
+  T (*Bs)[SB + 1] = As + SB;
+  const int t = threadIdx.x, tr = t & 15, tc = t >> 4;
+  // X_jj = D_jb
+  for (int e = t; e < SB * SB; e += blockDim.x) {
+    int r = e & (SB - 1), q = e >> 6;
+    int gr = SB * jb + r, gq = SB * jb + q;
+    if (gr < kw && gq < kw) X[gr + (int64_t)kw * gq] = Dv[(int64_t)jb * SB * SB + r + SB * q];
+  }
+  __syncthreads();
+  for (int i = jb + 1; i < nblk; ++i) {
+    double acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    for (int k = jb; k < i; ++k) {
+      for (int e = t; e < SB * SB; e += blockDim.x) {
+        int r = e & (SB - 1), q = e >> 6;
+        int ar = SB * i + r, aq = SB * k + q, br = SB * k + r, bq = SB * jb + q;
+        As[r][q] = (ar < kw && aq < kw) ? P[(j0 + ar) + (int64_t)m * (j0 + aq)] : (T)0;
+        Bs[r][q] = (br < kw && bq < kw) ? X[br + (int64_t)kw * bq] : (T)0;
+      }
+      __syncthreads();
+#pragma unroll 8
+      for (int q = 0; q < SB; ++q) {
+        double av[4], bv[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) av[a] = (double)As[tr + 16 * a][q];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) bv[b] = (double)Bs[q][tc + 16 * b];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
+      }
+      __syncthreads();
+    }
+    // X_ij = -D_i * acc
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) Bs[tr + 16 * a][tc + 16 * b] = (T)acc[a][b];
+    for (int e = t; e < SB * SB; e += blockDim.x) {
+      int r = e & (SB - 1), q = e >> 6;
+      As[r][q] = Dv[(int64_t)i * SB * SB + r + SB * q];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+#pragma unroll 8
+    for (int q = 0; q < SB; ++q) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) av[a] = (double)As[tr + 16 * a][q];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) bv[b] = (double)Bs[q][tc + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        int gr = SB * i + tr + 16 * a, gq = SB * jb + tc + 16 * b;
+        if (gr < kw && gq < kw) X[gr + (int64_t)kw * gq] = (T)(-acc[a][b]);
+      }
+    __syncthreads();   // X_ij visible to the CTA before it is read as an operand
+  }
+}
+
+// The diagonal product of a strip is spread over ceil(kw / 32) CTAs, each
+// owning 32 rows (forward) or 32 output columns (backward).  The forward
+// reads b from xp and writes y to the vector tt; the backward reads y from tt
+// and writes x to xp.  No CTA overwrites values another CTA of the same
+// launch reads, and at the end of the backward sweep xp holds the solution.
+// forward (a): y = X b on the rows of strip kb; CTA (g, front) owns rows
+// [32g, 32g + 32) and its 8 warps split the columns j (stride 8)
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_fwd_sdiag(const int32_t* __restrict__ list, const int32_t* __restrict__ first, const int64_t* __restrict__ Sptr,
+            const T* __restrict__ Sinv, int kb, int nr, int64_t n, const double* __restrict__ xp,
+            double* __restrict__ tt) {
+  int s = list[blockIdx.y];
+  int f = first[s], c = first[s + 1] - f;
   int j0 = kb * SW;
   if (j0 >= c) return;
-  const T* P = L + Lptr[s];
-  __shared__ double ys[SW][8];
-  
-  int nsub = min(SW / SB, (c - j0 + SB - 1) / SB);
-  __shared__ double red[8][SB][8];
-  double (*bs)[8] = red[0];   // each (l, k) is reduced and rewritten by one thread
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int t = 0; t < nsub; ++t) {
-    int jt = j0 + t * SB, kt = min(SB, c - jt);
-    // couplings to the earlier sub-blocks: each warp takes a slice of the
-    // columns [j0, jt); lanes cover the SB rows (coalesced column loads)
-    double acc0[8] = {0, 0, 0, 0, 0, 0, 0, 0}, acc1[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int q = j0 + warp; q < jt; q += 8) {
-      const T* colp = P + (int64_t)m * q + jt;
-      double y8[8];
+  int kw = min(SW, c - j0);
+  int g = blockIdx.x, r0 = 32 * g;
+  if (r0 >= kw) return;
+  const T* X = Sinv + Sptr[s] + (int64_t)kb * SW * SW;
+  int rmax = min(kw, r0 + 32);          // columns j < rmax can touch the slab
+  __shared__ double bs[SW][8];
+  __shared__ double red[8][32][9];
+  for (int e = threadIdx.x; e < rmax * 8; e += blockDim.x) {
+    int l = e % rmax, k = e / rmax;
+    bs[l][k] = k < nr ? xp[f + j0 + l + n * k] : 0.0;
+  }
+  __syncthreads();
+  int lane = threadIdx.x & 31, cg = threadIdx.x >> 5;
+  int r = r0 + lane;
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (r < kw) {
+    const T* xr = X + r;
+#pragma unroll 4
+    for (int j = cg; j <= r; j += 8) {
+      double x = (double)xr[(int64_t)kw * j];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) y8[k] = ys[q - j0][k];
-      double l0v = lane < kt ? (double)colp[lane] : 0.0;
-      double l1v = lane + 32 < kt ? (double)colp[lane + 32] : 0.0;
-#pragma unroll
-      for (int k = 0; k < 8; ++k) { acc0[k] += l0v * y8[k]; acc1[k] += l1v * y8[k]; }
+      for (int k = 0; k < 8; ++k) acc[k] += x * bs[j][k];
     }
+  }
 #pragma unroll
-    for (int k = 0; k < 8; ++k) { red[warp][lane][k] = acc0[k]; red[warp][lane + 32][k] = acc1[k]; }
-    __syncthreads();
-    for (int e = threadIdx.x; e < SB * 8; e += blockDim.x) {
-      int l = e / 8, k = e % 8;
+  for (int k = 0; k < 8; ++k) red[cg][lane][k] = acc[k];
+  __syncthreads();
+  for (int e = threadIdx.x; e < 32 * 8; e += blockDim.x) {
+    int l = e & 31, k = e >> 5;
+    if (r0 + l < kw && k < nr) {
       double v = 0.0;
-      if (l < kt && k < nr) {
-        v = xp[f + jt + l + n * k];
-        for (int w = 0; w < 8; ++w) v -= red[w][l][k];
-      }
-      bs[l][k] = v;
+#pragma unroll
+      for (int w = 0; w < 8; ++w) v += red[w][l][k];
+      tt[f + j0 + r0 + l + n * k] = v;
     }
-    __syncthreads();
-    const T* Dv = Dinv + Dptr[s] + (int64_t)(jt / SB) * SB * SB;
-    for (int e = threadIdx.x; e < SB * 8; e += blockDim.x) {
-      int l = e % SB, k = e / SB;
-      double acc = 0.0;
-      if (l < kt && k < nr) {
-        for (int q = 0; q <= l; ++q) acc += (double)Dv[l + SB * q] * bs[q][k];
-        xp[f + jt + l + n * k] = acc;
-      }
-      ys[t * SB + l][k] = acc;
-    }
-    __syncthreads();
   }
 }
 
@@ -529,7 +622,8 @@ template <typename T>
 __global__ void __launch_bounds__(256)
 k_fwd_supdate(const int32_t* __restrict__ list, const int32_t* __restrict__ first, const int32_t* __restrict__ mrows,
               const int64_t* __restrict__ Lptr, const int64_t* __restrict__ relptr, const T* __restrict__ L, int kb,
-              int nr, int64_t n, double* __restrict__ xp, double* __restrict__ V) {
+              int nr, int64_t n, const double* __restrict__ tt, double* __restrict__ xp,
+              double* __restrict__ V) {
   int s = list[blockIdx.y];
   int f = first[s], c = first[s + 1] - f, m = mrows[s], r = m - c;
   int j0 = kb * SW;
@@ -540,8 +634,8 @@ k_fwd_supdate(const int32_t* __restrict__ list, const int32_t* __restrict__ firs
   __shared__ double ys[SW][8];
   __shared__ double red[8][32][9];
   for (int e = threadIdx.x; e < SW * 8; e += blockDim.x) {
-    int l = e / 8, k = e % 8;
-    ys[l][k] = (l < kw && k < nr) ? xp[f + j0 + l + n * k] : 0.0;
+    int l = e & (SW - 1), k = e >> 8;
+    ys[l][k] = (l < kw && k < nr) ? tt[f + j0 + l + n * k] : 0.0;
   }
   __syncthreads();
   int rr = threadIdx.x & 31, g = threadIdx.x >> 5;   // row, column group of SW/8
@@ -550,6 +644,7 @@ k_fwd_supdate(const int32_t* __restrict__ list, const int32_t* __restrict__ firs
   if (i < m) {
     const T* P = L + Lptr[s] + i;
     int l0 = g * (SW / 8), l1 = min(l0 + SW / 8, kw);
+#pragma unroll 8
     for (int l = l0; l < l1; ++l) {
       double lv = (double)P[(int64_t)m * (j0 + l)];
 #pragma unroll
@@ -616,7 +711,7 @@ k_bwd_spartial(const int32_t* __restrict__ list, const int32_t* __restrict__ fir
   __shared__ double xs[256][8];
   const int32_t* R = rows + rows_ptr[s];
   for (int e = threadIdx.x; e < 256 * 8; e += blockDim.x) {
-    int ii = e / 8, k = e % 8;
+    int ii = e & 255, k = e >> 8;
     int i = row0 + ii;
     xs[ii][k] = (i < m && k < nr) ? xp[(int64_t)R[i] + n * k] : 0.0;
   }
@@ -641,75 +736,58 @@ k_bwd_spartial(const int32_t* __restrict__ list, const int32_t* __restrict__ fir
   }
 }
 
-// backward (b): x for the SB-blocks of strip kb in reverse (one CTA per front)
+// backward (b): x = X^T (b - sum of the partial dots) on the rows of strip kb;
+// CTA (g, front) owns outputs [32g, 32g + 32), a warp per output with lanes
+// along column i of X
 template <typename T>
 __global__ void __launch_bounds__(256)
 k_bwd_sdiag(const int32_t* __restrict__ list, const int32_t* __restrict__ first, const int32_t* __restrict__ mrows,
-            const int64_t* __restrict__ Lptr, const int64_t* __restrict__ Dptr, const int64_t* __restrict__ part_off,
-            const T* __restrict__ L, const T* __restrict__ Dinv, int kb, int nr, int64_t n,
-            const double* __restrict__ part, double* __restrict__ xp) {
-  int s = list[blockIdx.x];
+            const int64_t* __restrict__ Sptr, const int64_t* __restrict__ part_off, const T* __restrict__ Sinv,
+            int kb, int nr, int64_t n, const double* __restrict__ part, const double* __restrict__ tt,
+            double* __restrict__ xp) {
+  int s = list[blockIdx.y];
   int f = first[s], c = first[s + 1] - f, m = mrows[s];
   int j0 = kb * SW;
   if (j0 >= c) return;
   int kw = min(SW, c - j0);
+  int g = blockIdx.x, i0 = 32 * g;
+  if (i0 >= kw) return;
   int nrb = (m - (j0 + kw) + 255) / 256;
-  const T* P = L + Lptr[s];
-  const double* pp = part + part_off[blockIdx.x];
-  __shared__ double xs[SW][8];
-  __shared__ double bs[SB][8];
-  int nsub = (kw + SB - 1) / SB;
-  __shared__ double tsum[SB][8];
+  const double* pp = part + part_off[blockIdx.y];
+  const T* X = Sinv + Sptr[s] + (int64_t)kb * SW * SW;
+  __shared__ double bs[SW][8];
+  for (int e = threadIdx.x; e < (kw - i0) * 8; e += blockDim.x) {
+    int l = i0 + (e >> 3), k = e & 7;
+    double v = 0.0;
+    if (k < nr) {
+      // independent partial sums: four loads in flight per step
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      const double* q = pp + l * 8 + k;
+      int rb = 0;
+      for (; rb + 4 <= nrb; rb += 4) {
+        a0 += q[(int64_t)rb * SW * 8];
+        a1 += q[(int64_t)(rb + 1) * SW * 8];
+        a2 += q[(int64_t)(rb + 2) * SW * 8];
+        a3 += q[(int64_t)(rb + 3) * SW * 8];
+      }
+      for (; rb < nrb; ++rb) a0 += q[(int64_t)rb * SW * 8];
+      v = tt[f + j0 + l + n * k] - ((a0 + a1) + (a2 + a3));
+    }
+    bs[l][k] = v;
+  }
+  __syncthreads();
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int t = nsub - 1; t >= 0; --t) {
-    int jt = j0 + t * SB, kt = min(SB, c - jt);
-    // couplings to the later sub-blocks: column l of this sub-block dotted
-    // with x over rows [jt+kt, j0+kw); one warp per column, lanes over rows
-    for (int l = warp; l < SB; l += 8) {
-      double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      if (l < kt) {
-        const T* colp = P + (int64_t)m * (jt + l);
-        for (int q = jt + kt + lane; q < j0 + kw; q += 32) {
-          double lv = (double)colp[q];
+  for (int i = i0 + warp; i < min(kw, i0 + 32); i += 8) {
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const T* col = X + (int64_t)kw * i;
+    for (int j = i + lane; j < kw; j += 32) {
+      double x = (double)col[j];
 #pragma unroll
-          for (int k = 0; k < 8; ++k) acc[k] += lv * xs[q - j0][k];
-        }
-      }
-      double v = warp_sum8(acc, lane);
-      if ((lane & 3) == 0) tsum[l][lane >> 2] = v;
+      for (int k = 0; k < 8; ++k) acc[k] += x * bs[j][k];
     }
-    __syncthreads();
-    for (int e = threadIdx.x; e < SB * 8; e += blockDim.x) {
-      int l = e / 8, k = e % 8;
-      double v = 0.0;
-      if (l < kt && k < nr) {
-        v = xp[f + jt + l + n * k] - tsum[l][k];
-        for (int rb = 0; rb < nrb; ++rb) v -= pp[(int64_t)rb * SW * 8 + (t * SB + l) * 8 + k];
-      }
-      bs[l][k] = v;
-    }
-    __syncthreads();
-    const T* Dv = Dinv + Dptr[s] + (int64_t)(jt / SB) * SB * SB;
-    // x_l = sum_{q >= l} Dinv[q][l] b_q: column l of Dinv is contiguous, so a
-    // warp takes one l and its lanes stride over q
-    for (int l = warp; l < SB; l += 8) {
-      double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      if (l < kt) {
-        const T* colD = Dv + SB * l;
-        for (int q = l + lane; q < kt; q += 32) {
-          double dv = (double)colD[q];
-#pragma unroll
-          for (int k = 0; k < 8; ++k) acc[k] += dv * bs[q][k];
-        }
-      }
-      double v = warp_sum8(acc, lane);
-      if ((lane & 3) == 0) {
-        int k = lane >> 2;
-        if (l < kt && k < nr) xp[f + jt + l + n * k] = v;
-        xs[t * SB + l][k] = (l < kt && k < nr) ? v : 0.0;
-      }
-    }
-    __syncthreads();
+    double v = warp_sum8(acc, lane);
+    int k = lane >> 2;
+    if ((lane & 3) == 0 && k < nr) xp[f + j0 + i + n * k] = v;
   }
 }
 
@@ -891,8 +969,28 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, c
   return JFG_OK;
 }
 
+// Inverses of every strip's diagonal block, one launch over all fronts once
+// the factor is complete (the blocks are independent of each other).
 template <typename T>
-void solve_inner(jfg_model* m, NumericFactor* F, const T* Lf, const T* Dv, int nr, cudaStream_t st) {
+jfg_status strip_inverses(NumericFactor* F, const T* Lf, const T* Dvf, T* Svf, cudaStream_t st) {
+  if (F->n_inv_items == 0) return JFG_OK;
+  static bool attr_set = false;
+  const int bytes = 2 * SB * (SB + 1) * (int)sizeof(T);
+  if (!attr_set) {
+    JFG_CUDA(cudaFuncSetAttribute(k_strip_inverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    attr_set = true;
+  }
+  int ps = fine_prof() ? prof_start(st) : -1;
+  { k_strip_inverse<T><<<(unsigned)F->n_inv_items, 256, bytes, st>>>(F->inv_sn, F->inv_kb, F->inv_jb, F->first,
+                                                                  F->mrows, F->Lptr, F->Dptr, F->Sptr, Lf, Dvf, Svf);
+    count_launch(); }
+  prof_end(ps, st, KS_F_POTRF, 0.0);
+  JFG_CUDA(cudaGetLastError());
+  return JFG_OK;
+}
+
+template <typename T>
+void solve_inner(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int nr, cudaStream_t st) {
   const Symbolic& S = m->sym;
   int64_t n = S.n;
   int ps = prof_start(st);
@@ -903,17 +1001,17 @@ void solve_inner(jfg_model* m, NumericFactor* F, const T* Lf, const T* Dv, int n
     { int ps_ = fine_prof() ? prof_start(st) : -1; { k_zero_V<<<lv.count, 256, 0, st>>>(list, F->first, F->mrows, F->relptr, nr, F->V); count_launch(); } prof_end(ps_, st, KS_S_VEC, 0.0); }
     for (const auto& seg : lv.ea)
       if (seg.second > 0)
-        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_vec_extend_add<<<seg.second, 256, 0, st>>>(F->ea_child + seg.first, F->first, F->mrows, F->parent,
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_vec_extend_add<<<dim3(seg.second, std::max(1, (lv.ea_max_r + 255) / 256)), 256, 0, st>>>(F->ea_child + seg.first, F->first, F->mrows, F->parent,
                                                      F->relptr, F->rel, nr, n, F->xp, F->V); count_launch(); } prof_end(ps_, st, KS_S_VEC, 0.0); }
     int nstrip = (lv.max_c + SW - 1) / SW;
     for (int kb = 0; kb < nstrip; ++kb) {
-      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_fwd_sdiag<T><<<lv.count, 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->Dptr, Lf, Dv, kb, nr, n, F->xp);
+      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_fwd_sdiag<T><<<dim3(SW / 32, lv.count), 256, 0, st>>>(list, F->first, F->Sptr, Sv, kb, nr, n, F->xp, F->tt);
         count_launch(); } prof_end(ps_, st, KS_S_FDIAG, 0.0); }
       int rows = lv.max_m - kb * SW;
       if (rows > 0) {
         unsigned gx = (unsigned)((rows + 31) / 32);
         { int ps_ = fine_prof() ? prof_start(st) : -1; { k_fwd_supdate<T><<<dim3(gx, lv.count), 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->relptr, Lf, kb,
-                                                              nr, n, F->xp, F->V); count_launch(); } prof_end(ps_, st, KS_S_FUPD, 0.0); }
+                                                              nr, n, F->tt, F->xp, F->V); count_launch(); } prof_end(ps_, st, KS_S_FUPD, 0.0); }
       }
     }
   }
@@ -930,8 +1028,8 @@ void solve_inner(jfg_model* m, NumericFactor* F, const T* Lf, const T* Dv, int n
         { int ps_ = fine_prof() ? prof_start(st) : -1; { k_bwd_spartial<T><<<dim3(gx, lv.count), 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->rows_ptr, F->rows,
                                                                poff, Lf, kb, nr, n, F->xp, F->part); count_launch(); } prof_end(ps_, st, KS_S_BPART, 0.0); }
       }
-      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_bwd_sdiag<T><<<lv.count, 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->Dptr, poff, Lf, Dv, kb, nr, n,
-                                                 F->part, F->xp); count_launch(); } prof_end(ps_, st, KS_S_BDIAG, 0.0); }
+      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_bwd_sdiag<T><<<dim3(SW / 32, lv.count), 256, 0, st>>>(list, F->first, F->mrows, F->Sptr, poff, Sv, kb, nr, n,
+                                                 F->part, F->tt, F->xp); count_launch(); } prof_end(ps_, st, KS_S_BDIAG, 0.0); }
     }
   }
   // algorithmic bytes: the factor read twice (forward and backward) plus the
@@ -1075,17 +1173,25 @@ jfg_status numeric_create(jfg_model* m) {
       }
     }
   }
-  // strip metadata: inverse-block offsets and per-level partial-sum offsets
+  // strip metadata: 64-block inverse offsets, 256-strip inverse offsets with
+  // their work items (front, strip, block column), per-level partial offsets
   {
-    std::vector<int32_t> ssn, sidx;
-    std::vector<int64_t> dptr(S.ns, 0), poff(S.ns, 0);
-    int64_t dl = 0;
+    std::vector<int64_t> dptr(S.ns, 0), sptr(S.ns, 0), poff(S.ns, 0);
+    std::vector<int32_t> isn, ikb, ijb;
+    int64_t dl = 0, sl = 0;
     for (int64_t sn = 0; sn < S.ns; ++sn) {
       int64_t cc = S.sn_first[sn + 1] - S.sn_first[sn];
       int64_t nb = (cc + 63) / 64;
       dptr[sn] = dl;
       dl += nb * 64 * 64;
-      for (int64_t b = 0; b < nb; ++b) { ssn.push_back((int32_t)sn); sidx.push_back((int32_t)b); }
+      sptr[sn] = sl;
+      for (int64_t kb = 0; kb * 256 < cc; ++kb) {
+        int64_t kw = std::min<int64_t>(256, cc - 256 * kb);
+        sl += (kw == 256) ? 256 * 256 : kw * kw;
+        for (int64_t jb = 0; jb * 64 < kw; ++jb) {
+          isn.push_back((int32_t)sn); ikb.push_back((int32_t)kb); ijb.push_back((int32_t)jb);
+        }
+      }
     }
     int64_t pmax = 0;
     for (int64_t l = 0; l < S.n_levels; ++l) {
@@ -1100,12 +1206,15 @@ jfg_status numeric_create(jfg_model* m) {
       }
       pmax = std::max(pmax, acc);
     }
-    F->n_strips = (int64_t)ssn.size();
     F->dinv_len = std::max<int64_t>(dl, 1);
+    F->sinv_len = std::max<int64_t>(sl, 1);
+    F->n_inv_items = (int64_t)isn.size();
     F->part_len = std::max<int64_t>(pmax, 1);
-    upload(ssn, &F->strip_sn, c, st);
-    upload(sidx, &F->strip_idx, c, st);
     upload(dptr, &F->Dptr, c, st);
+    upload(sptr, &F->Sptr, c, st);
+    upload(isn, &F->inv_sn, c, st);
+    upload(ikb, &F->inv_kb, c, st);
+    upload(ijb, &F->inv_jb, c, st);
     upload(poff, &F->part_off, c, st);
     if (st != JFG_OK) return st;
     JFG_TRY(dev_alloc(c, (void**)&F->part, sizeof(double) * F->part_len));
@@ -1146,9 +1255,11 @@ void numeric_destroy(jfg_model* m) {
     fr(F->dD, 8 * S.n * oc); fr(F->dZ, 8 * m->ndof * oc); fr(F->dP, 8 * m->ndof * oc); fr(F->dQ, 8 * m->ndof * oc);
   }
   fr(F->free_mask, m->ndof);
-  fr(F->strip_sn, 4 * std::max<int64_t>(F->n_strips, 1)); fr(F->strip_idx, 4 * std::max<int64_t>(F->n_strips, 1));
-  fr(F->Dptr, 8 * S.ns); fr(F->part_off, 8 * S.ns);
+  fr(F->Dptr, 8 * S.ns); fr(F->Sptr, 8 * S.ns); fr(F->part_off, 8 * S.ns);
+  int64_t ni = std::max<int64_t>(F->n_inv_items, 1);
+  fr(F->inv_sn, 4 * ni); fr(F->inv_kb, 4 * ni); fr(F->inv_jb, 4 * ni);
   fr(F->Dinv64, 8 * F->dinv_len); fr(F->Dinv32, 4 * F->dinv_len); fr(F->part, 8 * F->part_len);
+  fr(F->Sinv64, 8 * F->sinv_len); fr(F->Sinv32, 4 * F->sinv_len);
   fr(F->err, sizeof(DevError));
   fr(F->norms, 8 * (256 * 64 + 64));
   if (F->ev0) cudaEventDestroy(F->ev0);
@@ -1178,7 +1289,9 @@ jfg_status numeric_factor(jfg_model* m, int precision) {
                                               m->d_nzval, nullptr, F->L64); count_launch(); }
     F->have64 = false;
     if (!F->Dinv64) JFG_TRY(dev_alloc(c, (void**)&F->Dinv64, sizeof(double) * F->dinv_len));
+    if (!F->Sinv64) JFG_TRY(dev_alloc(c, (void**)&F->Sinv64, sizeof(double) * F->sinv_len));
     JFG_TRY(factor_levels<double>(m, F, F->L64, F->U64, F->Dinv64, st));
+    JFG_TRY(strip_inverses<double>(F, F->L64, F->Dinv64, F->Sinv64, st));
   } else if (precision == JFG_PREC_MIXED) {
     if (!F->L32) {
       JFG_TRY(dev_alloc(c, (void**)&F->L32, sizeof(float) * S.nnz_L));
@@ -1194,7 +1307,9 @@ jfg_status numeric_factor(jfg_model* m, int precision) {
                                              m->d_nzval, F->scale, F->L32); count_launch(); }
     F->have32 = false;
     if (!F->Dinv32) JFG_TRY(dev_alloc(c, (void**)&F->Dinv32, sizeof(float) * F->dinv_len));
+    if (!F->Sinv32) JFG_TRY(dev_alloc(c, (void**)&F->Sinv32, sizeof(float) * F->sinv_len));
     JFG_TRY(factor_levels<float>(m, F, F->L32, F->U32, F->Dinv32, st));
+    JFG_TRY(strip_inverses<float>(F, F->L32, F->Dinv32, F->Sinv32, st));
   } else {
     set_error("unknown precision");
     return JFG_BAD_INPUT;
@@ -1264,8 +1379,8 @@ jfg_status numeric_solve(jfg_model* m, int nrhs, const double* hF, double* hU, d
     auto precond = [&](const double* rin, double* zout) -> jfg_status {
       const double* sc = use32 ? F->scale : nullptr;
       { k_gather_perm<<<gn, 256, 0, st>>>(n, nr, F->perm_dof, sc, rin, ndof, F->xp, 1.0); count_launch(); }
-      if (use32) solve_inner<float>(m, F, F->L32, F->Dinv32, nr, st);
-      else solve_inner<double>(m, F, F->L64, F->Dinv64, nr, st);
+      if (use32) solve_inner<float>(m, F, F->L32, F->Sinv32, nr, st);
+      else solve_inner<double>(m, F, F->L64, F->Sinv64, nr, st);
       JFG_CUDA(cudaMemsetAsync(zout, 0, sizeof(double) * ndof * nr, st));
       { k_scatter_add_perm<<<gn, 256, 0, st>>>(n, nr, F->perm_dof, sc, F->xp, zout, ndof); count_launch(); }
       return JFG_OK;
