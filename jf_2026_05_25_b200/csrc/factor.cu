@@ -947,7 +947,7 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, c
       int ps = prof_start(st);
       if constexpr (sizeof(T) == 4) {
         done = tc::schur_update_tf32x3(list, lv.count, F->first, F->mrows, F->Lptr, F->Uptr, Lf, Uf,
-                                       lv.max_r, lv.max_c, st);
+                                       lv.max_r, lv.max_c, F->err, st);
       }
       if (!done)
         { k_front_update<T><<<dim3((unsigned)tiles, lv.count), 256, 0, st>>>(list, F->first, F->mrows, F->Lptr,
@@ -1072,6 +1072,12 @@ jfg_status check_err(NumericFactor* F, const char* what) {
     set_error(std::string(what) + ": non-positive pivot in permuted column " + std::to_string(h.index), h.index);
     JFG_CUDA(cudaMemset(F->err, 0, sizeof(DevError)));
     return JFG_NOT_SPD;
+  }
+  if (h.code == EE_TC_TIMEOUT) {
+    set_error(std::string(what) + ": tensor-core pipeline wait expired (front " + std::to_string(h.index) + ")",
+              h.index);
+    JFG_CUDA(cudaMemset(F->err, 0, sizeof(DevError)));
+    return JFG_TIMEOUT;
   }
   return JFG_OK;
 }

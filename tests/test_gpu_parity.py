@@ -183,3 +183,26 @@ def test_thickness_update_resolve(ctx, oracle_mod):
     U, rep = dm.solve(m.load_matrix())
     ref = oracle_mod.solve_reference(m)
     assert _rel(U, ref["u"]) <= DISP_RTOL
+
+
+def test_tensor_core_schur_update(ctx, monkeypatch):
+    """The tcgen05 3xTF32 Schur-update kernel (switched on with
+    JFG_TENSOR_CORES=1) against the SIMT FP32 kernel on a model whose
+    update matrices span several 128 x 128 tiles: the mixed-factor diagonals
+    agree to tensor-core FP32 accuracy and both mixed solves refine to the
+    FP64 residual bar and the FP64 displacements."""
+    m = M.solid_block(n=8, n_cases=1)
+    F = m.load_matrix()
+    out = {}
+    for flag in ("0", "1"):
+        monkeypatch.setenv("JFG_TENSOR_CORES", flag)
+        be = B.JFEMGPUBackend(precision=lib.PREC_MIXED)
+        be._ctx = ctx
+        st = B.prepare(be, m)
+        d = st["dm"].factor_diag()
+        U, rep = st["dm"].solve(F, tol=RESID_TOL, max_ir=30)
+        assert rep["rel_residual"] <= RESID_TOL
+        out[flag] = (d, U)
+    rel = np.abs(out["1"][0] - out["0"][0]) / np.abs(out["0"][0])
+    assert rel.max() <= 1e-4, rel.max()
+    assert _rel(out["1"][1], out["0"][1]) <= DISP_RTOL
