@@ -117,6 +117,9 @@ jfg_status read_elem_error(jfg_model* m) {
     case EE_ENRICH: what = "CQUAD4 internal-mode block is singular"; break;
     case EE_T10_JAC: what = "CTETRA10 has a nonpositive Jacobian at an integration point"; break;
     case EE_T10_MAT: what = "CTETRA10 needs finite E > 0 and -1 < nu < 0.5"; break;
+    case EE_Q8_SHAPE: what = "CQUAD8 is not a flat parallelogram with mid-side nodes at the edge midpoints"; st = JFG_UNSUPPORTED; break;
+    case EE_Q8_DREF: what = "CQUAD8 bending section needs a positive reference stiffness D11"; break;
+    case EE_Q8_SINGULAR: what = "CQUAD8 transverse-shear flexibility is singular"; break;
     default:
       if (h.code >= EE_SHEAR && h.code < EE_SHEAR + 10) what = "CQUAD4 MacNeal shear block is degenerate";
       else what = "element kernel error " + std::to_string(h.code);

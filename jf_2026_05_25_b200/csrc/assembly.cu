@@ -28,7 +28,7 @@ uint64_t mask_t10() {
 }
 
 struct ElemRef {
-  int64_t e;        // global element order: Q4 first, then T10
+  int64_t e;        // global element order: Q4 first, then T10, then Q8
   int8_t local;     // local index of the column node in the element
 };
 
@@ -127,19 +127,47 @@ void residual_dd(const jfg_model* m, int nrhs, const double* x, const double* f,
 }
 
 jfg_status build_pattern(jfg_model* m) {
-  if (m->n_q8 > 0) {
-    set_error("CQUAD8 pattern requires the CQUAD8 device kernel");
-    return JFG_UNSUPPORTED;
-  }
   const int64_t nn = m->n_nodes, ndof = m->ndof;
-  const int64_t nq4 = m->n_q4, nt10 = m->n_t10;
+  const int64_t nq4 = m->n_q4, nt10 = m->n_t10, nq8 = m->n_q8;
   const uint64_t mt10 = mask_t10();
+  // CQUAD8 emits only its nonzero entries (assembly.jl:5912-5916), so its
+  // part of the pattern depends on the element values computed just before:
+  // per element and node pair a 6x6 component mask, per column a 48-bit row
+  // mask and the number of nonzeros in the earlier columns.
+  std::vector<uint64_t> q8pair(64 * nq8), q8col(48 * nq8);
+  std::vector<int32_t> q8pref(49 * nq8);
+  std::vector<int64_t> q8off(nq8 + 1, 0);
+  if (nq8 > 0) {
+    std::vector<double> v(2304 * nq8);
+    JFG_CUDA(cudaMemcpy(v.data(), m->d_ev + m->ev_q8_off, sizeof(double) * v.size(), cudaMemcpyDeviceToHost));
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < nq8; ++e) {
+      const double* K = v.data() + 2304 * e;
+      int32_t run = 0;
+      for (int cc = 0; cc < 48; ++cc) {
+        q8pref[49 * e + cc] = run;
+        uint64_t rm = 0;
+        for (int rr = 0; rr < 48; ++rr)
+          if (K[rr + 48 * cc] != 0.0) {
+            rm |= 1ull << rr;
+            ++run;
+            q8pair[64 * e + 8 * (rr / 6) + cc / 6] |= 1ull << ((rr % 6) + 6 * (cc % 6));
+          }
+        q8col[48 * e + cc] = rm;
+      }
+      q8pref[49 * e + 48] = run;
+    }
+    for (int64_t e = 0; e < nq8; ++e) q8off[e + 1] = q8off[e] + q8pref[49 * e + 48];
+  }
+  const int64_t g8 = nq4 + nt10;   // first global index of the CQUAD8 elements
   // node -> incident elements (ascending global order)
   std::vector<int64_t> iptr(nn + 1, 0);
   for (int64_t e = 0; e < nq4; ++e)
     for (int k = 0; k < 4; ++k) iptr[m->h_q4n[4 * e + k] + 1]++;
   for (int64_t e = 0; e < nt10; ++e)
     for (int k = 0; k < 10; ++k) iptr[m->h_t10n[10 * e + k] + 1]++;
+  for (int64_t e = 0; e < nq8; ++e)
+    for (int k = 0; k < 8; ++k) iptr[m->h_q8n[8 * e + k] + 1]++;
   for (int64_t v = 0; v < nn; ++v) iptr[v + 1] += iptr[v];
   std::vector<ElemRef> inc(iptr[nn]);
   {
@@ -148,13 +176,21 @@ jfg_status build_pattern(jfg_model* m) {
       for (int k = 0; k < 4; ++k) inc[pos[m->h_q4n[4 * e + k]]++] = {e, (int8_t)k};
     for (int64_t e = 0; e < nt10; ++e)
       for (int k = 0; k < 10; ++k) inc[pos[m->h_t10n[10 * e + k]]++] = {nq4 + e, (int8_t)k};
+    for (int64_t e = 0; e < nq8; ++e)
+      for (int k = 0; k < 8; ++k) inc[pos[m->h_q8n[8 * e + k]]++] = {g8 + e, (int8_t)k};
   }
   auto enodes = [&](int64_t ge, int& nnd) -> const int32_t* {
     if (ge < nq4) { nnd = 4; return m->h_q4n.data() + 4 * ge; }
-    nnd = 10;
-    return m->h_t10n.data() + 10 * (ge - nq4);
+    if (ge < g8) { nnd = 10; return m->h_t10n.data() + 10 * (ge - nq4); }
+    nnd = 8;
+    return m->h_q8n.data() + 8 * (ge - g8);
   };
-  auto emask = [&](int64_t ge) { return ge < nq4 ? MASK_Q4 : mt10; };
+  // 6x6 component mask of the (row node la, column node lb) block of element ge
+  auto pmask = [&](int64_t ge, int la, int lb) -> uint64_t {
+    if (ge < nq4) return MASK_Q4;
+    if (ge < g8) return mt10;
+    return q8pair[64 * (ge - g8) + 8 * la + lb];
+  };
   // per column node: sorted (row node, mask)
   struct Blk { int32_t a; uint64_t mask; };
   auto node_blocks = [&](int64_t b, std::vector<Blk>& out) {
@@ -162,8 +198,7 @@ jfg_status build_pattern(jfg_model* m) {
     for (int64_t p = iptr[b]; p < iptr[b + 1]; ++p) {
       int nnd;
       const int32_t* en = enodes(inc[p].e, nnd);
-      uint64_t mk = emask(inc[p].e);
-      for (int k = 0; k < nnd; ++k) out.push_back({en[k], mk});
+      for (int k = 0; k < nnd; ++k) out.push_back({en[k], pmask(inc[p].e, k, inc[p].local)});
     }
     std::sort(out.begin(), out.end(), [](const Blk& x, const Blk& y) { return x.a < y.a; });
     size_t w = 0;
@@ -194,8 +229,8 @@ jfg_status build_pattern(jfg_model* m) {
   m->nnz = nnz;
   m->rowval.resize(nnz);
   m->diag_pos.assign(ndof, -1);
-  m->n_trip = 576 * nq4 + 900 * nt10;
-  if (m->n_trip >= (int64_t)INT32_MAX) {
+  m->n_trip = 576 * nq4 + 900 * nt10 + q8off[nq8];
+  if (m->n_trip >= (int64_t)INT32_MAX || m->n_ev >= (int64_t)INT32_MAX) {
     set_error("triplet count exceeds the 32-bit slot-map range");
     return JFG_UNSUPPORTED;
   }
@@ -218,11 +253,13 @@ jfg_status build_pattern(jfg_model* m) {
             // cover the (i, j) component pair
             int32_t c = 0;
             for (int64_t p = iptr[b]; p < iptr[b + 1]; ++p) {
-              if (!((emask(inc[p].e) >> (i + 6 * j)) & 1)) continue;
               int nnd;
               const int32_t* en = enodes(inc[p].e, nnd);
               for (int k = 0; k < nnd; ++k)
-                if (en[k] == x.a) { ++c; break; }
+                if (en[k] == x.a) {
+                  if ((pmask(inc[p].e, k, inc[p].local) >> (i + 6 * j)) & 1) ++c;
+                  break;
+                }
             }
             cnt[q + 1] = c;
             ++q;
@@ -252,7 +289,6 @@ jfg_status build_pattern(jfg_model* m) {
             int32_t w = cnt[q];
             for (int64_t p = iptr[b]; p < iptr[b + 1]; ++p) {
               int64_t ge = inc[p].e;
-              if (!((emask(ge) >> (i + 6 * j)) & 1)) continue;
               int nnd;
               const int32_t* en = enodes(ge, nnd);
               int la = -1;
@@ -260,15 +296,24 @@ jfg_status build_pattern(jfg_model* m) {
                 if (en[k] == x.a) { la = k; break; }
               if (la < 0) continue;
               int lb = inc[p].local;
-              int64_t t;
+              if (!((pmask(ge, la, lb) >> (i + 6 * j)) & 1)) continue;
+              // t: the triplet's position in the reference's triplet order;
+              // src: the element value it reads (equal for Q4 and T10)
+              int64_t t, src;
               if (ge < nq4) {
                 int rr = 6 * la + i, cc = 6 * lb + j;
-                t = 576 * ge + rr + 24 * cc;
-              } else {
+                t = src = 576 * ge + rr + 24 * cc;
+              } else if (ge < g8) {
                 int rr = 3 * la + i, cc = 3 * lb + j;
-                t = 576 * nq4 + 900 * (ge - nq4) + rr + 30 * cc;
+                t = src = 576 * nq4 + 900 * (ge - nq4) + rr + 30 * cc;
+              } else {
+                int64_t e8 = ge - g8;
+                int rr = 6 * la + i, cc = 6 * lb + j;
+                uint64_t below = q8col[48 * e8 + cc] & ((1ull << rr) - 1);
+                t = 576 * nq4 + 900 * nt10 + q8off[e8] + q8pref[49 * e8 + cc] + __builtin_popcountll(below);
+                src = m->ev_q8_off + 2304 * e8 + rr + 48 * cc;
               }
-              trip[w++] = (int32_t)t;
+              trip[w++] = (int32_t)src;
               m->slot[t] = q;
             }
             ++q;

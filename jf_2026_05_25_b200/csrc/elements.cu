@@ -729,6 +729,353 @@ k_t10(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ m
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// CQUAD8 native shell (quad8_shell.jl:34-204; frame and congruences
+// assembly.jl:5893-5915).  One CTA of 128 threads per element:
+//   * thread 0: flat-parallelogram test, element frame, local coordinates;
+//   * threads 0..24: shape functions, derivatives and Jacobians at the 25
+//     points of the 2- and 3-point Gauss abscissas (every integration point
+//     of the element is one of them);
+//   * every thread owns 18 of the 48 x 48 entries and accumulates membrane
+//     (2x2 plus the 3-point excess corrections), bending (2x2 with the twist
+//     split and the 2x3 / 3x2 twist passes) and the shear term
+//     Bs^T F^{-1} Bs (F: 8 x 8 sampled flexibility, inverted by thread 0);
+//   * T^T K T with the element frame, symmetrisation, then the node_R
+//     congruence, each as 9-term block sums out of shared memory.
+// Section record: A (9), D (9), shear = G3 TS/T t, dref = D11, hasA, hasD.
+constexpr int Q8_THREADS = 128;
+
+__device__ __forceinline__ void q8_shape(double r, double s, double N[8], double dr[8], double ds[8]) {
+  const double rc[4] = {-1, 1, 1, -1}, sc[4] = {-1, -1, 1, 1};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    double a = 1 + rc[k] * r, b = 1 + sc[k] * s, c = rc[k] * r + sc[k] * s - 1;
+    N[k] = 0.25 * a * b * c;
+    dr[k] = 0.25 * rc[k] * b * (c + a);
+    ds[k] = 0.25 * sc[k] * a * (c + b);
+  }
+  N[4] = 0.5 * (1 - r * r) * (1 - s); dr[4] = -r * (1 - s);     ds[4] = -0.5 * (1 - r * r);
+  N[5] = 0.5 * (1 + r) * (1 - s * s); dr[5] = 0.5 * (1 - s * s); ds[5] = -s * (1 + r);
+  N[6] = 0.5 * (1 - r * r) * (1 + s); dr[6] = -r * (1 + s);     ds[6] = 0.5 * (1 - r * r);
+  N[7] = 0.5 * (1 - r) * (1 - s * s); dr[7] = -0.5 * (1 - s * s); ds[7] = -s * (1 - r);
+}
+
+__device__ __forceinline__ double q8_norm3(const double* a) { return sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); }
+
+struct Q8Point {
+  double N[8], dx[8], dy[8], det, jac[4];
+};
+
+// membrane / curvature strain-displacement column p (3 components)
+__device__ __forceinline__ void q8_bm(const Q8Point& P, int p, double b[3]) {
+  int k = p / 6, c = p % 6;
+  b[0] = (c == 0) ? P.dx[k] : 0.0;
+  b[1] = (c == 1) ? P.dy[k] : 0.0;
+  b[2] = (c == 0) ? P.dy[k] : (c == 1 ? P.dx[k] : 0.0);
+}
+__device__ __forceinline__ void q8_bb(const Q8Point& P, int p, double b[3]) {
+  int k = p / 6, c = p % 6;
+  b[0] = (c == 4) ? P.dx[k] : 0.0;
+  b[1] = (c == 3) ? -P.dy[k] : 0.0;
+  b[2] = (c == 4) ? P.dy[k] : (c == 3 ? -P.dx[k] : 0.0);
+}
+// b_p^T D b_q, D 3 x 3 column-major
+__device__ __forceinline__ double q8_bdb(const double bp[3], const double* D, const double bq[3]) {
+  double v = 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    double t = D[a] * bq[0] + D[a + 3] * bq[1] + D[a + 6] * bq[2];
+    v += bp[a] * t;
+  }
+  return v;
+}
+
+__global__ void __launch_bounds__(Q8_THREADS)
+k_q8(int64_t n, const int32_t* __restrict__ q8n, const double* __restrict__ q8s, const double* __restrict__ xyz,
+     const double* __restrict__ nodeR, double* __restrict__ ev, DevError* __restrict__ err) {
+  const int64_t e = blockIdx.x;
+  if (e >= n) return;
+  const int t = threadIdx.x;
+  __shared__ double X[24], RN[72], S[22], xy[16], Rf[9];
+  __shared__ Q8Point PT[25];
+  __shared__ double Kl[48 * 48], W[48 * 48];
+  __shared__ double Bs[8][48], Fi[64];
+  double (*Y)[48] = reinterpret_cast<double (*)[48]>(W);   // W is free until the frame transform
+  __shared__ int status;
+  if (t < 24) X[t] = xyz[3 * (int64_t)q8n[8 * e + t / 3] + t % 3];
+  if (t < 72) RN[t] = nodeR[9 * (int64_t)q8n[8 * e + t / 9] + t % 9];
+  if (t < 22) S[t] = q8s[22 * e + t];
+  if (t == 0) status = 0;
+  __syncthreads();
+  if (t == 0) {
+    // flat parallelogram with mid-side nodes at the edge midpoints
+    auto P = [&](int k, int a) { return X[3 * k + a]; };
+    double d21[3], d41[3], tv[3];
+    for (int a = 0; a < 3; ++a) { d21[a] = P(1, a) - P(0, a); d41[a] = P(3, a) - P(0, a); }
+    double scale = fmax(q8_norm3(d21), q8_norm3(d41));
+    bool ok = scale > 0;
+    double lim = 1e-6 * scale;
+    for (int a = 0; a < 3; ++a) tv[a] = P(0, a) + P(2, a) - P(1, a) - P(3, a);
+    if (q8_norm3(tv) > lim) ok = false;
+    const int mab[4][3] = {{4, 0, 1}, {5, 1, 2}, {6, 2, 3}, {7, 3, 0}};
+    for (int q = 0; q < 4; ++q) {
+      for (int a = 0; a < 3; ++a) tv[a] = P(mab[q][0], a) - (P(mab[q][1], a) + P(mab[q][2], a)) / 2;
+      if (q8_norm3(tv) > lim) ok = false;
+    }
+    double nn[3] = {d21[1] * d41[2] - d21[2] * d41[1], d21[2] * d41[0] - d21[0] * d41[2],
+                    d21[0] * d41[1] - d21[1] * d41[0]};
+    if (!(q8_norm3(nn) > 1e-12 * scale * scale)) ok = false;
+    if (!ok) {
+      status = EE_Q8_SHAPE;
+    } else {
+      double gxi[3], geta[3], cen[3], ez[3], av[3], bv[3], ex[3], ey[3];
+      for (int q = 0; q < 3; ++q) {
+        gxi[q] = (P(1, q) + P(2, q) - P(0, q) - P(3, q)) / 4;
+        geta[q] = (P(2, q) + P(3, q) - P(0, q) - P(1, q)) / 4;
+        cen[q] = (P(0, q) + P(1, q) + P(2, q) + P(3, q)) / 4;
+      }
+      ez[0] = gxi[1] * geta[2] - gxi[2] * geta[1];
+      ez[1] = gxi[2] * geta[0] - gxi[0] * geta[2];
+      ez[2] = gxi[0] * geta[1] - gxi[1] * geta[0];
+      double l = q8_norm3(ez);
+      for (int q = 0; q < 3; ++q) ez[q] /= l;
+      double lg = q8_norm3(gxi), le = q8_norm3(geta);
+      for (int q = 0; q < 3; ++q) av[q] = gxi[q] / lg + geta[q] / le;
+      l = q8_norm3(av);
+      for (int q = 0; q < 3; ++q) av[q] /= l;
+      bv[0] = ez[1] * av[2] - ez[2] * av[1];
+      bv[1] = ez[2] * av[0] - ez[0] * av[2];
+      bv[2] = ez[0] * av[1] - ez[1] * av[0];
+      const double rs2 = sqrt(2.0);
+      for (int q = 0; q < 3; ++q) { ex[q] = (av[q] - bv[q]) / rs2; ey[q] = (av[q] + bv[q]) / rs2; }
+      for (int q = 0; q < 3; ++q) { Rf[q] = ex[q]; Rf[3 + q] = ey[q]; Rf[6 + q] = ez[q]; }
+      for (int k = 0; k < 8; ++k) {
+        double d[3] = {P(k, 0) - cen[0], P(k, 1) - cen[1], P(k, 2) - cen[2]};
+        xy[k] = d[0] * ex[0] + d[1] * ex[1] + d[2] * ex[2];
+        xy[k + 8] = d[0] * ey[0] + d[1] * ey[1] + d[2] * ey[2];
+      }
+    }
+  }
+  __syncthreads();
+  if (status) {
+    if (t == 0 && atomicCAS(&err->code, 0, status) == 0) err->index = e;
+    return;
+  }
+  // shape data at the 25 points: abscissas {-1/sqrt3, 1/sqrt3, -sqrt0.6, 0, sqrt0.6}
+  const double g5[5] = {-1.0 / sqrt(3.0), 1.0 / sqrt(3.0), -sqrt(0.6), 0.0, sqrt(0.6)};
+  if (t < 25) {
+    double r = g5[t / 5], sv = g5[t % 5];
+    Q8Point& P = PT[t];
+    double dr[8], ds[8];
+    q8_shape(r, sv, P.N, dr, ds);
+    double j11 = 0, j12 = 0, j21 = 0, j22 = 0;
+    for (int k = 0; k < 8; ++k) {
+      j11 += dr[k] * xy[k]; j12 += dr[k] * xy[k + 8];
+      j21 += ds[k] * xy[k]; j22 += ds[k] * xy[k + 8];
+    }
+    double det = j11 * j22 - j12 * j21;
+    for (int k = 0; k < 8; ++k) {
+      P.dx[k] = (j22 * dr[k] - j12 * ds[k]) / det;
+      P.dy[k] = (-j21 * dr[k] + j11 * ds[k]) / det;
+    }
+    P.det = det;
+    P.jac[0] = j11; P.jac[1] = j12; P.jac[2] = j21; P.jac[3] = j22;
+  }
+  __syncthreads();
+  const double* A = S;
+  const double* Dm = S + 9;
+  const double shear = S[18], dref = S[19];
+  const bool hasA = S[20] != 0.0, hasD = S[21] != 0.0;
+  const double w3[3] = {5.0 / 9, 8.0 / 9, 5.0 / 9};
+  double acc[18];
+#pragma unroll
+  for (int u = 0; u < 18; ++u) acc[u] = 0.0;
+  if (hasA) {
+    for (int ir = 0; ir < 2; ++ir)
+      for (int is = 0; is < 2; ++is) {
+        const Q8Point& P = PT[ir * 5 + is];
+#pragma unroll
+        for (int u = 0; u < 18; ++u) {
+          int ent = t + Q8_THREADS * u, p = ent % 48, q = ent / 48;
+          double bp[3], bq[3];
+          q8_bm(P, p, bp); q8_bm(P, q, bq);
+          acc[u] += P.det * q8_bdb(bp, A, bq);
+        }
+      }
+    // 3-point excess corrections of the normal membrane strains
+    for (int row = 1; row <= 2; ++row) {
+      const double modulus = row == 1 ? A[0] : A[4];
+      for (int pass = 0; pass < 2; ++pass) {
+        const double sign = pass == 0 ? 1.0 : -1.0;
+        // row 1: r on 2 points, s on 3 (pass 0) or 2; row 2: r on 3 (pass 0) or 2, s on 2
+        const bool r3 = (row == 2 && pass == 0), s3 = (row == 1 && pass == 0);
+        const int nr = r3 ? 3 : 2, ns = s3 ? 3 : 2;
+        for (int i = 0; i < nr; ++i)
+          for (int j = 0; j < ns; ++j) {
+            const int pr = r3 ? 2 + i : i, ps = s3 ? 2 + j : j;
+            const double wr = r3 ? w3[i] : 1.0, ws = s3 ? w3[j] : 1.0;
+            const Q8Point& P = PT[pr * 5 + ps];
+            const double f = 0.25 * sign * wr * ws * P.det * modulus;
+#pragma unroll
+            for (int u = 0; u < 18; ++u) {
+              int ent = t + Q8_THREADS * u, p = ent % 48, q = ent / 48;
+              double vp = (p % 6 == row - 1) ? (row == 1 ? P.dx[p / 6] : P.dy[p / 6]) : 0.0;
+              double vq = (q % 6 == row - 1) ? (row == 1 ? P.dx[q / 6] : P.dy[q / 6]) : 0.0;
+              acc[u] += f * (vp * vq);
+            }
+          }
+      }
+    }
+  }
+  if (hasD) {
+    double Dx[9] = {Dm[0], Dm[3], 0.0, Dm[3], Dm[4], 0.0, 0.0, 0.0, 4 * Dm[8]};
+    for (int ir = 0; ir < 2; ++ir)
+      for (int is = 0; is < 2; ++is) {
+        const Q8Point& P = PT[ir * 5 + is];
+#pragma unroll
+        for (int u = 0; u < 18; ++u) {
+          int ent = t + Q8_THREADS * u, p = ent % 48, q = ent / 48;
+          double bp[3], bq[3];
+          q8_bb(P, p, bp); q8_bb(P, q, bq);
+          acc[u] += P.det * q8_bdb(bp, Dm, bq) - (2 * P.det) * q8_bdb(bp, Dx, bq);
+        }
+      }
+    for (int pass = 0; pass < 2; ++pass) {
+      const int nr = pass == 0 ? 2 : 3, ns = pass == 0 ? 3 : 2;
+      for (int i = 0; i < nr; ++i)
+        for (int j = 0; j < ns; ++j) {
+          const int pr = pass == 0 ? i : 2 + i, ps = pass == 0 ? 2 + j : j;
+          const double wr = pass == 0 ? 1.0 : w3[i], ws = pass == 0 ? w3[j] : 1.0;
+          const Q8Point& P = PT[pr * 5 + ps];
+          const double f = wr * ws * P.det;
+#pragma unroll
+          for (int u = 0; u < 18; ++u) {
+            int ent = t + Q8_THREADS * u, p = ent % 48, q = ent / 48;
+            double bp[3], bq[3];
+            q8_bb(P, p, bp); q8_bb(P, q, bq);
+            acc[u] += f * q8_bdb(bp, Dx, bq);
+          }
+        }
+    }
+    // transverse shear: sampled at the 2x2 points; flexibility from the last
+    if (t == 0) {
+      int st = 0;
+      if (!(dref > 0)) st = EE_Q8_DREF;
+      const Q8Point& P0 = PT[1 * 5 + 1];
+      const double detJ0 = P0.det;
+      const double rx = detJ0 / (P0.jac[0] * P0.jac[0]), ry = detJ0 / (P0.jac[3] * P0.jac[3]);
+      const double pat[4][4] = {{1, 1, 1, 1}, {-1, -1, 1, 1}, {-1, 1, -1, 1}, {1, -1, -1, 1}};
+      const double sx[4] = {12 * rx + 1200 * ry, 9.6 * rx, 12 * rx + 400 * ry, 12 * rx + 120 * ry};
+      const double sy[4] = {12 * ry + 1200 * rx, 12 * ry + 400 * rx, 9.6 * ry, 12 * ry + 120 * rx};
+      double F[64], M[64];
+      for (int q = 0; q < 64; ++q) F[q] = 0.0;
+      const double base = isfinite(shear) ? 1 / (shear * detJ0) : 0.0;
+      for (int q = 0; q < 8; ++q) F[q + 8 * q] = base;
+      for (int comp = 1; comp <= 2; ++comp)
+        for (int k = 0; k < 4; ++k) {
+          double stiff = comp == 1 ? sx[k] : sy[k];
+          double f = 1 / (stiff * dref) / 4;
+          for (int aa = 0; aa < 4; ++aa)
+            for (int cc = 0; cc < 4; ++cc)
+              F[(2 * aa + comp - 1) + 8 * (2 * cc + comp - 1)] += f * pat[k][aa] * pat[k][cc];
+        }
+      // Gauss-Jordan with partial pivoting
+      for (int q = 0; q < 64; ++q) { M[q] = F[q]; Fi[q] = (q % 9 == 0) ? 1.0 : 0.0; }
+      for (int k = 0; k < 8 && !st; ++k) {
+        int pv = k;
+        double best = fabs(M[k + 8 * k]);
+        for (int i = k + 1; i < 8; ++i)
+          if (fabs(M[i + 8 * k]) > best) { best = fabs(M[i + 8 * k]); pv = i; }
+        if (best == 0.0 || !isfinite(best)) { st = EE_Q8_SINGULAR; break; }
+        if (pv != k)
+          for (int j = 0; j < 8; ++j) {
+            double a = M[k + 8 * j]; M[k + 8 * j] = M[pv + 8 * j]; M[pv + 8 * j] = a;
+            double b = Fi[k + 8 * j]; Fi[k + 8 * j] = Fi[pv + 8 * j]; Fi[pv + 8 * j] = b;
+          }
+        double piv = M[k + 8 * k];
+        for (int j = 0; j < 8; ++j) { M[k + 8 * j] /= piv; Fi[k + 8 * j] /= piv; }
+        for (int i = 0; i < 8; ++i) {
+          if (i == k) continue;
+          double f = M[i + 8 * k];
+          if (f == 0.0) continue;
+          for (int j = 0; j < 8; ++j) { M[i + 8 * j] -= f * M[k + 8 * j]; Fi[i + 8 * j] -= f * Fi[k + 8 * j]; }
+        }
+      }
+      status = st;
+    }
+    // Bs (8 x 48): sample s = 2 ir + is, rows 2s (dx, N on w, theta_y) and 2s+1 (dy, -N on theta_x)
+    for (int q = t; q < 8 * 48; q += Q8_THREADS) {
+      int a = q / 48, col = q % 48, smp = a / 2, k = col / 6, c = col % 6;
+      const Q8Point& P = PT[(smp / 2) * 5 + (smp % 2)];
+      double v = 0.0;
+      if (a % 2 == 0) v = (c == 2) ? P.dx[k] : (c == 4 ? P.N[k] : 0.0);
+      else v = (c == 2) ? P.dy[k] : (c == 3 ? -P.N[k] : 0.0);
+      Bs[a][col] = v;
+    }
+    __syncthreads();
+    if (status) {
+      if (t == 0 && atomicCAS(&err->code, 0, status) == 0) err->index = e;
+      return;
+    }
+    for (int q = t; q < 8 * 48; q += Q8_THREADS) {
+      int a = q / 48, col = q % 48;
+      double v = 0.0;
+      for (int b = 0; b < 8; ++b) v += Fi[a + 8 * b] * Bs[b][col];
+      Y[a][col] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < 18; ++u) {
+      int ent = t + Q8_THREADS * u, p = ent % 48, q = ent / 48;
+      double v = 0.0;
+      for (int a = 0; a < 8; ++a) v += Bs[a][p] * Y[a][q];
+      acc[u] += v;
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < 18; ++u) Kl[t + Q8_THREADS * u] = acc[u];
+  __syncthreads();
+  // K = T^T Kl T, T block-diagonal with T(c + a, c + b) = e_a[b] (element axes)
+#pragma unroll
+  for (int u = 0; u < 18; ++u) {
+    int ent = t + Q8_THREADS * u, i = ent % 48, j = ent / 48;
+    int ci = i - i % 3, cj = j - j % 3;
+    double v = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      double ta = Rf[(i - ci) + 3 * a];
+      double row = 0.0;
+      for (int b = 0; b < 3; ++b) row += Kl[(ci + a) + 48 * (cj + b)] * Rf[(j - cj) + 3 * b];
+      v += ta * row;
+    }
+    W[ent] = v;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < 18; ++u) {
+    int ent = t + Q8_THREADS * u, i = ent % 48, j = ent / 48;
+    Kl[ent] = (W[i + 48 * j] + W[j + 48 * i]) / 2;
+  }
+  __syncthreads();
+  // node_R congruence: Tn(r0 + a, r0 + b) = R_node(a, b)
+  double* out = ev + 2304 * e;
+#pragma unroll
+  for (int u = 0; u < 18; ++u) {
+    int ent = t + Q8_THREADS * u, i = ent % 48, j = ent / 48;
+    int ci = i - i % 3, cj = j - j % 3;
+    const double* Ri = RN + 9 * (i / 6);
+    const double* Rj = RN + 9 * (j / 6);
+    double v = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      double ta = Ri[a + 3 * (i - ci)];
+      double row = 0.0;
+      for (int b = 0; b < 3; ++b) row += Kl[(ci + a) + 48 * (cj + b)] * Rj[b + 3 * (j - cj)];
+      v += ta * row;
+    }
+    out[ent] = v;
+  }
+}
+
 }  // namespace
 
 jfg_status launch_elements(jfg_model* m, cudaStream_t st) {
@@ -756,8 +1103,11 @@ jfg_status launch_elements(jfg_model* m, cudaStream_t st) {
     JFG_CUDA(cudaGetLastError());
   }
   if (m->n_q8 > 0) {
-    set_error("CQUAD8 device kernel not built into this library version");
-    return JFG_UNSUPPORTED;
+    int ps = prof_start(st);
+    { k_q8<<<(unsigned)m->n_q8, Q8_THREADS, 0, st>>>(m->n_q8, m->d_q8n, m->d_q8s, m->d_xyz, m->d_R,
+                                                   m->d_ev + m->ev_q8_off, m->d_err); count_launch(); }
+    prof_end(ps, st, KS_T10, (double)m->n_q8 * (32 + 8 * 22 + 8 * 2304) + 24.0 * m->n_nodes);
+    JFG_CUDA(cudaGetLastError());
   }
   return JFG_OK;
 }
@@ -766,10 +1116,6 @@ jfg_status launch_elements(jfg_model* m, cudaStream_t st) {
 // `ev` (n_ev doubles) and the first element error to `err` instead of the
 // model's own buffers; no profiling events.
 jfg_status launch_elements_into(const jfg_model* m, cudaStream_t st, double* ev, DevError* err) {
-  if (m->n_q8 > 0) {
-    set_error("CQUAD8 device kernel not built into this library version");
-    return JFG_UNSUPPORTED;
-  }
   if (m->n_q4 > 0) {
     int64_t blocks = (m->n_q4 + WARPS - 1) / WARPS;
     { k_q4<<<(unsigned)blocks, WARPS * 32, 0, st>>>(m->n_q4, m->d_q4n, m->d_q4s, m->d_xyz, m->d_R, ev, err);
@@ -787,6 +1133,11 @@ jfg_status launch_elements_into(const jfg_model* m, cudaStream_t st, double* ev,
     { k_t10<<<(unsigned)blocks, WARPS * 32, 0, st>>>(m->n_t10, m->d_t10n, m->d_t10m, m->d_xyz, m->d_R,
                                                   ident ? 1 : 0, ev + m->ev_t10_off, err);
       count_launch(); }
+    JFG_CUDA(cudaGetLastError());
+  }
+  if (m->n_q8 > 0) {
+    { k_q8<<<(unsigned)m->n_q8, Q8_THREADS, 0, st>>>(m->n_q8, m->d_q8n, m->d_q8s, m->d_xyz, m->d_R,
+                                                   ev + m->ev_q8_off, err); count_launch(); }
     JFG_CUDA(cudaGetLastError());
   }
   return JFG_OK;

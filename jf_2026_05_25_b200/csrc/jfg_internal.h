@@ -73,6 +73,7 @@ enum ElemErr : int32_t {
   EE_T10_JAC = 200,
   EE_T10_MAT = 202,
   EE_Q8_SHAPE = 300,
+  EE_Q8_DREF = 301,
   EE_Q8_SINGULAR = 302,
   EE_PIVOT = 500,
   EE_TC_TIMEOUT = 600,   // a bounded tensor-core pipeline wait expired

@@ -289,6 +289,54 @@ def flat_plate(nx: int = 20, ny: int = 20, a: float = 0.5, b: float = 0.5,
     return m
 
 
+def quad8_plate(nx: int = 8, ny: int = 6, a: float = 0.4, b: float = 0.3, t: float = 0.003,
+                E: float = 70e9, nu: float = 0.33, skew: float = 0.0, tilt_deg: float = 0.0,
+                n_cases: int = 1, force_sigma: float = 50.0, seed: int = 11) -> Sol101Model:
+    """Cantilever plate of CQUAD8 (native shell path, quad8_shell.jl).
+
+    Corner and mid-side nodes on the (2nx+1) x (2ny+1) lattice of the
+    parallelogram spanned by (a, 0) and (skew * b, b); element centres are not
+    nodes.  ``tilt_deg`` rotates the whole plate about the x axis and then about
+    z by half that angle, so the elements lie in a general plane.  PSHELL
+    MID1 = MID2 = MID3 = 1 with MAT1 G given.  SPC1 123456 on the edge x = 0.
+    Subcase k: seeded N(0, force_sigma) nodal forces on every free node.
+    """
+    idx = {}
+    pts = []
+    for j in range(2 * ny + 1):
+        for i in range(2 * nx + 1):
+            if i % 2 == 1 and j % 2 == 1:
+                continue
+            u, v = i / (2 * nx), j / (2 * ny)
+            idx[(i, j)] = len(pts)
+            pts.append([u * a + skew * b * v, v * b, 0.0])
+    xyz = np.asarray(pts, float)
+    if tilt_deg:
+        th = math.radians(tilt_deg)
+        Rx = np.array([[1, 0, 0], [0, math.cos(th), -math.sin(th)], [0, math.sin(th), math.cos(th)]])
+        ph = th / 2
+        Rz = np.array([[math.cos(ph), -math.sin(ph), 0], [math.sin(ph), math.cos(ph), 0], [0, 0, 1]])
+        xyz = xyz @ (Rz @ Rx).T
+    q8 = []
+    for j in range(ny):
+        for i in range(nx):
+            I, J = 2 * i, 2 * j
+            q8.append([idx[(I, J)], idx[(I + 2, J)], idx[(I + 2, J + 2)], idx[(I, J + 2)],
+                       idx[(I + 1, J)], idx[(I + 2, J + 1)], idx[(I + 1, J + 2)], idx[(I, J + 1)]])
+    q8 = np.asarray(q8, np.int32)
+    clamp = np.array([idx[(0, j)] for j in range(2 * ny + 1)], np.int64)
+    free = np.setdiff1d(np.arange(len(xyz)), clamp)
+    rng = _rng(seed)
+    cases = [LoadCase(sid=k + 1, forces=(free, rng.normal(0.0, force_sigma, (len(free), 3))))
+             for k in range(n_cases)]
+    return Sol101Model(
+        name=f"quad8_plate_{nx}x{ny}", grid_ids=np.arange(1, len(xyz) + 1, dtype=np.int64), xyz=xyz,
+        q8_nodes=q8, q8_pid=np.ones(len(q8), np.int64),
+        pshells={1: PShell(T=t, MID1=1, MID2=1, MID3=1)},
+        mats={1: Mat1(E=E, NU=nu, G=E / (2 * (1 + nu)))},
+        spc1=[("123456", clamp)], load_cases=cases, seed=seed)
+
+
 def wing_panel(nx: int = 200, ny: int = 400, lx: float = 1.0, ly: float = 2.0,
                n_blades: int = 9, blade_nz: int = 20, blade_h: float = 0.1,
                t_skin=(1.5e-3, 4.0e-3), t_blade: float = 3e-3, n_cases: int = 8,

@@ -76,6 +76,54 @@ def test_quad4_element_matrices(ctx, oracle_mod):
     assert worst <= ELEM_RTOL, worst
 
 
+def test_quad8_element_matrices(ctx, oracle_mod):
+    """CQUAD8 parallelograms in random planes, with random node_R frames on
+    half of the grids, against the oracle restatement of quad8_shell.jl."""
+    rng = np.random.default_rng(5)
+    xyz, q8, nodeR = [], [], []
+    for e in range(24):
+        a, b = rng.uniform(0.01, 0.06, 2)
+        ang = rng.uniform(50, 130)
+        th = np.radians(ang)
+        c = np.array([[0, 0, 0], [a, 0, 0], [a + b * np.cos(th), b * np.sin(th), 0], [b * np.cos(th), b * np.sin(th), 0]])
+        P = np.vstack([c, (c[0] + c[1]) / 2, (c[1] + c[2]) / 2, (c[2] + c[3]) / 2, (c[3] + c[0]) / 2])
+        R = _rot(0, rng.uniform(0, 180)) @ _rot(1, rng.uniform(0, 180)) @ _rot(2, rng.uniform(0, 360))
+        xyz.append(P @ R.T + rng.uniform(-1, 1, 3))
+        q8.append(np.arange(8 * e, 8 * e + 8))
+        for k in range(8):
+            Rn = _rot(2, rng.uniform(0, 360)) @ _rot(0, rng.uniform(0, 90)) if k % 2 else np.eye(3)
+            nodeR.append(Rn.ravel(order="F"))
+    xyz = np.vstack(xyz)
+    q8 = np.asarray(q8, np.int32)
+    nodeR = np.asarray(nodeR)
+    pids = np.arange(len(q8)) % 2 + 1
+    m = M.Sol101Model(name="q8set", grid_ids=np.arange(1, len(xyz) + 1), xyz=xyz, node_R=nodeR, q8_nodes=q8,
+                      q8_pid=pids,
+                      pshells={1: M.PShell(T=0.003, MID1=1, MID2=1, MID3=1),
+                               2: M.PShell(T=0.006, MID1=1, MID2=1, MID3=1, BEND_RATIO=0.9, TS_T=0.8)},
+                      mats={1: M.Mat1(E=70e9, NU=0.33, G=70e9 / 2.66)})
+    dm = lib.DeviceModel(ctx, m)
+    dm.assemble()
+    sect = m.q8_sections()
+    worst = 0.0
+    for e in range(len(q8)):
+        Kd = dm.element_matrix(1, e)
+        Ko = oracle_mod.q8_element(xyz[q8[e]], sect[e], nodeR[q8[e]])
+        worst = max(worst, _rel(Kd, Ko))
+    assert worst <= ELEM_RTOL, worst
+
+
+def test_quad8_rejects_curved_element(ctx):
+    m = M.quad8_plate(2, 2)
+    m.xyz = m.xyz.copy()
+    m.xyz[m.q8_nodes[0, 4], 2] += 0.01       # lift a mid-side node off the edge
+    dm = lib.DeviceModel(ctx, m)
+    with pytest.raises(lib.JfgError) as e:
+        dm.assemble()
+    assert e.value.status_name == "UNSUPPORTED"
+    assert e.value.detail == 0
+
+
 def test_tetra10_element_matrices(ctx, oracle_mod):
     m = M.solid_block(n=2, n_cases=1)
     rng = np.random.default_rng(3)
@@ -92,6 +140,8 @@ def test_tetra10_element_matrices(ctx, oracle_mod):
 
 MODELS = {
     "plate": lambda: M.flat_plate(),
+    "q8_flat": lambda: M.quad8_plate(8, 6, skew=0.3, n_cases=2),
+    "q8_tilted": lambda: M.quad8_plate(6, 5, skew=0.2, tilt_deg=30, n_cases=2),
     "wing_small": lambda: M.wing_panel(nx=24, ny=36, n_blades=3, blade_nz=4, n_cases=3, seed=5),
     "solid_small": lambda: M.solid_block(n=4, n_cases=2),
 }
