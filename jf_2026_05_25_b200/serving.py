@@ -1,0 +1,413 @@
+"""Device-resident SOL101 serving: packed batches, a resident-model registry
+and continuous batching over several device streams.
+
+The reference keeps one warm model per worker process and re-solves it
+(utils/julia_tools/warm_model_session.jl:5-99, jfem_worker_jsonl.jl:77-100,
+boundary_conditions.jl:62-75).  Here:
+
+* ``PackedModel`` packs independent small models into one block-diagonal
+  model (disjoint node sets, coordinates shifted apart).  Its element
+  kernels, assembly, level-scheduled factor and strip solves then run as one
+  set of launches for the whole batch: every level launch carries the fronts
+  of all models.  Load case c of every member goes to column c, scaled to unit
+  norm, and the refinement tolerance is divided by sqrt(members), so every
+  member meets the requested relative residual on its own; the split undoes
+  the scaling.
+* ``SolveServer`` keeps models (or packs) resident on the device: their
+  pattern, symbolic analysis and factor stay in HBM for re-solves with new
+  loads or thickness updates.  Resident bytes are charged against an HBM
+  budget and the least recently used models are freed to admit new ones.
+* Continuous batching: ``slots`` worker threads each own a library context
+  (its own CUDA stream); a free slot takes the next request, or every queued
+  new small model up to a DOF limit as one pack, while the other slots'
+  work is still on the device, so their kernels overlap.  Each request's
+  latency runs from submission to its result; ``stats()`` gives p50/p99.
+"""
+from __future__ import annotations
+
+import math
+import queue
+import threading
+import time
+from concurrent.futures import Future
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import backend as B
+from . import lib
+
+
+class PackedModel:
+    """Block-diagonal union of independent models (the batch unit)."""
+
+    def __init__(self, models: Sequence, gap: float = 1.0):
+        self.members = list(models)
+        xyz, R, q4n, q4s, q8n, q8s, t10n, t10m, spc = [], [], [], [], [], [], [], [], []
+        self.node_off, self.q4_off = [], []
+        n_off = 0
+        q4_off = 0
+        x0 = 0.0
+        for m in self.members:
+            p = np.asarray(m.xyz, float)
+            lo, hi = p.min(axis=0), p.max(axis=0)
+            shift = np.array([x0 - lo[0], -lo[1], -lo[2]])
+            xyz.append(p + shift)
+            x0 += (hi[0] - lo[0]) + gap
+            R.append(np.asarray(m.node_R, float))
+            q4n.append(np.asarray(m.q4_nodes, np.int32) + n_off)
+            q4s.append(m.q4_sections())
+            q8n.append(np.asarray(m.q8_nodes, np.int32) + n_off)
+            q8s.append(m.q8_sections())
+            t10n.append(np.asarray(m.t10_nodes, np.int32) + n_off)
+            t10m.append(m.t10_materials())
+            spc.append(np.asarray(m.spc_dofs(), np.int64) + 6 * n_off)
+            self.node_off.append(n_off)
+            self.q4_off.append(q4_off)
+            n_off += m.n_nodes
+            q4_off += len(m.q4_nodes)
+        self.node_off.append(n_off)
+        self.q4_off.append(q4_off)
+        self.xyz = np.vstack(xyz)
+        self.node_R = np.vstack(R)
+        self.q4_nodes = np.vstack(q4n).reshape(-1, 4)
+        self._q4s = np.vstack(q4s).reshape(-1, 26)
+        self.q8_nodes = np.vstack(q8n).reshape(-1, 8)
+        self._q8s = np.vstack(q8s).reshape(-1, 22)
+        self.t10_nodes = np.vstack(t10n).reshape(-1, 10)
+        self._t10m = np.vstack(t10m).reshape(-1, 2)
+        self._spc = np.unique(np.concatenate(spc))
+        self.name = f"pack_{len(self.members)}"
+
+    # attributes the device binding and the partition read
+    @property
+    def n_nodes(self) -> int:
+        return int(self.node_off[-1])
+
+    @property
+    def ndof(self) -> int:
+        return 6 * self.n_nodes
+
+    def q4_sections(self):
+        return self._q4s
+
+    def q8_sections(self):
+        return self._q8s
+
+    def t10_materials(self):
+        return self._t10m
+
+    def spc_dofs(self):
+        return self._spc
+
+    def dof_slice(self, k: int) -> slice:
+        return slice(6 * self.node_off[k], 6 * self.node_off[k + 1])
+
+    def load_columns(self, loads: Optional[Sequence[np.ndarray]] = None):
+        """Packed load matrix: column c holds case c of every member, each
+        scaled to unit norm.  Returns (F, scales[member][case])."""
+        loads = [m.load_matrix() if loads is None or loads[k] is None else np.asarray(loads[k])
+                 for k, m in enumerate(self.members)]
+        ncol = max(L.shape[1] for L in loads)
+        F = np.zeros((self.ndof, ncol), order="F")
+        scales = []
+        for k, L in enumerate(loads):
+            sl = self.dof_slice(k)
+            sc = []
+            for c in range(L.shape[1]):
+                nrm = float(np.linalg.norm(L[:, c]))
+                s = 1.0 / nrm if nrm > 0 else 1.0
+                F[sl, c] = L[:, c] * s
+                sc.append(s)
+            scales.append(sc)
+        return F, scales
+
+    def split(self, U: np.ndarray, scales) -> List[np.ndarray]:
+        out = []
+        for k, sc in enumerate(scales):
+            sl = self.dof_slice(k)
+            out.append(np.asfortranarray(U[sl, :len(sc)] / np.asarray(sc)[None, :]))
+        return out
+
+
+def member_residuals(dm, pack: PackedModel, U: np.ndarray, F: np.ndarray, free: np.ndarray,
+                     ncases: Sequence[int]) -> List[np.ndarray]:
+    """Relative residual |K u - f| / |f| of every member and case, on the
+    member's own free DOFs (the reference's measure, boundary_conditions.jl:1858-1866)."""
+    R = dm.residual(U, F)
+    mask = np.zeros(pack.ndof, bool)
+    mask[free] = True
+    out = []
+    for k, nc in enumerate(ncases):
+        sl = pack.dof_slice(k)
+        mk = mask[sl]
+        r = np.linalg.norm(R[sl][mk, :nc], axis=0)
+        f = np.linalg.norm(F[sl][mk, :nc], axis=0)
+        out.append(r / np.where(f > 0, f, 1.0))
+    return out
+
+
+def solve_pack(be: B.JFEMGPUBackend, models: Sequence, tol: float = 1e-10) -> Dict:
+    """Prepare and solve a pack of independent models in one set of launches.
+    Returns dict(state, pack, U (list per member), residuals (list per member))."""
+    pack = PackedModel(models)
+    st = B.prepare(be, pack)
+    F, scales = pack.load_columns()
+    # each column mixes the members' unit-norm loads: tol / sqrt(members)
+    # bounds every member's own relative residual by tol
+    tol_c = tol / math.sqrt(max(1, len(models)))
+    U, rep = st["dm"].solve(F, tol_c, max(be.max_ir, 30), raise_on_stall=False)
+    res = member_residuals(st["dm"], pack, U, F, st["free"], [len(sc) for sc in scales])
+    return dict(state=st, pack=pack, U=pack.split(U, scales), residuals=res, report=rep, F=F, scales=scales)
+
+
+# ----------------------------------------------------------------------------
+# server
+# ----------------------------------------------------------------------------
+
+@dataclass
+class Request:
+    kind: str                          # "solve" (new model), "resolve" (new loads), "update" (thickness)
+    model: object = None               # Sol101Model for "solve"
+    key: Optional[str] = None          # registry key (returned by "solve", used by the others)
+    loads: Optional[np.ndarray] = None # ndof x nrhs for "resolve"/"update" (None: the model's own cases)
+    elems: Optional[np.ndarray] = None # CQUAD4 indices for "update"
+    sections: Optional[np.ndarray] = None
+    t_submit: float = 0.0
+    future: Future = field(default_factory=Future)
+
+
+@dataclass
+class Resident:
+    dm: object
+    state: Dict
+    pack: Optional[PackedModel]
+    index: int                         # member index inside the pack (0 for a single model)
+    model: object
+    nbytes: int
+    lock: threading.Lock
+    last_used: float = 0.0
+
+
+class SolveServer:
+    """Continuous-batching SOL101 server on one device (see module docstring)."""
+
+    def __init__(self, device: int = 0, slots: int = 4, hbm_budget_bytes: float = 150e9,
+                 precision: int = lib.PREC_FP64, tol: float = 1e-10, small_dof: int = 60000,
+                 pack_dof: int = 400000, pack_models: int = 64):
+        self.device, self.precision, self.tol = device, precision, tol
+        self.small_dof, self.pack_dof, self.pack_models = small_dof, pack_dof, pack_models
+        self.budget = float(hbm_budget_bytes)
+        self.q: "queue.Queue[Request]" = queue.Queue()
+        self.pending: List[Request] = []
+        self.plock = threading.Condition()
+        self.registry: Dict[str, Resident] = {}
+        self.groups: Dict[int, List[str]] = {}      # pack id -> member keys (freed together)
+        self.rlock = threading.Lock()
+        self.resident_bytes = 0
+        self.latencies: List[float] = []
+        self.subcase_solves = 0
+        self._next_key = 0
+        self._stop = False
+        self.backends = []
+        for _ in range(slots):
+            be = B.JFEMGPUBackend(device=device, precision=precision, tol=tol)
+            be._ctx = lib.Context(device)
+            self.backends.append(be)
+        self.threads = [threading.Thread(target=self._worker, args=(i,), daemon=True) for i in range(slots)]
+        for t in self.threads:
+            t.start()
+
+    # ---------------------------------------------------------------- client API
+    def submit(self, req: Request) -> Future:
+        req.t_submit = time.perf_counter()
+        with self.plock:
+            self.pending.append(req)
+            self.plock.notify()
+        return req.future
+
+    def solve(self, model) -> Future:
+        return self.submit(Request("solve", model=model))
+
+    def resolve(self, key: str, loads: Optional[np.ndarray] = None) -> Future:
+        return self.submit(Request("resolve", key=key, loads=loads))
+
+    def update(self, key: str, elems: np.ndarray, sections: np.ndarray, loads: Optional[np.ndarray] = None) -> Future:
+        return self.submit(Request("update", key=key, elems=elems, sections=sections, loads=loads))
+
+    def close(self):
+        with self.plock:
+            self._stop = True
+            self.plock.notify_all()
+        for t in self.threads:
+            t.join(timeout=30)
+        with self.rlock:
+            for r in list(self.registry.values()):
+                r.dm.close()
+            self.registry.clear()
+        for be in self.backends:
+            be._ctx.close()
+
+    def stats(self) -> Dict:
+        lat = np.asarray(self.latencies)
+        if lat.size == 0:
+            return {"requests": 0}
+        return {"requests": int(lat.size), "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3),
+                "subcase_solves": int(self.subcase_solves), "resident_bytes": int(self.resident_bytes)}
+
+    # ---------------------------------------------------------------- scheduling
+    def _take(self) -> Optional[List[Request]]:
+        """Next unit of work: one request, or every queued new small model up
+        to the pack limits (continuous batching: whatever arrived meanwhile)."""
+        with self.plock:
+            while not self.pending and not self._stop:
+                self.plock.wait(timeout=0.5)
+            if self._stop and not self.pending:
+                return None
+            first = self.pending.pop(0)
+            if first.kind != "solve" or first.model.ndof > self.small_dof:
+                return [first]
+            batch, dof = [first], first.model.ndof
+            rest = []
+            for r in self.pending:
+                if (r.kind == "solve" and r.model.ndof <= self.small_dof and len(batch) < self.pack_models
+                        and dof + r.model.ndof <= self.pack_dof):
+                    batch.append(r)
+                    dof += r.model.ndof
+                else:
+                    rest.append(r)
+            self.pending = rest
+            return batch
+
+    def _worker(self, slot: int):
+        be = self.backends[slot]
+        while True:
+            work = self._take()
+            if work is None:
+                return
+            try:
+                if work[0].kind == "solve":
+                    self._do_solve(be, work)
+                elif work[0].kind == "resolve":
+                    self._do_resolve(work[0])
+                else:
+                    self._do_update(work[0])
+            except Exception as exc:   # report to every waiting client
+                for r in work:
+                    if not r.future.done():
+                        r.future.set_exception(exc)
+
+    def _finish(self, req: Request, result: Dict):
+        dt = time.perf_counter() - req.t_submit
+        with self.rlock:
+            self.latencies.append(dt)
+            self.subcase_solves += int(result["U"].shape[1])
+        result["latency_s"] = dt
+        req.future.set_result(result)
+
+    # ---------------------------------------------------------------- memory
+    @staticmethod
+    def _bytes_of(dm) -> int:
+        info = dm.symbolic_info()
+        _, nnz, ntrip = dm.sizes()
+        return int(info["factor_bytes"] * 1.6 + 24 * nnz + 8 * ntrip + 200 * dm.ndof)
+
+    def _admit(self, need: int):
+        """Free least-recently-used residents until `need` more bytes fit."""
+        with self.rlock:
+            while self.resident_bytes + need > self.budget and self.registry:
+                # evict the least recently used group (a pack is freed as a unit)
+                key = min(self.registry, key=lambda k: self.registry[k].last_used)
+                r = self.registry[key]
+                gid = id(r.dm)
+                keys = self.groups.pop(gid, [key])
+                if not r.lock.acquire(blocking=False):
+                    break   # in use: admit over budget rather than wait
+                try:
+                    for k in keys:
+                        self.registry.pop(k, None)
+                    self.resident_bytes -= r.nbytes
+                    r.dm.close()
+                finally:
+                    r.lock.release()
+
+    def _register(self, dm, state, pack, models) -> List[str]:
+        nbytes = self._bytes_of(dm)
+        self._admit(0)
+        lock = threading.Lock()
+        keys = []
+        with self.rlock:
+            for i, m in enumerate(models):
+                key = f"m{self._next_key}"
+                self._next_key += 1
+                self.registry[key] = Resident(dm, state, pack, i, m, nbytes, lock, time.perf_counter())
+                keys.append(key)
+            self.groups[id(dm)] = keys
+            self.resident_bytes += nbytes
+        return keys
+
+    # ---------------------------------------------------------------- work
+    def _do_solve(self, be, reqs: List[Request]):
+        models = [r.model for r in reqs]
+        est = sum(24 * 6 * m.n_nodes * 60 for m in models)   # rough pre-analysis estimate
+        self._admit(est)
+        out = solve_pack(be, models, self.tol)
+        keys = self._register(out["state"]["dm"], out["state"], out["pack"], models)
+        for k, r in enumerate(reqs):
+            self._finish(r, {"key": keys[k], "U": out["U"][k], "rel_residual": out["residuals"][k],
+                             "batch": len(reqs)})
+
+    def _member_solve(self, res: Resident, loads: Optional[np.ndarray]):
+        pack = res.pack
+        L = [None] * len(pack.members)
+        L[res.index] = res.model.load_matrix() if loads is None else loads
+        # only this member carries load; the others' columns are zero
+        F = np.zeros((pack.ndof, L[res.index].shape[1]), order="F")
+        sl = pack.dof_slice(res.index)
+        sc = []
+        for c in range(F.shape[1]):
+            nrm = float(np.linalg.norm(L[res.index][:, c]))
+            s = 1.0 / nrm if nrm > 0 else 1.0
+            F[sl, c] = L[res.index][:, c] * s
+            sc.append(s)
+        U, rep = res.dm.solve(F, self.tol, 30, raise_on_stall=False)
+        R = res.dm.residual(U, F)
+        free = res.state["free"]
+        mask = np.zeros(pack.ndof, bool)
+        mask[free] = True
+        mk = mask[sl]
+        rel = np.linalg.norm(R[sl][mk], axis=0) / np.maximum(np.linalg.norm(F[sl][mk], axis=0), 1e-300)
+        Um = np.asfortranarray(U[sl] / np.asarray(sc)[None, :])
+        return {"U": Um, "rel_residual": rel}
+
+    def _lookup(self, key: str) -> Resident:
+        with self.rlock:
+            res = self.registry.get(key)
+            if res is None:
+                raise KeyError(f"model {key} is not resident (evicted or unknown)")
+            res.last_used = time.perf_counter()
+            return res
+
+    def _do_resolve(self, req: Request):
+        res = self._lookup(req.key)
+        with res.lock:
+            out = self._member_solve(res, req.loads)
+        out["key"] = req.key
+        self._finish(req, out)
+
+    def _do_update(self, req: Request):
+        """Thickness (section) update of a resident model: element kernels,
+        assembly and the numeric factor rerun on the resident pattern and
+        symbolic analysis, then the solve."""
+        res = self._lookup(req.key)
+        with res.lock:
+            off = res.pack.q4_off[res.index]
+            res.dm.update_q4_sections(np.asarray(req.elems, np.int32) + off, req.sections)
+            res.pack._q4s[np.asarray(req.elems) + off] = req.sections
+            res.dm.assemble()
+            res.dm.factor(self.precision)
+            out = self._member_solve(res, req.loads)
+        out["key"] = req.key
+        self._finish(req, out)

@@ -119,3 +119,27 @@ def test_backend_names():
     assert B.backend_from_model(None, env={"JFEM_BACKEND": "b200"}) == "jfem_gpu"
     with pytest.raises(ValueError):
         B.normalize_backend_name("nope")
+
+
+def test_packed_model_matches_members(oracle_mod):
+    """A pack of independent panels is block diagonal: the host symbolic
+    analysis of the pack (a forest) with the oracle Cholesky reproduces every
+    member's own solution, and the unit-norm column scaling is undone."""
+    from jf_2026_05_25_b200 import serving as S
+    ms = [M.stiffened_panel(s) for s in (3, 11)]
+    pk = S.PackedModel(ms)
+    assert pk.ndof == sum(m.ndof for m in ms)
+    asm = oracle_mod.assemble(pk)
+    K = oracle_mod.csc_matrix(asm)
+    free, _, _ = oracle_mod.partition(pk, K)
+    info, perm = lib.symbolic_dry_run(asm["colptr"], asm["rowval"], free, pk.xyz)
+    Kff = K[free][:, free].tocsc()
+    F, sc = pk.load_columns()
+    U, _ = oracle_mod.chol_solve(len(free), Kff.indptr, Kff.indices, Kff.data, perm, F[free])
+    Uf = np.zeros((pk.ndof, F.shape[1]))
+    Uf[free] = U
+    for k, m in enumerate(ms):
+        ref = oracle_mod.solve_reference(m)
+        Uk = pk.split(Uf, sc)[k]
+        assert Uk.shape == ref["u"].shape
+        assert np.abs(Uk - ref["u"]).max() <= 1e-8 * np.abs(ref["u"]).max()

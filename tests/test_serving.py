@@ -1,0 +1,96 @@
+"""Serving on the device (gpu): packed batches and the continuous-batching
+server give every model the same result as solving it alone, within the
+parity tolerance, and meet the residual bar on each model's own DOFs."""
+import numpy as np
+import pytest
+
+from jf_2026_05_25_b200 import backend as B
+from jf_2026_05_25_b200 import build as jbuild
+from jf_2026_05_25_b200 import lib
+from jf_2026_05_25_b200 import model as M
+from jf_2026_05_25_b200 import serving as S
+
+pytestmark = pytest.mark.gpu
+
+DISP_RTOL = 1e-8
+RESID_TOL = 1e-10
+SEEDS = (3, 11, 25, 29, 23)
+
+
+@pytest.fixture(scope="module")
+def alone():
+    jbuild.build()
+    ctx = lib.Context(0)
+    out = {}
+    for s in SEEDS:
+        m = M.stiffened_panel(s)
+        be = B.JFEMGPUBackend(tol=RESID_TOL)
+        be._ctx = ctx
+        res = B.solve_model(be, m)
+        out[s] = np.stack([sc["raw_displacement"] for sc in res["subcases"]], axis=1)
+        res["state"]["dm"].close()
+    yield out
+    ctx.close()
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def test_packed_batch_matches_alone(alone):
+    models = [M.stiffened_panel(s) for s in SEEDS]
+    be = B.JFEMGPUBackend(tol=RESID_TOL)
+    out = S.solve_pack(be, models, RESID_TOL)
+    for k, s in enumerate(SEEDS):
+        assert out["U"][k].shape == alone[s].shape
+        assert _rel(out["U"][k], alone[s]) <= DISP_RTOL
+        assert out["residuals"][k].max() <= RESID_TOL
+    out["state"]["dm"].close()
+
+
+def test_server_mix_resolve_update_and_latency(alone):
+    srv = S.SolveServer(slots=2, tol=RESID_TOL, small_dof=20000, pack_dof=40000)
+    try:
+        futs = {s: srv.solve(M.stiffened_panel(s)) for s in SEEDS}
+        res = {s: f.result(timeout=600) for s, f in futs.items()}
+        for s in SEEDS:
+            assert _rel(res[s]["U"], alone[s]) <= DISP_RTOL
+            assert res[s]["rel_residual"].max() <= RESID_TOL
+        # re-solve of a resident model with doubled loads: linear response
+        s0 = SEEDS[0]
+        m0 = M.stiffened_panel(s0)
+        r2 = srv.resolve(res[s0]["key"], 2.0 * m0.load_matrix()).result(timeout=600)
+        assert _rel(r2["U"], 2.0 * alone[s0]) <= DISP_RTOL
+        assert r2["rel_residual"].max() <= RESID_TOL
+        # thickness update of every CQUAD4 of a resident model: same result as
+        # a fresh solve of the updated model
+        s1 = SEEDS[1]
+        m1 = M.stiffened_panel(s1)
+        sect = m1.q4_sections()
+        ref_model = M.stiffened_panel(s1)
+        for p in ref_model.pshells.values():
+            p.T *= 1.1
+        new_sect = ref_model.q4_sections()
+        r3 = srv.update(res[s1]["key"], np.arange(len(sect)), new_sect).result(timeout=600)
+        be = B.JFEMGPUBackend(tol=RESID_TOL)
+        fresh = B.solve_model(be, ref_model)
+        Uref = np.stack([sc["raw_displacement"] for sc in fresh["subcases"]], axis=1)
+        assert _rel(r3["U"], Uref) <= DISP_RTOL
+        st = srv.stats()
+        assert st["requests"] == len(SEEDS) + 2
+        assert 0 < st["p50_ms"] <= st["p99_ms"]
+    finally:
+        srv.close()
+
+
+def test_server_evicts_under_budget():
+    srv = S.SolveServer(slots=1, tol=RESID_TOL, hbm_budget_bytes=1.0, small_dof=0)
+    try:
+        a = srv.solve(M.stiffened_panel(SEEDS[0])).result(timeout=600)
+        b = srv.solve(M.stiffened_panel(SEEDS[1])).result(timeout=600)
+        assert a["key"] != b["key"]
+        with pytest.raises(KeyError):
+            srv.resolve(a["key"]).result(timeout=600)
+        srv.resolve(b["key"]).result(timeout=600)
+    finally:
+        srv.close()
