@@ -318,8 +318,8 @@ def run_ours(args, rank, world, local_rank):
             "data": "synthetic",
             "config": dict(cfg, parallelism=f"replicas{world}", precision=args.precision,
                            l2="inputs larger than L2 (factor %.1f GB)" % (sym["nnz_L"] * (8 if prec == 0 else 4) / 1e9)),
-            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(F.nbytes),
-                    "d2h_bytes_per_step": int(F.nbytes)},
+            "e2e": None if args.no_e2e else {"value": e2e_value, "unit": "solves/s",
+                                             "h2d_bytes_per_step": int(F.nbytes), "d2h_bytes_per_step": int(F.nbytes)},
             "gpu_launches": int(launches),
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
             "detail": {"rel_residual": rep["rel_residual"], "ir_iters": rep["ir_iters"],

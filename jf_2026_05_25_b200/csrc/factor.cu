@@ -14,6 +14,7 @@
 // scaling (mixed path); the mixed factor is the preconditioner of an FP64
 // iterative refinement on the FP64 CSC matrix.
 #include <algorithm>
+#include <climits>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -30,6 +31,7 @@ struct NumericFactor {
           *amap_pr = nullptr, *amap_pc = nullptr;
   int64_t *Lptr = nullptr, *Uptr = nullptr, *rows_ptr = nullptr, *relptr = nullptr, *amap_dst = nullptr;
   int64_t n_amap = 0;
+  const int32_t* level_sn_cur = nullptr;   // the level the factor loop is on
   // host launch metadata
   struct Level {
     int32_t off, count;
@@ -84,6 +86,7 @@ inline bool fine_prof() {
 
 constexpr int NB = 64;       // panel block width
 constexpr int TILE = 64;     // Schur-update tile
+constexpr int PW = 256;      // super-panel width of the blocked front factorisation
 
 __device__ inline void rec_err(DevError* e, int32_t code, int64_t idx) {
   if (atomicCAS(&e->code, 0, code) == 0) e->index = idx;
@@ -351,7 +354,8 @@ template <typename T>
 __global__ void __launch_bounds__(256)
 k_front_update(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
                const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
-               const int64_t* __restrict__ Uptr, T* __restrict__ L, T* __restrict__ U, int mode, int k0) {
+               const int64_t* __restrict__ Uptr, T* __restrict__ L, T* __restrict__ U, int mode, int kbeg,
+               int kend, int cend) {
   int s = list[blockIdx.y];
   int c = first[s + 1] - first[s];
   int m = mrows[s];
@@ -360,9 +364,11 @@ k_front_update(const int32_t* __restrict__ list, const int32_t* __restrict__ fir
   T* C;
   int64_t ldc;
   if (mode == 0) {
-    int k1 = min(k0 + NB, c);
-    if (k0 >= c || k1 >= c) return;
-    row0 = k1; col0 = k1; nrow = m - k1; ncol = c - k1; kb = k0; ke = k1;
+    // columns [k1, min(cend, c)) and rows [k1, m) of the front, K = [kbeg, k1)
+    int k1 = min(kend, c);
+    int ce = min(cend, c);
+    if (kbeg >= c || k1 >= ce) return;
+    row0 = k1; col0 = k1; nrow = m - k1; ncol = ce - k1; kb = kbeg; ke = k1;
     C = L + Lptr[s] + row0 + (int64_t)m * col0;
     ldc = m;
   } else {
@@ -421,6 +427,142 @@ k_front_update(const int32_t* __restrict__ list, const int32_t* __restrict__ fir
         else C[i + ldc * j] = -acc[a][b];      // U = -L21 L21^T; children are added after
       }
     }
+}
+
+// FP64 tensor-core (DMMA, mma.sync m8n8k4 f64) version of k_front_update for
+// the FP64 factor: the same 64 x 64 tiles and modes, 4 warps per CTA, each
+// warp a 32 x 32 block of 4 x 4 m8n8 accumulators; K in slices of 16 staged
+// through double-buffered shared memory (row stride 68 doubles keeps the
+// fragment loads free of bank conflicts).  tcgen05 has no FP64 kind, so this
+// is the tensor-core route for FP64.
+__device__ __forceinline__ void dmma_884(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+constexpr int DM_LD = TILE + 4;
+
+__global__ void __launch_bounds__(128)
+k_front_update_dmma(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
+                    const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
+                    const int64_t* __restrict__ Uptr, double* __restrict__ L, double* __restrict__ U, int mode,
+                    int kbeg, int kend, int cend) {
+  int s = list[blockIdx.y];
+  int c = first[s + 1] - first[s];
+  int m = mrows[s];
+  const double* P = L + Lptr[s];
+  int row0, col0, nrow, ncol, kb, ke;
+  double* C;
+  int64_t ldc;
+  if (mode == 0) {
+    int k1 = min(kend, c);
+    int ce = min(cend, c);
+    if (kbeg >= c || k1 >= ce) return;
+    row0 = k1; col0 = k1; nrow = m - k1; ncol = ce - k1; kb = kbeg; ke = k1;
+    C = L + Lptr[s] + row0 + (int64_t)m * col0;
+    ldc = m;
+  } else {
+    int r = m - c;
+    if (r <= 0 || Uptr[s] < 0) return;
+    row0 = c; col0 = c; nrow = r; ncol = r; kb = 0; ke = c;
+    C = U + Uptr[s];
+    ldc = r;
+  }
+  int ntj = (ncol + TILE - 1) / TILE, nti = (nrow + TILE - 1) / TILE;
+  int t = blockIdx.x;
+  if (t >= nti * ntj) return;
+  int ti = t / ntj, tj = t % ntj;
+  if (ti * TILE + TILE - 1 + row0 < tj * TILE + col0) return;   // strictly upper tile
+  __shared__ double As[2][16][DM_LD];
+  __shared__ double Bs[2][16][DM_LD];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wr = warp >> 1, wc = warp & 1;
+  const int g = lane >> 2, q = lane & 3;
+  // loader: element e = tid + 128 j -> row e & 63, k (e >> 6) in [0, 16)
+  const int64_t abase = row0 + (int64_t)ti * TILE, bbase = col0 + (int64_t)tj * TILE;
+  double ra[8], rb[8];
+  auto gload = [&](int k) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      int e = tid + 128 * j, r = e & 63, kk = e >> 6;
+      int kg = k + kk;
+      bool kok = kg < ke;
+      ra[j] = (kok && ti * TILE + r < nrow) ? P[abase + r + (int64_t)m * kg] : 0.0;
+      rb[j] = (kok && tj * TILE + r < ncol) ? P[bbase + r + (int64_t)m * kg] : 0.0;
+    }
+  };
+  auto sstore = [&](int buf) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      int e = tid + 128 * j, r = e & 63, kk = e >> 6;
+      As[buf][kk][r] = ra[j];
+      Bs[buf][kk][r] = rb[j];
+    }
+  };
+  double acc[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+  gload(kb);
+  sstore(0);
+  __syncthreads();
+  int buf = 0;
+  for (int k = kb; k < ke; k += 16) {
+    const bool more = k + 16 < ke;
+    if (more) gload(k + 16);
+#pragma unroll
+    for (int k4 = 0; k4 < 16; k4 += 4) {
+      double af[4], bf[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) af[a] = As[buf][k4 + q][wr * 32 + a * 8 + g];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) bf[b] = Bs[buf][k4 + q][wc * 32 + b * 8 + g];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) dmma_884(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+    }
+    if (more) sstore(buf ^ 1);
+    __syncthreads();
+    buf ^= 1;
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        int i = ti * TILE + wr * 32 + a * 8 + g, j = tj * TILE + wc * 32 + b * 8 + 2 * q + h;
+        if (i < nrow && j < ncol && row0 + i >= col0 + j) {
+          if (mode == 0) C[i + ldc * j] -= acc[a][b][h];
+          else C[i + ldc * j] = -acc[a][b][h];
+        }
+      }
+}
+
+inline bool dmma_enabled() {
+  const char* e = std::getenv("JFG_DMMA");
+  return !(e && e[0] == '0');
+}
+
+// one launch of the front update for a level: DMMA for the FP64 factor,
+// SIMT tiles otherwise (and for the FP64 factor with JFG_DMMA=0)
+template <typename T>
+void launch_front_update(unsigned tiles, int count, NumericFactor* F, T* Lf, T* Uf, int mode, int kbeg, int kend,
+                         int cend, cudaStream_t st) {
+  if constexpr (sizeof(T) == 8) {
+    if (dmma_enabled()) {
+      k_front_update_dmma<<<dim3(tiles, count), 128, 0, st>>>(F->level_sn_cur, F->first, F->mrows, F->Lptr, F->Uptr,
+                                                              Lf, Uf, mode, kbeg, kend, cend);
+      count_launch();
+      return;
+    }
+  }
+  k_front_update<T><<<dim3(tiles, count), 256, 0, st>>>(F->level_sn_cur, F->first, F->mrows, F->Lptr, F->Uptr, Lf, Uf,
+                                                        mode, kbeg, kend, cend);
+  count_launch();
 }
 
 // ---------------------------------------------------------------- solves
@@ -910,6 +1052,7 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, c
   const Symbolic& S = m->sym;
   for (const auto& lv : F->levels) {
     const int32_t* list = F->level_sn + lv.off;
+    F->level_sn_cur = list;
     // extend-add, pass 0: children columns that land in this level's panels
     for (const auto& seg : lv.ea) {
       if (seg.second == 0) continue;
@@ -919,25 +1062,37 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, c
                                                             F->parent, F->Lptr, F->Uptr, F->relptr, F->rel, Lf, Uf, 0);
         count_launch(); } prof_end(ps_, st, KS_F_EA, 0.0); }
     }
-    // blocked partial factorisation of every front of the level
-    for (int k0 = 0; k0 < lv.max_c; k0 += NB) {
-      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_potrf_diag<T><<<lv.count, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr,
-                                                                             F->Dptr, Lf, Dvf, k0, F->err);
-        count_launch(); } prof_end(ps_, st, KS_F_POTRF, 0.0); }
-      int rows_max = lv.max_m - k0 - 1;
-      if (rows_max > 0) {
+    // blocked partial factorisation of every front of the level, in
+    // super-panels of PW columns: inside a super-panel the 64-column steps
+    // update only the super-panel's own later columns; the columns after it
+    // take one update with K = PW, so the trailing part of a wide front is
+    // read and written once per PW columns instead of once per 64
+    for (int P0 = 0; P0 < lv.max_c; P0 += PW) {
+      const int P1 = P0 + PW;
+      for (int k0 = P0; k0 < std::min(P1, lv.max_c); k0 += NB) {
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_potrf_diag<T><<<lv.count, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr,
+                                                                               F->Dptr, Lf, Dvf, k0, F->err);
+          count_launch(); } prof_end(ps_, st, KS_F_POTRF, 0.0); }
+        int rows_max = lv.max_m - k0 - 1;
+        if (rows_max <= 0) continue;
         unsigned gx = (unsigned)((rows_max + 63) / 64);
         { int ps_ = fine_prof() ? prof_start(st) : -1; { k_trsm_panel<T><<<dim3(gx, lv.count), 256, 2 * NB * (NB + 1) * sizeof(T), st>>>(list, F->first, F->mrows,
-                                                                                          F->Lptr, F->Dptr, Lf, Dvf, k0);
+                                                                                        F->Lptr, F->Dptr, Lf, Dvf, k0);
           count_launch(); } prof_end(ps_, st, KS_F_TRSM, 0.0); }
-        int nrow = lv.max_m - k0 - NB, ncol = lv.max_c - k0 - NB;
+        int nrow = lv.max_m - k0 - NB, ncol = std::min(P1, lv.max_c) - k0 - NB;
         if (nrow > 0 && ncol > 0) {
           int64_t tiles = (int64_t)((nrow + TILE - 1) / TILE) * ((ncol + TILE - 1) / TILE);
           { int ps_ = fine_prof() ? prof_start(st) : -1;
-            { k_front_update<T><<<dim3((unsigned)tiles, lv.count), 256, 0, st>>>(list, F->first, F->mrows, F->Lptr,
-                                                                            F->Uptr, Lf, Uf, 0, k0); count_launch(); }
+            launch_front_update<T>((unsigned)tiles, lv.count, F, Lf, Uf, 0, k0, k0 + NB, P1, st);
             prof_end(ps_, st, KS_F_PANEL, 0.0); }
         }
+      }
+      int nrow = lv.max_m - P1, ncol = lv.max_c - P1;
+      if (nrow > 0 && ncol > 0) {
+        int64_t tiles = (int64_t)((nrow + TILE - 1) / TILE) * ((ncol + TILE - 1) / TILE);
+        { int ps_ = fine_prof() ? prof_start(st) : -1;
+          launch_front_update<T>((unsigned)tiles, lv.count, F, Lf, Uf, 0, P0, P1, INT_MAX, st);
+          prof_end(ps_, st, KS_F_PANEL, 0.0); }
       }
     }
     if (lv.max_r > 0) {
@@ -950,8 +1105,7 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, c
                                        lv.max_r, lv.max_c, F->err, st);
       }
       if (!done)
-        { k_front_update<T><<<dim3((unsigned)tiles, lv.count), 256, 0, st>>>(list, F->first, F->mrows, F->Lptr,
-                                                                        F->Uptr, Lf, Uf, 1, 0); count_launch(); }
+        launch_front_update<T>((unsigned)tiles, lv.count, F, Lf, Uf, 1, 0, 0, 0, st);
       prof_end(ps, st, KS_SCHUR, lv.schur_flops);
     }
     // extend-add, pass 1: children columns that land in the U of this level

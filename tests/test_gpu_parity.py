@@ -256,3 +256,23 @@ def test_tensor_core_schur_update(ctx, monkeypatch):
     rel = np.abs(out["1"][0] - out["0"][0]) / np.abs(out["0"][0])
     assert rel.max() <= 1e-4, rel.max()
     assert _rel(out["1"][1], out["0"][1]) <= DISP_RTOL
+
+
+def test_dmma_front_update_matches_simt(ctx, monkeypatch):
+    """The FP64 tensor-core (DMMA) update kernel against the SIMT FP64
+    kernel (JFG_DMMA=0): the same factor diagonal to FP64 rounding and the
+    same displacements."""
+    m = M.solid_block(n=8, n_cases=1)
+    F = m.load_matrix()
+    out = {}
+    for flag in ("0", "1"):
+        monkeypatch.setenv("JFG_DMMA", flag)
+        be = B.JFEMGPUBackend(precision=lib.PREC_FP64)
+        be._ctx = ctx
+        st = B.prepare(be, m)
+        U, rep = st["dm"].solve(F, tol=RESID_TOL)
+        assert rep["rel_residual"] <= RESID_TOL
+        out[flag] = (st["dm"].factor_diag(), U)
+    rel = np.abs(out["1"][0] - out["0"][0]) / np.abs(out["0"][0])
+    assert rel.max() <= 1e-10, rel.max()
+    assert _rel(out["1"][1], out["0"][1]) <= 1e-10
