@@ -491,9 +491,9 @@ def stiffened_panel(seed: int) -> Sol101Model:
     blades of depth U{4..8} elements, t ~ U[1,6] mm, edges clamped or simply
     supported, 1-16 subcases of PLOAD4 U[1,20] kPa + N(0,50 N) nodal forces.
 
-    Simply supported edges take SPC 3 on the edge plus the minimum in-plane
-    restraint (SPC 12 at the first edge node, SPC 1 at the last) so that the
-    panel has no in-plane rigid-body motion.
+    Simply supported edges take SPC 3 on the edge; when no edge is clamped,
+    SPC 12 at the skin corner (0, 0) and SPC 2 at the skin corner (lx, 0)
+    remove the in-plane rigid-body motions.
     """
     rng = _rng(seed)
     nx = int(rng.integers(8, 65)); ny = int(rng.integers(8, 65))
@@ -518,10 +518,11 @@ def stiffened_panel(seed: int) -> Sol101Model:
         else:
             spc.append(("3", nodes))
     if not any_clamped:
-        e0 = np.where(edges[2])[0]
-        spc.append(("12", e0[:1])); spc.append(("1", e0[-1:]))
-        e1 = np.where(edges[0])[0]
-        spc.append(("2", e1[-1:]))
+        # in-plane rigid motions: u, v at the skin corner (0, 0) and v at the
+        # skin corner (lx, 0) (the in-plane rotation about z)
+        c00 = np.where(edges[0] & edges[2])[0]
+        c10 = np.where(edges[1] & edges[2])[0]
+        spc.append(("12", c00[:1])); spc.append(("2", c10[:1]))
     n_cases = int(rng.integers(1, 17))
     n_skin_el = nx * ny
     free_nodes = np.setdiff1d(np.arange(len(xyz)), np.concatenate([s[1] for s in spc]))
