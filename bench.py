@@ -372,7 +372,7 @@ def run_batched(args):
         pk = S.PackedModel(p)
         st = B.prepare(be, pk)
         F, sc = pk.load_columns()
-        work.append((i % args.slots, pk, st, F, sc, 1e-10 / np.sqrt(len(p))))
+        work.append((i % args.slots, pk, st, F, sc, 0.5e-10 / np.sqrt(len(p))))
     done = [0.0] * len(work)
     worst = [0.0]
 
@@ -543,7 +543,7 @@ def main():
     ap.add_argument("--slots", type=int, default=4, help="batched/serving: device streams")
     ap.add_argument("--baseline-models", type=int, default=128, help="batched: per-model FP64 sample")
     ap.add_argument("--requests", type=int, default=160, help="serving: requests in the stream")
-    ap.add_argument("--rate", type=float, default=20.0, help="serving: Poisson arrival rate (requests/s)")
+    ap.add_argument("--rate", type=float, default=5.0, help="serving: Poisson arrival rate (requests/s)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
     args = ap.parse_args()
