@@ -177,6 +177,25 @@ def _openblas():
     return os.path.abspath(c[0]) if c else ""
 
 
+# ---------------------------------------------------------------- replicas
+def slowest_rank(seconds: float, world: int, device: str) -> float:
+    """Max over ranks of a per-rank time: with replicas the job ends when the
+    slowest rank does (every rank takes this collective at the same point)."""
+    if world <= 1:
+        return seconds
+    import torch
+    import torch.distributed as dist
+    tt = torch.tensor([seconds], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def replica_throughput(steps: int, world: int, seconds: float) -> float:
+    """Whole-job throughput of N independent replicas: every rank solved
+    `steps` analyses, the job took the slowest rank's time."""
+    return world * steps / seconds
+
+
 # ---------------------------------------------------------------- device arm
 def run_ours(args, rank, world, local_rank):
     import torch
@@ -244,10 +263,8 @@ def run_ours(args, rank, world, local_rank):
     # the device work of the K steps; the torch events on the current stream
     # give the same interval on the device clock.
     ms_dev = max(e0.elapsed_time(e1), 1000.0 * t_wall)
+    ms_dev = slowest_rank(ms_dev, world, "cuda")
     if world > 1:
-        tt = torch.tensor([ms_dev], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_dev = float(tt.item())
         dist.barrier()
     clk = clocks.stop()
     stats = {}
@@ -260,7 +277,7 @@ def run_ours(args, rank, world, local_rank):
         if o[0] > 0:
             stats[name] = {"launches": int(o[0]), "ms": float(o[1]), "units": float(o[2])}
     ms_step = ms_dev / args.steps
-    value = world * args.steps / (ms_dev / 1000.0)
+    value = replica_throughput(args.steps, world, ms_dev / 1000.0)
     # ---- e2e through the public API with host buffers
     if not args.no_e2e:
         step_e2e()
@@ -272,11 +289,8 @@ def run_ours(args, rank, world, local_rank):
         step_e2e()
     torch.cuda.synchronize()
     e2e_s = max(time.perf_counter() - t0, 1e-9)
-    if world > 1:
-        tt = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
-    e2e_value = world * args.steps / e2e_s
+    e2e_s = slowest_rank(e2e_s, world, "cuda")
+    e2e_value = replica_throughput(args.steps, world, e2e_s)
     # ---- roofline of the dominant kernel
     peaks = _peaks()
     # the roofline reports the dominant single kernel among the coarse classes
