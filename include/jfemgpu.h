@@ -44,8 +44,9 @@ typedef enum {
 
 typedef enum {
   JFG_PREC_FP64 = 0,        /* plain FP64 supernodal Cholesky                      */
-  JFG_PREC_MIXED = 1        /* FP32-storage factor, 3xTF32 tensor-core updates,
-                               FP64 iterative refinement on the FP64 CSR matrix   */
+  JFG_PREC_MIXED = 1        /* FP32-storage factor (FP32 updates; 3xTF32 tensor-
+                               core updates with JFG_TENSOR_CORES=1), FP64
+                               iterative refinement on the FP64 CSR matrix      */
 } jfg_precision;
 
 typedef struct jfg_ctx jfg_ctx;
@@ -173,7 +174,7 @@ jfg_status jfg_get_timings(jfg_model* model, double* seconds4);
  * between solves (device memory held by another framework's caching pool,
  * or other streams that a device-wide cudaMalloc/cudaFree would stall).
  * The element matrices live in one fixed 16 MiB device array of the
- * library, so models needing more element storage (about 3,600 CQUAD4 or
+ * library, so models needing more element storage (about 2,600 CQUAD4 or
  * 2,300 CTETRA10) get JFG_BAD_INPUT.  jfg_assemble must have been called
  * once on the model (it builds the pattern).  All calls on a device share
  * that array: calls that overlap on the GPU race and must be serialised.

@@ -213,6 +213,7 @@ jfg_status jfg_model_upload(jfg_ctx* c, int64_t n_nodes, const double* xyz, cons
   m->ev_q8_off = m->ev_t10_off + 900 * n_t10;
   m->n_ev = m->ev_q8_off + 2304 * n_q8;
   if ((st = dev_alloc(c, (void**)&m->d_ev, sizeof(double) * std::max<int64_t>(m->n_ev, 1))) ||
+      (st = dev_alloc(c, (void**)&m->d_q4prep, sizeof(double) * Q4_PREP_STRIDE * std::max<int64_t>(n_q4, 1))) ||
       (st = dev_alloc(c, (void**)&m->d_err, sizeof(DevError)))) {
     jfg_model_free(m);
     return st;
@@ -231,6 +232,7 @@ jfg_status jfg_model_free(jfg_model* m) {
   dev_free(c, m->d_q8n, 4 * m->h_q8n.size()); dev_free(c, m->d_q8s, 8 * m->h_q8s.size());
   dev_free(c, m->d_t10n, 4 * m->h_t10n.size()); dev_free(c, m->d_t10m, 8 * m->h_t10m.size());
   dev_free(c, m->d_ev, 8 * std::max<int64_t>(m->n_ev, 1)); dev_free(c, m->d_err, sizeof(DevError));
+  dev_free(c, m->d_q4prep, 8 * Q4_PREP_STRIDE * std::max<int64_t>(m->n_q4, 1));
   if (m->pattern_built) {
     dev_free(c, m->d_colptr, 8 * (m->ndof + 1)); dev_free(c, m->d_rowval, 4 * m->nnz);
     dev_free(c, m->d_nzptr, 4 * (m->nnz + 1)); dev_free(c, m->d_trip, 4 * m->n_trip);

@@ -96,17 +96,9 @@ __device__ bool inv_small(const double* A, double* Ai) {
   return true;
 }
 
-struct Q4Slab {
-  double Kab[96], Kbb[16], Kabs[96], Kbbs[16], Kabb[96], Kbbb[16];
-  double D[48], sol[48], Ci[32];
-  double Pm[96], Pb[96];
-  double Ke[576];
-  double T[36];
-  int status;
-};
 
-// MacNeal shear operator D (4 x 12) and sol = Z^-1 D; single lane.
-__device__ int macneal_operator(const double lc[8], const double* Cb, const double* Cs, Q4Slab& S) {
+// MacNeal shear operator D (4 x 12) and sol = Z^-1 D (one thread).
+__device__ int macneal_operator(const double lc[8], const double* Cb, const double* Cs, double* D, double* sol) {
   const double pt = 0.57735026918962573;  // 1/sqrt(3)
   const double sxi[4] = {0.0, 0.0, -pt, pt}, seta[4] = {-pt, pt, 0.0, 0.0};
   double Ce[4][12], Je[4][4];
@@ -127,7 +119,6 @@ __device__ int macneal_operator(const double lc[8], const double* Cb, const doub
       Ce[sp][3 * k + 2] = N[k] * tx;
     }
   }
-  double* D = S.D;
   for (int sp = 0; sp < 4; ++sp) {
     double J11 = Je[sp][0], J12 = Je[sp][1], J21 = Je[sp][2], J22 = Je[sp][3];
     double det = J11 * J22 - J12 * J21;
@@ -210,20 +201,32 @@ __device__ int macneal_operator(const double lc[8], const double* Cb, const doub
     for (int i = 0; i < 4; ++i) {
       double s = 0.0;
       for (int k = 0; k < 4; ++k) s += Zi[i + 4 * k] * D[k + 4 * j];
-      S.sol[i + 4 * j] = s;
+      sol[i + 4 * j] = s;
     }
   return 0;
 }
 
-__global__ void __launch_bounds__(WARPS * 32)
-k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ sect,
-     const double* __restrict__ xyz, const double* __restrict__ nodeR, double* __restrict__ ev,
-     DevError* err) {
-  __shared__ Q4Slab slabs[WARPS];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t e = (int64_t)blockIdx.x * WARPS + w;
+// CQUAD4 in two passes.  k_q4_prep, one thread per element, does the scalar
+// work: element frame and local coordinates, the PSHELL material rotation,
+// the MacNeal shear operator D and Z^{-1} D, and the 4 x 4 internal-mode
+// blocks with their inverses.  k_q4, one warp per element, then accumulates
+// the 24 x 24 stiffness with every lane busy (18 entries each): Gauss-point
+// membrane and bending, the shear term, lumped drilling, the
+// section-kinematic enrichment and the node-frame transform.  The prep record
+// per element is Q4P doubles of scratch.
+constexpr int Q4P_LC = 0, Q4P_V = 8, Q4P_CM = 17, Q4P_CB = 26, Q4P_CS = 35, Q4P_SHP = 39, Q4P_DETJC = 40,
+              Q4P_IJC = 41, Q4P_K6 = 45, Q4P_H = 46, Q4P_SHEAR = 47, Q4P_D = 48, Q4P_SOL = 96, Q4P_CI = 144,
+              Q4P_KBB = 176, Q4P_KBBB = 192, Q4P_STATUS = 208;
+constexpr int Q4P = Q4_PREP_STRIDE;
+static_assert(Q4P_STATUS < Q4P, "CQUAD4 prep record layout");
+
+__global__ void __launch_bounds__(128)
+k_q4_prep(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ sect,
+          const double* __restrict__ xyz, double* __restrict__ prep, DevError* err) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n) return;
-  Q4Slab& S = slabs[w];
+  double* out = prep + Q4P * e;
+  out[Q4P_STATUS] = 0.0;
   int nd[4];
   double p[4][3];
 #pragma unroll
@@ -291,11 +294,13 @@ k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ se
   }
   const double* sc = sect + 26 * e;
   if (!(zmax <= 1e-12 * fmax(xmax, 1e-30))) {
-    if (lane == 0) record_error(err, EE_NOT_FLAT, e);
+    record_error(err, EE_NOT_FLAT, e);
+    out[Q4P_STATUS] = 1.0;
     return;
   }
   if (sc[25] != 0.0) {
-    if (lane == 0) record_error(err, EE_FLAGS, e);
+    record_error(err, EE_FLAGS, e);
+    out[Q4P_STATUS] = 1.0;
     return;
   }
   double Cm[9], Cb[9], Cs[4];
@@ -343,22 +348,151 @@ k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ se
 #pragma unroll
   for (int i = 0; i < 9; ++i) cmmax = fmax(cmmax, fabs(Cm[i]));
   const double* shp = cmmax > 0 ? Cm : Cb;
-  // ---- center Jacobian
   const double dNr_c[4] = {-0.25, 0.25, 0.25, -0.25}, dNs_c[4] = {-0.25, -0.25, 0.25, 0.25};
   double J11c, J12c, J21c, J22c;
   jac4(lc, dNr_c, dNs_c, J11c, J12c, J21c, J22c);
   const double detJc = J11c * J22c - J12c * J21c;
   const double idc = 1.0 / detJc;
   const double iJ11c = J22c * idc, iJ12c = -J12c * idc, iJ21c = -J21c * idc, iJ22c = J11c * idc;
-  // ---- owned accumulators
-  double ke[18], kab[3], kabs[3], kabb[3], kbb = 0, kbbs = 0, kbbb = 0;
+  // internal-mode blocks over the 2 x 2 Gauss points
+  double kbb[16], kbbs[16], kbbb[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) kbb[q] = kbbs[q] = kbbb[q] = 0.0;
+  const double pt = 0.57735026918962573;
+  const double gr[4] = {-pt, pt, pt, -pt}, gs[4] = {-pt, -pt, pt, pt};
+  bool ok = true;
+  for (int g = 0; g < 4; ++g) {
+    double r = gr[g], sv = gs[g];
+    double dNr[4], dNs[4];
+    shape_d(r, sv, dNr, dNs);
+    double J11, J12, J21, J22;
+    jac4(lc, dNr, dNs, J11, J12, J21, J22);
+    double detJ = J11 * J22 - J12 * J21;
+    if (!jac_ok(detJ, J11, J12, J21, J22)) ok = false;
+    double wgt = fabs(detJ), id = 1.0 / detJ;
+    double iJ11 = J22 * id, iJ12 = -J12 * id, iJ21 = -J21 * id, iJ22 = J11 * id;
+    double ratio = (iJ11 * iJ22 - iJ12 * iJ21) / (iJ11c * iJ22c - iJ12c * iJ21c);
+    double p1x = ratio * iJ11c * (-2 * r), p1y = ratio * iJ21c * (-2 * r);
+    double p2x = ratio * iJ12c * (-2 * sv), p2y = ratio * iJ22c * (-2 * sv);
+    double gq = detJc / detJ;
+    double b1x = (iJ11c * (-2 * r)) * gq, b1y = (iJ21c * (-2 * r)) * gq;
+    double b2x = (iJ12c * (-2 * sv)) * gq, b2y = (iJ22c * (-2 * sv)) * gq;
+    auto bi = [&](int q, double o[3]) {
+      if (q == 0) { o[0] = p1x; o[1] = 0; o[2] = p1y; }
+      else if (q == 1) { o[0] = 0; o[1] = p1y; o[2] = p1x; }
+      else if (q == 2) { o[0] = p2x; o[1] = 0; o[2] = p2y; }
+      else { o[0] = 0; o[1] = p2y; o[2] = p2x; }
+    };
+    auto bib = [&](int q, double o[3]) {
+      if (q == 0) { o[0] = 0; o[1] = -b1y; o[2] = -b1x; }
+      else if (q == 1) { o[0] = 0; o[1] = -b2y; o[2] = -b2x; }
+      else if (q == 2) { o[0] = b1x; o[1] = 0; o[2] = b1y; }
+      else { o[0] = b2x; o[1] = 0; o[2] = b2y; }
+    };
+    for (int l = 0; l < 16; ++l) {
+      int i = l % 4, q = l / 4;
+      double u[3], v[3];
+      bi(i, u); bi(q, v);
+      kbb[l] += wgt * qf3(u, Cm, v);
+      bib(i, u); bib(q, v);
+      kbbs[l] += wgt * qf3(u, shp, v);
+      kbbb[l] += wgt * qf3(u, Cb, v);
+    }
+  }
+  if (!ok) {
+    record_error(err, EE_JACOBIAN, e);
+    out[Q4P_STATUS] = 1.0;
+    return;
+  }
+  double csmax = fmax(fmax(fabs(Cs[0]), fabs(Cs[1])), fmax(fabs(Cs[2]), fabs(Cs[3])));
+  bool do_shear = !(h < 1e-30 || csmax < 1e-30);
+  if (do_shear) {
+    int st = macneal_operator(lc, Cb, Cs, out + Q4P_D, out + Q4P_SOL);
+    if (st != 0) {
+      record_error(err, EE_SHEAR + st, e);
+      out[Q4P_STATUS] = 1.0;
+      return;
+    }
+  }
+  // drilling corners must have valid Jacobians
+  const double alphaL = (k6rot * 1e-6) * Cm[8] * (4.0 * fabs(detJc));
+  if (alphaL != 0.0) {
+    const double cr[4] = {-1, 1, 1, -1}, cs4[4] = {-1, -1, 1, 1};
+    for (int corner = 0; corner < 4; ++corner) {
+      double dNr[4], dNs[4];
+      shape_d(cr[corner], cs4[corner], dNr, dNs);
+      double J11, J12, J21, J22;
+      jac4(lc, dNr, dNs, J11, J12, J21, J22);
+      if (!jac_ok(J11 * J22 - J12 * J21, J11, J12, J21, J22)) ok = false;
+    }
+    if (!ok) {
+      record_error(err, EE_JACOBIAN, e);
+      out[Q4P_STATUS] = 1.0;
+      return;
+    }
+  }
+  // enrichment inverses
+  {
+    double mx = 0, mb = 0;
+    for (int i = 0; i < 16; ++i) { mx = fmax(mx, fabs(kbb[i])); mb = fmax(mb, fabs(kbbs[i])); }
+    bool good = true;
+    if (mx > 0) { if (!inv_small<4>(kbb, out + Q4P_CI)) good = false; }
+    else for (int i = 0; i < 16; ++i) out[Q4P_CI + i] = 0.0;
+    if (mb > 0) { if (!inv_small<4>(kbbs, out + Q4P_CI + 16)) good = false; }
+    else for (int i = 0; i < 16; ++i) out[Q4P_CI + 16 + i] = 0.0;
+    if (!good) {
+      record_error(err, EE_ENRICH, e);
+      out[Q4P_STATUS] = 1.0;
+      return;
+    }
+  }
+  for (int i = 0; i < 8; ++i) out[Q4P_LC + i] = lc[i];
+  for (int a = 0; a < 3; ++a) { out[Q4P_V + a] = v1[a]; out[Q4P_V + 3 + a] = v2[a]; out[Q4P_V + 6 + a] = v3[a]; }
+  for (int i = 0; i < 9; ++i) { out[Q4P_CM + i] = Cm[i]; out[Q4P_CB + i] = Cb[i]; }
+  for (int i = 0; i < 4; ++i) out[Q4P_CS + i] = Cs[i];
+  out[Q4P_SHP] = cmmax > 0 ? 1.0 : 0.0;
+  out[Q4P_DETJC] = detJc;
+  out[Q4P_IJC] = iJ11c; out[Q4P_IJC + 1] = iJ12c; out[Q4P_IJC + 2] = iJ21c; out[Q4P_IJC + 3] = iJ22c;
+  out[Q4P_K6] = k6rot;
+  out[Q4P_H] = h;
+  out[Q4P_SHEAR] = do_shear ? 1.0 : 0.0;
+  for (int i = 0; i < 16; ++i) { out[Q4P_KBB + i] = kbb[i]; out[Q4P_KBBB + i] = kbbb[i]; }
+}
+
+struct Q4Slab {
+  double P[Q4P];
+  double Kab[96], Kabs[96], Kabb[96];
+  double Pm[96], Pb[96];
+  double Ke[576];
+  double T[36];
+};
+
+__global__ void __launch_bounds__(WARPS * 32)
+k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ prep,
+     const double* __restrict__ nodeR, double* __restrict__ ev) {
+  __shared__ Q4Slab slabs[WARPS];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t e = (int64_t)blockIdx.x * WARPS + w;
+  if (e >= n) return;
+  Q4Slab& S = slabs[w];
+  const double* src = prep + Q4P * e;
+  for (int i = lane; i < Q4P; i += 32) S.P[i] = src[i];
+  __syncwarp();
+  if (S.P[Q4P_STATUS] != 0.0) return;
+  const double* lc = S.P + Q4P_LC;
+  const double* Cm = S.P + Q4P_CM;
+  const double* Cb = S.P + Q4P_CB;
+  const double* shp = S.P[Q4P_SHP] != 0.0 ? Cm : Cb;
+  const double detJc = S.P[Q4P_DETJC];
+  const double iJ11c = S.P[Q4P_IJC], iJ12c = S.P[Q4P_IJC + 1], iJ21c = S.P[Q4P_IJC + 2], iJ22c = S.P[Q4P_IJC + 3];
+  const double k6rot = S.P[Q4P_K6];
+  double ke[18], kab[3], kabs[3], kabb[3];
 #pragma unroll
   for (int t = 0; t < 18; ++t) ke[t] = 0.0;
 #pragma unroll
   for (int t = 0; t < 3; ++t) { kab[t] = 0.0; kabs[t] = 0.0; kabb[t] = 0.0; }
   const double pt = 0.57735026918962573;
   const double gr[4] = {-pt, pt, pt, -pt}, gs[4] = {-pt, -pt, pt, pt};
-  bool ok = true;
   for (int g = 0; g < 4; ++g) {
     double r = gr[g], s = gs[g];
     double dNr[4], dNs[4];
@@ -366,7 +500,6 @@ k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ se
     double J11, J12, J21, J22;
     jac4(lc, dNr, dNs, J11, J12, J21, J22);
     double detJ = J11 * J22 - J12 * J21;
-    if (!jac_ok(detJ, J11, J12, J21, J22)) ok = false;
     double wgt = fabs(detJ), id = 1.0 / detJ;
     double iJ11 = J22 * id, iJ12 = -J12 * id, iJ21 = -J21 * id, iJ22 = J11 * id;
     double dx[4], dy[4];
@@ -436,19 +569,6 @@ k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ se
         kabb[t] += wgt * qf3(u, Cb, v);
       }
     }
-    if (lane < 16) {
-      int i = lane % 4, q = lane / 4;
-      double u[3], v[3];
-      bi(i, u); bi(q, v);
-      kbb += wgt * qf3(u, Cm, v);
-      bib(i, u); bib(q, v);
-      kbbs += wgt * qf3(u, shp, v);
-      kbbb += wgt * qf3(u, Cb, v);
-    }
-  }
-  if (!ok) {
-    if (lane == 0) record_error(err, EE_JACOBIAN, e);
-    return;
   }
 #pragma unroll
   for (int t = 0; t < 3; ++t) {
@@ -456,17 +576,10 @@ k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ se
     S.Kabs[lane + 32 * t] = kabs[t];
     S.Kabb[lane + 32 * t] = kabb[t];
   }
-  if (lane < 16) { S.Kbb[lane] = kbb; S.Kbbs[lane] = kbbs; S.Kbbb[lane] = kbbb; }
-  // ---- MacNeal shear operator (lane 0), needs only lc/Cb/Cs
-  double csmax = fmax(fmax(fabs(Cs[0]), fabs(Cs[1])), fmax(fabs(Cs[2]), fabs(Cs[3])));
-  bool do_shear = !(h < 1e-30 || csmax < 1e-30);
-  if (lane == 0) S.status = do_shear ? macneal_operator(lc, Cb, Cs, S) : 0;
-  __syncwarp();
-  if (S.status != 0) {
-    if (lane == 0) record_error(err, EE_SHEAR + S.status, e);
-    return;
-  }
-  if (do_shear) {
+  // ---- MacNeal shear term
+  if (S.P[Q4P_SHEAR] != 0.0) {
+    const double* D = S.P + Q4P_D;
+    const double* sol = S.P + Q4P_SOL;
 #pragma unroll
     for (int t = 0; t < 18; ++t) {
       int idx = lane + 32 * t;
@@ -477,8 +590,8 @@ k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ se
         double a = 0.0, b = 0.0;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          a += S.D[q + 4 * ii] * S.sol[q + 4 * jj];
-          b += S.D[q + 4 * jj] * S.sol[q + 4 * ii];
+          a += D[q + 4 * ii] * sol[q + 4 * jj];
+          b += D[q + 4 * jj] * sol[q + 4 * ii];
         }
         ke[t] += 0.5 * (a + b);
       }
@@ -494,7 +607,6 @@ k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ se
       double J11, J12, J21, J22;
       jac4(lc, dNr, dNs, J11, J12, J21, J22);
       double detJ = J11 * J22 - J12 * J21;
-      if (!jac_ok(detJ, J11, J12, J21, J22)) ok = false;
       double id = 1.0 / detJ;
       double iJ11 = J22 * id, iJ12 = -J12 * id, iJ21 = -J21 * id, iJ22 = J11 * id;
       double wc = alphaL * (fabs(detJ) / fmax(fabs(detJc), 1e-30));
@@ -513,28 +625,10 @@ k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ se
         if (bi_ != 0.0) ke[t] += wc * (bi_ * bd(j));
       }
     }
-    if (!ok) {
-      if (lane == 0) record_error(err, EE_JACOBIAN, e);
-      return;
-    }
   }
   // ---- section-kinematic enrichment
   __syncwarp();
-  if (lane == 0) {
-    double mx = 0, mb = 0;
-    for (int i = 0; i < 16; ++i) { mx = fmax(mx, fabs(S.Kbb[i])); mb = fmax(mb, fabs(S.Kbbs[i])); }
-    int st = 0;
-    if (mx > 0) { if (!inv_small<4>(S.Kbb, S.Ci)) st = 1; }
-    else for (int i = 0; i < 16; ++i) S.Ci[i] = 0.0;
-    if (mb > 0) { if (!inv_small<4>(S.Kbbs, S.Ci + 16)) st = 1; }
-    else for (int i = 0; i < 16; ++i) S.Ci[16 + i] = 0.0;
-    S.status = st;
-  }
-  __syncwarp();
-  if (S.status != 0) {
-    if (lane == 0) record_error(err, EE_ENRICH, e);
-    return;
-  }
+  const double* Ci = S.P + Q4P_CI;
 #pragma unroll
   for (int t = 0; t < 3; ++t) {
     int idx = lane + 32 * t;      // (q, j) of a 4 x 24 map
@@ -542,13 +636,15 @@ k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ se
     double pm = 0.0, pb = 0.0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      pm -= S.Ci[q + 4 * k] * S.Kab[j + 24 * k];
-      pb -= S.Ci[16 + q + 4 * k] * S.Kabs[j + 24 * k];
+      pm -= Ci[q + 4 * k] * S.Kab[j + 24 * k];
+      pb -= Ci[16 + q + 4 * k] * S.Kabs[j + 24 * k];
     }
     S.Pm[idx] = pm;
     S.Pb[idx] = pb;
   }
   __syncwarp();
+  const double* Kbb = S.P + Q4P_KBB;
+  const double* Kbbb = S.P + Q4P_KBBB;
 #pragma unroll
   for (int t = 0; t < 18; ++t) {
     int idx = lane + 32 * t;
@@ -560,8 +656,8 @@ k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ se
            S.Kabb[i + 24 * k] * S.Pb[k + 4 * j] + S.Pb[k + 4 * i] * S.Kabb[j + 24 * k];
 #pragma unroll
       for (int l = 0; l < 4; ++l)
-        v += S.Pm[k + 4 * i] * S.Kbb[k + 4 * l] * S.Pm[l + 4 * j] +
-             S.Pb[k + 4 * i] * S.Kbbb[k + 4 * l] * S.Pb[l + 4 * j];
+        v += S.Pm[k + 4 * i] * Kbb[k + 4 * l] * S.Pm[l + 4 * j] +
+             S.Pb[k + 4 * i] * Kbbb[k + 4 * l] * S.Pb[l + 4 * j];
     }
     ke[t] += v;
   }
@@ -569,8 +665,9 @@ k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ se
 #pragma unroll
   for (int t = 0; t < 18; ++t) S.Ke[lane + 32 * t] = ke[t];
   if (lane < 4) {
-    const double* R = nodeR + 9 * (int64_t)nd[lane];
-    const double Rel[3][3] = {{v1[0], v1[1], v1[2]}, {v2[0], v2[1], v2[2]}, {v3[0], v3[1], v3[2]}};
+    const double* R = nodeR + 9 * (int64_t)nodes[4 * e + lane];
+    const double* V = S.P + Q4P_V;
+    const double Rel[3][3] = {{V[0], V[1], V[2]}, {V[3], V[4], V[5]}, {V[6], V[7], V[8]}};
     for (int rr = 0; rr < 3; ++rr)
       for (int cc = 0; cc < 3; ++cc)
         S.T[9 * lane + rr + 3 * cc] =
@@ -1082,8 +1179,10 @@ jfg_status launch_elements(jfg_model* m, cudaStream_t st) {
   if (m->n_q4 > 0) {
     int64_t blocks = (m->n_q4 + WARPS - 1) / WARPS;
     int ps = prof_start(st);
-    { k_q4<<<(unsigned)blocks, WARPS * 32, 0, st>>>(m->n_q4, m->d_q4n, m->d_q4s, m->d_xyz, m->d_R,
-                                                 m->d_ev, m->d_err); count_launch(); }
+    { k_q4_prep<<<(unsigned)((m->n_q4 + 127) / 128), 128, 0, st>>>(m->n_q4, m->d_q4n, m->d_q4s, m->d_xyz,
+                                                                 m->d_q4prep, m->d_err); count_launch(); }
+    { k_q4<<<(unsigned)blocks, WARPS * 32, 0, st>>>(m->n_q4, m->d_q4n, m->d_q4prep, m->d_R, m->d_ev);
+      count_launch(); }
     // algorithmic bytes: connectivity + section in, matrix out, coordinates once
     prof_end(ps, st, KS_Q4, (double)m->n_q4 * (16 + 8 * 26 + 8 * 576) + 24.0 * m->n_nodes);
     JFG_CUDA(cudaGetLastError());
@@ -1113,13 +1212,15 @@ jfg_status launch_elements(jfg_model* m, cudaStream_t st) {
 }
 
 // Same element kernels as launch_elements, writing the element matrices to
-// `ev` (n_ev doubles) and the first element error to `err` instead of the
-// model's own buffers; no profiling events.
-jfg_status launch_elements_into(const jfg_model* m, cudaStream_t st, double* ev, DevError* err) {
+// `ev` (n_ev doubles), the CQUAD4 prep records to `q4prep` (n_q4 x
+// Q4_PREP_STRIDE doubles) and the first element error to `err` instead of
+// the model's own buffers; no profiling events.
+jfg_status launch_elements_into(const jfg_model* m, cudaStream_t st, double* ev, double* q4prep, DevError* err) {
   if (m->n_q4 > 0) {
     int64_t blocks = (m->n_q4 + WARPS - 1) / WARPS;
-    { k_q4<<<(unsigned)blocks, WARPS * 32, 0, st>>>(m->n_q4, m->d_q4n, m->d_q4s, m->d_xyz, m->d_R, ev, err);
-      count_launch(); }
+    { k_q4_prep<<<(unsigned)((m->n_q4 + 127) / 128), 128, 0, st>>>(m->n_q4, m->d_q4n, m->d_q4s, m->d_xyz, q4prep,
+                                                                 err); count_launch(); }
+    { k_q4<<<(unsigned)blocks, WARPS * 32, 0, st>>>(m->n_q4, m->d_q4n, q4prep, m->d_R, ev); count_launch(); }
     JFG_CUDA(cudaGetLastError());
   }
   if (m->n_t10 > 0) {

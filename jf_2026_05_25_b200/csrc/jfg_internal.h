@@ -56,6 +56,10 @@ struct DevMem {
 };
 
 // Error record written by device kernels (first failing element / pivot).
+// doubles per CQUAD4 of the scratch record passed from the thread-per-element
+// pass to the warp-per-element pass of the element kernel
+constexpr int Q4_PREP_STRIDE = 210;
+
 struct DevError {
   int32_t code;        // 0 = none
   int32_t pad;
@@ -103,6 +107,7 @@ struct jfg_model {
   // element values: Q4 576 / T10 900 / Q8 2304 doubles per element
   int64_t ev_t10_off = 0, ev_q8_off = 0, n_ev = 0;
   double* d_ev = nullptr;
+  double* d_q4prep = nullptr;   // n_q4 x Q4_PREP_STRIDE scratch between the two CQUAD4 passes
   jfg::DevError* d_err = nullptr;
   // pattern + slot map (built once)
   bool pattern_built = false;
@@ -131,7 +136,7 @@ namespace jfg {
 
 // elements.cu
 jfg_status launch_elements(jfg_model* m, cudaStream_t st);
-jfg_status launch_elements_into(const jfg_model* m, cudaStream_t st, double* ev, DevError* err);
+jfg_status launch_elements_into(const jfg_model* m, cudaStream_t st, double* ev, double* q4prep, DevError* err);
 // assembly.cu
 jfg_status build_pattern(jfg_model* m);
 jfg_status launch_assembly(jfg_model* m, cudaStream_t st);

@@ -13,14 +13,15 @@
 //
 // Limits and sharing:
 //   * the scratch array holds at most kScratchBytes (16 MiB); a model whose
-//     element matrices need more (roughly 3,600 CQUAD4 or 2,300 CTETRA10
-//     elements) is rejected with JFG_BAD_INPUT before any launch;
+//     element matrices and CQUAD4 prep records need more (roughly 2,600
+//     CQUAD4 or 2,300 CTETRA10 elements) is rejected with JFG_BAD_INPUT
+//     before any launch;
 //   * every GPU that loads the library holds the 16 MiB array until the
 //     process exits;
 //   * every call on a device shares the same array and it keeps the previous
 //     call's contents.  The element-error record at its head must start at
 //     zero and is cleared by each call (cudaMemsetAsync); the element
-//     matrices are overwritten in full by each call.  Calls whose work
+//     matrices and prep records are overwritten in full by each call.  Calls whose work
 //     overlaps on the same GPU (two host threads, or two contexts on
 //     different streams) race on the array: serialise them;
 //   * the first call on each device looks up the array's device address
@@ -97,7 +98,8 @@ jfg_status jfg_assemble_values_noalloc(jfg_model* m, double* nzval_dev) {
     set_error("pattern not built: call jfg_assemble once before the no-allocation variant");
     return JFG_NOT_READY;
   }
-  const size_t need = kHeaderBytes + sizeof(double) * (size_t)m->n_ev;
+  const size_t ev_bytes = (sizeof(double) * (size_t)m->n_ev + 255) / 256 * 256;
+  const size_t need = kHeaderBytes + ev_bytes + sizeof(double) * Q4_PREP_STRIDE * (size_t)m->n_q4;
   if (need > kScratchBytes) {
     set_error("model needs " + std::to_string(need) + " bytes of element scratch; the no-allocation path holds " +
               std::to_string(kScratchBytes) + " bytes (use jfg_assemble)", (int64_t)need);
@@ -109,9 +111,10 @@ jfg_status jfg_assemble_values_noalloc(jfg_model* m, double* nzval_dev) {
   JFG_TRY(scratch_address(m->ctx->device, &base));
   DevError* err = reinterpret_cast<DevError*>(base);
   double* ev = reinterpret_cast<double*>(base + kHeaderBytes);
+  double* q4prep = reinterpret_cast<double*>(base + kHeaderBytes + ev_bytes);
   cudaStream_t st = m->ctx->stream;
   JFG_CUDA(cudaMemsetAsync(err, 0, sizeof(DevError), st));
-  JFG_TRY(launch_elements_into(m, st, ev, err));
+  JFG_TRY(launch_elements_into(m, st, ev, q4prep, err));
   JFG_TRY(launch_gather_into(m, st, ev, nzval_dev));
   DevError h{};
   JFG_CUDA(cudaMemcpyAsync(&h, err, sizeof(DevError), cudaMemcpyDeviceToHost, st));
