@@ -32,6 +32,13 @@ struct NumericFactor {
   int64_t *Lptr = nullptr, *Uptr = nullptr, *rows_ptr = nullptr, *relptr = nullptr, *amap_dst = nullptr;
   int64_t n_amap = 0;
   const int32_t* level_sn_cur = nullptr;   // the level the factor loop is on
+  // CUDA graphs of the factorisation (per precision) and of one preconditioner
+  // application (per precision and right-hand-side count 1..8)
+  cudaGraphExec_t factor_graph[2] = {nullptr, nullptr};
+  int64_t factor_graph_nodes[2] = {0, 0};
+  int factor_calls[2] = {0, 0};
+  cudaGraphExec_t solve_graph[2][9] = {};
+  int64_t solve_graph_nodes[2][9] = {};
   // host launch metadata
   struct Level {
     int32_t off, count;
@@ -82,6 +89,50 @@ inline bool fine_prof() {
   static int v = -1;
   if (v < 0) v = std::getenv("JFG_FINE_PROFILE") ? 1 : 0;
   return v == 1 && profiling_enabled();
+}
+
+// Launch-bound sequences (the level loop of the factorisation, the level and
+// strip loop of a preconditioner application) are captured once into a CUDA
+// graph and replayed: one graph launch instead of hundreds of kernel launches.
+// JFG_GRAPHS=0 or kernel-class profiling runs them eagerly.
+inline bool graphs_enabled() {
+  const char* e = std::getenv("JFG_GRAPHS");
+  return !(e && e[0] == '0') && !profiling_enabled();
+}
+
+template <typename Fn>
+jfg_status run_graph(cudaGraphExec_t& ge, int64_t& nodes, cudaStream_t st, Fn&& body) {
+  if (!ge) {
+    const int64_t c0 = launch_count();
+    cudaGraph_t g = nullptr;
+    JFG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    jfg_status s = body();
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    const int64_t k = launch_count() - c0;
+    count_launch(-(int)k);   // nothing ran while capturing
+    if (s != JFG_OK || e != cudaSuccess || g == nullptr) {
+      if (g) cudaGraphDestroy(g);
+      (void)cudaGetLastError();
+      return body();          // run eagerly instead
+    }
+    e = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      ge = nullptr;
+      (void)cudaGetLastError();
+      return body();
+    }
+    nodes = k;
+  }
+  JFG_CUDA(cudaGraphLaunch(ge, st));
+  count_launch((int)nodes);
+  return JFG_OK;
+}
+
+void drop_solve_graphs(NumericFactor* F) {
+  for (auto& row : F->solve_graph)
+    for (auto& g : row)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
 }
 
 constexpr int NB = 64;       // panel block width
@@ -1199,6 +1250,7 @@ jfg_status ensure_workspace(jfg_model* m, NumericFactor* F, int nrhs) {
     p = nullptr;
   };
   int64_t n = m->sym.n, ndof = m->ndof;
+  drop_solve_graphs(F);
   if (F->nrhs_cap > 0) {
     int oc = F->nrhs_cap;
     fr(F->xp, n * oc); fr(F->tt, n * oc); fr(F->V, F->v_total * oc); fr(F->dF, ndof * oc); fr(F->dU, ndof * oc);
@@ -1424,6 +1476,9 @@ void numeric_destroy(jfg_model* m) {
   fr(F->norms, 8 * (256 * 64 + 64));
   if (F->ev0) cudaEventDestroy(F->ev0);
   if (F->ev1) cudaEventDestroy(F->ev1);
+  drop_solve_graphs(F);
+  for (auto& g : F->factor_graph)
+    if (g) cudaGraphExecDestroy(g);
   delete F;
   m->num = nullptr;
 }
@@ -1450,8 +1505,16 @@ jfg_status numeric_factor(jfg_model* m, int precision) {
     F->have64 = false;
     if (!F->Dinv64) JFG_TRY(dev_alloc(c, (void**)&F->Dinv64, sizeof(double) * F->dinv_len));
     if (!F->Sinv64) JFG_TRY(dev_alloc(c, (void**)&F->Sinv64, sizeof(double) * F->sinv_len));
-    JFG_TRY(factor_levels<double>(m, F, F->L64, F->U64, F->Dinv64, st));
-    JFG_TRY(strip_inverses<double>(F, F->L64, F->Dinv64, F->Sinv64, st));
+    auto body = [&]() -> jfg_status {
+      JFG_TRY(factor_levels<double>(m, F, F->L64, F->U64, F->Dinv64, st));
+      return strip_inverses<double>(F, F->L64, F->Dinv64, F->Sinv64, st);
+    };
+    // the first factorisation runs eagerly (one-time kernel attributes);
+    // later ones replay its graph
+    if (F->factor_calls[0]++ > 0 && graphs_enabled())
+      JFG_TRY(run_graph(F->factor_graph[0], F->factor_graph_nodes[0], st, body));
+    else
+      JFG_TRY(body());
   } else if (precision == JFG_PREC_MIXED) {
     if (!F->L32) {
       JFG_TRY(dev_alloc(c, (void**)&F->L32, sizeof(float) * S.nnz_L));
@@ -1468,8 +1531,14 @@ jfg_status numeric_factor(jfg_model* m, int precision) {
     F->have32 = false;
     if (!F->Dinv32) JFG_TRY(dev_alloc(c, (void**)&F->Dinv32, sizeof(float) * F->dinv_len));
     if (!F->Sinv32) JFG_TRY(dev_alloc(c, (void**)&F->Sinv32, sizeof(float) * F->sinv_len));
-    JFG_TRY(factor_levels<float>(m, F, F->L32, F->U32, F->Dinv32, st));
-    JFG_TRY(strip_inverses<float>(F, F->L32, F->Dinv32, F->Sinv32, st));
+    auto body = [&]() -> jfg_status {
+      JFG_TRY(factor_levels<float>(m, F, F->L32, F->U32, F->Dinv32, st));
+      return strip_inverses<float>(F, F->L32, F->Dinv32, F->Sinv32, st);
+    };
+    if (F->factor_calls[1]++ > 0 && graphs_enabled())
+      JFG_TRY(run_graph(F->factor_graph[1], F->factor_graph_nodes[1], st, body));
+    else
+      JFG_TRY(body());
   } else {
     set_error("unknown precision");
     return JFG_BAD_INPUT;
@@ -1539,8 +1608,13 @@ jfg_status numeric_solve(jfg_model* m, int nrhs, const double* hF, double* hU, d
     auto precond = [&](const double* rin, double* zout) -> jfg_status {
       const double* sc = use32 ? F->scale : nullptr;
       { k_gather_perm<<<gn, 256, 0, st>>>(n, nr, F->perm_dof, sc, rin, ndof, F->xp, 1.0); count_launch(); }
-      if (use32) solve_inner<float>(m, F, F->L32, F->Sinv32, nr, st);
-      else solve_inner<double>(m, F, F->L64, F->Sinv64, nr, st);
+      auto body = [&]() -> jfg_status {
+        if (use32) solve_inner<float>(m, F, F->L32, F->Sinv32, nr, st);
+        else solve_inner<double>(m, F, F->L64, F->Sinv64, nr, st);
+        return JFG_OK;
+      };
+      if (graphs_enabled()) JFG_TRY(run_graph(F->solve_graph[use32][nr], F->solve_graph_nodes[use32][nr], st, body));
+      else JFG_TRY(body());
       JFG_CUDA(cudaMemsetAsync(zout, 0, sizeof(double) * ndof * nr, st));
       { k_scatter_add_perm<<<gn, 256, 0, st>>>(n, nr, F->perm_dof, sc, F->xp, zout, ndof); count_launch(); }
       return JFG_OK;
