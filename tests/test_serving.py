@@ -94,3 +94,25 @@ def test_server_evicts_under_budget():
         srv.resolve(b["key"]).result(timeout=600)
     finally:
         srv.close()
+
+
+def test_autotune_picks_a_candidate_and_keeps_results(alone):
+    """The autotuner times candidate schedules (nested-dissection leaf size,
+    amalgamation thresholds, DMMA or SIMT updates) and every candidate gives
+    the same displacements; the tuned options are cached per size class."""
+    from jf_2026_05_25_b200 import autotune as AT
+    m = M.stiffened_panel(SEEDS[0])
+    cands = [{"JFG_ND_LEAF": "16", "JFG_RELAX_COLS": "16,48,128", "JFG_RELAX_ZEROS": "0.5,0.1,0.03", "JFG_DMMA": "1"},
+             {"JFG_ND_LEAF": "48", "JFG_RELAX_COLS": "32,96,256", "JFG_RELAX_ZEROS": "0.7,0.2,0.08", "JFG_DMMA": "0"}]
+    out = AT.tune(m, cands, repeats=1)
+    assert out["best"] in cands
+    assert AT.tuned_options(m) == out["best"]
+    for opt in cands:
+        AT.apply(opt)
+        try:
+            be = B.JFEMGPUBackend(tol=RESID_TOL)
+            res = B.solve_model(be, m)
+            U = np.stack([sc["raw_displacement"] for sc in res["subcases"]], axis=1)
+            assert _rel(U, alone[SEEDS[0]]) <= DISP_RTOL
+        finally:
+            AT.apply({})
