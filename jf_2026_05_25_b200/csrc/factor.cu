@@ -646,11 +646,16 @@ __global__ void k_vec_extend_add(const int32_t* __restrict__ child, const int32_
   int a = blockIdx.y * 256 + threadIdx.x;
   if (a >= rc) return;
   int ra = rl[a];
-  for (int k = 0; k < nr; ++k) {
-    double v = src[a + (int64_t)rc * k];
-    if (ra < cp) xp[first[p] + ra + n * k] += v;
-    else vp[(ra - cp) + (int64_t)rp * k] += v;
-  }
+  double* dst = (ra < cp) ? xp + first[p] + ra : vp + (ra - cp);
+  const int64_t ld = (ra < cp) ? n : (int64_t)rp;
+  double v[8], d[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) v[k] = k < nr ? src[a + (int64_t)rc * k] : 0.0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) d[k] = k < nr ? dst[ld * k] : 0.0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    if (k < nr) dst[ld * k] = d[k] + v[k];
 }
 
 // ---------------------------------------------------------------- strip solves
