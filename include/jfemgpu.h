@@ -44,9 +44,11 @@ typedef enum {
 
 typedef enum {
   JFG_PREC_FP64 = 0,        /* plain FP64 supernodal Cholesky                      */
-  JFG_PREC_MIXED = 1        /* FP32-storage factor (FP32 updates; 3xTF32 tensor-
-                               core updates with JFG_TENSOR_CORES=1), FP64
-                               iterative refinement on the FP64 CSR matrix      */
+  JFG_PREC_MIXED = 1        /* FP32-storage factor, FP64 iterative refinement on
+                               the FP64 CSR matrix; front updates on the tensor
+                               cores in 3xTF32 for solid-only models, SIMT FP32
+                               where shells are present (JFG_TENSOR_CORES=1/0
+                               forces either)                                   */
 } jfg_precision;
 
 typedef struct jfg_ctx jfg_ctx;

@@ -8,8 +8,10 @@ analysis (csrc/symbolic.cpp SymbolicOptions::from_env):
   thresholds, which set front widths and so the tile shapes the factor and
   strip-solve kernels see;
 
-and the FP64 update-kernel choice (``JFG_DMMA``: tensor-core DMMA tiles or
-SIMT tiles).  ``tune`` times symbolic analysis + numeric factor + solve of a
+the FP64 update-kernel choice (``JFG_DMMA``: tensor-core DMMA tiles or
+SIMT tiles) and, for the mixed factor, the FP32 update-kernel choice
+(``JFG_TENSOR_CORES``: tcgen05 3xTF32 tiles or SIMT FP32 tiles; the time
+includes the refinement iterations each choice needs).  ``tune`` times symbolic analysis + numeric factor + solve of a
 representative model for every candidate and returns the fastest; the
 choice is cached per size class (element kind, DOF bucket) so that a serving
 process tunes once per class.  The options are process-wide environment
@@ -28,7 +30,7 @@ import numpy as np
 from . import backend as B
 from . import lib
 
-KNOBS = ("JFG_ND_LEAF", "JFG_RELAX_COLS", "JFG_RELAX_ZEROS", "JFG_DMMA")
+KNOBS = ("JFG_ND_LEAF", "JFG_RELAX_COLS", "JFG_RELAX_ZEROS", "JFG_DMMA", "JFG_TENSOR_CORES")
 
 DEFAULT_CANDIDATES: List[Dict[str, str]] = [
     {"JFG_ND_LEAF": leaf, "JFG_RELAX_COLS": cols, "JFG_RELAX_ZEROS": zeros, "JFG_DMMA": dmma}
@@ -60,6 +62,8 @@ def tune(model, candidates: Optional[Sequence[Dict[str, str]]] = None, repeats: 
     """Time every candidate on `model`; returns dict(best, timings) and caches
     the best options for the model's size class."""
     cands = list(candidates or DEFAULT_CANDIDATES)
+    if candidates is None and precision == lib.PREC_MIXED:
+        cands = [dict(c, JFG_TENSOR_CORES=t) for c in cands for t in ("1", "0")]
     saved = {k: os.environ.get(k) for k in KNOBS}
     own_ctx = ctx is None
     ctx = ctx or lib.Context(0)

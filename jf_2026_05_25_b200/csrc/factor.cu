@@ -52,6 +52,7 @@ struct NumericFactor {
   double* L64 = nullptr;
   double* U64 = nullptr;
   float* L32 = nullptr;
+  float* L32lo = nullptr;     // v - trunc19(v) of every L32 entry (tensor-core updates only)
   float* U32 = nullptr;
   double* scale = nullptr;    // n, symmetric diagonal scaling of the mixed factor
   // inverse diagonal blocks of the strip solve
@@ -357,7 +358,7 @@ template <typename T>
 __global__ void __launch_bounds__(256)
 k_trsm_panel(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
              const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr, const int64_t* __restrict__ Dptr,
-             T* __restrict__ L, const T* __restrict__ Dinv, int k0) {
+             T* __restrict__ L, const T* __restrict__ Dinv, int k0, float* __restrict__ Llo) {
   int s = list[blockIdx.y];
   int c = first[s + 1] - first[s];
   if (k0 >= c) return;
@@ -395,6 +396,24 @@ k_trsm_panel(const int32_t* __restrict__ list, const int32_t* __restrict__ first
     for (int t = 0; t < 16; ++t) {
       int l = g * 16 + t;
       if (l < kn) P[row + (int64_t)m * (k0 + l)] = acc[t];
+    }
+    if constexpr (sizeof(T) == 4) {
+      // low parts for the 3xTF32 updates: the tensor core reads the upper
+      // 19 bits of v (truncation), so lo = v - trunc19(v), exact in FP32,
+      // stored rounded to nearest in 19 bits so that the tensor core's own
+      // truncation of lo adds no one-sided error
+      if (Llo) {
+        float* Q = Llo + Lptr[s];
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+          int l = g * 16 + t;
+          if (l < kn) {
+            const float v = acc[t];
+            const float lo = v - __uint_as_float(__float_as_uint(v) & 0xFFFFE000u);
+            Q[row + (int64_t)m * (k0 + l)] = __uint_as_float((__float_as_uint(lo) + 0x1000u) & 0xFFFFE000u);
+          }
+        }
+      }
     }
   }
 }
@@ -591,6 +610,12 @@ k_front_update_dmma(const int32_t* __restrict__ list, const int32_t* __restrict_
           else C[i + ldc * j] = -acc[a][b][h];
         }
       }
+}
+
+// smallest level output (rows) handed to the tensor-core update kernel
+inline int tc_min_dim() {
+  const char* e = std::getenv("JFG_TC_MIN");
+  return e ? std::max(1, std::atoi(e)) : 256;
 }
 
 inline bool dmma_enabled() {
@@ -1096,8 +1121,10 @@ void upload(std::vector<T>& h, T** d, jfg_ctx* c, jfg_status& st) {
   }
 }
 
+// Llo: low parts of the FP32 factor for the tensor-core updates (nullptr:
+// SIMT / DMMA updates only)
 template <typename T>
-jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, cudaStream_t st) {
+jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, float* Llo, cudaStream_t st) {
   static bool attr_set = false;
   if (!attr_set) {
     int bytes = 2 * NB * (NB + 1) * (int)sizeof(T);
@@ -1106,9 +1133,22 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, c
     attr_set = true;
   }
   const Symbolic& S = m->sym;
+  const int tc_min = tc_min_dim();
   for (const auto& lv : F->levels) {
     const int32_t* list = F->level_sn + lv.off;
     F->level_sn_cur = list;
+    // one front update of the level: the tensor-core 3xTF32 kernel for the
+    // FP32 factor when its low parts exist and the level's output is large
+    // enough for 128 x 128 tiles, else the SIMT / DMMA tiles
+    auto update = [&](int mode, int kbeg, int kend, int cend, int max_rows, int max_cols, int64_t tiles) {
+      if constexpr (sizeof(T) == 4) {
+        if (Llo && max_rows >= tc_min && max_cols >= tc_min / 2 &&
+            tc::front_update_tf32x3(list, lv.count, F->first, F->mrows, F->Lptr, F->Uptr, Lf, Llo, Uf, mode, kbeg,
+                                    kend, cend, max_rows, max_cols, F->err, st))
+          return;
+      }
+      launch_front_update<T>((unsigned)tiles, lv.count, F, Lf, Uf, mode, kbeg, kend, cend, st);
+    };
     // extend-add, pass 0: children columns that land in this level's panels
     for (const auto& seg : lv.ea) {
       if (seg.second == 0) continue;
@@ -1133,13 +1173,13 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, c
         if (rows_max <= 0) continue;
         unsigned gx = (unsigned)((rows_max + 63) / 64);
         { int ps_ = fine_prof() ? prof_start(st) : -1; { k_trsm_panel<T><<<dim3(gx, lv.count), 256, 2 * NB * (NB + 1) * sizeof(T), st>>>(list, F->first, F->mrows,
-                                                                                        F->Lptr, F->Dptr, Lf, Dvf, k0);
+                                                                                        F->Lptr, F->Dptr, Lf, Dvf, k0, Llo);
           count_launch(); } prof_end(ps_, st, KS_F_TRSM, 0.0); }
         int nrow = lv.max_m - k0 - NB, ncol = std::min(P1, lv.max_c) - k0 - NB;
         if (nrow > 0 && ncol > 0) {
           int64_t tiles = (int64_t)((nrow + TILE - 1) / TILE) * ((ncol + TILE - 1) / TILE);
           { int ps_ = fine_prof() ? prof_start(st) : -1;
-            launch_front_update<T>((unsigned)tiles, lv.count, F, Lf, Uf, 0, k0, k0 + NB, P1, st);
+            update(0, k0, k0 + NB, P1, nrow, ncol, tiles);
             prof_end(ps_, st, KS_F_PANEL, 0.0); }
         }
       }
@@ -1147,21 +1187,15 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, c
       if (nrow > 0 && ncol > 0) {
         int64_t tiles = (int64_t)((nrow + TILE - 1) / TILE) * ((ncol + TILE - 1) / TILE);
         { int ps_ = fine_prof() ? prof_start(st) : -1;
-          launch_front_update<T>((unsigned)tiles, lv.count, F, Lf, Uf, 0, P0, P1, INT_MAX, st);
+          update(0, P0, P1, INT_MAX, nrow, ncol, tiles);
           prof_end(ps_, st, KS_F_PANEL, 0.0); }
       }
     }
     if (lv.max_r > 0) {
       int64_t nt = (lv.max_r + TILE - 1) / TILE;
       int64_t tiles = nt * nt;
-      bool done = false;
       int ps = prof_start(st);
-      if constexpr (sizeof(T) == 4) {
-        done = tc::schur_update_tf32x3(list, lv.count, F->first, F->mrows, F->Lptr, F->Uptr, Lf, Uf,
-                                       lv.max_r, lv.max_c, F->err, st);
-      }
-      if (!done)
-        launch_front_update<T>((unsigned)tiles, lv.count, F, Lf, Uf, 1, 0, 0, 0, st);
+      update(1, 0, 0, 0, lv.max_r, lv.max_r, tiles);
       prof_end(ps, st, KS_SCHUR, lv.schur_flops);
     }
     // extend-add, pass 1: children columns that land in the U of this level
@@ -1463,7 +1497,7 @@ void numeric_destroy(jfg_model* m) {
   fr(F->rows_ptr, 8 * (S.ns + 1)); fr(F->relptr, 8 * (S.ns + 1)); fr(F->amap_dst, 8 * S.amap_dst.size());
   fr(F->amap_pr, 4 * S.amap_dst.size()); fr(F->amap_pc, 4 * S.amap_dst.size());
   fr(F->L64, 8 * S.nnz_L); fr(F->U64, 8 * std::max<int64_t>(S.u_arena, 1));
-  fr(F->L32, 4 * S.nnz_L); fr(F->U32, 4 * std::max<int64_t>(S.u_arena, 1));
+  fr(F->L32, 4 * S.nnz_L); fr(F->L32lo, 4 * S.nnz_L); fr(F->U32, 4 * std::max<int64_t>(S.u_arena, 1));
   fr(F->scale, 8 * S.n);
   int oc = F->nrhs_cap;
   if (oc > 0) {
@@ -1511,7 +1545,7 @@ jfg_status numeric_factor(jfg_model* m, int precision) {
     if (!F->Dinv64) JFG_TRY(dev_alloc(c, (void**)&F->Dinv64, sizeof(double) * F->dinv_len));
     if (!F->Sinv64) JFG_TRY(dev_alloc(c, (void**)&F->Sinv64, sizeof(double) * F->sinv_len));
     auto body = [&]() -> jfg_status {
-      JFG_TRY(factor_levels<double>(m, F, F->L64, F->U64, F->Dinv64, st));
+      JFG_TRY(factor_levels<double>(m, F, F->L64, F->U64, F->Dinv64, nullptr, st));
       return strip_inverses<double>(F, F->L64, F->Dinv64, F->Sinv64, st);
     };
     // the first factorisation runs eagerly (one-time kernel attributes);
@@ -1534,10 +1568,22 @@ jfg_status numeric_factor(jfg_model* m, int precision) {
       { k_scatter_A<float><<<ga, 256, 0, st>>>(F->n_amap, F->amap_src, F->amap_dst, F->amap_pr, F->amap_pc,
                                              m->d_nzval, F->scale, F->L32); count_launch(); }
     F->have32 = false;
+    // tensor-core updates by default for solid-only models; shell models
+    // (drilling DOFs, thin-shell conditioning) keep the FP32 SIMT updates:
+    // the 3xTF32 tensor-core sums carry one-sided errors of about 1e-6 per
+    // K-slice (truncating accumulation in tensor memory, missing lo*lo), which
+    // on the 914k-DOF wing panel raise refinement from 8 to 13 iterations
+    // while on the CTETRA10 block the iteration count is unchanged
+    const int tcs = tc::setting();
+    float* tc_lo = nullptr;
+    if (tcs == 1 || (tcs < 0 && m->n_q4 + m->n_q8 == 0)) {
+      if (!F->L32lo) JFG_TRY(dev_alloc(c, (void**)&F->L32lo, sizeof(float) * S.nnz_L));
+      tc_lo = F->L32lo;
+    }
     if (!F->Dinv32) JFG_TRY(dev_alloc(c, (void**)&F->Dinv32, sizeof(float) * F->dinv_len));
     if (!F->Sinv32) JFG_TRY(dev_alloc(c, (void**)&F->Sinv32, sizeof(float) * F->sinv_len));
     auto body = [&]() -> jfg_status {
-      JFG_TRY(factor_levels<float>(m, F, F->L32, F->U32, F->Dinv32, st));
+      JFG_TRY(factor_levels<float>(m, F, F->L32, F->U32, F->Dinv32, tc_lo, st));
       return strip_inverses<float>(F, F->L32, F->Dinv32, F->Sinv32, st);
     };
     if (F->factor_calls[1]++ > 0 && graphs_enabled())

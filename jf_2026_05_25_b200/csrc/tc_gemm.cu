@@ -1,26 +1,10 @@
-// tc_gemm.cu -- tensor-core Schur-complement update (3xTF32) for the mixed
-// factor: U = -L21 L21^T for every front of a level, lower-triangular
-// 128 x 128 tiles, on the sm_100a 5th-generation tensor cores.
-//
-// Per CTA (128 threads, one output tile):
-//   * all threads stream K-slices of 16 columns of L21 from global memory
-//     (column-major, coalesced along rows), split every value into
-//     hi = tf32(v) and lo = tf32(v - hi), and store hi/lo of both operands
-//     into shared memory in the no-swizzle K-major core-matrix layout
-//     (8 rows x 16 bytes per core matrix);
-//   * one thread issues tcgen05.mma kind::tf32 (M = N = 128, K = 8):
-//     lo*hi + hi*lo + hi*hi accumulate in FP32 in tensor memory, and
-//     tcgen05.commit arrives on the stage's mbarrier;
-//   * two shared-memory stages: the loads of slice k+1 overlap the MMAs of
-//     slice k; a stage is refilled only after its mbarrier has completed;
-//   * every few K-slices the accumulator is read with tcgen05.ld (warp w
-//     owns TMEM lanes 32w..32w+31 = tile rows) and added into an FP32
-//     register row per thread; the epilogue writes -acc into the
-//     column-major update matrix, lower triangle only.
-// Every mbarrier wait is bounded (about two seconds of clock); on expiry the
-// CTA records EE_TC_TIMEOUT in the device error record, waits (bounded) for
-// its own MMAs, frees its tensor memory and returns.  No TMA and no cluster
-// multicast are used.
+// tc_gemm.cu -- tensor-core (tcgen05, kind::tf32) front updates of the
+// mixed-precision supernodal factor: C -= A B^T on 128 x 128 tiles of the
+// panel columns of a front (mode 0) and U = -L21 L21^T (mode 1), in 3xTF32
+// split precision with FP32 accumulation.  Operands are streamed with
+// cp.async into a shared-memory ring; accumulators live in tensor memory and
+// are drained into FP32 registers every K-slice.  No TMA and no cluster
+// multicast are used; every wait is bounded.
 #include "tc_gemm.cuh"
 
 #include <cstdlib>
@@ -31,39 +15,10 @@ namespace jfg {
 namespace tc {
 namespace {
 
-constexpr int TM = 128;                        // tile rows (M) and columns (N)
-constexpr int TK = 16;                         // K columns per shared-memory stage
-constexpr int PART = TM * TK * 4;              // bytes of one operand part (hi or lo)
-constexpr int NSPLIT = 2;                      // tf32 terms per operand value (hi, lo)
-constexpr int STAGE = 2 * NSPLIT * PART;       // A_hi, A_lo, B_hi, B_lo
-constexpr int NSTAGE = 2;
-constexpr int SMEM_BYTES = NSTAGE * STAGE + 64;
-constexpr uint32_t TMEM_COLS = 128;
-// instruction descriptor: D f32, A/B tf32, both K-major, N = 128, M = 128
-constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TM >> 3) << 17) |
-                           ((uint32_t)(TM >> 4) << 24);
 constexpr long long WAIT_CYCLES = 4000000000LL;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-// shared-memory matrix descriptor, K-major without swizzle: core matrices of
-// 8 rows x 16 bytes; 128 bytes between 8-row groups (SBO) and 2048 bytes
-// between the two 16-byte K halves of one K = 8 instruction (LBO)
-__device__ __forceinline__ uint64_t mat_desc(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)((2048u >> 4) & 0x3FFFu) << 16;
-  d |= (uint64_t)((128u >> 4) & 0x3FFFu) << 32;
-  d |= (uint64_t)1 << 46;   // descriptor version for sm_100
-  return d;
-}
-
-__device__ __forceinline__ float tf32_round(float v) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
-  return __uint_as_float(r);
 }
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
@@ -89,15 +44,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity)
   return true;
 }
 
-__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
-      ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate)
-      : "memory");
-}
-
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                : "memory");
@@ -106,66 +52,147 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// byte offset of element (row i, column k) inside one operand part
-__device__ __forceinline__ uint32_t part_off(int i, int k) {
-  return (uint32_t)(((k >> 2) * (TM / 8) + (i >> 3)) * 128 + (i & 7) * 16 + (k & 3) * 4);
+// ---------------------------------------------------------------------------
+// Front updates of the mixed factor on the tensor cores, operands streamed
+// by asynchronous copies.  The trsm kernel stores next to every FP32 panel
+// value v its low part lo = rn19(v - trunc19(v)) (L32lo); the tensor core
+// reads v itself as the high part (kind::tf32 uses the upper 19 bits of an
+// FP32 word), so both operand terms are plain copies from global memory.
+//
+// One CTA per 128 x 128 output tile, warp-specialised:
+//   * warps 0-7 (drain): warp w reads TMEM lanes 32(w%4).. +32 (tile rows)
+//     and columns 64(w/4).. +64; every UDR K-slices of 16 columns are
+//     accumulated by the tensor core into one of two TMEM accumulators and
+//     added here into FP32 registers once complete, so the tensor core never
+//     sums more than 16 UDR columns of products; the epilogue writes
+//     C -= acc (mode 0, panel columns of the front) or C = -acc (mode 1,
+//     the update matrix U);
+//   * warps 8..8+UPW-1 (producers): 4-byte cp.async of hi and lo of both
+//     operands into a UST-stage ring in the no-swizzle K-major core-matrix
+//     layout, completion signalled per stage with
+//     cp.async.mbarrier.arrive.noinc on the stage's "full" barrier;
+//   * the last warp (one thread): waits for a full stage and a free
+//     accumulator, issues lo*hi + hi*lo + hi*hi (K = 8 per instruction) and
+//     commits to the stage's "empty" barrier and the accumulator's "full"
+//     barrier.
+// Every wait is bounded (about two seconds of clock) and also gives up as
+// soon as another warp has given up; the CTA then records EE_TC_TIMEOUT,
+// waits (bounded) for its own copies and MMAs and frees its tensor memory.
+constexpr int UM = 128;
+constexpr int UK = 16;
+#ifndef JFG_TC_STAGES
+#define JFG_TC_STAGES 4
+#endif
+#ifndef JFG_TC_DRAIN
+#define JFG_TC_DRAIN 1
+#endif
+constexpr int UST = JFG_TC_STAGES;
+constexpr int UDR = JFG_TC_DRAIN;               // K-slices per accumulator use
+constexpr int UDW = 8;                          // drain warps: 4 lane quarters x 2 column halves
+constexpr int UPW = 4;                          // producer warps
+constexpr int UTHREADS = (UDW + UPW + 1) * 32;
+constexpr uint32_t UTMEM = 2 * UM;              // two FP32 accumulators of 128 columns
+// K-major without swizzle: core matrix = 8 rows x 4 columns (16 bytes);
+// 4-column groups 2048 bytes apart (LBO), 8-row groups 128 bytes (SBO)
+constexpr int UPART = UM * UK * 4;
+constexpr uint32_t U_LBO = 2048, U_SBO = 128, U_KSTEP = 4096;
+constexpr int USTAGE = 4 * UPART;               // A hi, A lo, B hi, B lo
+constexpr int UBAR = UST * USTAGE;
+constexpr int USMEM = UBAR + 8 * (2 * UST + 5) + 16;
+constexpr uint32_t UIDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(UM >> 3) << 17) |
+                            ((uint32_t)(UM >> 4) << 24);
+
+__device__ __forceinline__ uint64_t u_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((U_LBO >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((U_SBO >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
 }
 
-// loads columns [k, k + TK) of rows [row, row + 128) of the column-major panel
-// (rows past nrows or columns past kend read as zero), splits every value
-// into hi = tf32(v) and lo = tf32(v - hi) and stores hi into the first part,
-// lo into the second
-__device__ __forceinline__ void load_split(const float* __restrict__ P, int64_t ld, int64_t row, int nrows,
-                                           int k, int kend, unsigned char* parts) {
-  const int t = threadIdx.x;   // one row per thread
-  const bool rok = t < nrows;
-#pragma unroll
-  for (int q = 0; q < TK / 4; ++q) {
-    float v[4], h[4], l[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      int kk = k + 4 * q + e;
-      v[e] = (rok && kk < kend) ? P[row + t + ld * kk] : 0.0f;
-      h[e] = tf32_round(v[e]);
-      l[e] = tf32_round(v[e] - h[e]);
-    }
-    const uint32_t off = part_off(t, 4 * q);
-    *reinterpret_cast<float4*>(parts + off) = make_float4(h[0], h[1], h[2], h[3]);
-    *reinterpret_cast<float4*>(parts + PART + off) = make_float4(l[0], l[1], l[2], l[3]);
+__device__ __forceinline__ void u_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
+      ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(UIDESC), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void cp4(uint32_t dst, const float* src, uint32_t bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// bounded wait that also gives up once another warp has set *abort
+__device__ __forceinline__ bool u_wait(uint32_t bar, uint32_t parity, volatile int* abort) {
+  const long long t0 = clock64();
+  while (!mbar_try(bar, parity)) {
+    if (*abort) return false;
+    if (clock64() - t0 > WAIT_CYCLES) { *abort = 1; return false; }
   }
+  return true;
 }
 
-__global__ void __launch_bounds__(128)
-k_schur_tf32x3(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
-               const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
-               const int64_t* __restrict__ Uptr, const float* __restrict__ L, float* __restrict__ U,
-               int drain, DevError* err) {
+__global__ void __launch_bounds__(UTHREADS, 1)
+k_update_tf32x3(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
+                const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
+                const int64_t* __restrict__ Uptr, float* __restrict__ L, const float* __restrict__ Llo,
+                float* __restrict__ U, int mode, int kbeg, int kend, int cend, int terms, DevError* err) {
   const int s = list[blockIdx.y];
   const int c = first[s + 1] - first[s];
   const int m = mrows[s];
-  const int r = m - c;
-  if (r <= 0 || Uptr[s] < 0) return;
-  const int nt = (r + TM - 1) / TM;
-  // lower-triangular tile (ti, tj), tj <= ti, from the linear index
-  int t = blockIdx.x;
-  if (t >= nt * (nt + 1) / 2) return;
-  int ti = (int)((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
-  while (ti * (ti + 1) / 2 > t) --ti;
-  while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
-  const int tj = t - ti * (ti + 1) / 2;
-
+  int row0, col0, nrow, ncol, kb, ke;
+  float* C;
+  int64_t ldc;
+  if (mode == 0) {
+    int k1 = min(kend, c);
+    int ce = min(cend, c);
+    if (kbeg >= c || k1 >= ce) return;
+    row0 = k1; col0 = k1; nrow = m - k1; ncol = ce - k1; kb = kbeg; ke = k1;
+    C = L + Lptr[s] + row0 + (int64_t)m * col0;
+    ldc = m;
+  } else {
+    int r = m - c;
+    if (r <= 0 || Uptr[s] < 0) return;
+    row0 = c; col0 = c; nrow = r; ncol = r; kb = 0; ke = c;
+    C = U + Uptr[s];
+    ldc = r;
+  }
+  const int ntj = (ncol + UM - 1) / UM, nti = (nrow + UM - 1) / UM;
+  const int t = blockIdx.x;
+  if (t >= nti * ntj) return;
+  const int ti = t / ntj, tj = t % ntj;
+  if (ti * UM + UM - 1 + row0 < tj * UM + col0) return;   // strictly upper tile
   extern __shared__ __align__(1024) unsigned char smem[];
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + NSTAGE * STAGE);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + NSTAGE * STAGE + 32);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-
-  if (threadIdx.x == 0) {
-    for (int q = 0; q < NSTAGE; ++q) mbar_init(smem_addr(&bars[q]), 1);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + UBAR);
+  uint64_t* empty = full + UST;
+  uint64_t* accfull = empty + UST;
+  uint64_t* accempty = accfull + 2;
+  uint64_t* spare = accempty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(spare + 1);
+  volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    for (int q = 0; q < UST; ++q) {
+      mbar_init(smem_addr(&full[q]), UPW * 32);
+      mbar_init(smem_addr(&empty[q]), 1);
+    }
+    mbar_init(smem_addr(spare), 1);
+    for (int q = 0; q < 2; ++q) {
+      mbar_init(smem_addr(&accfull[q]), 1);
+      mbar_init(smem_addr(&accempty[q]), UDW * 32);
+    }
+    *abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
-                 "r"(TMEM_COLS)
+                 "r"(UTMEM)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -173,124 +200,170 @@ k_schur_tf32x3(const int32_t* __restrict__ list, const int32_t* __restrict__ fir
   __syncthreads();
   fence_after();
   const uint32_t tmem = *tmem_slot;
+  const int nk = (ke - kb + UK - 1) / UK;
+  const uint32_t sbase = smem_addr(smem);
 
-  const float* P = L + Lptr[s];
-  const int64_t arow = (int64_t)c + (int64_t)ti * TM, brow = (int64_t)c + (int64_t)tj * TM;
-  const int anr = min(TM, r - ti * TM), bnr = min(TM, r - tj * TM);
-  const int nk = (c + TK - 1) / TK;
-  bool ok = true;
-  int issued = 0;   // K-slices whose MMAs were committed
-  // FP32 accumulator of this thread's tile row: tensor memory is drained into
-  // it every `drain` K-slices, so no tensor-memory sum runs over more than
-  // drain * 16 products (the tensor-core accumulation is not round-to-nearest)
-  float acc[TM];
+  if (warp >= UDW && warp < UDW + UPW) {
+    // ---------------------------------------------------------- producers
+    const int pw = warp - UDW;
+    const int64_t arow0 = row0 + (int64_t)ti * UM, brow0 = col0 + (int64_t)tj * UM;
+    const float* P = L + Lptr[s];
+    const int64_t dlo = (Llo + Lptr[s]) - P;
+    // rows past the tile's valid rows re-read the tile's first row: such
+    // rows only reach output rows / columns that are not stored
+    int64_t ra[4], rb[4];
+    // warp pw: row groups pw + 4 rg, columns lane / 8 + 4 g (one 8 x 4 block,
+    // four full 32-byte sectors, per instruction)
 #pragma unroll
-  for (int j = 0; j < TM; ++j) acc[j] = 0.0f;
-  int fresh = 1;    // the next MMA starts a new tensor-memory sum
-  for (int kt = 0; kt < nk; ++kt) {
-    const int stg = kt & 1;
-    unsigned char* base = smem + stg * STAGE;
-    if (kt >= NSTAGE) {
-      // the MMAs that read this stage (slice kt - 2) must have completed
-      if (!mbar_wait_bounded(smem_addr(&bars[stg]), (uint32_t)(((kt - NSTAGE) / NSTAGE) & 1))) ok = false;
+    for (int rg = 0; rg < 4; ++rg) {
+      const int i = (pw + 4 * rg) * 8 + (lane & 7);
+      ra[rg] = arow0 + (ti * UM + i < nrow ? i : 0);
+      rb[rg] = brow0 + (tj * UM + i < ncol ? i : 0);
     }
-    if (__syncthreads_or(!ok)) { ok = false; break; }
-    load_split(P, m, arow, anr, kt * TK, c, base);
-    load_split(P, m, brow, bnr, kt * TK, c, base + NSPLIT * PART);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      fence_after();
-      const uint32_t a0 = smem_addr(base), b0 = a0 + NSPLIT * PART;
+    const uint32_t soff = (uint32_t)(pw * 128 + (lane & 7) * 16 + (lane >> 3) * 4);
+    for (int j = 0; j < nk; ++j) {
+      const int st = j % UST, n = j / UST;
+      if (n >= 1 && !u_wait(smem_addr(&empty[st]), (uint32_t)((n - 1) & 1), abort)) break;
+      const uint32_t base = sbase + (uint32_t)(st * USTAGE) + soff;
 #pragma unroll
-      for (int q = 0; q < TK / 8; ++q) {
-        const uint32_t o = (uint32_t)q * 2 * (TM / 8) * 128;
-        // lo*hi + hi*lo + hi*hi (3xTF32), small terms first
-        mma_tf32(tmem, mat_desc(a0 + PART + o), mat_desc(b0 + o), (fresh && q == 0) ? 0u : 1u);
-        mma_tf32(tmem, mat_desc(a0 + o), mat_desc(b0 + PART + o), 1u);
-        mma_tf32(tmem, mat_desc(a0 + o), mat_desc(b0 + o), 1u);
+      for (int g = 0; g < 4; ++g) {
+        const int k = kb + j * UK + (lane >> 3) + 4 * g;
+        const uint32_t sg = base + (uint32_t)(g * 2048);
+        const bool kv = k < ke;
+        const float* col = P + (int64_t)m * (kv ? k : kb);   // columns past ke: zero-filled
+        const uint32_t nb = kv ? 4u : 0u;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const uint32_t o = sg + (uint32_t)(r * 512);
+          cp4(o, col + ra[r], nb);
+          cp4(o + UPART, col + dlo + ra[r], nb);
+          cp4(o + 2 * UPART, col + rb[r], nb);
+          cp4(o + 3 * UPART, col + dlo + rb[r], nb);
+        }
       }
-      mma_commit(smem_addr(&bars[stg]));
+      asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_addr(&full[st])) : "memory");
     }
-    issued = kt + 1;
-    fresh = 0;
-    if ((kt + 1) % drain == 0 || kt == nk - 1) {
-      if (!mbar_wait_bounded(smem_addr(&bars[stg]), (uint32_t)((kt / NSTAGE) & 1))) ok = false;
-      if (__syncthreads_or(!ok)) { ok = false; break; }
-      fence_after();
-      const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+    asm volatile("cp.async.wait_all;" ::: "memory");
+  } else if (warp == UDW + UPW) {
+    // ---------------------------------------------------------- MMA issue
+    if (lane == 0) {
+      int issued = 0;
+      for (int j = 0; j < nk; ++j) {
+        const int st = j % UST, n = j / UST, use = j / UDR, slot = use & 1, q = use >> 1;
+        const bool first_of_use = (j % UDR) == 0, last_of_use = (j % UDR) == UDR - 1 || j == nk - 1;
+        if (!u_wait(smem_addr(&full[st]), (uint32_t)(n & 1), abort)) break;
+        if (first_of_use && q >= 1 && !u_wait(smem_addr(&accempty[slot]), (uint32_t)((q - 1) & 1), abort)) break;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        fence_after();
+        const uint32_t a_hi = sbase + (uint32_t)(st * USTAGE), a_lo = a_hi + UPART;
+        const uint32_t b_hi = a_hi + 2 * UPART, b_lo = a_hi + 3 * UPART;
+        const uint32_t d = tmem + (uint32_t)(slot * UM);
 #pragma unroll
-      for (int j0 = 0; j0 < TM; j0 += 16) {
-        uint32_t v[16];
+        for (int kq = 0; kq < UK / 8; ++kq) {
+          const uint32_t o = (uint32_t)kq * U_KSTEP;
+          u_mma(d, u_desc(a_lo + o), u_desc(b_hi + o), (first_of_use && kq == 0) ? 0u : 1u);
+          u_mma(d, u_desc(a_hi + o), u_desc(b_lo + o), 1u);
+          u_mma(d, u_desc(a_hi + o), u_desc(b_hi + o), 1u);
+          if (terms > 3) u_mma(d, u_desc(a_lo + o), u_desc(b_lo + o), 1u);
+        }
+        mma_commit(smem_addr(&empty[st]));
+        if (last_of_use) mma_commit(smem_addr(&accfull[slot]));
+        issued = j + 1;
+      }
+      if (issued < nk && issued > 0) {
+        // gave up: let the MMAs already issued finish before TMEM is freed
+        mma_commit(smem_addr(spare));
+        const long long t0 = clock64();
+        while (!mbar_try(smem_addr(spare), 0u) && clock64() - t0 < WAIT_CYCLES) {
+        }
+      }
+    }
+    __syncwarp();
+  } else {
+    // ---------------------------------------------------------- drain + epilogue
+    constexpr int HC = UM / 2;
+    float acc[HC];
+#pragma unroll
+    for (int jj = 0; jj < HC; ++jj) acc[jj] = 0.0f;
+    const uint32_t tlane = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)((warp >> 2) * HC);
+    const int nuse = (nk + UDR - 1) / UDR;
+    int drained = 0;
+    for (int u = 0; u < nuse; ++u) {
+      const int slot = u & 1, q = u >> 1;
+      bool ok = lane == 0 ? u_wait(smem_addr(&accfull[slot]), (uint32_t)(q & 1), abort) : true;
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) break;
+      fence_after();
+      const uint32_t tb = tlane + (uint32_t)(slot * UM);
+#pragma unroll
+      for (int j0 = 0; j0 < HC; j0 += 32) {
+        uint32_t v[32];
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
               "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-            : "r"(lane_base + (uint32_t)j0));
+            : "r"(tb + (uint32_t)j0));
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+              "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+            : "r"(tb + (uint32_t)(j0 + 16)));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int e = 0; e < 16; ++e) acc[j0 + e] += __uint_as_float(v[e]);
+        for (int e = 0; e < 32; ++e) acc[j0 + e] += __uint_as_float(v[e]);
       }
       fence_before();
-      fresh = 1;
+      mbar_arrive(smem_addr(&accempty[slot]));
+      drained = u + 1;
     }
-  }
-  // the last slice was drained inside the loop; after a timeout, wait
-  // (bounded) for whatever MMAs were committed before freeing tensor memory
-  if (!ok && issued > 0) {
-    const int last = issued - 1;
-    mbar_wait_bounded(smem_addr(&bars[last & 1]), (uint32_t)((last / NSTAGE) & 1));
-  }
-  if (!ok && threadIdx.x == 0 && atomicCAS(&err->code, 0, (int32_t)EE_TC_TIMEOUT) == 0) err->index = s;
-  if (ok && issued == nk) {
-    float* Ud = U + Uptr[s];
-    const int li = warp * 32 + lane;              // row inside the tile
-    const int64_t gi = (int64_t)ti * TM + li;     // row inside U
+    if (drained == nuse && nk > 0) {
+      const int64_t gi = (int64_t)ti * UM + (warp & 3) * 32 + lane;
+      if (gi < nrow) {
 #pragma unroll
-    for (int j = 0; j < TM; ++j) {
-      const int64_t gj = (int64_t)tj * TM + j;
-      if (li < anr && j < bnr && gi >= gj) Ud[gi + (int64_t)r * gj] = -acc[j];
+        for (int jj = 0; jj < HC; ++jj) {
+          const int64_t gj = (int64_t)tj * UM + (warp >> 2) * HC + jj;
+          if (gj < ncol && row0 + gi >= col0 + gj) {
+            float* dst = C + gi + ldc * gj;
+            if (mode == 0) *dst -= acc[jj];
+            else *dst = -acc[jj];
+          }
+        }
+      }
     }
   }
   fence_before();
   __syncthreads();
+  if (tid == 0 && *abort && atomicCAS(&err->code, 0, (int32_t)EE_TC_TIMEOUT) == 0) err->index = s;
   if (warp == 0) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(UTMEM) : "memory");
   }
 }
 
 }  // namespace
 
-// Off unless JFG_TENSOR_CORES=1.  Measured on the 914k-DOF wing panel: the
-// tensor-core update takes about as long as the SIMT FP32 kernel (its loads
-// are the bottleneck, not the MMAs) and its FP32 accumulation in tensor
-// memory is less accurate (a mixed-factor diagonal about 4x further from the
-// FP64 one, even with a three-term split), so refinement needs more
-// iterations (13 instead of 8).
-bool enabled() {
+int setting() {
   const char* e = std::getenv("JFG_TENSOR_CORES");
-  return e && e[0] == '1';
+  if (!e || !e[0]) return -1;
+  return e[0] == '0' ? 0 : 1;
 }
 
-bool schur_update_tf32x3(const int32_t* list, int count, const int32_t* first, const int32_t* mrows,
-                         const int64_t* Lptr, const int64_t* Uptr, float* L, float* U, int max_r, int max_c,
-                         DevError* err, cudaStream_t st) {
-  (void)max_c;
-  if (!enabled() || count <= 0 || max_r <= 0) return false;
+bool enabled() { return setting() != 0; }
+
+bool front_update_tf32x3(const int32_t* list, int count, const int32_t* first, const int32_t* mrows,
+                         const int64_t* Lptr, const int64_t* Uptr, float* L, const float* Llo, float* U, int mode,
+                         int kbeg, int kend, int cend, int max_rows, int max_cols, DevError* err, cudaStream_t st) {
+  if (!enabled() || !Llo || count <= 0 || max_rows <= 0 || max_cols <= 0) return false;
   static bool attr = false;
   if (!attr) {
-    if (cudaFuncSetAttribute(k_schur_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES) !=
-        cudaSuccess)
+    if (cudaFuncSetAttribute(k_update_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, USMEM) != cudaSuccess)
       return false;
     attr = true;
   }
-  const int nt = (max_r + TM - 1) / TM;
-  const unsigned tiles = (unsigned)(nt * (nt + 1) / 2);
-  const char* d = std::getenv("JFG_TC_DRAIN");
-  int drain = d ? std::atoi(d) : 1;
-  if (drain < 1) drain = 1 << 30;
-  k_schur_tf32x3<<<dim3(tiles, (unsigned)count), 128, SMEM_BYTES, st>>>(list, first, mrows, Lptr, Uptr, L, U, drain,
-                                                                      err);
+  const char* te = std::getenv("JFG_TC_TERMS");   // 4: add lo*lo
+  const int terms = (te && te[0] == '4') ? 4 : 3;
+  const int64_t tiles = (int64_t)((max_rows + UM - 1) / UM) * ((max_cols + UM - 1) / UM);
+  k_update_tf32x3<<<dim3((unsigned)tiles, (unsigned)count), UTHREADS, USMEM, st>>>(list, first, mrows, Lptr, Uptr, L, Llo,
+                                                                             U, mode, kbeg, kend, cend, terms, err);
   count_launch();
   return cudaGetLastError() == cudaSuccess;
 }
