@@ -487,16 +487,34 @@ k_front_update(const int32_t* __restrict__ list, const int32_t* __restrict__ fir
     }
     __syncthreads();
   }
+  // epilogue; for mode 0 every load of C is issued before the first store.
+  // Mode 1 writes U = -L21 L21^T; the children are added after.
+  auto inside = [&](int i, int j) { return i < nrow && j < ncol && row0 + i >= col0 + j; };
+  if (mode == 0) {
+    T cv[4][4];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      int i = ti * TILE + ty + 16 * a, j = tj * TILE + tx + 16 * b;
-      if (i < nrow && j < ncol && row0 + i >= col0 + j) {
-        if (mode == 0) C[i + ldc * j] -= acc[a][b];
-        else C[i + ldc * j] = -acc[a][b];      // U = -L21 L21^T; children are added after
+      for (int b = 0; b < 4; ++b) {
+        int i = ti * TILE + ty + 16 * a, j = tj * TILE + tx + 16 * b;
+        cv[a][b] = inside(i, j) ? C[i + ldc * j] : (T)0;
       }
-    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        int i = ti * TILE + ty + 16 * a, j = tj * TILE + tx + 16 * b;
+        if (inside(i, j)) C[i + ldc * j] = cv[a][b] - acc[a][b];
+      }
+  } else {
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        int i = ti * TILE + ty + 16 * a, j = tj * TILE + tx + 16 * b;
+        if (inside(i, j)) C[i + ldc * j] = -acc[a][b];
+      }
+  }
 }
 
 // FP64 tensor-core (DMMA, mma.sync m8n8k4 f64) version of k_front_update for
@@ -598,18 +616,39 @@ k_front_update_dmma(const int32_t* __restrict__ list, const int32_t* __restrict_
     __syncthreads();
     buf ^= 1;
   }
+  // epilogue; for mode 0 every load of C is issued before the first store
+  auto inside = [&](int i, int j) { return i < nrow && j < ncol && row0 + i >= col0 + j; };
+  if (mode == 0) {
+    double cv[4][4][2];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b)
+      for (int b = 0; b < 4; ++b)
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        int i = ti * TILE + wr * 32 + a * 8 + g, j = tj * TILE + wc * 32 + b * 8 + 2 * q + h;
-        if (i < nrow && j < ncol && row0 + i >= col0 + j) {
-          if (mode == 0) C[i + ldc * j] -= acc[a][b][h];
-          else C[i + ldc * j] = -acc[a][b][h];
+        for (int h = 0; h < 2; ++h) {
+          int i = ti * TILE + wr * 32 + a * 8 + g, j = tj * TILE + wc * 32 + b * 8 + 2 * q + h;
+          cv[a][b][h] = inside(i, j) ? C[i + ldc * j] : 0.0;
         }
-      }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          int i = ti * TILE + wr * 32 + a * 8 + g, j = tj * TILE + wc * 32 + b * 8 + 2 * q + h;
+          if (inside(i, j)) C[i + ldc * j] = cv[a][b][h] - acc[a][b][h];
+        }
+  } else {
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          int i = ti * TILE + wr * 32 + a * 8 + g, j = tj * TILE + wc * 32 + b * 8 + 2 * q + h;
+          if (inside(i, j)) C[i + ldc * j] = -acc[a][b][h];
+        }
+  }
 }
 
 // smallest level output (rows) handed to the tensor-core update kernel

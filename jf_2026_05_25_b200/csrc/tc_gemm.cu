@@ -37,12 +37,6 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
-  long long t0 = clock64();
-  while (!mbar_try(bar, parity))
-    if (clock64() - t0 > WAIT_CYCLES) return false;
-  return true;
-}
 
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
@@ -317,15 +311,27 @@ k_update_tf32x3(const int32_t* __restrict__ list, const int32_t* __restrict__ fi
       drained = u + 1;
     }
     if (drained == nuse && nk > 0) {
+      // this thread's row of the tile, columns j0g .. j0g + HC - 1; stored
+      // are the columns below ncol on or below the front's diagonal.  All
+      // loads of a 16-column group are issued before its stores.
       const int64_t gi = (int64_t)ti * UM + (warp & 3) * 32 + lane;
-      if (gi < nrow) {
+      const int64_t j0g = (int64_t)tj * UM + (warp >> 2) * HC;
+      const int64_t jlast = min((int64_t)ncol - 1, row0 + gi - col0) - j0g;
+      if (gi < nrow && jlast >= 0) {
+        float* crow = C + gi + ldc * j0g;
 #pragma unroll
-        for (int jj = 0; jj < HC; ++jj) {
-          const int64_t gj = (int64_t)tj * UM + (warp >> 2) * HC + jj;
-          if (gj < ncol && row0 + gi >= col0 + gj) {
-            float* dst = C + gi + ldc * gj;
-            if (mode == 0) *dst -= acc[jj];
-            else *dst = -acc[jj];
+        for (int h = 0; h < HC; h += 16) {
+          if (mode == 0) {
+            float cv[16];
+#pragma unroll
+            for (int e = 0; e < 16; ++e) cv[e] = (h + e <= jlast) ? crow[ldc * (h + e)] : 0.0f;
+#pragma unroll
+            for (int e = 0; e < 16; ++e)
+              if (h + e <= jlast) crow[ldc * (h + e)] = cv[e] - acc[h + e];
+          } else {
+#pragma unroll
+            for (int e = 0; e < 16; ++e)
+              if (h + e <= jlast) crow[ldc * (h + e)] = -acc[h + e];
           }
         }
       }
