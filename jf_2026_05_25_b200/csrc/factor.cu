@@ -52,7 +52,13 @@ struct NumericFactor {
   double* L64 = nullptr;
   double* U64 = nullptr;
   float* L32 = nullptr;
-  float* L32lo = nullptr;     // v - trunc19(v) of every L32 entry (tensor-core updates only)
+  // tensor-core operand copies of L32 (mixed factor with tcgen05 updates):
+  // hi = rn19(v), lo = rn19(v - hi), packed per front (offset PKptr[s]) in
+  // 512-byte 64-byte-swizzled atoms of 8 rows x 16 columns, slice-block
+  // major; padding zeroed once at allocation.  tc_zero: 8 KB of zeros.
+  float *Phi = nullptr, *Plo = nullptr, *tc_zero = nullptr;
+  int64_t* PKptr = nullptr;
+  int64_t pk_len = 0;
   float* U32 = nullptr;
   double* scale = nullptr;    // n, symmetric diagonal scaling of the mixed factor
   // inverse diagonal blocks of the strip solve
@@ -358,7 +364,8 @@ template <typename T>
 __global__ void __launch_bounds__(256)
 k_trsm_panel(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
              const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr, const int64_t* __restrict__ Dptr,
-             T* __restrict__ L, const T* __restrict__ Dinv, int k0, float* __restrict__ Llo) {
+             T* __restrict__ L, const T* __restrict__ Dinv, int k0, float* __restrict__ Phi,
+             float* __restrict__ Plo, const int64_t* __restrict__ PKptr) {
   int s = list[blockIdx.y];
   int c = first[s + 1] - first[s];
   if (k0 >= c) return;
@@ -398,19 +405,32 @@ k_trsm_panel(const int32_t* __restrict__ list, const int32_t* __restrict__ first
       if (l < kn) P[row + (int64_t)m * (k0 + l)] = acc[t];
     }
     if constexpr (sizeof(T) == 4) {
-      // low parts for the 3xTF32 updates: the tensor core reads the upper
-      // 19 bits of v (truncation), so lo = v - trunc19(v), exact in FP32,
-      // stored rounded to nearest in 19 bits so that the tensor core's own
-      // truncation of lo adds no one-sided error
-      if (Llo) {
-        float* Q = Llo + Lptr[s];
+      // packed tensor-core operands: hi = rn19(v), lo = rn19(v - hi), in the
+      // 64-byte-swizzled atoms of 8 rows x 16 columns (this thread's 16
+      // columns are one slice block; its row is 64 contiguous bytes)
+      if (Phi) {
+        const int64_t nrg = (m + 7) / 8;
+        const int ri = row & 7, sw = (ri >> 1) & 3;
+        const int64_t base = PKptr[s] + ((int64_t)((k0 + 16 * g) >> 4) * nrg + (row >> 3)) * 128 + ri * 16;
 #pragma unroll
-        for (int t = 0; t < 16; ++t) {
-          int l = g * 16 + t;
-          if (l < kn) {
-            const float v = acc[t];
-            const float lo = v - __uint_as_float(__float_as_uint(v) & 0xFFFFE000u);
-            Q[row + (int64_t)m * (k0 + l)] = __uint_as_float((__float_as_uint(lo) + 0x1000u) & 0xFFFFE000u);
+        for (int q = 0; q < 4; ++q) {
+          float h[4], l[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const float v = acc[4 * q + e];
+            h[e] = __uint_as_float((__float_as_uint(v) + 0x1000u) & 0xFFFFE000u);
+            const float rem = v - h[e];
+            l[e] = __uint_as_float((__float_as_uint(rem) + 0x1000u) & 0xFFFFE000u);
+          }
+          const int l0 = g * 16 + 4 * q;                   // first panel column of the chunk
+          const int64_t off = base + (int64_t)((q ^ sw) * 4);
+          if (l0 + 3 < kn) {
+            *reinterpret_cast<float4*>(Phi + off) = make_float4(h[0], h[1], h[2], h[3]);
+            *reinterpret_cast<float4*>(Plo + off) = make_float4(l[0], l[1], l[2], l[3]);
+          } else {
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+              if (l0 + e < kn) { Phi[off + e] = h[e]; Plo[off + e] = l[e]; }
           }
         }
       }
@@ -1160,10 +1180,11 @@ void upload(std::vector<T>& h, T** d, jfg_ctx* c, jfg_status& st) {
   }
 }
 
-// Llo: low parts of the FP32 factor for the tensor-core updates (nullptr:
-// SIMT / DMMA updates only)
+// tc: the FP32 factor's updates go to the tensor-core kernel (where the
+// level's output is large enough); the trsm then also writes the packed
+// operand copies F->Phi / F->Plo
 template <typename T>
-jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, float* Llo, cudaStream_t st) {
+jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, bool tc, cudaStream_t st) {
   static bool attr_set = false;
   if (!attr_set) {
     int bytes = 2 * NB * (NB + 1) * (int)sizeof(T);
@@ -1181,9 +1202,9 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, f
     // enough for 128 x 128 tiles, else the SIMT / DMMA tiles
     auto update = [&](int mode, int kbeg, int kend, int cend, int max_rows, int max_cols, int64_t tiles) {
       if constexpr (sizeof(T) == 4) {
-        if (Llo && max_rows >= tc_min && max_cols >= tc_min / 2 &&
-            tc::front_update_tf32x3(list, lv.count, F->first, F->mrows, F->Lptr, F->Uptr, Lf, Llo, Uf, mode, kbeg,
-                                    kend, cend, max_rows, max_cols, F->err, st))
+        if (tc && max_rows >= tc_min && max_cols >= tc_min / 2 &&
+            tc::front_update_tf32x3(list, lv.count, F->first, F->mrows, F->Lptr, F->Uptr, Lf, F->Phi, F->Plo,
+                                    F->PKptr, F->tc_zero, Uf, mode, kbeg, kend, cend, max_rows, max_cols, F->err, st))
           return;
       }
       launch_front_update<T>((unsigned)tiles, lv.count, F, Lf, Uf, mode, kbeg, kend, cend, st);
@@ -1212,7 +1233,8 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, f
         if (rows_max <= 0) continue;
         unsigned gx = (unsigned)((rows_max + 63) / 64);
         { int ps_ = fine_prof() ? prof_start(st) : -1; { k_trsm_panel<T><<<dim3(gx, lv.count), 256, 2 * NB * (NB + 1) * sizeof(T), st>>>(list, F->first, F->mrows,
-                                                                                        F->Lptr, F->Dptr, Lf, Dvf, k0, Llo);
+                                                                                        F->Lptr, F->Dptr, Lf, Dvf, k0,
+                                                                                        tc ? F->Phi : nullptr, F->Plo, F->PKptr);
           count_launch(); } prof_end(ps_, st, KS_F_TRSM, 0.0); }
         int nrow = lv.max_m - k0 - NB, ncol = std::min(P1, lv.max_c) - k0 - NB;
         if (nrow > 0 && ncol > 0) {
@@ -1536,7 +1558,8 @@ void numeric_destroy(jfg_model* m) {
   fr(F->rows_ptr, 8 * (S.ns + 1)); fr(F->relptr, 8 * (S.ns + 1)); fr(F->amap_dst, 8 * S.amap_dst.size());
   fr(F->amap_pr, 4 * S.amap_dst.size()); fr(F->amap_pc, 4 * S.amap_dst.size());
   fr(F->L64, 8 * S.nnz_L); fr(F->U64, 8 * std::max<int64_t>(S.u_arena, 1));
-  fr(F->L32, 4 * S.nnz_L); fr(F->L32lo, 4 * S.nnz_L); fr(F->U32, 4 * std::max<int64_t>(S.u_arena, 1));
+  fr(F->L32, 4 * S.nnz_L); fr(F->Phi, 4 * F->pk_len); fr(F->Plo, 4 * F->pk_len);
+  fr(F->PKptr, 8 * (S.ns + 1)); fr(F->tc_zero, 8192); fr(F->U32, 4 * std::max<int64_t>(S.u_arena, 1));
   fr(F->scale, 8 * S.n);
   int oc = F->nrhs_cap;
   if (oc > 0) {
@@ -1584,7 +1607,7 @@ jfg_status numeric_factor(jfg_model* m, int precision) {
     if (!F->Dinv64) JFG_TRY(dev_alloc(c, (void**)&F->Dinv64, sizeof(double) * F->dinv_len));
     if (!F->Sinv64) JFG_TRY(dev_alloc(c, (void**)&F->Sinv64, sizeof(double) * F->sinv_len));
     auto body = [&]() -> jfg_status {
-      JFG_TRY(factor_levels<double>(m, F, F->L64, F->U64, F->Dinv64, nullptr, st));
+      JFG_TRY(factor_levels<double>(m, F, F->L64, F->U64, F->Dinv64, false, st));
       return strip_inverses<double>(F, F->L64, F->Dinv64, F->Sinv64, st);
     };
     // the first factorisation runs eagerly (one-time kernel attributes);
@@ -1614,15 +1637,29 @@ jfg_status numeric_factor(jfg_model* m, int precision) {
     // on the 914k-DOF wing panel raise refinement from 8 to 13 iterations
     // while on the CTETRA10 block the iteration count is unchanged
     const int tcs = tc::setting();
-    float* tc_lo = nullptr;
-    if (tcs == 1 || (tcs < 0 && m->n_q4 + m->n_q8 == 0)) {
-      if (!F->L32lo) JFG_TRY(dev_alloc(c, (void**)&F->L32lo, sizeof(float) * S.nnz_L));
-      tc_lo = F->L32lo;
+    const bool use_tc = tcs == 1 || (tcs < 0 && m->n_q4 + m->n_q8 == 0);
+    if (use_tc && !F->Phi) {
+      // packed operand arrays: ceil(c/16) x ceil(m/8) atoms of 128 floats
+      std::vector<int64_t> pk(S.ns + 1, 0);
+      for (int64_t s = 0; s < S.ns; ++s) {
+        const int64_t cs = S.sn_first[s + 1] - S.sn_first[s], ms = S.sn_m[s];
+        pk[s + 1] = pk[s] + ((cs + 15) / 16) * ((ms + 7) / 8) * 128;
+      }
+      F->pk_len = std::max<int64_t>(pk[S.ns], 128);
+      JFG_TRY(dev_alloc(c, (void**)&F->PKptr, sizeof(int64_t) * (S.ns + 1)));
+      JFG_TRY(dev_alloc(c, (void**)&F->Phi, sizeof(float) * F->pk_len));
+      JFG_TRY(dev_alloc(c, (void**)&F->Plo, sizeof(float) * F->pk_len));
+      JFG_TRY(dev_alloc(c, (void**)&F->tc_zero, 8192));
+      JFG_CUDA(cudaMemcpyAsync(F->PKptr, pk.data(), sizeof(int64_t) * (S.ns + 1), cudaMemcpyHostToDevice, st));
+      JFG_CUDA(cudaMemsetAsync(F->Phi, 0, sizeof(float) * F->pk_len, st));
+      JFG_CUDA(cudaMemsetAsync(F->Plo, 0, sizeof(float) * F->pk_len, st));
+      JFG_CUDA(cudaMemsetAsync(F->tc_zero, 0, 8192, st));
+      JFG_CUDA(cudaStreamSynchronize(st));   // pk is a host temporary
     }
     if (!F->Dinv32) JFG_TRY(dev_alloc(c, (void**)&F->Dinv32, sizeof(float) * F->dinv_len));
     if (!F->Sinv32) JFG_TRY(dev_alloc(c, (void**)&F->Sinv32, sizeof(float) * F->sinv_len));
     auto body = [&]() -> jfg_status {
-      JFG_TRY(factor_levels<float>(m, F, F->L32, F->U32, F->Dinv32, tc_lo, st));
+      JFG_TRY(factor_levels<float>(m, F, F->L32, F->U32, F->Dinv32, use_tc, st));
       return strip_inverses<float>(F, F->L32, F->Dinv32, F->Sinv32, st);
     };
     if (F->factor_calls[1]++ > 0 && graphs_enabled())

@@ -47,28 +47,33 @@ __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::be
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
 // ---------------------------------------------------------------------------
-// Front updates of the mixed factor on the tensor cores, operands streamed
-// by asynchronous copies.  The trsm kernel stores next to every FP32 panel
-// value v its low part lo = rn19(v - trunc19(v)) (L32lo); the tensor core
-// reads v itself as the high part (kind::tf32 uses the upper 19 bits of an
-// FP32 word), so both operand terms are plain copies from global memory.
+// Front updates of the mixed factor on the tensor cores.  The trsm kernel
+// writes every FP32 panel value v a second time as hi = rn19(v) and
+// lo = rn19(v - hi) into two packed operand arrays laid out as the shared-
+// memory image the tensor core reads: per front, 512-byte atoms of 8 rows x
+// 16 columns in the 64-byte-swizzled K-major layout, slice-block major, so
+// that 128 rows of one 16-column K-slice are 8 KB of contiguous memory.
 //
 // One CTA per 128 x 128 output tile, warp-specialised:
 //   * warps 0-7 (drain): warp w reads TMEM lanes 32(w%4).. +32 (tile rows)
 //     and columns 64(w/4).. +64; every UDR K-slices of 16 columns are
-//     accumulated by the tensor core into one of two TMEM accumulators and
+//     accumulated by the tensor core into one of USL TMEM accumulators
+//     (round robin, so the MMAs run up to USL - 1 uses ahead of the drain) and
 //     added here into FP32 registers once complete, so the tensor core never
 //     sums more than 16 UDR columns of products; the epilogue writes
 //     C -= acc (mode 0, panel columns of the front) or C = -acc (mode 1,
-//     the update matrix U);
-//   * warps 8..8+UPW-1 (producers): 4-byte cp.async of hi and lo of both
-//     operands into a UST-stage ring in the no-swizzle K-major core-matrix
-//     layout, completion signalled per stage with
-//     cp.async.mbarrier.arrive.noinc on the stage's "full" barrier;
-//   * the last warp (one thread): waits for a full stage and a free
-//     accumulator, issues lo*hi + hi*lo + hi*hi (K = 8 per instruction) and
-//     commits to the stage's "empty" barrier and the accumulator's "full"
-//     barrier.
+//     the update matrix U), all loads of a column group before its stores;
+//   * warp 8 (one thread): per K-slice 4 bulk copies (cp.async.bulk, no
+//     multicast) of 8 KB (A hi, A lo, B hi, B lo) into a UST-stage ring,
+//     completion counted in bytes on the stage's mbarrier;
+//   * warp 9 (one thread): waits for a full stage and a free accumulator,
+//     issues lo*hi + hi*lo + hi*hi (kind::tf32, M = N = 128, K = 8) and
+//     commits to the stage's "empty" and the accumulator's "full" barriers.
+// Tile origins are multiples of 8 rows: mode 1 (origin c) starts the tile
+// grid c mod 8 rows early and stores nothing above row c.  Rows past the
+// front come from stale shared memory or zeroed padding and reach only output
+// rows that are not stored; columns past the K range are zeroed padding of
+// the packed arrays (or an 8 KB zero page).
 // Every wait is bounded (about two seconds of clock) and also gives up as
 // soon as another warp has given up; the CTA then records EE_TC_TIMEOUT,
 // waits (bounded) for its own copies and MMAs and frees its tensor memory.
@@ -83,16 +88,22 @@ constexpr int UK = 16;
 constexpr int UST = JFG_TC_STAGES;
 constexpr int UDR = JFG_TC_DRAIN;               // K-slices per accumulator use
 constexpr int UDW = 8;                          // drain warps: 4 lane quarters x 2 column halves
-constexpr int UPW = 4;                          // producer warps
-constexpr int UTHREADS = (UDW + UPW + 1) * 32;
-constexpr uint32_t UTMEM = 2 * UM;              // two FP32 accumulators of 128 columns
-// K-major without swizzle: core matrix = 8 rows x 4 columns (16 bytes);
-// 4-column groups 2048 bytes apart (LBO), 8-row groups 128 bytes (SBO)
+constexpr int UTHREADS = (UDW + 2) * 32;        // + producer warp + MMA warp
+#ifndef JFG_TC_SLOTS
+#define JFG_TC_SLOTS 4
+#endif
+constexpr int USL = JFG_TC_SLOTS;               // TMEM accumulators of 128 columns
+constexpr uint32_t UTMEM = USL * UM;
+// K-major, 64-byte swizzle: an 8-row x 16-column atom of 512 bytes, row i at
+// i*64, its 16-byte chunk c (4 columns) at chunk position c ^ ((i >> 1) & 3);
+// 16 atoms (128 rows) stacked 512 bytes apart (SBO) form one operand part
+// of a K-slice.  The two K = 8 halves of a slice start 32 bytes apart.
 constexpr int UPART = UM * UK * 4;
-constexpr uint32_t U_LBO = 2048, U_SBO = 128, U_KSTEP = 4096;
+constexpr uint32_t U_LBO = 16, U_SBO = 512, U_KSTEP = 32;
+constexpr uint64_t U_SWIZZLE_64B = 4;
 constexpr int USTAGE = 4 * UPART;               // A hi, A lo, B hi, B lo
 constexpr int UBAR = UST * USTAGE;
-constexpr int USMEM = UBAR + 8 * (2 * UST + 5) + 16;
+constexpr int USMEM = UBAR + 8 * (2 * UST + 2 * USL + 1) + 16;
 constexpr uint32_t UIDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(UM >> 3) << 17) |
                             ((uint32_t)(UM >> 4) << 24);
 
@@ -102,6 +113,7 @@ __device__ __forceinline__ uint64_t u_desc(uint32_t saddr) {
   d |= (uint64_t)((U_LBO >> 4) & 0x3FFFu) << 16;
   d |= (uint64_t)((U_SBO >> 4) & 0x3FFFu) << 32;
   d |= (uint64_t)1 << 46;
+  d |= U_SWIZZLE_64B << 61;
   return d;
 }
 
@@ -114,8 +126,14 @@ __device__ __forceinline__ void u_mma(uint32_t tmem_d, uint64_t adesc, uint64_t 
       : "memory");
 }
 
-__device__ __forceinline__ void cp4(uint32_t dst, const float* src, uint32_t bytes) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+__device__ __forceinline__ void bulk_load(uint32_t dst, const float* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
@@ -135,7 +153,8 @@ __device__ __forceinline__ bool u_wait(uint32_t bar, uint32_t parity, volatile i
 __global__ void __launch_bounds__(UTHREADS, 1)
 k_update_tf32x3(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
                 const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
-                const int64_t* __restrict__ Uptr, float* __restrict__ L, const float* __restrict__ Llo,
+                const int64_t* __restrict__ Uptr, float* __restrict__ L, const float* __restrict__ Phi,
+                const float* __restrict__ Plo, const int64_t* __restrict__ PKptr, const float* __restrict__ zero,
                 float* __restrict__ U, int mode, int kbeg, int kend, int cend, int terms, DevError* err) {
   const int s = list[blockIdx.y];
   const int c = first[s + 1] - first[s];
@@ -157,27 +176,30 @@ k_update_tf32x3(const int32_t* __restrict__ list, const int32_t* __restrict__ fi
     C = U + Uptr[s];
     ldc = r;
   }
-  const int ntj = (ncol + UM - 1) / UM, nti = (nrow + UM - 1) / UM;
+  // tile grid from a row origin that is a multiple of 8 (row0 == col0)
+  const int sh = row0 & 7;
+  const int row0e = row0 - sh, col0e = col0 - sh, nrowe = nrow + sh, ncole = ncol + sh;
+  const int ntj = (ncole + UM - 1) / UM, nti = (nrowe + UM - 1) / UM;
   const int t = blockIdx.x;
   if (t >= nti * ntj) return;
   const int ti = t / ntj, tj = t % ntj;
-  if (ti * UM + UM - 1 + row0 < tj * UM + col0) return;   // strictly upper tile
+  if (ti * UM + UM - 1 + row0e < tj * UM + col0e) return;   // strictly upper tile
   extern __shared__ __align__(1024) unsigned char smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + UBAR);
   uint64_t* empty = full + UST;
   uint64_t* accfull = empty + UST;
-  uint64_t* accempty = accfull + 2;
-  uint64_t* spare = accempty + 2;
+  uint64_t* accempty = accfull + USL;
+  uint64_t* spare = accempty + USL;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(spare + 1);
   volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
     for (int q = 0; q < UST; ++q) {
-      mbar_init(smem_addr(&full[q]), UPW * 32);
+      mbar_init(smem_addr(&full[q]), 1);
       mbar_init(smem_addr(&empty[q]), 1);
     }
     mbar_init(smem_addr(spare), 1);
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < USL; ++q) {
       mbar_init(smem_addr(&accfull[q]), 1);
       mbar_init(smem_addr(&accempty[q]), UDW * 32);
     }
@@ -197,53 +219,48 @@ k_update_tf32x3(const int32_t* __restrict__ list, const int32_t* __restrict__ fi
   const int nk = (ke - kb + UK - 1) / UK;
   const uint32_t sbase = smem_addr(smem);
 
-  if (warp >= UDW && warp < UDW + UPW) {
-    // ---------------------------------------------------------- producers
-    const int pw = warp - UDW;
-    const int64_t arow0 = row0 + (int64_t)ti * UM, brow0 = col0 + (int64_t)tj * UM;
-    const float* P = L + Lptr[s];
-    const int64_t dlo = (Llo + Lptr[s]) - P;
-    // rows past the tile's valid rows re-read the tile's first row: such
-    // rows only reach output rows / columns that are not stored
-    int64_t ra[4], rb[4];
-    // warp pw: row groups pw + 4 rg, columns lane / 8 + 4 g (one 8 x 4 block,
-    // four full 32-byte sectors, per instruction)
+  if (warp == UDW) {
+    // ---------------------------------------------------------- producer
+    if (lane == 0) {
+      const int64_t pk = PKptr[s], nrg = (m + 7) / 8;
+      const int64_t rga = (row0e + (int64_t)ti * UM) >> 3, rgb = (col0e + (int64_t)tj * UM) >> 3;
+      const uint32_t na = (uint32_t)min((int64_t)16, nrg - rga) * 512u;
+      const uint32_t nb = (uint32_t)min((int64_t)16, nrg - rgb) * 512u;
+      int issued = 0;
+      for (int j = 0; j < nk; ++j) {
+        const int st = j % UST, n = j / UST;
+        if (n >= 1 && !u_wait(smem_addr(&empty[st]), (uint32_t)((n - 1) & 1), abort)) break;
+        const uint32_t dst = sbase + (uint32_t)(st * USTAGE), bar = smem_addr(&full[st]);
+        const int64_t sb = (kb + j * UK) >> 4;   // 16-column slice block
+        if (16 * sb < ke) {
+          const int64_t oa = pk + (sb * nrg + rga) * 128, ob = pk + (sb * nrg + rgb) * 128;
+          mbar_expect_tx(bar, 2 * (na + nb));
+          bulk_load(dst, Phi + oa, na, bar);
+          bulk_load(dst + UPART, Plo + oa, na, bar);
+          bulk_load(dst + 2 * UPART, Phi + ob, nb, bar);
+          bulk_load(dst + 3 * UPART, Plo + ob, nb, bar);
+        } else {   // columns past the K range: zeros
+          mbar_expect_tx(bar, 4 * UPART);
 #pragma unroll
-    for (int rg = 0; rg < 4; ++rg) {
-      const int i = (pw + 4 * rg) * 8 + (lane & 7);
-      ra[rg] = arow0 + (ti * UM + i < nrow ? i : 0);
-      rb[rg] = brow0 + (tj * UM + i < ncol ? i : 0);
-    }
-    const uint32_t soff = (uint32_t)(pw * 128 + (lane & 7) * 16 + (lane >> 3) * 4);
-    for (int j = 0; j < nk; ++j) {
-      const int st = j % UST, n = j / UST;
-      if (n >= 1 && !u_wait(smem_addr(&empty[st]), (uint32_t)((n - 1) & 1), abort)) break;
-      const uint32_t base = sbase + (uint32_t)(st * USTAGE) + soff;
-#pragma unroll
-      for (int g = 0; g < 4; ++g) {
-        const int k = kb + j * UK + (lane >> 3) + 4 * g;
-        const uint32_t sg = base + (uint32_t)(g * 2048);
-        const bool kv = k < ke;
-        const float* col = P + (int64_t)m * (kv ? k : kb);   // columns past ke: zero-filled
-        const uint32_t nb = kv ? 4u : 0u;
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          const uint32_t o = sg + (uint32_t)(r * 512);
-          cp4(o, col + ra[r], nb);
-          cp4(o + UPART, col + dlo + ra[r], nb);
-          cp4(o + 2 * UPART, col + rb[r], nb);
-          cp4(o + 3 * UPART, col + dlo + rb[r], nb);
+          for (int q = 0; q < 4; ++q) bulk_load(dst + q * UPART, zero, UPART, bar);
+        }
+        issued = j + 1;
+      }
+      if (issued < nk && issued > 0) {
+        // gave up: let the copies already issued land before the CTA exits
+        const int l = issued - 1;
+        const long long t0 = clock64();
+        while (!mbar_try(smem_addr(&full[l % UST]), (uint32_t)((l / UST) & 1)) && clock64() - t0 < WAIT_CYCLES) {
         }
       }
-      asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_addr(&full[st])) : "memory");
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");
-  } else if (warp == UDW + UPW) {
+    __syncwarp();
+  } else if (warp == UDW + 1) {
     // ---------------------------------------------------------- MMA issue
     if (lane == 0) {
       int issued = 0;
       for (int j = 0; j < nk; ++j) {
-        const int st = j % UST, n = j / UST, use = j / UDR, slot = use & 1, q = use >> 1;
+        const int st = j % UST, n = j / UST, use = j / UDR, slot = use % USL, q = use / USL;
         const bool first_of_use = (j % UDR) == 0, last_of_use = (j % UDR) == UDR - 1 || j == nk - 1;
         if (!u_wait(smem_addr(&full[st]), (uint32_t)(n & 1), abort)) break;
         if (first_of_use && q >= 1 && !u_wait(smem_addr(&accempty[slot]), (uint32_t)((q - 1) & 1), abort)) break;
@@ -283,7 +300,7 @@ k_update_tf32x3(const int32_t* __restrict__ list, const int32_t* __restrict__ fi
     const int nuse = (nk + UDR - 1) / UDR;
     int drained = 0;
     for (int u = 0; u < nuse; ++u) {
-      const int slot = u & 1, q = u >> 1;
+      const int slot = u % USL, q = u / USL;
       bool ok = lane == 0 ? u_wait(smem_addr(&accfull[slot]), (uint32_t)(q & 1), abort) : true;
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) break;
@@ -311,27 +328,29 @@ k_update_tf32x3(const int32_t* __restrict__ list, const int32_t* __restrict__ fi
       drained = u + 1;
     }
     if (drained == nuse && nk > 0) {
-      // this thread's row of the tile, columns j0g .. j0g + HC - 1; stored
-      // are the columns below ncol on or below the front's diagonal.  All
-      // loads of a 16-column group are issued before its stores.
-      const int64_t gi = (int64_t)ti * UM + (warp & 3) * 32 + lane;
-      const int64_t j0g = (int64_t)tj * UM + (warp >> 2) * HC;
+      // this thread's row of the tile and columns j0g .. j0g + HC - 1 (front
+      // coordinates relative to C); stored are rows in [0, nrow) and columns
+      // in [0, ncol) on or below the front's diagonal.  All loads of a
+      // 16-column group are issued before its stores.
+      const int64_t gi = (int64_t)ti * UM + (warp & 3) * 32 + lane - sh;
+      const int64_t j0g = (int64_t)tj * UM + (warp >> 2) * HC - sh;
+      const int64_t jfirst = -j0g;
       const int64_t jlast = min((int64_t)ncol - 1, row0 + gi - col0) - j0g;
-      if (gi < nrow && jlast >= 0) {
-        float* crow = C + gi + ldc * j0g;
+      if (gi >= 0 && gi < nrow && jlast >= 0) {
 #pragma unroll
         for (int h = 0; h < HC; h += 16) {
           if (mode == 0) {
             float cv[16];
 #pragma unroll
-            for (int e = 0; e < 16; ++e) cv[e] = (h + e <= jlast) ? crow[ldc * (h + e)] : 0.0f;
+            for (int e = 0; e < 16; ++e)
+              cv[e] = (h + e >= jfirst && h + e <= jlast) ? C[gi + ldc * (j0g + h + e)] : 0.0f;
 #pragma unroll
             for (int e = 0; e < 16; ++e)
-              if (h + e <= jlast) crow[ldc * (h + e)] = cv[e] - acc[h + e];
+              if (h + e >= jfirst && h + e <= jlast) C[gi + ldc * (j0g + h + e)] = cv[e] - acc[h + e];
           } else {
 #pragma unroll
             for (int e = 0; e < 16; ++e)
-              if (h + e <= jlast) crow[ldc * (h + e)] = -acc[h + e];
+              if (h + e >= jfirst && h + e <= jlast) C[gi + ldc * (j0g + h + e)] = -acc[h + e];
           }
         }
       }
@@ -356,9 +375,10 @@ int setting() {
 bool enabled() { return setting() != 0; }
 
 bool front_update_tf32x3(const int32_t* list, int count, const int32_t* first, const int32_t* mrows,
-                         const int64_t* Lptr, const int64_t* Uptr, float* L, const float* Llo, float* U, int mode,
-                         int kbeg, int kend, int cend, int max_rows, int max_cols, DevError* err, cudaStream_t st) {
-  if (!enabled() || !Llo || count <= 0 || max_rows <= 0 || max_cols <= 0) return false;
+                         const int64_t* Lptr, const int64_t* Uptr, float* L, const float* Phi, const float* Plo,
+                         const int64_t* PKptr, const float* zero, float* U, int mode, int kbeg, int kend, int cend,
+                         int max_rows, int max_cols, DevError* err, cudaStream_t st) {
+  if (!enabled() || !Phi || !Plo || !PKptr || !zero || count <= 0 || max_rows <= 0 || max_cols <= 0) return false;
   static bool attr = false;
   if (!attr) {
     if (cudaFuncSetAttribute(k_update_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, USMEM) != cudaSuccess)
@@ -367,9 +387,10 @@ bool front_update_tf32x3(const int32_t* list, int count, const int32_t* first, c
   }
   const char* te = std::getenv("JFG_TC_TERMS");   // 4: add lo*lo
   const int terms = (te && te[0] == '4') ? 4 : 3;
-  const int64_t tiles = (int64_t)((max_rows + UM - 1) / UM) * ((max_cols + UM - 1) / UM);
-  k_update_tf32x3<<<dim3((unsigned)tiles, (unsigned)count), UTHREADS, USMEM, st>>>(list, first, mrows, Lptr, Uptr, L, Llo,
-                                                                             U, mode, kbeg, kend, cend, terms, err);
+  const int ext = mode == 1 ? 7 : 0;              // the mode-1 grid starts up to 7 rows early
+  const int64_t tiles = (int64_t)((max_rows + ext + UM - 1) / UM) * ((max_cols + ext + UM - 1) / UM);
+  k_update_tf32x3<<<dim3((unsigned)tiles, (unsigned)count), UTHREADS, USMEM, st>>>(
+      list, first, mrows, Lptr, Uptr, L, Phi, Plo, PKptr, zero, U, mode, kbeg, kend, cend, terms, err);
   count_launch();
   return cudaGetLastError() == cudaSuccess;
 }
