@@ -990,12 +990,14 @@ k_bwd_spartial(const int32_t* __restrict__ list, const int32_t* __restrict__ fir
   int rb = blockIdx.x / (SW / 32), cg = blockIdx.x % (SW / 32);
   if (rb >= nrb || cg * 32 >= kw) return;
   int row0 = j0 + kw + rb * 256;
-  __shared__ double xs[256][8];
+  // right-hand-side major, so that lanes reading consecutive rows hit
+  // consecutive banks
+  __shared__ double xs[8][256];
   const int32_t* R = rows + rows_ptr[s];
   for (int e = threadIdx.x; e < 256 * 8; e += blockDim.x) {
     int ii = e & 255, k = e >> 8;
     int i = row0 + ii;
-    xs[ii][k] = (i < m && k < nr) ? xp[(int64_t)R[i] + n * k] : 0.0;
+    xs[k][ii] = (i < m && k < nr) ? xp[(int64_t)R[i] + n * k] : 0.0;
   }
   __syncthreads();
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1005,13 +1007,16 @@ k_bwd_spartial(const int32_t* __restrict__ list, const int32_t* __restrict__ fir
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (jj < kw) {
       const T* col = L + Lptr[s] + (int64_t)m * (j0 + jj);
-      for (int ii = lane; ii < 256; ii += 32) {
-        int i = row0 + ii;
-        if (i >= m) break;
-        double lv = (double)col[i];
+      double lv[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) acc[k] += lv * xs[ii][k];
+      for (int u = 0; u < 8; ++u) {   // all eight loads in flight
+        int i = row0 + lane + 32 * u;
+        lv[u] = i < m ? (double)col[i] : 0.0;
       }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] += lv[u] * xs[k][lane + 32 * u];
     }
     double v = warp_sum8(acc, lane);
     if ((lane & 3) == 0 && jj < SW) out[jj * 8 + (lane >> 2)] = v;
@@ -1037,7 +1042,7 @@ k_bwd_sdiag(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
   int nrb = (m - (j0 + kw) + 255) / 256;
   const double* pp = part + part_off[blockIdx.y];
   const T* X = Sinv + Sptr[s] + (int64_t)kb * SW * SW;
-  __shared__ double bs[SW][8];
+  __shared__ double bs[8][SW];   // right-hand-side major (conflict-free row reads)
   for (int e = threadIdx.x; e < (kw - i0) * 8; e += blockDim.x) {
     int l = i0 + (e >> 3), k = e & 7;
     double v = 0.0;
@@ -1055,17 +1060,26 @@ k_bwd_sdiag(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
       for (; rb < nrb; ++rb) a0 += q[(int64_t)rb * SW * 8];
       v = tt[f + j0 + l + n * k] - ((a0 + a1) + (a2 + a3));
     }
-    bs[l][k] = v;
+    bs[k][l] = v;
   }
   __syncthreads();
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int i = i0 + warp; i < min(kw, i0 + 32); i += 8) {
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     const T* col = X + (int64_t)kw * i;
-    for (int j = i + lane; j < kw; j += 32) {
-      double x = (double)col[j];
+    double x[SW / 32];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) acc[k] += x * bs[j][k];
+    for (int u = 0; u < SW / 32; ++u) {   // all loads in flight
+      int j = i + lane + 32 * u;
+      x[u] = j < kw ? (double)col[j] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < SW / 32; ++u) {
+      int j = i + lane + 32 * u;   // bs holds columns [i0, kw) only
+      if (j < kw) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] += x[u] * bs[k][j];
+      }
     }
     double v = warp_sum8(acc, lane);
     int k = lane >> 2;
