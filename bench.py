@@ -52,6 +52,10 @@ def make_workload(name: str):
     if name == "solid_block":
         return M.solid_block(), {"workload": "solid_block_40cube_ctetra10", "grids": 531441, "ctetra10": 384000,
                                  "ndof": 3188646, "subcases": 4}
+    if name == "solid_block_small":   # profiling-sized case of the same kernels
+        m = M.solid_block(n=16)
+        return m, {"workload": "solid_block_16cube_ctetra10", "grids": m.n_nodes, "ctetra10": len(m.t10_nodes),
+                   "ndof": m.ndof, "subcases": len(m.load_cases)}
     raise ValueError(name)
 
 
@@ -551,7 +555,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--workload", default="wing_panel",
-                    choices=["wing_panel", "wing_panel_small", "plate", "solid_block", "batched", "serving"])
+                    choices=["wing_panel", "wing_panel_small", "plate", "solid_block", "solid_block_small", "batched",
+                             "serving"])
     ap.add_argument("--models", type=int, default=1024, help="batched: number of panels")
     ap.add_argument("--pack-dof", type=int, default=400000, help="batched: DOF per pack")
     ap.add_argument("--slots", type=int, default=4, help="batched/serving: device streams")

@@ -915,9 +915,11 @@ k_fwd_supdate(const int32_t* __restrict__ list, const int32_t* __restrict__ firs
   if (row0 >= m) return;
   __shared__ double ys[SW][8];
   __shared__ double red[8][32][9];
-  for (int e = threadIdx.x; e < SW * 8; e += blockDim.x) {
-    int l = e & (SW - 1), k = e >> 8;
-    ys[l][k] = (l < kw && k < nr) ? tt[f + j0 + l + n * k] : 0.0;
+  // only the strip's kw columns and nr right-hand sides are read below (the
+  // accumulators of right-hand sides past nr are never stored)
+  for (int e = threadIdx.x; e < kw * nr; e += blockDim.x) {
+    int l = e % kw, k = e / kw;
+    ys[l][k] = tt[f + j0 + l + n * k];
   }
   __syncthreads();
   int rr = threadIdx.x & 31, g = threadIdx.x >> 5;   // row, column group of SW/8
