@@ -193,12 +193,23 @@ __global__ void k_extend_add(const int32_t* __restrict__ child, const int32_t* _
   int rb = rl[cb];
   if ((pass == 0) != (rb < cp)) return;
   const T* src = U + uc + (int64_t)rc * cb;
-  if (rb < cp) {
-    T* dst = L + Lptr[p] + (int64_t)mp * rb;
-    for (int a = cb + lane; a < rc; a += 32) dst[rl[a]] += src[a];
-  } else {
-    T* dst = U + Uptr[p] + (int64_t)rp * (rb - cp) - cp;
-    for (int a = cb + lane; a < rc; a += 32) dst[rl[a]] += src[a];
+  T* dst = rb < cp ? L + Lptr[p] + (int64_t)mp * rb : U + Uptr[p] + (int64_t)rp * (rb - cp) - cp;
+  // groups of 8 entries per lane: every load of a group (map, source,
+  // destination) is issued before its stores
+  for (int a0 = cb + lane; a0 < rc; a0 += 32 * 8) {
+    int idx[8];
+    T sv[8], dv[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      int a = a0 + 32 * u;
+      idx[u] = a < rc ? rl[a] : -1;
+      sv[u] = a < rc ? src[a] : (T)0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) dv[u] = idx[u] >= 0 ? dst[idx[u]] : (T)0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (idx[u] >= 0) dst[idx[u]] = dv[u] + sv[u];
   }
 }
 
@@ -285,7 +296,10 @@ k_potrf_diag(const int32_t* __restrict__ list, const int32_t* __restrict__ first
   T* P = L + Lptr[s] + k0 + (int64_t)m * k0;
   const int t = threadIdx.x, w = t >> 5, lane = t & 31;
   if (t == 0) bad_idx = NB;
-  for (int e = t; e < NB * NB; e += blockDim.x) {
+  // 256 threads: all 16 loads of a thread in flight together
+#pragma unroll
+  for (int u = 0; u < NB * NB / 256; ++u) {
+    int e = t + 256 * u;
     int i = e & (NB - 1), j = e >> 6;
     A[i][j] = (i < kn && j < kn) ? (i >= j ? P[i + (int64_t)m * j] : (T)0) : (i == j ? (T)1 : (T)0);
   }
@@ -378,7 +392,10 @@ k_trsm_panel(const int32_t* __restrict__ list, const int32_t* __restrict__ first
   T (*X)[NB + 1] = Di + NB;
   const T* Dv = Dinv + Dptr[s] + (int64_t)(k0 / NB) * NB * NB;
   T* P = L + Lptr[s];
-  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+  // 256 threads: all 32 loads of a thread in flight together
+#pragma unroll
+  for (int u = 0; u < NB * NB / 256; ++u) {
+    int e = threadIdx.x + 256 * u;
     int i = e % NB, j = e / NB;
     Di[i][j] = Dv[i + NB * j];
     int row = row0 + i;
