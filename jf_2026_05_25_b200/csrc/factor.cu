@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 
 #include "jfg_internal.h"
 #include "tc_gemm.cuh"
@@ -46,6 +47,14 @@ struct NumericFactor {
     std::vector<std::pair<int32_t, int32_t>> ea;   // (offset into ea_child, count), per child rank
     int32_t ea_max_r;
     double schur_flops;   // sum over fronts of r(r+1) c (lower SYRK, 2 flops per FMA)
+    // the level's fronts are listed by decreasing width: cs[i] is the width
+    // of the i-th, pm[i] the largest row count among the first i + 1
+    std::vector<int32_t> cs, pm;
+    // fronts wider than kmin (a prefix of the list)
+    int active(int kmin) const {
+      return (int)(std::upper_bound(cs.begin(), cs.end(), kmin, std::greater<int32_t>()) - cs.begin());
+    }
+    int maxm(int na) const { return na > 0 ? pm[na - 1] : 0; }
   };
   std::vector<Level> levels;
   // factor storage
@@ -1233,14 +1242,14 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
     // one front update of the level: the tensor-core 3xTF32 kernel for the
     // FP32 factor when its low parts exist and the level's output is large
     // enough for 128 x 128 tiles, else the SIMT / DMMA tiles
-    auto update = [&](int mode, int kbeg, int kend, int cend, int max_rows, int max_cols, int64_t tiles) {
+    auto update = [&](int mode, int kbeg, int kend, int cend, int max_rows, int max_cols, int64_t tiles, int cnt) {
       if constexpr (sizeof(T) == 4) {
         if (tc && max_rows >= tc_min && max_cols >= tc_min / 2 &&
-            tc::front_update_tf32x3(list, lv.count, F->first, F->mrows, F->Lptr, F->Uptr, Lf, F->Phi, F->Plo,
+            tc::front_update_tf32x3(list, cnt, F->first, F->mrows, F->Lptr, F->Uptr, Lf, F->Phi, F->Plo,
                                     F->PKptr, F->tc_zero, Uf, mode, kbeg, kend, cend, max_rows, max_cols, F->err, st))
           return;
       }
-      launch_front_update<T>((unsigned)tiles, lv.count, F, Lf, Uf, mode, kbeg, kend, cend, st);
+      launch_front_update<T>((unsigned)tiles, cnt, F, Lf, Uf, mode, kbeg, kend, cend, st);
     };
     // extend-add, pass 0: children columns that land in this level's panels
     for (const auto& seg : lv.ea) {
@@ -1259,29 +1268,32 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
     for (int P0 = 0; P0 < lv.max_c; P0 += PW) {
       const int P1 = P0 + PW;
       for (int k0 = P0; k0 < std::min(P1, lv.max_c); k0 += NB) {
-        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_potrf_diag<T><<<lv.count, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr,
+        const int na = lv.active(k0);   // fronts wider than k0: a prefix of the list
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_potrf_diag<T><<<na, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr,
                                                                                F->Dptr, Lf, Dvf, k0, F->err);
           count_launch(); } prof_end(ps_, st, KS_F_POTRF, 0.0); }
-        int rows_max = lv.max_m - k0 - 1;
+        int rows_max = lv.maxm(na) - k0 - 1;
         if (rows_max <= 0) continue;
         unsigned gx = (unsigned)((rows_max + 63) / 64);
-        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_trsm_panel<T><<<dim3(gx, lv.count), 256, 2 * NB * (NB + 1) * sizeof(T), st>>>(list, F->first, F->mrows,
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_trsm_panel<T><<<dim3(gx, na), 256, 2 * NB * (NB + 1) * sizeof(T), st>>>(list, F->first, F->mrows,
                                                                                         F->Lptr, F->Dptr, Lf, Dvf, k0,
                                                                                         tc ? F->Phi : nullptr, F->Plo, F->PKptr);
           count_launch(); } prof_end(ps_, st, KS_F_TRSM, 0.0); }
-        int nrow = lv.max_m - k0 - NB, ncol = std::min(P1, lv.max_c) - k0 - NB;
-        if (nrow > 0 && ncol > 0) {
+        const int nu = lv.active(k0 + NB);   // fronts with columns after this block
+        int nrow = lv.maxm(nu) - k0 - NB, ncol = std::min(P1, lv.max_c) - k0 - NB;
+        if (nu > 0 && nrow > 0 && ncol > 0) {
           int64_t tiles = (int64_t)((nrow + TILE - 1) / TILE) * ((ncol + TILE - 1) / TILE);
           { int ps_ = fine_prof() ? prof_start(st) : -1;
-            update(0, k0, k0 + NB, P1, nrow, ncol, tiles);
+            update(0, k0, k0 + NB, P1, nrow, ncol, tiles, nu);
             prof_end(ps_, st, KS_F_PANEL, 0.0); }
         }
       }
-      int nrow = lv.max_m - P1, ncol = lv.max_c - P1;
-      if (nrow > 0 && ncol > 0) {
+      const int nt = lv.active(P1);   // fronts with columns after the super-panel
+      int nrow = lv.maxm(nt) - P1, ncol = lv.max_c - P1;
+      if (nt > 0 && nrow > 0 && ncol > 0) {
         int64_t tiles = (int64_t)((nrow + TILE - 1) / TILE) * ((ncol + TILE - 1) / TILE);
         { int ps_ = fine_prof() ? prof_start(st) : -1;
-          update(0, P0, P1, INT_MAX, nrow, ncol, tiles);
+          update(0, P0, P1, INT_MAX, nrow, ncol, tiles, nt);
           prof_end(ps_, st, KS_F_PANEL, 0.0); }
       }
     }
@@ -1289,7 +1301,7 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
       int64_t nt = (lv.max_r + TILE - 1) / TILE;
       int64_t tiles = nt * nt;
       int ps = prof_start(st);
-      update(1, 0, 0, 0, lv.max_r, lv.max_r, tiles);
+      update(1, 0, 0, 0, lv.max_r, lv.max_r, tiles, lv.count);
       prof_end(ps, st, KS_SCHUR, lv.schur_flops);
     }
     // extend-add, pass 1: children columns that land in the U of this level
@@ -1343,12 +1355,13 @@ void solve_inner(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int n
                                                      F->relptr, F->rel, nr, n, F->xp, F->V); count_launch(); } prof_end(ps_, st, KS_S_VEC, 0.0); }
     int nstrip = (lv.max_c + SW - 1) / SW;
     for (int kb = 0; kb < nstrip; ++kb) {
-      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_fwd_sdiag<T><<<dim3(SW / 32, lv.count), 256, 0, st>>>(list, F->first, F->Sptr, Sv, kb, nr, n, F->xp, F->tt);
+      const int na = lv.active(kb * SW);   // fronts that have strip kb: a prefix of the list
+      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_fwd_sdiag<T><<<dim3(SW / 32, na), 256, 0, st>>>(list, F->first, F->Sptr, Sv, kb, nr, n, F->xp, F->tt);
         count_launch(); } prof_end(ps_, st, KS_S_FDIAG, 0.0); }
-      int rows = lv.max_m - kb * SW;
+      int rows = lv.maxm(na) - kb * SW;
       if (rows > 0) {
         unsigned gx = (unsigned)((rows + 31) / 32);
-        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_fwd_supdate<T><<<dim3(gx, lv.count), 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->relptr, Lf, kb,
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_fwd_supdate<T><<<dim3(gx, na), 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->relptr, Lf, kb,
                                                               nr, n, F->tt, F->xp, F->V); count_launch(); } prof_end(ps_, st, KS_S_FUPD, 0.0); }
       }
     }
@@ -1360,13 +1373,14 @@ void solve_inner(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int n
     const int64_t* poff = F->part_off + lv.off;
     int nstrip = (lv.max_c + SW - 1) / SW;
     for (int kb = nstrip - 1; kb >= 0; --kb) {
-      int rows = lv.max_m - kb * SW;
+      const int na = lv.active(kb * SW);
+      int rows = lv.maxm(na) - kb * SW;
       if (rows > 0) {
         unsigned gx = (unsigned)(((rows + 255) / 256) * (SW / 32));
-        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_bwd_spartial<T><<<dim3(gx, lv.count), 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->rows_ptr, F->rows,
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_bwd_spartial<T><<<dim3(gx, na), 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->rows_ptr, F->rows,
                                                                poff, Lf, kb, nr, n, F->xp, F->part); count_launch(); } prof_end(ps_, st, KS_S_BPART, 0.0); }
       }
-      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_bwd_sdiag<T><<<dim3(SW / 32, lv.count), 256, 0, st>>>(list, F->first, F->mrows, F->Sptr, poff, Sv, kb, nr, n,
+      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_bwd_sdiag<T><<<dim3(SW / 32, na), 256, 0, st>>>(list, F->first, F->mrows, F->Sptr, poff, Sv, kb, nr, n,
                                                  F->part, F->tt, F->xp); count_launch(); } prof_end(ps_, st, KS_S_BDIAG, 0.0); }
     }
   }
@@ -1452,6 +1466,16 @@ jfg_status numeric_create(jfg_model* m) {
   jfg_status st = JFG_OK;
   upload(S.sn_first, &F->first, c, st);
   upload(S.sn_m, &F->mrows, c, st);
+  // fronts of a level by decreasing width (then by index), so that the
+  // fronts still active at a column step are a prefix of the level's list
+  // and each step launches only them
+  for (int64_t l = 0; l < S.n_levels; ++l) {
+    auto b = S.level_sn.begin() + S.level_ptr[l], e = S.level_sn.begin() + S.level_ptr[l + 1];
+    std::sort(b, e, [&](int32_t x, int32_t y) {
+      const int32_t cx = S.sn_first[x + 1] - S.sn_first[x], cy = S.sn_first[y + 1] - S.sn_first[y];
+      return cx != cy ? cx > cy : x < y;
+    });
+  }
   upload(S.level_sn, &F->level_sn, c, st);
   upload(S.ea_child, &F->ea_child, c, st);
   upload(S.rel, &F->rel, c, st);
@@ -1494,12 +1518,16 @@ jfg_status numeric_create(jfg_model* m) {
     lv.off = S.level_ptr[l];
     lv.count = S.level_ptr[l + 1] - S.level_ptr[l];
     lv.max_c = lv.max_m = lv.max_r = 0;
+    lv.cs.clear();
+    lv.pm.clear();
     for (int32_t q = lv.off; q < lv.off + lv.count; ++q) {
       int32_t s = S.level_sn[q];
       int32_t cc = S.sn_first[s + 1] - S.sn_first[s];
       lv.max_c = std::max(lv.max_c, cc);
       lv.max_m = std::max(lv.max_m, S.sn_m[s]);
       if (S.sn_parent[s] >= 0) lv.max_r = std::max(lv.max_r, S.sn_m[s] - cc);
+      lv.cs.push_back(cc);
+      lv.pm.push_back(lv.max_m);
     }
     lv.schur_flops = 0;
     for (int32_t q = lv.off; q < lv.off + lv.count; ++q) {
