@@ -229,9 +229,12 @@ __global__ void k_extend_add(const int32_t* __restrict__ child, const int32_t* _
 // right-looking by rows with lane j holding column o+j of X = L^{-1}.
 // Pivots that are not positive and finite are replaced by 1 and the smallest
 // such column index is recorded in *bad_idx.
+// Not inlined: the two calls of k_potrf_diag share one copy of this long,
+// fully unrolled body (the kernel runs one CTA per front and is bound by
+// its serial chain, where instruction-cache misses showed as stalls).
 template <typename T>
-__device__ __forceinline__ void chol32_inv(T (*A)[NB + 1], T (*B)[NB + 1], T* sv, T* pv, int o, int kn,
-                                           int* bad_idx) {
+__device__ __noinline__ void chol32_inv(T (*A)[NB + 1], T (*B)[NB + 1], T* sv, T* pv, int o, int kn,
+                                        int* bad_idx) {
   const int lane = threadIdx.x & 31;
   const int gi = o + lane;
   T a[32];
