@@ -57,13 +57,21 @@ def apply(options: Dict[str, str]):
             os.environ.pop(k, None)
 
 
+def candidate_list(precision: int, candidates: Optional[Sequence[Dict[str, str]]] = None) -> List[Dict[str, str]]:
+    """The schedules `tune` times: the given ones, or the default grid; for the
+    mixed factor the default grid is doubled with the FP32 update choice
+    (tensor cores on / off)."""
+    cands = [dict(c) for c in (candidates or DEFAULT_CANDIDATES)]
+    if candidates is None and precision == lib.PREC_MIXED:
+        cands = [dict(c, JFG_TENSOR_CORES=t) for c in cands for t in ("1", "0")]
+    return cands
+
+
 def tune(model, candidates: Optional[Sequence[Dict[str, str]]] = None, repeats: int = 2,
          ctx: Optional[lib.Context] = None, precision: int = lib.PREC_FP64) -> Dict:
     """Time every candidate on `model`; returns dict(best, timings) and caches
     the best options for the model's size class."""
-    cands = list(candidates or DEFAULT_CANDIDATES)
-    if candidates is None and precision == lib.PREC_MIXED:
-        cands = [dict(c, JFG_TENSOR_CORES=t) for c in cands for t in ("1", "0")]
+    cands = candidate_list(precision, candidates)
     saved = {k: os.environ.get(k) for k in KNOBS}
     own_ctx = ctx is None
     ctx = ctx or lib.Context(0)

@@ -143,3 +143,21 @@ def test_packed_model_matches_members(oracle_mod):
         Uk = pk.split(Uf, sc)[k]
         assert Uk.shape == ref["u"].shape
         assert np.abs(Uk - ref["u"]).max() <= 1e-8 * np.abs(ref["u"]).max()
+
+
+def test_autotune_candidates_cover_update_kernels():
+    """The default tuning grid covers leaf size x amalgamation thresholds x
+    FP64 update kernel; for the mixed factor every schedule is also timed with
+    the tensor-core FP32 updates on and off, and explicit candidates are
+    taken as given."""
+    from jf_2026_05_25_b200 import autotune as AT
+    from jf_2026_05_25_b200 import lib
+    base = AT.candidate_list(lib.PREC_FP64)
+    assert base == AT.DEFAULT_CANDIDATES and len(base) == 18
+    mixed = AT.candidate_list(lib.PREC_MIXED)
+    assert len(mixed) == 2 * len(base)
+    assert {c["JFG_TENSOR_CORES"] for c in mixed} == {"0", "1"}
+    assert all({k: v for k, v in c.items() if k != "JFG_TENSOR_CORES"} in base for c in mixed)
+    given = [{"JFG_ND_LEAF": "16"}]
+    assert AT.candidate_list(lib.PREC_MIXED, given) == given
+    assert "JFG_TENSOR_CORES" in AT.KNOBS
