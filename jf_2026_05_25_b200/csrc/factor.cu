@@ -1138,23 +1138,8 @@ __global__ void k_scatter_add_perm(int64_t n, int nr, const int32_t* __restrict_
   for (int q = 0; q < nr; ++q) dst[g + lddst * q] += xp[k + n * q] * sc;
 }
 
-// Per-column sums of squares of an n x nr block (deterministic two-level tree).
-__global__ void k_colnorm2_partial(int64_t n, int nr, const double* __restrict__ x, double* __restrict__ part) {
-  __shared__ double sh[256];
-  int q = blockIdx.y;
-  double s = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    double v = x[i + n * q];
-    s += v * v;
-  }
-  sh[threadIdx.x] = s;
-  __syncthreads();
-  for (int o = 128; o > 0; o >>= 1) {
-    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) part[q * gridDim.x + blockIdx.x] = sh[0];
-}
+// Second level of the per-column dot products: the nb partial sums of each
+// column added in a fixed order (deterministic two-level tree).
 __global__ void k_colnorm2_final(int nb, int nr, const double* __restrict__ part, double* __restrict__ out) {
   int q = threadIdx.x;
   if (q >= nr) return;
@@ -1442,16 +1427,6 @@ jfg_status coldot(NumericFactor* F, int64_t len, int nr, const double* a, const 
                   cudaStream_t st) {
   const int nb = 256;
   { k_coldot_partial<<<dim3(nb, nr), 256, 0, st>>>(len, nr, a, b, F->norms); count_launch(); }
-  { k_colnorm2_final<<<1, 64, 0, st>>>(nb, nr, F->norms, F->norms + nb * 64); count_launch(); }
-  JFG_CUDA(cudaMemcpyAsync(out_host, F->norms + nb * 64, sizeof(double) * nr, cudaMemcpyDeviceToHost, st));
-  JFG_CUDA(cudaStreamSynchronize(st));
-  return JFG_OK;
-}
-
-// per-RHS squared norms of the n x nr block x (result on host)
-jfg_status colnorm2(NumericFactor* F, int64_t n, int nr, const double* x, double* out_host, cudaStream_t st) {
-  const int nb = 256;
-  { k_colnorm2_partial<<<dim3(nb, nr), 256, 0, st>>>(n, nr, x, F->norms); count_launch(); }
   { k_colnorm2_final<<<1, 64, 0, st>>>(nb, nr, F->norms, F->norms + nb * 64); count_launch(); }
   JFG_CUDA(cudaMemcpyAsync(out_host, F->norms + nb * 64, sizeof(double) * nr, cudaMemcpyDeviceToHost, st));
   JFG_CUDA(cudaStreamSynchronize(st));
