@@ -1,10 +1,11 @@
 // tc_gemm.cu -- tensor-core (tcgen05, kind::tf32) front updates of the
 // mixed-precision supernodal factor: C -= A B^T on 128 x 128 tiles of the
 // panel columns of a front (mode 0) and U = -L21 L21^T (mode 1), in 3xTF32
-// split precision with FP32 accumulation.  Operands are streamed with
-// cp.async into a shared-memory ring; accumulators live in tensor memory and
-// are drained into FP32 registers every K-slice.  No TMA and no cluster
-// multicast are used; every wait is bounded.
+// split precision with FP32 accumulation.  Operands (packed hi/lo images
+// written by the panel trsm) are streamed with bulk asynchronous copies
+// (cp.async.bulk, global -> shared, no tensor maps, no cluster multicast)
+// into a shared-memory ring; accumulators live in tensor memory and are
+// drained into FP32 registers every K-slice.  Every wait is bounded.
 #include "tc_gemm.cuh"
 
 #include <cstdlib>
