@@ -25,8 +25,10 @@
 //     overlaps on the same GPU (two host threads, or two contexts on
 //     different streams) race on the array: serialise them;
 //   * the first call on each device looks up the array's device address
-//     (cudaGetSymbolAddress, with that device current); make that first call
-//     before any stream capture is started on that device.
+//     (cudaGetSymbolAddress, with that device current; with lazy module
+//     loading this is also when the 16 MiB are taken); make that first call
+//     before any stream capture is started on that device.  The address is
+//     looked up again if the device's context has been re-created since.
 #include <mutex>
 #include <string>
 
@@ -42,16 +44,54 @@ constexpr int kMaxDevices = 64;
 // kernels get the device address from cudaGetSymbolAddress below.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
+// The array's address is looked up once per device and context.  A context
+// that is destroyed and created again (cudaDeviceReset, or the primary
+// context released and retained) reloads the module, which can move the
+// array, so each cached address is tagged with the id of the context it was
+// taken in (cuCtxGetId: unique for the life of the process) and looked up
+// again when the current context's id differs.
+using CtxGetCurrentFn = int (*)(void**);
+using CtxGetIdFn = int (*)(void*, unsigned long long*);
+
+struct ScratchAddr {
+  unsigned long long ctx_id = 0;
+  void* ptr = nullptr;
+};
+
 std::mutex g_addr_mu;
-void* g_addr[kMaxDevices] = {};
+ScratchAddr g_addr[kMaxDevices];
+
+// Id of the calling thread's current context, 0 when it cannot be read (the
+// address is then looked up again on every call, which is still allocation-free).
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, nullptr) == cudaSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, nullptr) == cudaSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+  });
+  if (!get_current || !get_id) return 0;
+  void* ctx = nullptr;
+  if (get_current(&ctx) != 0 || !ctx) return 0;
+  unsigned long long id = 0;
+  if (get_id(ctx, &id) != 0) return 0;
+  return id;
+}
 
 jfg_status scratch_address(int dev, unsigned char** out) {
   if (dev < 0 || dev >= kMaxDevices) {
     jfg::set_error("device ordinal out of range for the no-allocation scratch");
     return JFG_BAD_INPUT;
   }
+  const unsigned long long ctx_id = current_context_id();
   std::lock_guard<std::mutex> lk(g_addr_mu);
-  if (!g_addr[dev]) {
+  ScratchAddr& a = g_addr[dev];
+  if (!a.ptr || ctx_id == 0 || a.ctx_id != ctx_id) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
@@ -59,9 +99,10 @@ jfg_status scratch_address(int dev, unsigned char** out) {
                      cudaGetErrorString(e));
       return JFG_CUDA_ERROR;
     }
-    g_addr[dev] = p;
+    a.ptr = p;
+    a.ctx_id = ctx_id;
   }
-  *out = static_cast<unsigned char*>(g_addr[dev]);
+  *out = static_cast<unsigned char*>(a.ptr);
   return JFG_OK;
 }
 

@@ -190,6 +190,7 @@ class Resident:
     nbytes: int
     lock: threading.Lock
     last_used: float = 0.0
+    evicted: bool = False              # set under `lock` when the group is freed
 
 
 class SolveServer:
@@ -317,19 +318,33 @@ class SolveServer:
         return int(info["factor_bytes"] * 1.6 + 24 * nnz + 8 * ntrip + 200 * dm.ndof)
 
     def _admit(self, need: int):
-        """Free least-recently-used residents until `need` more bytes fit."""
+        """Free least-recently-used residents until `need` more bytes fit.
+
+        A pack is freed as a unit.  A group whose lock is held (a re-solve or
+        an update is running on it) is skipped, so in-flight work is never
+        freed under it; when every remaining group is busy the request is
+        admitted over budget rather than waiting.  The group's bytes are
+        released once, and its registry entries go only after its lock is held.
+        """
         with self.rlock:
-            while self.resident_bytes + need > self.budget and self.registry:
-                # evict the least recently used group (a pack is freed as a unit)
-                key = min(self.registry, key=lambda k: self.registry[k].last_used)
+            busy = set()
+            while self.resident_bytes + need > self.budget:
+                cands = [k for k in self.registry if id(self.registry[k].dm) not in busy]
+                if not cands:
+                    break
+                key = min(cands, key=lambda k: self.registry[k].last_used)
                 r = self.registry[key]
                 gid = id(r.dm)
-                keys = self.groups.pop(gid, [key])
                 if not r.lock.acquire(blocking=False):
-                    break   # in use: admit over budget rather than wait
+                    busy.add(gid)
+                    continue
                 try:
+                    keys = self.groups.pop(gid, [key])
                     for k in keys:
-                        self.registry.pop(k, None)
+                        member = self.registry.pop(k, None)
+                        if member is not None:
+                            member.evicted = True
+                    r.evicted = True
                     self.resident_bytes -= r.nbytes
                     r.dm.close()
                 finally:
@@ -392,9 +407,17 @@ class SolveServer:
             res.last_used = time.perf_counter()
             return res
 
+    @staticmethod
+    def _check_live(res: Resident, key: str):
+        """Called with res.lock held: the group may have been evicted between
+        the registry lookup and taking the lock."""
+        if res.evicted:
+            raise KeyError(f"model {key} is not resident (evicted or unknown)")
+
     def _do_resolve(self, req: Request):
         res = self._lookup(req.key)
         with res.lock:
+            self._check_live(res, req.key)
             out = self._member_solve(res, req.loads)
         out["key"] = req.key
         self._finish(req, out)
@@ -405,6 +428,7 @@ class SolveServer:
         symbolic analysis, then the solve."""
         res = self._lookup(req.key)
         with res.lock:
+            self._check_live(res, req.key)
             off = res.pack.q4_off[res.index]
             res.dm.update_q4_sections(np.asarray(req.elems, np.int32) + off, req.sections)
             res.pack._q4s[np.asarray(req.elems) + off] = req.sections

@@ -201,6 +201,60 @@ def partition(model, K, eps_zero: float = 1e-8) -> Tuple[np.ndarray, np.ndarray,
     return free, np.where(fixed)[0], {"autospc_zero": int(zero.sum()), "autospc_gpst": n_gpst}
 
 
+# ----------------------------------------------------------------------------
+# Applied loads (loads.jl:497-586 resolve_loads, solve_case.jl:57-91)
+# ----------------------------------------------------------------------------
+
+def load_vector(model, case) -> np.ndarray:
+    """Global force vector of one subcase, restated from the reference.
+
+    PLOAD4 on a 4-node shell (loads.jl:546-585): the face normal is
+    (x3 - x1) x (x4 - x2), area = |normal| / 2, and each of the 4 nodes gets
+    area * p / 4 along the unit normal (no nodal moments).  FORCE and the
+    consistent C3D10 face loads (delivered as nodal forces, abaqus_input.jl:
+    347-405) add their vectors to the translational DOFs.  The accumulated
+    global vector is then expressed in each node's displacement frame,
+    F_node = node_R' * F_global, per 3-block (solve_case.jl:78-82).
+    """
+    n_nodes = model.n_nodes
+    acc = np.zeros((n_nodes, 6))
+    X = np.asarray(model.xyz, float)
+    if case.pload4 is not None:
+        eidx, pres = case.pload4
+        q4 = np.asarray(model.q4_nodes)[np.asarray(eidx)]
+        a = X[q4[:, 2]] - X[q4[:, 0]]
+        b = X[q4[:, 3]] - X[q4[:, 1]]
+        nx = a[:, 1] * b[:, 2] - a[:, 2] * b[:, 1]
+        ny = a[:, 2] * b[:, 0] - a[:, 0] * b[:, 2]
+        nz = a[:, 0] * b[:, 1] - a[:, 1] * b[:, 0]
+        nrm = np.sqrt(nx * nx + ny * ny + nz * nz)
+        ok = 0.5 * nrm > 1e-30
+        share = np.where(ok, 0.5 * nrm * np.asarray(pres, float) / 4.0, 0.0)
+        unit = np.stack([nx, ny, nz], axis=1) / np.where(nrm > 0, nrm, 1.0)[:, None]
+        fnode = unit * share[:, None]
+        for k in range(4):
+            for c in range(3):
+                acc[:, c] += np.bincount(q4[:, k], weights=fnode[:, c], minlength=n_nodes)
+    for item in (case.forces, case.cload):
+        if item is None:
+            continue
+        nidx, vec = item
+        for c in range(3):
+            acc[:, c] += np.bincount(np.asarray(nidx), weights=np.asarray(vec, float)[:, c], minlength=n_nodes)
+    R = np.asarray(model.node_R, float).reshape(n_nodes, 3, 3, order="C")   # R[n, col, row]
+    out = np.empty_like(acc)
+    for blk in (0, 3):
+        g = acc[:, blk:blk + 3]
+        # (node_R' g)_j = sum_i node_R[i, j] g_i, node_R column-major: R[n, j, i] = node_R[i, j]
+        out[:, blk:blk + 3] = np.einsum("nji,ni->nj", R, g)
+    return out.reshape(-1)
+
+
+def load_matrix(model) -> np.ndarray:
+    """ndof x nsubcases (column-major) of every subcase's force vector."""
+    return np.asfortranarray(np.stack([load_vector(model, c) for c in model.load_cases], axis=1))
+
+
 def solve_reference(model, asm=None, free=None):
     """FP64 SOL101 on the CPU with SciPy's SuperLU (independent small-case checker).
 
@@ -212,7 +266,7 @@ def solve_reference(model, asm=None, free=None):
     K = csc_matrix(asm)
     if free is None:
         free, _, _ = partition(model, K)
-    F = model.load_matrix()
+    F = load_matrix(model)
     Kff = K[free][:, free].tocsc()
     # Symmetric(K_ff) (upper triangle) is what the reference factorises
     import scipy.sparse as sp

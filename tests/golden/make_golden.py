@@ -1,7 +1,7 @@
 """Regenerate the golden fixtures in this directory from the reference tree.
 
-Run in a container that has the OpenJFEM reference checked out (argument 1,
-default /root/reference).  It reads test and validation files as text only:
+Run in a container that has the OpenJFEM reference checked out; its path is
+the one required argument.  It reads test and validation files as text only:
 
 * utils/test/quad8_shell_test.jl -- CQUAD8 single-element stiffness entries
   produced by an external reference solver (rtol 2e-6 in the reference test).
@@ -139,7 +139,9 @@ def curved_beams(ref):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_golden.py <path of the OpenJFEM reference checkout>")
+    ref = sys.argv[1]
     here = os.path.dirname(os.path.abspath(__file__))
     json.dump(quad8_tables(ref), open(os.path.join(here, "quad8_entries.json"), "w"), indent=1)
     json.dump(mystran(ref), open(os.path.join(here, "mystran_sol101_simple.json"), "w"), indent=1)

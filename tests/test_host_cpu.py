@@ -89,19 +89,31 @@ def test_partition_gpst_finds_oblique_drilling(oracle_mod):
     assert np.array_equal(free_b, free_o)
 
 
+def _node_pairs(conn, n_nodes):
+    """Distinct (row node, column node) pairs coupled by at least one element."""
+    conn = np.asarray(conn, np.int64)
+    k = conn.shape[1]
+    a = np.repeat(conn, k, axis=1).ravel()
+    b = np.tile(conn, (1, k)).ravel()
+    return len(np.unique(a * n_nodes + b))
+
+
 def test_wing_panel_counts():
+    """Sizes of the stiffened wing-box panel, including nnz(K) = 49,332,276:
+    every pair of grids sharing a CQUAD4 couples 6 x 6 DOFs."""
     m = M.wing_panel()
     assert m.n_nodes == 152781 and len(m.q4_nodes) == 152000
     assert m.ndof == 916686
     assert m.ndof - len(m.spc_dofs()) == 914400
     assert len(m.load_cases) == 8
+    assert 36 * _node_pairs(m.q4_nodes, m.n_nodes) == 49332276
 
 
 def test_flat_plate_counts(oracle_mod):
     m = M.flat_plate()
     assert m.n_nodes == 441 and m.ndof == 2646
     asm = oracle_mod.assemble(m)
-    assert len(asm["rowval"]) == 133956
+    assert len(asm["rowval"]) == 133956 == 36 * _node_pairs(m.q4_nodes, m.n_nodes)
     K = oracle_mod.csc_matrix(asm)
     free, _, _ = oracle_mod.partition(m, K)
     assert len(free) == 2166
@@ -111,6 +123,8 @@ def test_solid_block_counts():
     m = M.solid_block(n=40)
     assert m.n_nodes == 531441 and len(m.t10_nodes) == 384000
     assert 3 * (m.n_nodes - len(np.unique(m.spc_dofs() // 6))) == 1574640
+    # CTETRA10 triplets touch translational DOFs only: 3 x 3 per grid pair
+    assert 9 * _node_pairs(m.t10_nodes, m.n_nodes) == 134475849
 
 
 def test_backend_names():

@@ -1,0 +1,87 @@
+"""Resident-model registry of the serving loop (CPU, no device).
+
+The registry logic -- least-recently-used eviction against the HBM budget,
+packs freed as a unit, in-flight groups never freed under a running re-solve
+-- is host code; these tests drive it with stand-in device models.
+"""
+import threading
+
+import pytest
+
+from jf_2026_05_25_b200 import serving as S
+
+
+class FakeDM:
+    """Stand-in for lib.DeviceModel: the registry only sizes and frees it."""
+
+    def __init__(self, factor_bytes):
+        self.factor_bytes = factor_bytes
+        self.ndof = 0
+        self.closed = 0
+
+    def symbolic_info(self):
+        return {"factor_bytes": self.factor_bytes}
+
+    def sizes(self):
+        return 0, 0, 0
+
+    def close(self):
+        self.closed += 1
+
+
+@pytest.fixture
+def server():
+    srv = S.SolveServer(slots=0, hbm_budget_bytes=100.0)
+    yield srv
+    srv.close()
+
+
+def _group(srv, n_members, nbytes):
+    dm = FakeDM(nbytes / 1.6)
+    keys = srv._register(dm, {}, None, [object()] * n_members)
+    return dm, keys
+
+
+def test_eviction_skips_a_busy_pack_and_frees_whole_groups(server):
+    dm_a, keys_a = _group(server, 2, 50.0)     # a pack of two models
+    dm_b, keys_b = _group(server, 1, 50.0)
+    assert server.resident_bytes == pytest.approx(100.0)
+    res_a = server._lookup(keys_a[0])
+    server._lookup(keys_b[0])                  # b is now the most recently used
+    # a re-solve holds pack a's lock while a new model needs room: a is the
+    # least recently used but busy, so b goes instead
+    with res_a.lock:
+        server._admit(50.0)
+        assert dm_a.closed == 0 and dm_b.closed == 1
+        assert all(k in server.registry for k in keys_a)
+        assert keys_b[0] not in server.registry
+        assert server.resident_bytes == pytest.approx(50.0)
+    # once idle the pack is freed as one unit and its bytes released once
+    server._admit(60.0)
+    assert dm_a.closed == 1
+    assert not any(k in server.registry for k in keys_a)
+    assert server.resident_bytes == pytest.approx(0.0)
+
+
+def test_resolve_after_eviction_raises_key_error(server):
+    dm_a, keys_a = _group(server, 2, 60.0)
+    res = server._lookup(keys_a[1])            # looked up before the eviction
+    server._admit(80.0)
+    assert dm_a.closed == 1
+    with res.lock:
+        with pytest.raises(KeyError):
+            server._check_live(res, keys_a[1])
+    with pytest.raises(KeyError):
+        server._lookup(keys_a[0])
+
+
+def test_eviction_waits_for_nothing_when_every_group_is_busy(server):
+    dm_a, keys_a = _group(server, 1, 90.0)
+    res = server._lookup(keys_a[0])
+    done = threading.Event()
+    with res.lock:
+        t = threading.Thread(target=lambda: (server._admit(50.0), done.set()))
+        t.start()
+        assert done.wait(5.0), "admission blocked on a busy group"
+        t.join()
+    assert dm_a.closed == 0 and keys_a[0] in server.registry
