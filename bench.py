@@ -109,42 +109,34 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- CPU arms
-def cpu_sol101(mdl, free, perm, nthreads):
-    """The CPU restatement of the reference path (oracle): element loop,
-    sparse() CSC, K_ff, supernodal Cholesky with OpenBLAS, one RHS at a time."""
+def cpu_sol101(mdl, nthreads, u_keep=False):
+    """The CPU restatement of the reference path (oracle only; the device
+    library is not loaded): element loop and sparse() CSC, the SPC1 +
+    AUTOSPC partition, K_ff, the oracle's CHOLMOD-rule ordering (approximate
+    minimum degree, nested dissection when that is poor), supernodal
+    Cholesky with OpenBLAS, then one RHS at a time."""
     from oracle import oracle as O
     t0 = time.perf_counter()
     asm = O.assemble(mdl)
     K = O.csc_matrix(asm)
-    Kff = K[free][:, free].tocsc()
     t1 = time.perf_counter()
-    F = mdl.load_matrix()[free]
-    U, info = O.chol_solve(len(free), Kff.indptr.astype(np.int64), Kff.indices, Kff.data, perm, F, nthreads=nthreads)
+    free, _, _ = O.partition(mdl, K)
+    Kff = K[free][:, free].tocsc()
+    perm, oinfo = O.order(Kff, free, mdl.xyz)
     t2 = time.perf_counter()
-    return dict(assembly_s=t1 - t0, factor_s=info["factor_s"], solve_s=info["solve_s"], total_s=t2 - t0,
-                flops=info["flops"], nnz_L=info["nnz_L"])
-
-
-def free_and_perm_host(mdl):
-    """Free set and ordering computed by the host code (no device)."""
-    from jf_2026_05_25_b200 import lib
-    from jf_2026_05_25_b200 import backend as B
-    from oracle import oracle as O
-    asm = O.assemble(mdl)
-    K = O.csc_matrix(asm)
-    Kc = K.tocsc()
-    nn = mdl.n_nodes
-    blocks = np.zeros((nn, 18))
-    # node blocks from the CSC (vectorised over the 6x6 diagonal blocks)
-    for off in (0, 1):
-        for b in range(3):
-            for a in range(3):
-                rows = 6 * np.arange(nn) + 3 * off + a
-                cols = 6 * np.arange(nn) + 3 * off + b
-                blocks[:, 9 * off + a + 3 * b] = np.asarray(Kc[rows, cols]).ravel()
-    free, fixed, _ = B.compute_free_dofs(mdl, K.diagonal(), blocks)
-    _, perm = lib.symbolic_dry_run(asm["colptr"], asm["rowval"], free, mdl.xyz)
-    return free, perm
+    F = O.load_matrix(mdl)
+    U, info = O.chol_solve(len(free), Kff.indptr.astype(np.int64), Kff.indices, Kff.data, perm, F[free],
+                           nthreads=nthreads)
+    t3 = time.perf_counter()
+    out = dict(assembly_s=t1 - t0, constraints_ordering_s=t2 - t1, factor_s=info["factor_s"],
+               solve_s=info["solve_s"], total_s=t3 - t0, flops=info["flops"], nnz_L=info["nnz_L"],
+               ordering=oinfo["method"])
+    if u_keep:
+        u = np.zeros((mdl.ndof, F.shape[1]))
+        u[free] = U
+        out["u"] = u
+        out["free"] = free
+    return out
 
 
 def run_reference(args, rank, world):
@@ -153,10 +145,9 @@ def run_reference(args, rank, world):
     os.environ.setdefault("JFEM_ORACLE_OPENBLAS", _openblas())
     mdl, cfg = make_workload(args.workload)
     nthreads = os.cpu_count() or 1
-    free, perm = free_and_perm_host(mdl)
     times = []
     for k in range(args.warmup + args.steps):
-        r = cpu_sol101(mdl, free, perm, nthreads)
+        r = cpu_sol101(mdl, nthreads)
         if k >= args.warmup:
             times.append(r["total_s"])
     ms = 1000.0 * float(np.mean(times))
@@ -320,13 +311,20 @@ def run_ours(args, rank, world, local_rank):
                     "frac": achieved / peak, "traffic": None, "peak_source": peaks["src"] + " hbm_gbs",
                     "launches": s["launches"], "ms_total": s["ms"]}
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         os.environ.setdefault("JFEM_ORACLE_OPENBLAS", _openblas())
         nthreads = os.cpu_count() or 1
-        r = cpu_sol101(mdl, st["free"], dm.perm(), nthreads)
+        r = cpu_sol101(mdl, nthreads, u_keep=True)
+        u_ref = r.pop("u")
+        free_ref = r.pop("free")
+        U_dev = dU.double().cpu().numpy().T          # ndof x nrhs
+        parity = {"max_rel_disp_err_vs_fp64_oracle": float(np.abs(U_dev - u_ref).max() / np.abs(u_ref).max()),
+                  "same_free_set": bool(np.array_equal(free_ref, st["free"])),
+                  "oracle": "CPU restatement: oracle partition and ordering, supernodal FP64 Cholesky (OpenBLAS)"}
         cpu = {"value": 1.0 / r["total_s"], "unit": "solves/s", "cores": nthreads, "kind": "port",
-               "sample": f"one full {cfg['workload']} SOL101 (assembly, sparse(), K_ff, supernodal Cholesky with "
-                         f"OpenBLAS, {cfg['subcases']} single-RHS solves); same ordering as the device",
+               "sample": f"one full {cfg['workload']} SOL101 (assembly, sparse(), partition, ordering, K_ff, "
+                         f"supernodal Cholesky with OpenBLAS, {cfg['subcases']} single-RHS solves)",
                "stages_s": r}
     rep = reps[-1]
     tflops_factor = sym["flops"] / 1e12
@@ -340,6 +338,7 @@ def run_ours(args, rank, world, local_rank):
                                              "h2d_bytes_per_step": int(F.nbytes), "d2h_bytes_per_step": int(F.nbytes)},
             "gpu_launches": int(launches),
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+            "parity": parity,
             "detail": {"rel_residual": rep["rel_residual"], "ir_iters": rep["ir_iters"],
                        "fallback_used": rep["fallback_used"], "subcase_solves_per_s": value * nrhs,
                        "factor_tflop": tflops_factor, "factor_tflops_per_s": tflops_factor / (ms_step / 1000.0),

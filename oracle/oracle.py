@@ -21,7 +21,7 @@ _lib = None
 
 def build(force: bool = False) -> str:
     """Compile oracle_fem.cpp + oracle_chol.cpp into _build/liboracle.so."""
-    srcs = [os.path.join(HERE, f) for f in ("oracle_fem.cpp", "oracle_chol.cpp")]
+    srcs = [os.path.join(HERE, f) for f in ("oracle_fem.cpp", "oracle_chol.cpp", "oracle_order.cpp")]
     os.makedirs(os.path.dirname(LIB_PATH), exist_ok=True)
     if not force and os.path.exists(LIB_PATH):
         lib_m = os.path.getmtime(LIB_PATH)
@@ -53,6 +53,12 @@ def lib():
             getattr(L, name).restype = ctypes.c_int
         L.or_chol_factor_solve.argtypes = [i64, P, P, P, P, i32, P, P, i32, P]
         L.or_chol_factor_solve.restype = ctypes.c_int
+        L.or_chol_counts.argtypes = [i64, P, P, P, P]
+        L.or_chol_counts.restype = ctypes.c_int
+        L.or_amd_order.argtypes = [i32, P, P, P, P]
+        L.or_amd_order.restype = ctypes.c_int
+        L.or_nd_order.argtypes = [i32, P, P, P, P, i32, P]
+        L.or_nd_order.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -146,59 +152,170 @@ def csc_matrix(asm):
 # Partition (boundary_conditions.jl:1028-1138 diagonal AUTOSPC, :745-845 GPST)
 # ----------------------------------------------------------------------------
 
+def node_blocks(K, n_nodes: int) -> np.ndarray:
+    """(n_nodes, 2, 3, 3): every grid's translational and rotational 3x3
+    diagonal blocks of K (row, column)."""
+    Kc = K.tocsc()
+    out = np.zeros((n_nodes, 2, 3, 3))
+    base = 6 * np.arange(n_nodes)
+    for off in (0, 1):
+        for a in range(3):
+            for b in range(3):
+                out[:, off, a, b] = np.asarray(Kc[base + 3 * off + a, base + 3 * off + b]).ravel()
+    return out
+
+
+def _gpst_claim(vals, vecs, loc, eps_zero):
+    """The DOFs (positions in loc) that the singular eigenvalues of one block
+    fix: each eigenvalue below eps_zero * max|eigenvalue| claims the unclaimed
+    DOF its eigenvector lies closest to (ties to the lowest DOF)."""
+    lam = np.max(np.abs(vals))
+    if not lam > 0:
+        return []
+    claimed = []
+    for k in range(len(loc)):
+        if not abs(vals[k]) / lam < eps_zero:
+            continue
+        best_a, best_w = -1, -1.0
+        for ii in range(len(loc)):
+            if ii in claimed:
+                continue
+            w = abs(vecs[ii, k])
+            if w > best_w + 1e-12:
+                best_w, best_a = w, ii
+        if best_a >= 0:
+            claimed.append(best_a)
+    return claimed
+
+
 def partition(model, K, eps_zero: float = 1e-8) -> Tuple[np.ndarray, np.ndarray, dict]:
     """Fixed set = SPC1 u zero-diagonal AUTOSPC u grid-point singularities.
 
     With grid-point-singularity processing on (the reference default) the
-    diagonal pass fixes exact zeros only; GPST then eigen-decomposes every
-    node's free 3x3 translational / rotational block and fixes the DOF the
-    eigenvector of each eigenvalue below eps_zero * lambda_max lies closest to.
+    diagonal pass fixes exact zeros only (boundary_conditions.jl:1028-1138);
+    GPST then eigen-decomposes every grid's free 3x3 translational /
+    rotational block and fixes the DOF the eigenvector of each eigenvalue
+    below eps_zero * lambda_max lies closest to (:745-845).  Full blocks are
+    decomposed in one batched call, partly fixed ones one by one.
     Returns (free_dofs ascending, fixed_dofs ascending, diagnostics).
     """
     n = model.ndof
+    nn = n // 6
     fixed = np.zeros(n, bool)
     fixed[model.spc_dofs()] = True
     diag = np.asarray(K.diagonal()).copy()
     zero = (~fixed) & (diag == 0.0)
     fixed |= zero
+    blocks = node_blocks(K, nn)
+    fx = fixed.reshape(nn, 2, 3).copy()
     n_gpst = 0
-    Kc = K.tocsc()
-    nn = n // 6
-    for node in range(nn):
-        base = 6 * node
-        for off in (0, 3):
-            loc = [a for a in range(3) if not fixed[base + off + a]]
-            if not loc:
-                continue
-            idx = [base + off + a for a in loc]
-            blk = Kc[idx][:, idx].toarray()
-            S = 0.5 * (blk + blk.T)
-            vals, vecs = np.linalg.eigh(S)
-            lam = np.max(np.abs(vals))
-            if not lam > 0:
-                continue
-            claimed = set()
-            for k in range(len(loc)):
-                ratio = abs(vals[k]) / lam
-                if not ratio < eps_zero:
-                    continue
-                best_a, best_w = -1, -1.0
-                for ii, a in enumerate(loc):
-                    w = abs(vecs[ii, k])
-                    if a in claimed:
-                        continue
-                    if w > best_w + 1e-12:
-                        best_w, best_a = w, a
-                if best_a < 0:
-                    continue
-                g = base + off + best_a
-                if fixed[g]:
-                    continue
-                claimed.add(best_a)
-                fixed[g] = True
-                n_gpst += 1
+    for off in (0, 1):
+        free_blk = ~fx[:, off, :]
+        full = np.where(free_blk.all(axis=1))[0]
+        if len(full):
+            S = blocks[full, off]
+            vals, vecs = np.linalg.eigh(0.5 * (S + S.transpose(0, 2, 1)))
+            lam = np.abs(vals).max(axis=1)
+            sing = ((np.abs(vals) / np.where(lam > 0, lam, 1.0)[:, None]) < eps_zero) & (lam > 0)[:, None]
+            for r in np.where(sing.any(axis=1))[0]:
+                for a in _gpst_claim(vals[r], vecs[r], [0, 1, 2], eps_zero):
+                    fixed[6 * full[r] + 3 * off + a] = True
+                    n_gpst += 1
+        for node in np.where(free_blk.any(axis=1) & ~free_blk.all(axis=1))[0]:
+            loc = [a for a in range(3) if free_blk[node, a]]
+            blk = blocks[node, off][np.ix_(loc, loc)]
+            vals, vecs = np.linalg.eigh(0.5 * (blk + blk.T))
+            for ii in _gpst_claim(vals, vecs, loc, eps_zero):
+                g = 6 * node + 3 * off + loc[ii]
+                if not fixed[g]:
+                    fixed[g] = True
+                    n_gpst += 1
     free = np.where(~fixed)[0].astype(np.int32)
     return free, np.where(fixed)[0], {"autospc_zero": int(zero.sum()), "autospc_gpst": n_gpst}
+
+
+# ----------------------------------------------------------------------------
+# Fill-reducing ordering of K_ff (what CHOLMOD chooses inside cholesky())
+# ----------------------------------------------------------------------------
+
+def grid_graph(Kff, free: np.ndarray):
+    """Grid-point graph of K_ff: one vertex per grid with free DOFs (weight =
+    its free DOFs), an edge where two grids share a nonzero block.
+    Returns (ptr, adj, weights, grid of each vertex, vertex of each free DOF)."""
+    free = np.asarray(free, np.int64)
+    grid = free // 6
+    ugrid, vert_of = np.unique(grid, return_inverse=True)
+    Kc = Kff.tocsc()
+    cols = np.repeat(np.arange(Kc.shape[1]), np.diff(Kc.indptr))
+    a = vert_of[Kc.indices].astype(np.int64)
+    b = vert_of[cols].astype(np.int64)
+    keep = a != b
+    nv = len(ugrid)
+    code = np.unique(a[keep] * nv + b[keep])
+    src, dst = code // nv, code % nv
+    both = np.unique(np.concatenate([src * nv + dst, dst * nv + src]))
+    src, dst = both // nv, both % nv
+    ptr = np.zeros(nv + 1, np.int64)
+    np.add.at(ptr, src + 1, 1)
+    ptr = np.cumsum(ptr)
+    wt = np.bincount(vert_of, minlength=nv).astype(np.int32)
+    return ptr, dst.astype(np.int32), wt, ugrid, vert_of
+
+
+def chol_counts(Kff, perm) -> dict:
+    """nnz(L) and flops (sum of squared column counts) of Symmetric(K_ff) in order perm."""
+    Kc = Kff.tocsc()
+    info = np.zeros(3)
+    st = lib().or_chol_counts(Kc.shape[0], _p(np.ascontiguousarray(Kc.indptr, np.int64)),
+                              _p(np.ascontiguousarray(Kc.indices, np.int32)),
+                              _p(np.ascontiguousarray(perm, np.int32)), _p(info))
+    if st != 0:
+        raise ValueError("bad permutation")
+    return {"nnz_L": float(info[0]), "flops": float(info[1]), "nnz_A_lower": float(info[2])}
+
+
+def order(Kff, free, xyz, method: str = "cholmod", leaf: int = 64):
+    """Elimination order of K_ff's unknowns: perm[k] = position in `free` of
+    the k-th eliminated unknown (a grid's DOFs stay together, ascending).
+
+    method "amd": approximate minimum degree; "nd": nested dissection by
+    coordinate bisection; "cholmod": CHOLMOD's default rule -- take AMD, and
+    when its factor is poor (nnz(L) >= 5 nnz(A) and flops >= 500 nnz(L)) also
+    try nested dissection and keep the ordering with the fewer nonzeros in L.
+    Returns (perm, info dict with the method used, nnz_L and flops).
+    """
+    L = lib()
+    ptr, adj, wt, ugrid, vert_of = grid_graph(Kff, free)
+    nv = len(ugrid)
+
+    def expand(vorder):
+        rank = np.empty(nv, np.int64)
+        rank[vorder] = np.arange(nv)
+        # DOFs by their grid's rank, ascending DOF within a grid
+        return np.lexsort((np.arange(len(free)), rank[vert_of])).astype(np.int32)
+
+    def run(m):
+        vo = np.empty(nv, np.int32)
+        if m == "amd":
+            st = L.or_amd_order(nv, _p(ptr), _p(adj), _p(wt), _p(vo))
+        else:
+            X = np.ascontiguousarray(np.asarray(xyz, float)[ugrid])
+            st = L.or_nd_order(nv, _p(ptr), _p(adj), _p(wt), _p(X), int(leaf), _p(vo))
+        if st != 0:
+            raise RuntimeError(f"oracle ordering {m} failed")
+        perm = expand(vo)
+        info = chol_counts(Kff, perm)
+        info["method"] = m
+        return perm, info
+
+    if method in ("amd", "nd"):
+        return run(method)
+    perm, info = run("amd")
+    if info["nnz_L"] >= 5 * info["nnz_A_lower"] and info["flops"] >= 500 * info["nnz_L"]:
+        perm2, info2 = run("nd")
+        if info2["nnz_L"] < info["nnz_L"]:
+            return perm2, info2
+    return perm, info
 
 
 # ----------------------------------------------------------------------------

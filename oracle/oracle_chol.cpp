@@ -113,29 +113,19 @@ void syrk_ln(int n, int k, const double* A, int lda, double* C, int ldc) {
     }
 }
 
-}  // namespace
-
-extern "C" {
-
-// n: order of K_ff.  CSC (colptr, rowval, nzval) of K_ff; only entries with
-// row <= col are read (Symmetric(K_ff, :U)).  perm[k] = unknown eliminated
-// k-th.  F, U: n x nrhs column-major.  info[0..3] = factor seconds, solve
-// seconds, nnz(L), flops (sum c_j^2).  Returns 0, or -1 (bad input), or
-// k+1 (first non-positive pivot in permuted column k).
-int or_chol_factor_solve(int64_t n, const int64_t* colptr, const int32_t* rowval,
-                         const double* nzval, const int32_t* perm, int32_t nrhs,
-                         const double* F, double* U, int32_t nthreads, double* info) {
-  using clk = std::chrono::steady_clock;
-  Blas& bl = blas();
-  if (bl.ok && bl.set_threads) bl.set_threads(nthreads > 0 ? nthreads : 1);
-  auto t0 = clk::now();
+// Permuted lower triangle of Symmetric(K_ff, :U) (lp/li/lv, CSC by column),
+// Liu's elimination tree and the column counts of L by row subtrees.
+// Returns 0, or -1 for a bad permutation.
+int symbolic_counts(int64_t n, const int64_t* colptr, const int32_t* rowval, const double* nzval,
+                    const int32_t* perm, std::vector<int64_t>& lp, std::vector<int32_t>& li,
+                    std::vector<double>& lv, std::vector<int32_t>& parent, std::vector<int64_t>& cc) {
   std::vector<int32_t> iperm(n);
   for (int64_t k = 0; k < n; ++k) {
     if (perm[k] < 0 || perm[k] >= n) return -1;
     iperm[perm[k]] = (int32_t)k;
   }
   // permuted lower triangle, CSC by column
-  std::vector<int64_t> lp(n + 1, 0);
+  lp.assign(n + 1, 0);
   for (int64_t j = 0; j < n; ++j)
     for (int64_t p = colptr[j]; p < colptr[j + 1]; ++p) {
       int64_t i = rowval[p];
@@ -144,8 +134,8 @@ int or_chol_factor_solve(int64_t n, const int64_t* colptr, const int32_t* rowval
       lp[std::min(a, b) + 1]++;
     }
   for (int64_t j = 0; j < n; ++j) lp[j + 1] += lp[j];
-  std::vector<int32_t> li(lp[n]);
-  std::vector<double> lv(lp[n]);
+  li.assign(lp[n], 0);
+  lv.assign(nzval ? lp[n] : 0, 0.0);
   {
     std::vector<int64_t> pos(lp.begin(), lp.end() - 1);
     for (int64_t j = 0; j < n; ++j)
@@ -155,7 +145,8 @@ int or_chol_factor_solve(int64_t n, const int64_t* colptr, const int32_t* rowval
         int64_t a = iperm[i], b = iperm[j];
         int64_t c = std::min(a, b), r = std::max(a, b);
         li[pos[c]] = (int32_t)r;
-        lv[pos[c]++] = nzval[p];
+        if (nzval) lv[pos[c]] = nzval[p];
+        pos[c]++;
       }
   }
   // elimination tree (Liu) from the row structure: for column j, the rows
@@ -171,7 +162,8 @@ int or_chol_factor_solve(int64_t n, const int64_t* colptr, const int32_t* rowval
     for (int64_t j = 0; j < n; ++j)
       for (int64_t p = lp[j]; p < lp[j + 1]; ++p) rj[pos[li[p]]++] = (int32_t)j;
   }
-  std::vector<int32_t> parent(n, -1), anc(n, -1);
+  parent.assign(n, -1);
+  std::vector<int32_t> anc(n, -1);
   for (int64_t i = 0; i < n; ++i)
     for (int64_t p = rp[i]; p < rp[i + 1]; ++p) {
       int64_t j = rj[p];
@@ -184,7 +176,7 @@ int or_chol_factor_solve(int64_t n, const int64_t* colptr, const int32_t* rowval
       }
     }
   // column counts via row subtrees
-  std::vector<int64_t> cc(n, 1);
+  cc.assign(n, 1);
   std::vector<int64_t> mark(n, -1);
   for (int64_t i = 0; i < n; ++i) {
     mark[i] = i;
@@ -198,6 +190,45 @@ int or_chol_factor_solve(int64_t n, const int64_t* colptr, const int32_t* rowval
       }
     }
   }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+// n: order of K_ff.  CSC (colptr, rowval, nzval) of K_ff; only entries with
+// row <= col are read (Symmetric(K_ff, :U)).  perm[k] = unknown eliminated
+// k-th.  F, U: n x nrhs column-major.  info[0..3] = factor seconds, solve
+// seconds, nnz(L), flops (sum c_j^2).  Returns 0, or -1 (bad input), or
+// k+1 (first non-positive pivot in permuted column k).
+// Symbolic counts of the factor of Symmetric(K_ff) in the elimination order
+// perm: info[0] = nnz(L) (incl. diagonal), info[1] = flops (sum_j c_j^2),
+// info[2] = nnz of the lower triangle of K_ff.  Returns 0 or -1.
+int or_chol_counts(int64_t n, const int64_t* colptr, const int32_t* rowval, const int32_t* perm, double* info) {
+  std::vector<int64_t> lp, cc;
+  std::vector<int32_t> li, parent;
+  std::vector<double> lv;
+  if (symbolic_counts(n, colptr, rowval, nullptr, perm, lp, li, lv, parent, cc) != 0) return -1;
+  double nnzL = 0, flops = 0;
+  for (int64_t j = 0; j < n; ++j) { nnzL += (double)cc[j]; flops += (double)cc[j] * (double)cc[j]; }
+  info[0] = nnzL;
+  info[1] = flops;
+  info[2] = (double)lp[n];
+  return 0;
+}
+
+int or_chol_factor_solve(int64_t n, const int64_t* colptr, const int32_t* rowval,
+                         const double* nzval, const int32_t* perm, int32_t nrhs,
+                         const double* F, double* U, int32_t nthreads, double* info) {
+  using clk = std::chrono::steady_clock;
+  Blas& bl = blas();
+  if (bl.ok && bl.set_threads) bl.set_threads(nthreads > 0 ? nthreads : 1);
+  auto t0 = clk::now();
+  std::vector<int64_t> lp, cc;
+  std::vector<int32_t> li, parent;
+  std::vector<double> lv;
+  if (symbolic_counts(n, colptr, rowval, nzval, perm, lp, li, lv, parent, cc) != 0) return -1;
   std::vector<int32_t> nchild(n, 0);
   for (int64_t j = 0; j < n; ++j)
     if (parent[j] >= 0) nchild[parent[j]]++;
