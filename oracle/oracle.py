@@ -32,9 +32,22 @@ def build(force: bool = False) -> str:
     return LIB_PATH
 
 
+def _default_openblas():
+    """SciPy's bundled OpenBLAS (the checker's dense kernels), if present."""
+    import glob
+    try:
+        import scipy
+    except ImportError:
+        return None
+    c = glob.glob(os.path.join(os.path.dirname(scipy.__file__), "..", "scipy.libs", "libscipy_openblas-*.so"))
+    return os.path.abspath(c[0]) if c else None
+
+
 def lib():
     global _lib
     if _lib is None:
+        if "JFEM_ORACLE_OPENBLAS" not in os.environ and _default_openblas():
+            os.environ["JFEM_ORACLE_OPENBLAS"] = _default_openblas()
         build()
         L = ctypes.CDLL(LIB_PATH)
         d, i32, i64 = ctypes.c_double, ctypes.c_int32, ctypes.c_int64
@@ -53,6 +66,14 @@ def lib():
             getattr(L, name).restype = ctypes.c_int
         L.or_chol_factor_solve.argtypes = [i64, P, P, P, P, i32, P, P, i32, P]
         L.or_chol_factor_solve.restype = ctypes.c_int
+        L.or_chol_factor.argtypes = [i64, P, P, P, P, i32, ctypes.POINTER(P)]
+        L.or_chol_factor.restype = ctypes.c_int
+        L.or_chol_solve.argtypes = [P, i32, P, P]
+        L.or_chol_solve.restype = ctypes.c_int
+        L.or_chol_free.argtypes = [P]
+        L.or_chol_free.restype = None
+        L.or_csc_residual_dd.argtypes = [i64, i64, P, P, P, i32, P, P, P]
+        L.or_csc_residual_dd.restype = None
         L.or_chol_counts.argtypes = [i64, P, P, P, P]
         L.or_chol_counts.restype = ctypes.c_int
         L.or_amd_order.argtypes = [i32, P, P, P, P]
@@ -404,6 +425,76 @@ def solve_reference(model, asm=None, free=None):
     R = K @ u - F
     rel = np.linalg.norm(Kff @ u_ff - F[free], axis=0) / np.maximum(np.linalg.norm(F[free], axis=0), 1e-300)
     return dict(u=u, F=F, R=R, free=free, rel_residual=rel, asm=asm)
+
+
+def residual_dd(A, x, f) -> np.ndarray:
+    """f - A x, accumulated per row in double-double (compensated) arithmetic."""
+    A = A.tocsc()
+    x = np.asfortranarray(x, np.float64)
+    f = np.asfortranarray(f, np.float64)
+    if x.ndim == 1:
+        x, f = x[:, None], f[:, None]
+    r = np.zeros_like(f, order="F")
+    lib().or_csc_residual_dd(A.shape[0], A.shape[1], _p(np.ascontiguousarray(A.indptr, np.int64)),
+                             _p(np.ascontiguousarray(A.indices, np.int32)),
+                             _p(np.ascontiguousarray(A.data, np.float64)), x.shape[1], _p(x), _p(f), _p(r))
+    return r
+
+
+class CholFactor:
+    """The oracle's supernodal FP64 Cholesky of Symmetric(K_ff), factored once."""
+
+    def __init__(self, Kff, perm, nthreads: int = 0):
+        Kc = Kff.tocsc()
+        self.n = Kc.shape[0]
+        self.h = ctypes.c_void_p()
+        st = lib().or_chol_factor(self.n, _p(np.ascontiguousarray(Kc.indptr, np.int64)),
+                                  _p(np.ascontiguousarray(Kc.indices, np.int32)),
+                                  _p(np.ascontiguousarray(Kc.data, np.float64)),
+                                  _p(np.ascontiguousarray(perm, np.int32)), int(nthreads), ctypes.byref(self.h))
+        if st != 0:
+            raise RuntimeError(f"oracle cholesky failed: status {st}")
+
+    def solve(self, F):
+        F = np.asfortranarray(F, np.float64)
+        one = F.ndim == 1
+        if one:
+            F = F[:, None]
+        U = np.zeros_like(F, order="F")
+        lib().or_chol_solve(self.h, F.shape[1], _p(F), _p(U))
+        return U[:, 0] if one else U
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_chol_free(self.h)
+            self.h = None
+
+
+def solve_reference_chol(model, nthreads: int = 0, refine: int = 6):
+    """FP64 SOL101 on the CPU for large checks: the oracle's partition and
+    ordering, its supernodal Cholesky (OpenBLAS), and refinement on the
+    assembled K_ff with compensated residuals, so that the checker's
+    displacements are accurate to about the conditioning of the FP64 data.
+    Returns dict(u (ndof x nrhs), F, R = K u - F, free, rel_residual)."""
+    asm = assemble(model)
+    K = csc_matrix(asm)
+    free, _, _ = partition(model, K)
+    Kff = K[free][:, free].tocsc()
+    perm, _ = order(Kff, free, model.xyz)
+    F = load_matrix(model)
+    Fff = np.asfortranarray(F[free])
+    C = CholFactor(Kff, perm, nthreads)
+    u_ff = C.solve(Fff)
+    fn = np.maximum(np.linalg.norm(Fff, axis=0), 1e-300)
+    for _ in range(refine):
+        r = residual_dd(Kff, u_ff, Fff)
+        if np.all(np.linalg.norm(r, axis=0) <= 1e-16 * fn):
+            break
+        u_ff = u_ff + C.solve(r)
+    u = np.zeros_like(F)
+    u[free] = u_ff
+    rel = np.linalg.norm(residual_dd(Kff, u_ff, Fff), axis=0) / fn
+    return dict(u=u, F=F, R=K @ u - F, free=free, rel_residual=rel)
 
 
 def chol_solve(n, colptr, rowval, nzval, perm, F, nthreads=0):

@@ -193,38 +193,21 @@ int symbolic_counts(int64_t n, const int64_t* colptr, const int32_t* rowval, con
   return 0;
 }
 
-}  // namespace
-
-extern "C" {
-
-// n: order of K_ff.  CSC (colptr, rowval, nzval) of K_ff; only entries with
-// row <= col are read (Symmetric(K_ff, :U)).  perm[k] = unknown eliminated
-// k-th.  F, U: n x nrhs column-major.  info[0..3] = factor seconds, solve
-// seconds, nnz(L), flops (sum c_j^2).  Returns 0, or -1 (bad input), or
-// k+1 (first non-positive pivot in permuted column k).
-// Symbolic counts of the factor of Symmetric(K_ff) in the elimination order
-// perm: info[0] = nnz(L) (incl. diagonal), info[1] = flops (sum_j c_j^2),
-// info[2] = nnz of the lower triangle of K_ff.  Returns 0 or -1.
-int or_chol_counts(int64_t n, const int64_t* colptr, const int32_t* rowval, const int32_t* perm, double* info) {
-  std::vector<int64_t> lp, cc;
-  std::vector<int32_t> li, parent;
-  std::vector<double> lv;
-  if (symbolic_counts(n, colptr, rowval, nullptr, perm, lp, li, lv, parent, cc) != 0) return -1;
+struct CholFactor {
+  int64_t n = 0, ns = 0;
+  std::vector<int32_t> perm;
+  std::vector<int64_t> sfirst;
+  std::vector<std::vector<int32_t>> srows;
+  std::vector<std::vector<double>> panel;
   double nnzL = 0, flops = 0;
-  for (int64_t j = 0; j < n; ++j) { nnzL += (double)cc[j]; flops += (double)cc[j] * (double)cc[j]; }
-  info[0] = nnzL;
-  info[1] = flops;
-  info[2] = (double)lp[n];
-  return 0;
-}
+};
 
-int or_chol_factor_solve(int64_t n, const int64_t* colptr, const int32_t* rowval,
-                         const double* nzval, const int32_t* perm, int32_t nrhs,
-                         const double* F, double* U, int32_t nthreads, double* info) {
-  using clk = std::chrono::steady_clock;
+// Symbolic analysis and numeric multifrontal factorisation into C.
+// Returns 0, -1 (bad input) or k+1 (first non-positive pivot in column k).
+int factor_into(CholFactor& C, int64_t n, const int64_t* colptr, const int32_t* rowval, const double* nzval,
+                const int32_t* perm, int32_t nthreads) {
   Blas& bl = blas();
   if (bl.ok && bl.set_threads) bl.set_threads(nthreads > 0 ? nthreads : 1);
-  auto t0 = clk::now();
   std::vector<int64_t> lp, cc;
   std::vector<int32_t> li, parent;
   std::vector<double> lv;
@@ -233,7 +216,8 @@ int or_chol_factor_solve(int64_t n, const int64_t* colptr, const int32_t* rowval
   for (int64_t j = 0; j < n; ++j)
     if (parent[j] >= 0) nchild[parent[j]]++;
   // fundamental supernodes
-  std::vector<int64_t> sfirst;
+  std::vector<int64_t>& sfirst = C.sfirst;
+  sfirst.clear();
   for (int64_t j = 0; j < n; ++j) {
     bool merge = j > 0 && parent[j - 1] == j && cc[j - 1] == cc[j] + 1 && nchild[j] == 1;
     if (!merge) sfirst.push_back(j);
@@ -252,7 +236,8 @@ int or_chol_factor_solve(int64_t n, const int64_t* colptr, const int32_t* rowval
   for (int64_t s = 0; s < ns; ++s)
     if (sparent[s] >= 0) schildren[sparent[s]].push_back((int32_t)s);
   // supernode row structures (rows below the supernode), bottom-up
-  std::vector<std::vector<int32_t>> srows(ns);
+  std::vector<std::vector<int32_t>>& srows = C.srows;
+  srows.assign(ns, {});
   std::vector<int64_t> fmark(n, -1);
   double flops = 0;
   int64_t nnzL = 0;
@@ -276,7 +261,8 @@ int or_chol_factor_solve(int64_t n, const int64_t* colptr, const int32_t* rowval
     nnzL += c * (c + 1) / 2 + c * r;
   }
   // numeric multifrontal
-  std::vector<std::vector<double>> panel(ns);   // m x c, ld = m
+  std::vector<std::vector<double>>& panel = C.panel;   // m x c, ld = m
+  panel.assign(ns, {});
   std::vector<std::vector<double>> upd(ns);     // r x r
   std::vector<int64_t> rowpos(n, -1);
   for (int64_t s = 0; s < ns; ++s) {
@@ -307,7 +293,6 @@ int or_chol_factor_solve(int64_t n, const int64_t* colptr, const int32_t* rowval
     int ci = (int)c, mi = (int)m, ri = (int)r;
     potrf_lower(ci, front.data(), mi, &info_p);
     if (info_p != 0) {
-      info[0] = std::chrono::duration<double>(clk::now() - t0).count();
       return (int)(f + info_p);
     }
     if (r > 0) {
@@ -320,8 +305,22 @@ int or_chol_factor_solve(int64_t n, const int64_t* colptr, const int32_t* rowval
     }
     panel[s].assign(front.begin(), front.begin() + m * c);
   }
-  auto t1 = clk::now();
-  // solves, one right-hand side at a time (boundary_conditions.jl:1714)
+  C.n = n;
+  C.ns = ns;
+  C.perm.assign(perm, perm + n);
+  C.nnzL = (double)nnzL;
+  C.flops = flops;
+  return 0;
+}
+
+// Forward and backward substitution with C, one right-hand side at a time
+// (boundary_conditions.jl:1714).
+void solve_with(const CholFactor& C, int32_t nrhs, const double* F, double* U) {
+  const int64_t n = C.n, ns = C.ns;
+  const int32_t* perm = C.perm.data();
+  const std::vector<int64_t>& sfirst = C.sfirst;
+  const std::vector<std::vector<int32_t>>& srows = C.srows;
+  const std::vector<std::vector<double>>& panel = C.panel;
   std::vector<double> x(n);
   for (int32_t q = 0; q < nrhs; ++q) {
     for (int64_t k = 0; k < n; ++k) x[k] = F[(int64_t)q * n + perm[k]];
@@ -351,12 +350,65 @@ int or_chol_factor_solve(int64_t n, const int64_t* colptr, const int32_t* rowval
     }
     for (int64_t k = 0; k < n; ++k) U[(int64_t)q * n + perm[k]] = x[k];
   }
-  auto t2 = clk::now();
-  info[0] = std::chrono::duration<double>(t1 - t0).count();
-  info[1] = std::chrono::duration<double>(t2 - t1).count();
-  info[2] = (double)nnzL;
-  info[3] = flops;
+}
+
+}  // namespace
+
+extern "C" {
+
+// n: order of K_ff.  CSC (colptr, rowval, nzval) of K_ff; only entries with
+// row <= col are read (Symmetric(K_ff, :U)).  perm[k] = unknown eliminated
+// k-th.  F, U: n x nrhs column-major.  info[0..3] = factor seconds, solve
+// seconds, nnz(L), flops (sum c_j^2).  Returns 0, or -1 (bad input), or
+// k+1 (first non-positive pivot in permuted column k).
+// Symbolic counts of the factor of Symmetric(K_ff) in the elimination order
+// perm: info[0] = nnz(L) (incl. diagonal), info[1] = flops (sum_j c_j^2),
+// info[2] = nnz of the lower triangle of K_ff.  Returns 0 or -1.
+int or_chol_counts(int64_t n, const int64_t* colptr, const int32_t* rowval, const int32_t* perm, double* info) {
+  std::vector<int64_t> lp, cc;
+  std::vector<int32_t> li, parent;
+  std::vector<double> lv;
+  if (symbolic_counts(n, colptr, rowval, nullptr, perm, lp, li, lv, parent, cc) != 0) return -1;
+  double nnzL = 0, flops = 0;
+  for (int64_t j = 0; j < n; ++j) { nnzL += (double)cc[j]; flops += (double)cc[j] * (double)cc[j]; }
+  info[0] = nnzL;
+  info[1] = flops;
+  info[2] = (double)lp[n];
   return 0;
 }
+
+int or_chol_factor_solve(int64_t n, const int64_t* colptr, const int32_t* rowval,
+                         const double* nzval, const int32_t* perm, int32_t nrhs,
+                         const double* F, double* U, int32_t nthreads, double* info) {
+  using clk = std::chrono::steady_clock;
+  auto t0 = clk::now();
+  CholFactor C;
+  int st = factor_into(C, n, colptr, rowval, nzval, perm, nthreads);
+  auto t1 = clk::now();
+  info[0] = std::chrono::duration<double>(t1 - t0).count();
+  if (st != 0) return st;
+  solve_with(C, nrhs, F, U);
+  auto t2 = clk::now();
+  info[1] = std::chrono::duration<double>(t2 - t1).count();
+  info[2] = C.nnzL;
+  info[3] = C.flops;
+  return 0;
+}
+
+// Factor once, solve many times (the checker's iterative refinement).
+int or_chol_factor(int64_t n, const int64_t* colptr, const int32_t* rowval, const double* nzval,
+                   const int32_t* perm, int32_t nthreads, void** handle) {
+  CholFactor* C = new CholFactor();
+  int st = factor_into(*C, n, colptr, rowval, nzval, perm, nthreads);
+  if (st != 0) { delete C; *handle = nullptr; return st; }
+  *handle = C;
+  return 0;
+}
+int or_chol_solve(void* handle, int32_t nrhs, const double* F, double* U) {
+  if (!handle) return -1;
+  solve_with(*static_cast<CholFactor*>(handle), nrhs, F, U);
+  return 0;
+}
+void or_chol_free(void* handle) { delete static_cast<CholFactor*>(handle); }
 
 }  // extern "C"

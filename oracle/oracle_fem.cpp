@@ -960,6 +960,35 @@ int64_t or_build_csc(int64_t n, int64_t nt, const int64_t* I, const int64_t* J,
 }
 
 // y = K x for CSC K (ndof x ndof), x/y column-major with nrhs columns.
+// r = f - A x in double-double arithmetic (Knuth two-sum, FMA two-product)
+// per row: the checker's refinement residual carries only the final rounding,
+// so refinement can reach the accuracy of the FP64 data even where the row
+// sums of a stiffness matrix cancel.  A is m x n in CSC; f, r: m x nrhs.
+void or_csc_residual_dd(int64_t m, int64_t n, const int64_t* colptr, const int32_t* rowval,
+                        const double* nzval, int32_t nrhs, const double* x, const double* f, double* r) {
+  std::vector<double> hi(m), lo(m);
+  for (int32_t c = 0; c < nrhs; ++c) {
+    const double* xc = x + (int64_t)c * n;
+    const double* fc = f + (int64_t)c * m;
+    for (int64_t i = 0; i < m; ++i) { hi[i] = -fc[i]; lo[i] = 0.0; }
+    for (int64_t j = 0; j < n; ++j) {
+      const double xj = xc[j];
+      for (int64_t p = colptr[j]; p < colptr[j + 1]; ++p) {
+        const int64_t i = rowval[p];
+        const double prod = nzval[p] * xj;
+        const double perr = std::fma(nzval[p], xj, -prod);
+        const double s = hi[i] + prod;
+        const double bp = s - hi[i];
+        const double serr = (hi[i] - (s - bp)) + (prod - bp);
+        hi[i] = s;
+        lo[i] += serr + perr;
+      }
+    }
+    double* rc = r + (int64_t)c * m;
+    for (int64_t i = 0; i < m; ++i) rc[i] = -(hi[i] + lo[i]);
+  }
+}
+
 void or_csc_matvec(int64_t n, const int64_t* colptr, const int32_t* rowval,
                    const double* nzval, int32_t nrhs, const double* x, double* y) {
   for (int32_t c = 0; c < nrhs; ++c) {

@@ -290,3 +290,113 @@ def test_dmma_front_update_matches_simt(ctx, monkeypatch):
     rel = np.abs(out["1"][0] - out["0"][0]) / np.abs(out["0"][0])
     assert rel.max() <= 1e-10, rel.max()
     assert _rel(out["1"][1], out["0"][1]) <= 1e-10
+
+
+LARGE = {
+    # 25^3 lattice of CTETRA10 grids, 45,000 free DOF
+    "solid_12": lambda: M.solid_block(n=12, n_cases=2),
+    # 80 x 120 skin + 9 blades of 8 x 120: 110,160 free DOF
+    "wing_110k": lambda: M.wing_panel(nx=80, ny=120, blade_nz=8, n_cases=3, seed=9),
+}
+
+
+@pytest.fixture(scope="module")
+def large_refs(oracle_mod):
+    return {}
+
+
+@pytest.mark.parametrize("name", sorted(LARGE))
+@pytest.mark.parametrize("prec", [lib.PREC_FP64, lib.PREC_MIXED])
+def test_sol101_large_against_oracle(ctx, oracle_mod, large_refs, name, prec):
+    """Displacements of a CTETRA10 block and a >100k-DOF stiffened panel
+    against the FP64 oracle (its own partition, ordering and supernodal
+    Cholesky, refined with compensated residuals): 1e-8 relative to the field
+    maximum for the FP64 and the mixed path, relative residual <= 1e-10."""
+    m = LARGE[name]()
+    if name not in large_refs:
+        large_refs[name] = oracle_mod.solve_reference_chol(m)
+    ref = large_refs[name]
+    be = B.JFEMGPUBackend(precision=prec, tol=RESID_TOL, max_ir=40)
+    be._ctx = ctx
+    res = B.solve_model(be, m)
+    assert np.array_equal(res["state"]["free"], ref["free"])
+    U = np.stack([s["raw_displacement"] for s in res["subcases"]], axis=1)
+    for sc in res["subcases"]:
+        assert sc["solver_diagnostics"]["linear_solver"]["rel_residual"] <= RESID_TOL
+    assert _rel(U, ref["u"]) <= DISP_RTOL
+    fixed = res["state"]["fixed"]
+    Rdev = res["state"]["dm"].residual(U, m.load_matrix())[fixed]
+    assert _rel(Rdev, ref["R"][fixed]) <= DISP_RTOL
+    res["state"]["dm"].close()
+
+
+def _soft_root_plate():
+    """A plate clamped along y = 0 through one row of elements 1e-3 times as
+    thick as the rest: every grid's own 3x3 blocks are well conditioned (no
+    AUTOSPC, no grid-point singularity), but the stiff part's rotations about
+    the root line are held only by the soft row's bending (thickness cubed,
+    1e-9), so in any elimination order two or three pivot ratios L_ii^2 / K_ii
+    come out near 1e-10 while the next smallest stays above 1e-3."""
+    m = M.flat_plate(nx=6, ny=6)
+    soft = np.where(m.xyz[m.q4_nodes[:, 0], 1] < 1e-12)[0]
+    m.q4_pid = m.q4_pid.copy()
+    m.q4_pid[soft] = 2
+    m.pshells[2] = M.PShell(T=2e-6, MID1=1, MID2=1, MID3=1)
+    clamp = np.where(m.xyz[:, 1] < 1e-12)[0]
+    m.spc1 = [("123456", clamp)]
+    return m
+
+
+def test_post_factor_pivot_check_refactors(ctx, oracle_mod):
+    """The post-factorisation singular-pivot check of boundary_conditions.jl:
+    1662-1710: DOFs whose pivot ratio L_ii^2 / K_ii falls below 1e-7 join the
+    fixed set and K_ff is factored again.  The refactored solve meets the
+    residual bar and matches the oracle on the same reduced free set."""
+    m = _soft_root_plate()
+    be = B.JFEMGPUBackend(tol=RESID_TOL)
+    be._ctx = ctx
+    res = B.solve_model(be, m)
+    st = res["state"]
+    n_sing = st["bc"]["post_factorization_singular_dofs"]
+    assert n_sing > 0
+    # the first factor's partition fixed only the SPC1 DOFs
+    assert len(st["fixed"]) == len(m.spc_dofs()) + n_sing
+    for sc in res["subcases"]:
+        assert sc["solver_diagnostics"]["linear_solver"]["rel_residual"] <= RESID_TOL
+    U = np.stack([s["raw_displacement"] for s in res["subcases"]], axis=1)
+    assert np.all(U[st["fixed"]] == 0.0)
+    ref = oracle_mod.solve_reference(m, free=st["free"])
+    assert _rel(U, ref["u"]) <= DISP_RTOL
+    st["dm"].close()
+
+
+def test_warped_quad4_is_refused(ctx):
+    """A warped CQUAD4 (grid out of the element plane) is outside the device's
+    flat-element path: UNSUPPORTED, with the index of an offending element."""
+    m = M.flat_plate(nx=4, ny=4)
+    centre = int(np.argmin(np.linalg.norm(m.xyz - [0.25, 0.25, 0.0], axis=1)))
+    m.xyz = m.xyz.copy()
+    m.xyz[centre, 2] = 1e-3
+    touching = set(np.where((m.q4_nodes == centre).any(axis=1))[0].tolist())
+    dm = lib.DeviceModel(ctx, m)
+    with pytest.raises(lib.JfgError) as e:
+        dm.assemble()
+    assert e.value.status_name == "UNSUPPORTED"
+    assert e.value.detail in touching
+    dm.close()
+
+
+def test_non_default_quad4_flags_are_refused(ctx):
+    """A PSHELL with blank MID3 selects the rigid transverse-shear route of the
+    reference (assembly.jl:2780-2787), which the device does not implement:
+    UNSUPPORTED with the index of an element of that property."""
+    m = M.flat_plate(nx=4, ny=4)
+    m.q4_pid = m.q4_pid.copy()
+    m.q4_pid[5:] = 2
+    m.pshells[2] = M.PShell(T=0.002, MID1=1, MID2=1, MID3=0)
+    dm = lib.DeviceModel(ctx, m)
+    with pytest.raises(lib.JfgError) as e:
+        dm.assemble()
+    assert e.value.status_name == "UNSUPPORTED"
+    assert e.value.detail >= 5
+    dm.close()
