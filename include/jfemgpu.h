@@ -162,6 +162,17 @@ jfg_status jfg_solve(jfg_model* model, int32_t nrhs, const double* F,
 jfg_status jfg_residual(jfg_model* model, int32_t nrhs, const double* U,
                         const double* F, double* R);
 
+/* Element stresses and strains from displacement fields U (ndof x nrhs,
+ * column-major, the node-frame displacements jfg_solve returns), the step
+ * after the solve in _build_results_from_state (solve_case.jl:182-303).
+ * kind 2 = CTETRA10, at the element centroid as recover_solid_stresses!
+ * (src/solver/stress_recovery.jl:1823-1960): out is nrhs x n_t10 records of
+ * 13 doubles (load case major): sxx syy szz txy tyz tzx, exx eyy ezz gxy gyz
+ * gzx (engineering shears), von Mises, in the basic frame.  Other kinds
+ * return JFG_UNSUPPORTED.                                                  */
+jfg_status jfg_recover_stresses(jfg_model* model, int32_t kind, int32_t nrhs,
+                                const double* U, double* out);
+
 /* Same as jfg_solve with F and U in DEVICE memory (ndof x nrhs, column-major). */
 jfg_status jfg_solve_device(jfg_model* model, int32_t nrhs, const double* F_dev,
                             double* U_dev, double tol, int32_t max_ir,

@@ -432,6 +432,31 @@ jfg_status jfg_residual(jfg_model* m, int32_t nrhs, const double* U, const doubl
   return JFG_OK;
 }
 
+jfg_status jfg_recover_stresses(jfg_model* m, int32_t kind, int32_t nrhs, const double* U, double* out) {
+  JFG_TRY(check_model(m));
+  if (nrhs <= 0 || !U || !out) { set_error("nrhs must be positive and U, out non-null"); return JFG_BAD_INPUT; }
+  if (kind != 2) { set_error("stress recovery is available for CTETRA10 (kind 2)"); return JFG_UNSUPPORTED; }
+  const int64_t len = m->ndof * (int64_t)nrhs, olen = 13 * m->n_t10 * (int64_t)nrhs;
+  if (olen == 0) return JFG_OK;
+  double *dU = nullptr, *dO = nullptr;
+  JFG_TRY(dev_alloc(m->ctx, (void**)&dU, 8 * len));
+  jfg_status st = dev_alloc(m->ctx, (void**)&dO, 8 * olen);
+  if (st) { dev_free(m->ctx, dU, 8 * len); return st; }
+  cudaStream_t s = m->ctx->stream;
+  cudaError_t e = cudaMemcpyAsync(dU, U, 8 * len, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) st = recover_t10_stresses(m, nrhs, dU, dO, s);
+  if (e == cudaSuccess && st == JFG_OK) e = cudaMemcpyAsync(out, dO, 8 * olen, cudaMemcpyDeviceToHost, s);
+  cudaError_t e2 = cudaStreamSynchronize(s);
+  dev_free(m->ctx, dU, 8 * len);
+  dev_free(m->ctx, dO, 8 * olen);
+  if (st != JFG_OK) return st;
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    set_error(cudaGetErrorString(e != cudaSuccess ? e : e2));
+    return JFG_CUDA_ERROR;
+  }
+  return read_elem_error(m);
+}
+
 jfg_status jfg_update_q4_sections(jfg_model* m, int64_t n, const int32_t* elems, const double* sect) {
   JFG_TRY(check_model(m));
   for (int64_t k = 0; k < n; ++k) {

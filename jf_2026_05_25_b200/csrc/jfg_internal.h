@@ -151,6 +151,8 @@ jfg_status numeric_factor(jfg_model* m, int precision);
 jfg_status numeric_solve(jfg_model* m, int nrhs, const double* hF, double* hU, double tol,
                          int max_ir, jfg_solve_report* rep, bool device_io);
 jfg_status numeric_factor_diag(jfg_model* m, double* out);
+// stress.cu
+jfg_status recover_t10_stresses(jfg_model* m, int nrhs, const double* U_dev, double* out_dev, cudaStream_t st);
 // memory
 jfg_status dev_alloc(jfg_ctx* c, void** p, size_t bytes);
 void dev_free(jfg_ctx* c, void* p, size_t bytes);

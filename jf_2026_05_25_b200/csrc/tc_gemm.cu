@@ -83,11 +83,7 @@ constexpr int UK = 16;
 #ifndef JFG_TC_STAGES
 #define JFG_TC_STAGES 4
 #endif
-#ifndef JFG_TC_DRAIN
-#define JFG_TC_DRAIN 1
-#endif
 constexpr int UST = JFG_TC_STAGES;
-constexpr int UDR = JFG_TC_DRAIN;               // K-slices per accumulator use
 constexpr int UDW = 8;                          // drain warps: 4 lane quarters x 2 column halves
 constexpr int UTHREADS = (UDW + 2) * 32;        // + producer warp + MMA warp
 #ifndef JFG_TC_SLOTS
@@ -156,7 +152,8 @@ k_update_tf32x3(const int32_t* __restrict__ list, const int32_t* __restrict__ fi
                 const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
                 const int64_t* __restrict__ Uptr, float* __restrict__ L, const float* __restrict__ Phi,
                 const float* __restrict__ Plo, const int64_t* __restrict__ PKptr, const float* __restrict__ zero,
-                float* __restrict__ U, int mode, int kbeg, int kend, int cend, int terms, DevError* err) {
+                float* __restrict__ U, int mode, int kbeg, int kend, int cend, int terms, int udr, DevError* err) {
+  const int UDR = udr;   // K-slices of 16 summed by the tensor core per accumulator use
   const int s = list[blockIdx.y];
   const int c = first[s + 1] - first[s];
   const int m = mrows[s];
@@ -248,10 +245,14 @@ k_update_tf32x3(const int32_t* __restrict__ list, const int32_t* __restrict__ fi
         issued = j + 1;
       }
       if (issued < nk && issued > 0) {
-        // gave up: let the copies already issued land before the CTA exits
-        const int l = issued - 1;
-        const long long t0 = clock64();
-        while (!mbar_try(smem_addr(&full[l % UST]), (uint32_t)((l / UST) & 1)) && clock64() - t0 < WAIT_CYCLES) {
+        // gave up: let every copy still in flight land before the CTA exits.
+        // The last UST issued slices are the latest use of each stage; wait
+        // for each at its own phase (bounded; a phase already complete
+        // returns at once)
+        for (int l = max(0, issued - UST); l < issued; ++l) {
+          const long long t0 = clock64();
+          while (!mbar_try(smem_addr(&full[l % UST]), (uint32_t)((l / UST) & 1)) && clock64() - t0 < WAIT_CYCLES) {
+          }
         }
       }
     }
@@ -388,10 +389,18 @@ bool front_update_tf32x3(const int32_t* list, int count, const int32_t* first, c
   }
   const char* te = std::getenv("JFG_TC_TERMS");   // 4: add lo*lo
   const int terms = (te && te[0] == '4') ? 4 : 3;
+  // K-slices of 16 columns the tensor core sums per accumulator use before
+  // the drain warps add them in FP32 registers (JFG_TC_DRAIN, 1..16)
+  static int udr = -1;
+  if (udr < 0) {
+    const char* de = std::getenv("JFG_TC_DRAIN");
+    udr = de ? std::atoi(de) : 1;
+    udr = udr < 1 ? 1 : (udr > 16 ? 16 : udr);
+  }
   const int ext = mode == 1 ? 7 : 0;              // the mode-1 grid starts up to 7 rows early
   const int64_t tiles = (int64_t)((max_rows + ext + UM - 1) / UM) * ((max_cols + ext + UM - 1) / UM);
   k_update_tf32x3<<<dim3((unsigned)tiles, (unsigned)count), UTHREADS, USMEM, st>>>(
-      list, first, mrows, Lptr, Uptr, L, Phi, Plo, PKptr, zero, U, mode, kbeg, kend, cend, terms, err);
+      list, first, mrows, Lptr, Uptr, L, Phi, Plo, PKptr, zero, U, mode, kbeg, kend, cend, terms, udr, err);
   count_launch();
   return cudaGetLastError() == cudaSuccess;
 }

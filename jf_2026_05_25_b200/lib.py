@@ -92,6 +92,7 @@ def load():
         "jfg_get_timings": [P, P],
         "jfg_symbolic_dry_run": [I64, P, P, I64, P, P, P, P],
         "jfg_assemble_values_noalloc": [P, P],
+        "jfg_recover_stresses": [P, I32, I32, P, P],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -286,6 +287,16 @@ class DeviceModel:
         nr = 1 if U.ndim == 1 else U.shape[1]
         _check(load().jfg_residual(self.h, nr, _p(U), _p(F), _p(R)))
         return R
+
+    def t10_stresses(self, U: np.ndarray) -> np.ndarray:
+        """Centroid stress, strain and von Mises of every CTETRA10 for every
+        column of U: array (nrhs, n_t10, 13)."""
+        U = np.asfortranarray(U, np.float64)
+        if U.ndim == 1:
+            U = U[:, None]
+        out = np.empty((U.shape[1], len(self.model.t10_nodes), 13))
+        _check(load().jfg_recover_stresses(self.h, 2, U.shape[1], _p(U), _p(out)))
+        return out
 
     def update_q4_sections(self, elems: np.ndarray, sect: np.ndarray):
         elems = np.ascontiguousarray(elems, np.int32)

@@ -72,6 +72,8 @@ def lib():
         L.or_chol_solve.restype = ctypes.c_int
         L.or_chol_free.argtypes = [P]
         L.or_chol_free.restype = None
+        L.or_t10_stress.argtypes = [P, P, d, d, P, P]
+        L.or_t10_stress.restype = ctypes.c_int
         L.or_csc_residual_dd.argtypes = [i64, i64, P, P, P, i32, P, P, P]
         L.or_csc_residual_dd.restype = None
         L.or_chol_counts.argtypes = [i64, P, P, P, P]
@@ -131,6 +133,32 @@ def t10_element(xyz, E, nu, nodeR=None):
     if st:
         raise ValueError(f"or_t10_element status {st}")
     return Ke
+
+
+def t10_stresses(model, U) -> np.ndarray:
+    """Centroid stress / strain / von Mises of every CTETRA10 for every column
+    of U (ndof x nrhs): array (nrhs, n_t10, 13) = sxx syy szz txy tyz tzx,
+    exx eyy ezz gxy gyz gzx, von Mises (stress_recovery.jl:1823-1960)."""
+    U = np.asarray(U, float)
+    if U.ndim == 1:
+        U = U[:, None]
+    L = lib()
+    nodes = np.asarray(model.t10_nodes)
+    mat = model.t10_materials()
+    R = np.asarray(model.node_R, float)
+    X = np.asarray(model.xyz, float)
+    out = np.zeros((U.shape[1], len(nodes), 13))
+    rec = np.zeros(13)
+    for k in range(U.shape[1]):
+        un = U[:, k].reshape(-1, 6)[:, :3]
+        for e in range(len(nodes)):
+            nd = nodes[e]
+            st = L.or_t10_stress(_p(np.ascontiguousarray(X[nd])), _p(np.ascontiguousarray(R[nd])),
+                                 float(mat[e, 0]), float(mat[e, 1]), _p(np.ascontiguousarray(un[nd])), _p(rec))
+            if st:
+                raise ValueError(f"element {e}: or_t10_stress status {st}")
+            out[k, e] = rec
+    return out
 
 
 def assemble(model):

@@ -960,6 +960,75 @@ int64_t or_build_csc(int64_t n, int64_t nt, const int64_t* I, const int64_t* J,
 }
 
 // y = K x for CSC K (ndof x ndof), x/y column-major with nrhs columns.
+// CTETRA10 centroid stress and strain (recover_solid_stresses!,
+// src/solver/stress_recovery.jl:1823-1960, with solid_centroid_B_tetra10,
+// src/tetra10.jl:110-115, and stress_solid_3d, src/FEMKernels.jl:13067-13074):
+// element displacements are the nodes' translations rotated to the basic
+// frame (u = node_R * u_node); B at the centroid (r = s = t = 1/4);
+// strain = B u (engineering shears xy, yz, zx), stress = D strain,
+// von Mises from the six stress components.  xyz: 10 x 3 (row per node),
+// nodeR: 10 x 9 col-major blocks, u_node: 10 x 3 translations in the node
+// frames.  out: sxx syy szz txy tyz tzx, exx eyy ezz gxy gyz gzx, von Mises.
+int or_t10_stress(const double* xyz, const double* nodeR, double E, double nu, const double* u_node,
+                  double* out) {
+  if (!(std::isfinite(E) && E > 0 && std::isfinite(nu) && nu > -1 && nu < 0.5)) return 2;
+  const int edges[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
+  const double dL[3][4] = {{-1, 1, 0, 0}, {-1, 0, 1, 0}, {-1, 0, 0, 1}};
+  const double L[4] = {0.25, 0.25, 0.25, 0.25};
+  double dN[3][10];
+  for (int i = 0; i < 4; ++i)
+    for (int k = 0; k < 3; ++k) dN[k][i] = (4.0 * L[i] - 1.0) * dL[k][i];
+  for (int e = 0; e < 6; ++e) {
+    int i = edges[e][0], j = edges[e][1];
+    for (int k = 0; k < 3; ++k) dN[k][e + 4] = 4.0 * (L[j] * dL[k][i] + L[i] * dL[k][j]);
+  }
+  double J[9];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      double sm = 0;
+      for (int k = 0; k < 10; ++k) sm += dN[a][k] * xyz[3 * k + b];
+      J[a + 3 * b] = sm;
+    }
+  double det = J[0] * (J[4] * J[8] - J[7] * J[5]) - J[3] * (J[1] * J[8] - J[7] * J[2]) +
+               J[6] * (J[1] * J[5] - J[4] * J[2]);
+  if (!(std::isfinite(det) && det > 0.0)) return 1;
+  double Ji[9];
+  if (!inv_small(J, 3, Ji)) return 1;
+  double u[30];
+  for (int k = 0; k < 10; ++k)
+    for (int a = 0; a < 3; ++a) {
+      double sm = 0;
+      for (int b = 0; b < 3; ++b) sm += nodeR[9 * k + a + 3 * b] * u_node[3 * k + b];
+      u[3 * k + a] = sm;
+    }
+  double eps[6] = {0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < 10; ++i) {
+    double gx = Ji[0] * dN[0][i] + Ji[3] * dN[1][i] + Ji[6] * dN[2][i];
+    double gy = Ji[1] * dN[0][i] + Ji[4] * dN[1][i] + Ji[7] * dN[2][i];
+    double gz = Ji[2] * dN[0][i] + Ji[5] * dN[1][i] + Ji[8] * dN[2][i];
+    const double ux = u[3 * i], uy = u[3 * i + 1], uz = u[3 * i + 2];
+    eps[0] += gx * ux;
+    eps[1] += gy * uy;
+    eps[2] += gz * uz;
+    eps[3] += gy * ux + gx * uy;
+    eps[4] += gz * uy + gy * uz;
+    eps[5] += gz * ux + gx * uz;
+  }
+  double c = E / ((1.0 + nu) * (1.0 - 2.0 * nu)), d = 1.0 - nu, sh = (1.0 - 2.0 * nu) / 2.0;
+  double sig[6];
+  for (int i = 0; i < 3; ++i) {
+    double sm = 0;
+    for (int j = 0; j < 3; ++j) sm += (i == j ? c * d : c * nu) * eps[j];
+    sig[i] = sm;
+  }
+  for (int i = 3; i < 6; ++i) sig[i] = c * sh * eps[i];
+  double vm = sig[0] * sig[0] + sig[1] * sig[1] + sig[2] * sig[2] - sig[0] * sig[1] - sig[1] * sig[2] -
+              sig[2] * sig[0] + 3.0 * (sig[3] * sig[3] + sig[4] * sig[4] + sig[5] * sig[5]);
+  for (int i = 0; i < 6; ++i) { out[i] = sig[i]; out[6 + i] = eps[i]; }
+  out[12] = std::sqrt(std::max(0.0, vm));
+  return 0;
+}
+
 // r = f - A x in double-double arithmetic (Knuth two-sum, FMA two-product)
 // per row: the checker's refinement residual carries only the final rounding,
 // so refinement can reach the accuracy of the FP64 data even where the row

@@ -400,3 +400,29 @@ def test_non_default_quad4_flags_are_refused(ctx):
     assert e.value.status_name == "UNSUPPORTED"
     assert e.value.detail >= 5
     dm.close()
+
+
+def test_t10_stress_recovery_matches_oracle(ctx, oracle_mod):
+    """Device CTETRA10 centroid stresses, strains and von Mises
+    (stress_recovery.jl:1823-1960) against the oracle on random displacement
+    fields with rotated grid frames: 1e-12 relative to each field's maximum."""
+    m = M.solid_block(n=3, n_cases=1)
+    rng = np.random.default_rng(4)
+    R = np.zeros((m.n_nodes, 9))
+    for i in range(m.n_nodes):
+        Q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+        R[i] = Q.ravel(order="F")
+    m.node_R = R
+    U = rng.normal(scale=1e-4, size=(m.ndof, 3))
+    dm = lib.DeviceModel(ctx, m)
+    dm.assemble()
+    got = dm.t10_stresses(U)
+    ref = oracle_mod.t10_stresses(m, U)
+    for a, b in ((0, 6), (6, 12), (12, 13)):
+        assert _rel(got[..., a:b], ref[..., a:b]) <= ELEM_RTOL
+    u1 = U[:, :1].copy(order="F")
+    out = np.empty(13)
+    with pytest.raises(lib.JfgError) as e:
+        lib._check(lib.load().jfg_recover_stresses(dm.h, 0, 1, lib._p(u1), lib._p(out)))
+    assert e.value.status_name == "UNSUPPORTED"
+    dm.close()

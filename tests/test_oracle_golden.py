@@ -367,3 +367,29 @@ def test_pressure_and_face_load_totals(oracle_mod):
     assert F[:, 2].sum() == pytest.approx(-1e6 * 0.3 * 0.3, rel=1e-13)
     corner = np.all((np.round(s.xyz / (0.3 / 6)) % 2) == 0, axis=1)
     assert np.abs(F[corner, 2]).max() == 0.0
+
+
+def test_t10_stress_recovery_uniform_strain(oracle_mod):
+    """Known answer for the CTETRA10 centroid recovery (stress_recovery.jl:
+    1823-1960): an affine displacement u = A x gives every element the strain
+    sym(A) (engineering shears) and the stress D strain, also when the grids
+    carry rotated displacement frames (u_node = node_R' u)."""
+    m = M.solid_block(n=2, n_cases=1)
+    m.node_R = _random_frames(m.n_nodes, 3)
+    A = np.array([[.002, .001, -.0004], [-.0002, -.0007, .0003], [.0008, -.0006, .0011]])
+    ub = m.xyz @ A.T
+    R = m.node_R.reshape(-1, 3, 3).transpose(0, 2, 1)          # R[n] = node_R as a matrix
+    U = np.zeros((m.ndof, 1))
+    U.reshape(-1, 6)[:, :3] = np.einsum("nji,nj->ni", R, ub)   # node_R' u
+    S = oracle_mod.t10_stresses(m, U)[0]
+    eps = np.array([A[0, 0], A[1, 1], A[2, 2], A[0, 1] + A[1, 0], A[1, 2] + A[2, 1], A[2, 0] + A[0, 2]])
+    E, nu = 210e9, 0.3
+    c = E / ((1 + nu) * (1 - 2 * nu))
+    D = np.zeros((6, 6)); D[:3, :3] = c * nu; np.fill_diagonal(D[:3, :3], c * (1 - nu))
+    D[3, 3] = D[4, 4] = D[5, 5] = c * (1 - 2 * nu) / 2
+    sig = D @ eps
+    vm = np.sqrt(sig[0] ** 2 + sig[1] ** 2 + sig[2] ** 2 - sig[0] * sig[1] - sig[1] * sig[2] - sig[2] * sig[0]
+                 + 3 * (sig[3] ** 2 + sig[4] ** 2 + sig[5] ** 2))
+    assert np.allclose(S[:, 6:12], eps[None, :], rtol=1e-12, atol=1e-15)
+    assert np.allclose(S[:, 0:6], sig[None, :], rtol=1e-10, atol=1e-3)
+    assert np.allclose(S[:, 12], vm, rtol=1e-10)
