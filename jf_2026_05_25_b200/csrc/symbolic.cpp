@@ -25,6 +25,69 @@ struct NodeGraph {
   std::vector<int32_t> adj;
 };
 
+// Minimum-degree order of one nested-dissection leaf.  The leaf's nodes
+// are eliminated before every node outside it, so the elimination graph is
+// built over the leaf plus its halo (outside neighbours, never eliminated
+// here) and a node's degree counts both: the exact external degree of the
+// elimination graph, kept as bitsets (at most 512 vertices; larger leaves
+// keep their given order).  Ties go to the earlier node.
+void order_leaf(const NodeGraph& g, const std::vector<int32_t>& nodes, std::vector<int32_t>& mark,
+                std::vector<int32_t>& pos, int32_t* out) {
+  const int nl = (int)nodes.size();
+  constexpr int MAXV = 512, W = MAXV / 64;
+  std::vector<int32_t> verts(nodes.begin(), nodes.end());
+  for (int k = 0; k < nl; ++k) { mark[verts[k]] = 1; pos[verts[k]] = k; }
+  for (int k = 0; k < nl && (int)verts.size() <= MAXV; ++k) {
+    const int32_t v = verts[k];
+    for (int64_t p = g.ptr[v]; p < g.ptr[v + 1]; ++p) {
+      const int32_t w = g.adj[p];
+      if (mark[w] < 0) { mark[w] = 2; pos[w] = (int32_t)verts.size(); verts.push_back(w); }
+    }
+  }
+  const int nv = (int)verts.size();
+  if (nv > MAXV) {
+    for (int k = 0; k < nl; ++k) out[k] = nodes[k];
+  } else {
+    std::vector<uint64_t> adj((size_t)nv * W, 0);
+    for (int k = 0; k < nl; ++k) {
+      const int32_t v = verts[k];
+      for (int64_t p = g.ptr[v]; p < g.ptr[v + 1]; ++p) {
+        const int j = pos[g.adj[p]];
+        if (j == k) continue;
+        adj[(size_t)k * W + j / 64] |= 1ull << (j % 64);
+        adj[(size_t)j * W + k / 64] |= 1ull << (k % 64);
+      }
+    }
+    std::vector<uint8_t> done(nl, 0);
+    for (int step = 0; step < nl; ++step) {
+      int best = -1, bd = 1 << 30;
+      for (int k = 0; k < nl; ++k) {
+        if (done[k]) continue;
+        int d = 0;
+        for (int w = 0; w < W; ++w) d += __builtin_popcountll(adj[(size_t)k * W + w]);
+        if (d < bd) { bd = d; best = k; }
+      }
+      out[step] = verts[best];
+      done[best] = 1;
+      // eliminate best: its neighbours become a clique
+      const uint64_t* nb = &adj[(size_t)best * W];
+      for (int w = 0; w < W; ++w) {
+        uint64_t bits = nb[w];
+        while (bits) {
+          const int j = w * 64 + __builtin_ctzll(bits);
+          bits &= bits - 1;
+          uint64_t* aj = &adj[(size_t)j * W];
+          for (int x = 0; x < W; ++x) aj[x] |= nb[x];
+          aj[j / 64] &= ~(1ull << (j % 64));
+          aj[best / 64] &= ~(1ull << (best % 64));
+        }
+      }
+      for (int x = 0; x < W; ++x) adj[(size_t)best * W + x] = 0;
+    }
+  }
+  for (int32_t v : verts) { mark[v] = -1; pos[v] = -1; }
+}
+
 // Nested dissection by recursive coordinate bisection with a one-sided vertex
 // separator: split the node set at the median of its longest bounding-box
 // axis, take as separator the nodes of one half that touch the other half
@@ -34,6 +97,7 @@ void nested_dissection(const NodeGraph& g, const double* xyz, const std::vector<
   int64_t n_nodes = (int64_t)g.ptr.size() - 1;
   order.assign(active.size(), -1);
   std::vector<int64_t> tag(n_nodes, -1);
+  std::vector<int32_t> mark(n_nodes, -1), halo_pos(n_nodes, -1);
   struct Task { int64_t lo, hi; std::vector<int32_t> nodes; };
   std::vector<Task> st;
   st.push_back({0, (int64_t)active.size(), active});
@@ -44,7 +108,7 @@ void nested_dissection(const NodeGraph& g, const double* xyz, const std::vector<
     st.pop_back();
     int64_t sz = (int64_t)t.nodes.size();
     if (sz <= leaf) {
-      for (int64_t k = 0; k < sz; ++k) order[t.lo + k] = t.nodes[k];
+      order_leaf(g, t.nodes, mark, halo_pos, order.data() + t.lo);
       continue;
     }
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -60,12 +124,25 @@ void nested_dissection(const NodeGraph& g, const double* xyz, const std::vector<
     for (int64_t k = 0; k < sz; ++k) key[k] = {xyz[3 * (int64_t)t.nodes[k] + ax], t.nodes[k]};
     int64_t mid = sz / 2;
     std::nth_element(key.begin(), key.begin() + mid, key.end());
+    // the cut keeps every node at the median coordinate on one side, so a
+    // grid line of a structured mesh is never split between the halves (a
+    // split line would make a jagged, larger separator)
+    // (ties at the median go to the lower half, or to the upper half when
+    // the median is the largest coordinate; a split that leaves a half empty
+    // falls back to splitting by rank)
+    const double cut = key[mid].first;
+    int64_t n_le = 0, n_lt = 0;
+    for (int64_t k = 0; k < sz; ++k) { n_le += key[k].first <= cut; n_lt += key[k].first < cut; }
+    const int split_mode = (n_le < sz) ? 0 : (n_lt > 0 ? 1 : 2);
+    auto in_a = [&](int64_t k) {
+      return split_mode == 0 ? key[k].first <= cut : split_mode == 1 ? key[k].first < cut : k < mid;
+    };
     int64_t tA = next_tag++, tB = next_tag++;
-    for (int64_t k = 0; k < sz; ++k) tag[key[k].second] = k < mid ? tA : tB;
+    for (int64_t k = 0; k < sz; ++k) tag[key[k].second] = in_a(k) ? tA : tB;
     std::vector<int32_t> sepA, sepB, A, B;
     for (int64_t k = 0; k < sz; ++k) {
       int32_t v = key[k].second;
-      bool isA = k < mid;
+      bool isA = in_a(k);
       int64_t other = isA ? tB : tA;
       bool touch = false;
       for (int64_t p = g.ptr[v]; p < g.ptr[v + 1]; ++p)
