@@ -141,6 +141,16 @@ jfg_status jfg_get_element_matrix(jfg_model* model, int32_t kind, int64_t elem,
 jfg_status jfg_set_free_dofs(jfg_model* model, int64_t n_free,
                              const int32_t* free_dofs);
 jfg_status jfg_get_symbolic_info(jfg_model* model, jfg_symbolic_info* info);
+/* No counterpart in the reference, whose worker re-parses and re-analyses
+ * every request (warm_model_session.jl:5-99 keeps one model warm).  For a
+ * new model `dst` of the same mesh as a resident model `src` (same grid count
+ * and CQUAD4 / CTETRA10 connectivity, no CQUAD8, whose pattern depends on the
+ * element values): copies src's CSC pattern and slot map (device to device)
+ * and keeps src's symbolic analysis, so that the first jfg_assemble on dst
+ * skips the pattern build and jfg_set_free_dofs skips the ordering and
+ * analysis when its free set equals src's.  Call before dst's first
+ * jfg_assemble.  Different meshes give JFG_BAD_INPUT.                     */
+jfg_status jfg_model_share_structure(jfg_model* dst, const jfg_model* src);
 /* Fill-reducing permutation (F.p of the factor object, :1666): perm[k] = the
  * position in free_dofs of the k-th eliminated unknown.                   */
 jfg_status jfg_get_perm(jfg_model* model, int32_t* perm);

@@ -359,11 +359,68 @@ jfg_status jfg_set_free_dofs(jfg_model* m, int64_t n_free, const int32_t* free_d
   if (n_free <= 0 || !free_dofs) { set_error("empty free set"); return JFG_BAD_INPUT; }
   numeric_destroy(m);
   m->sym_ready = false;
-  SymbolicOptions opt = SymbolicOptions::from_env();
-  std::string e = analyze(m->ndof, m->colptr.data(), m->rowval.data(), n_free, free_dofs, m->h_xyz.data(), opt, m->sym);
-  if (!e.empty()) { set_error(e); return JFG_BAD_INPUT; }
+  if (m->has_sym_cache && (int64_t)m->sym_cache_free.size() == n_free &&
+      std::equal(m->sym_cache_free.begin(), m->sym_cache_free.end(), free_dofs)) {
+    // the shared analysis of this mesh and free set
+    m->sym = std::move(m->sym_cache);
+    m->sym_cache = Symbolic();
+    m->has_sym_cache = false;
+    std::vector<int32_t>().swap(m->sym_cache_free);
+  } else {
+    SymbolicOptions opt = SymbolicOptions::from_env();
+    std::string e =
+        analyze(m->ndof, m->colptr.data(), m->rowval.data(), n_free, free_dofs, m->h_xyz.data(), opt, m->sym);
+    if (!e.empty()) { set_error(e); return JFG_BAD_INPUT; }
+  }
   JFG_TRY(numeric_create(m));
   m->sym_ready = true;
+  return JFG_OK;
+}
+
+jfg_status jfg_model_share_structure(jfg_model* dst, const jfg_model* src) {
+  JFG_TRY(check_model(dst));
+  if (!src) { set_error("null source model"); return JFG_BAD_INPUT; }
+  if (!src->pattern_built) { set_error("source model has no pattern: call jfg_assemble on it first"); return JFG_NOT_READY; }
+  if (dst->pattern_built) { set_error("destination model already has a pattern"); return JFG_BAD_INPUT; }
+  if (dst->n_q8 > 0 || src->n_q8 > 0) {
+    set_error("CQUAD8 patterns depend on the element values and are not shared");
+    return JFG_UNSUPPORTED;
+  }
+  if (dst->n_nodes != src->n_nodes || dst->h_q4n != src->h_q4n || dst->h_t10n != src->h_t10n) {
+    set_error("models do not share a mesh (grid count or element connectivity differ)");
+    return JFG_BAD_INPUT;
+  }
+  jfg_ctx* c = dst->ctx;
+  const int64_t ndof = dst->ndof, nnz = src->nnz;
+  dst->nnz = nnz;
+  dst->n_trip = src->n_trip;
+  dst->colptr = src->colptr;
+  dst->rowval = src->rowval;
+  dst->slot = src->slot;
+  dst->diag_pos = src->diag_pos;
+  JFG_TRY(dev_alloc(c, (void**)&dst->d_colptr, sizeof(int64_t) * (ndof + 1)));
+  JFG_TRY(dev_alloc(c, (void**)&dst->d_rowval, sizeof(int32_t) * nnz));
+  JFG_TRY(dev_alloc(c, (void**)&dst->d_nzptr, sizeof(int32_t) * (nnz + 1)));
+  JFG_TRY(dev_alloc(c, (void**)&dst->d_trip, sizeof(int32_t) * dst->n_trip));
+  JFG_TRY(dev_alloc(c, (void**)&dst->d_tpos, sizeof(int64_t) * nnz));
+  JFG_TRY(dev_alloc(c, (void**)&dst->d_nzval, sizeof(double) * nnz));
+  JFG_TRY(up(c, dst->diag_pos, &dst->d_diag_pos));
+  cudaStream_t st = c->stream;
+  JFG_CUDA(cudaMemcpyAsync(dst->d_colptr, src->d_colptr, sizeof(int64_t) * (ndof + 1), cudaMemcpyDeviceToDevice, st));
+  JFG_CUDA(cudaMemcpyAsync(dst->d_rowval, src->d_rowval, sizeof(int32_t) * nnz, cudaMemcpyDeviceToDevice, st));
+  JFG_CUDA(cudaMemcpyAsync(dst->d_nzptr, src->d_nzptr, sizeof(int32_t) * (nnz + 1), cudaMemcpyDeviceToDevice, st));
+  JFG_CUDA(cudaMemcpyAsync(dst->d_trip, src->d_trip, sizeof(int32_t) * dst->n_trip, cudaMemcpyDeviceToDevice, st));
+  JFG_CUDA(cudaMemcpyAsync(dst->d_tpos, src->d_tpos, sizeof(int64_t) * nnz, cudaMemcpyDeviceToDevice, st));
+  JFG_CUDA(cudaStreamSynchronize(st));
+  dst->pattern_built = true;
+  if (src->sym_ready) {
+    dst->sym_cache = src->sym;
+    dst->sym_cache_free.clear();
+    dst->sym_cache_free.reserve(src->sym.n);
+    for (int64_t d = 0; d < ndof; ++d)
+      if (src->sym.gdof_to_perm[d] >= 0) dst->sym_cache_free.push_back((int32_t)d);
+    dst->has_sym_cache = true;
+  }
   return JFG_OK;
 }
 

@@ -47,6 +47,7 @@ struct NumericFactor {
     std::vector<std::pair<int32_t, int32_t>> ea;   // (offset into ea_child, count), per child rank
     int32_t ea_max_r;
     double schur_flops;   // sum over fronts of r(r+1) c (lower SYRK, 2 flops per FMA)
+    int64_t pk_len = 0;   // floats of the packed tensor-core operand images of the level's fronts
     // the level's fronts are listed by decreasing width: cs[i] is the width
     // of the i-th, pm[i] the largest row count among the first i + 1
     std::vector<int32_t> cs, pm;
@@ -64,7 +65,11 @@ struct NumericFactor {
   // tensor-core operand copies of L32 (mixed factor with tcgen05 updates):
   // hi = rn19(v), lo = rn19(v - hi), packed per front (offset PKptr[s]) in
   // 512-byte 64-byte-swizzled atoms of 8 rows x 16 columns, slice-block
-  // major; padding zeroed once at allocation.  tc_zero: 8 KB of zeros.
+  // major.  The images are only read by the updates of the front's own level,
+  // so one workspace sized for the largest level serves every level: PKptr[s]
+  // is the front's offset inside its level's region, which is zeroed (the
+  // padding must read as zero) before the level's panels write it.
+  // tc_zero: 8 KB of zeros.
   float *Phi = nullptr, *Plo = nullptr, *tc_zero = nullptr;
   int64_t* PKptr = nullptr;
   int64_t pk_len = 0;
@@ -1227,6 +1232,11 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
   for (const auto& lv : F->levels) {
     const int32_t* list = F->level_sn + lv.off;
     F->level_sn_cur = list;
+    if (sizeof(T) == 4 && tc && lv.pk_len > 0) {
+      // fresh zero padding for this level's operand images
+      JFG_CUDA(cudaMemsetAsync(F->Phi, 0, sizeof(float) * lv.pk_len, st));
+      JFG_CUDA(cudaMemsetAsync(F->Plo, 0, sizeof(float) * lv.pk_len, st));
+    }
     // one front update of the level: the tensor-core 3xTF32 kernel for the
     // FP32 factor when its low parts exist and the level's output is large
     // enough for 128 x 128 tiles, else the SIMT / DMMA tiles
@@ -1678,20 +1688,27 @@ jfg_status numeric_factor(jfg_model* m, int precision) {
     const int tcs = tc::setting();
     const bool use_tc = tcs == 1 || (tcs < 0 && m->n_q4 + m->n_q8 == 0);
     if (use_tc && !F->Phi) {
-      // packed operand arrays: ceil(c/16) x ceil(m/8) atoms of 128 floats
+      // packed operand images: ceil(c/16) x ceil(m/8) atoms of 128 floats per
+      // front, offsets relative to the front's level region
       std::vector<int64_t> pk(S.ns + 1, 0);
-      for (int64_t s = 0; s < S.ns; ++s) {
-        const int64_t cs = S.sn_first[s + 1] - S.sn_first[s], ms = S.sn_m[s];
-        pk[s + 1] = pk[s] + ((cs + 15) / 16) * ((ms + 7) / 8) * 128;
+      int64_t wmax = 0;
+      for (auto& lv : F->levels) {
+        int64_t acc = 0;
+        for (int32_t q = lv.off; q < lv.off + lv.count; ++q) {
+          const int32_t s = S.level_sn[q];
+          const int64_t cs = S.sn_first[s + 1] - S.sn_first[s], ms = S.sn_m[s];
+          pk[s] = acc;
+          acc += ((cs + 15) / 16) * ((ms + 7) / 8) * 128;
+        }
+        lv.pk_len = acc;
+        wmax = std::max(wmax, acc);
       }
-      F->pk_len = std::max<int64_t>(pk[S.ns], 128);
+      F->pk_len = std::max<int64_t>(wmax, 128);
       JFG_TRY(dev_alloc(c, (void**)&F->PKptr, sizeof(int64_t) * (S.ns + 1)));
       JFG_TRY(dev_alloc(c, (void**)&F->Phi, sizeof(float) * F->pk_len));
       JFG_TRY(dev_alloc(c, (void**)&F->Plo, sizeof(float) * F->pk_len));
       JFG_TRY(dev_alloc(c, (void**)&F->tc_zero, 8192));
       JFG_CUDA(cudaMemcpyAsync(F->PKptr, pk.data(), sizeof(int64_t) * (S.ns + 1), cudaMemcpyHostToDevice, st));
-      JFG_CUDA(cudaMemsetAsync(F->Phi, 0, sizeof(float) * F->pk_len, st));
-      JFG_CUDA(cudaMemsetAsync(F->Plo, 0, sizeof(float) * F->pk_len, st));
       JFG_CUDA(cudaMemsetAsync(F->tc_zero, 0, 8192, st));
       JFG_CUDA(cudaStreamSynchronize(st));   // pk is a host temporary
     }

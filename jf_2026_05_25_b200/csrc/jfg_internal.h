@@ -127,6 +127,12 @@ struct jfg_model {
   // symbolic
   bool sym_ready = false;
   jfg::Symbolic sym;
+  // analysis of the same mesh taken over from another model
+  // (jfg_model_share_structure): used by jfg_set_free_dofs when its free set
+  // is the one this analysis was made for
+  std::vector<int32_t> sym_cache_free;
+  jfg::Symbolic sym_cache;
+  bool has_sym_cache = false;
   NumericFactor* num = nullptr;
   // timings of the last calls (seconds, device events)
   double t_elements = 0, t_assembly = 0, t_factor = 0, t_solve = 0;

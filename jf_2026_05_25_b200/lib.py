@@ -93,6 +93,7 @@ def load():
         "jfg_symbolic_dry_run": [I64, P, P, I64, P, P, P, P],
         "jfg_assemble_values_noalloc": [P, P],
         "jfg_recover_stresses": [P, I32, I32, P, P],
+        "jfg_model_share_structure": [P, P],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -185,6 +186,11 @@ class DeviceModel:
             self.close()
         except Exception:
             pass
+
+    def share_structure(self, src: "DeviceModel"):
+        """Take over the pattern and the symbolic analysis of a resident model
+        of the same mesh (see jfg_model_share_structure)."""
+        _check(load().jfg_model_share_structure(self.h, src.h))
 
     # ---- assembly
     def assemble(self):

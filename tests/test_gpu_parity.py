@@ -426,3 +426,34 @@ def test_t10_stress_recovery_matches_oracle(ctx, oracle_mod):
         lib._check(lib.load().jfg_recover_stresses(dm.h, 0, 1, lib._p(u1), lib._p(out)))
     assert e.value.status_name == "UNSUPPORTED"
     dm.close()
+
+
+def test_share_structure_gives_the_same_solution(ctx):
+    """A second model of the same mesh (other thicknesses and loads) that
+    takes over a resident model's pattern and symbolic analysis
+    (jfg_model_share_structure) solves bit-for-bit like the same model
+    analysed on its own; a different mesh is refused."""
+    a = M.wing_panel(nx=24, ny=36, n_blades=3, blade_nz=4, n_cases=2, seed=5)
+    b = M.wing_panel(nx=24, ny=36, n_blades=3, blade_nz=4, n_cases=2, seed=6)
+    be = B.JFEMGPUBackend(tol=RESID_TOL)
+    be._ctx = ctx
+    st_a = B.prepare(be, a)
+    alone = B.solve_model(be, b)
+    U_alone = np.stack([sc["raw_displacement"] for sc in alone["subcases"]], axis=1)
+    dm = lib.DeviceModel(ctx, b)
+    dm.share_structure(st_a["dm"])
+    dm.assemble()
+    d, _ = dm.diag()
+    free, fixed, _ = B.compute_free_dofs(b, d, dm.node_blocks())
+    assert np.array_equal(free, st_a["free"])
+    dm.set_free_dofs(free)
+    assert np.array_equal(dm.perm(), st_a["dm"].perm())
+    dm.factor(lib.PREC_FP64)
+    U, rep = dm.solve(b.load_matrix())
+    assert np.array_equal(U, U_alone)
+    other = lib.DeviceModel(ctx, M.wing_panel(nx=20, ny=36, n_blades=3, blade_nz=4, n_cases=1))
+    with pytest.raises(lib.JfgError) as e:
+        other.share_structure(st_a["dm"])
+    assert e.value.status_name == "BAD_INPUT"
+    for x in (dm, other, st_a["dm"], alone["state"]["dm"]):
+        x.close()
