@@ -153,12 +153,23 @@ def compute_free_dofs(model, diag: np.ndarray, node_blocks: np.ndarray, eps_zero
 # solve_model
 # ----------------------------------------------------------------------------
 
-def prepare(backend: JFEMGPUBackend, model) -> Dict:
+def prepare(backend: JFEMGPUBackend, model, donor: Optional["lib.DeviceModel"] = None,
+            before_factor=None, dm: Optional["lib.DeviceModel"] = None) -> Dict:
     """Upload, assemble, partition, analyse and factor: the per-model state
-    that the reference caches in LinearSolveCacheEntry (boundary_conditions.jl:62-75)."""
+    that the reference caches in LinearSolveCacheEntry (boundary_conditions.jl:62-75).
+
+    ``donor``: a resident model of the same mesh whose pattern and symbolic
+    analysis the new model takes over (jfg_model_share_structure).
+    ``before_factor(dm)``: called once the symbolic analysis exists and before
+    the factor is allocated (the serving loop admits the model's bytes there).
+    ``dm``: the model already uploaded (and possibly given a donor's structure).
+    """
     timings = {}
     t0 = time.perf_counter()
-    dm = lib.DeviceModel(backend.ctx, model)
+    if dm is None:
+        dm = lib.DeviceModel(backend.ctx, model)
+        if donor is not None:
+            dm.share_structure(donor)
     dm.assemble()
     timings["assembly"] = time.perf_counter() - t0
     t1 = time.perf_counter()
@@ -167,6 +178,8 @@ def prepare(backend: JFEMGPUBackend, model) -> Dict:
     free, fixed, bc = compute_free_dofs(model, diag, blocks, backend.eps_zero)
     dm.set_free_dofs(free)
     timings["constraints"] = time.perf_counter() - t1
+    if before_factor is not None:
+        before_factor(dm)
     t2 = time.perf_counter()
     dm.factor(backend.precision)
     # post-factor pivot check L_ii^2 / K_ii < threshold (boundary_conditions.jl:1662-1710)

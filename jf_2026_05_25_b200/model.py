@@ -76,6 +76,9 @@ class Sol101Model:
     spc1: List[Tuple[str, np.ndarray]] = field(default_factory=list)
     load_cases: List[LoadCase] = field(default_factory=list)
     seed: Optional[int] = None
+    # per-element CQUAD4 section records set by a thickness update; when
+    # present they replace the records derived from the PSHELL cards
+    q4_sect_override: Optional[np.ndarray] = None
 
     def __post_init__(self):
         if self.node_R is None:
@@ -100,6 +103,8 @@ class Sol101Model:
         Cs = TS/T * h * G * I2, G = MAT(MID3).G or E/2(1+nu)       (:2085-2129)
         E_ref = E, k6rot = PARAM K6ROT (0 for membrane-only)       (:4008)
         """
+        if self.q4_sect_override is not None:
+            return self.q4_sect_override
         out = np.zeros((len(self.q4_pid), Q4_SECT_STRIDE))
         for pid in np.unique(self.q4_pid):
             rec = _q4_section_record(self, int(pid))
@@ -157,6 +162,7 @@ class Sol101Model:
         rotation of the reference is the identity for basic-frame grids.
         """
         F = np.zeros(self.ndof)
+        nn_tot = self.n_nodes
         if case.pload4 is not None:
             eidx, p = case.pload4
             nodes = self.q4_nodes[eidx]
@@ -169,17 +175,17 @@ class Sol101Model:
             ldir = nv / nn[:, None]
             tf = area * p
             fnode = ldir * (tf / 4.0)[:, None]
+            Fn = F.reshape(-1, 6)
             for k in range(4):
                 for a in range(3):
-                    np.add.at(F, 6 * nodes[:, k] + a, fnode[:, a])
-        if case.forces is not None:
-            nidx, vec = case.forces
+                    Fn[:, a] += np.bincount(nodes[:, k], weights=fnode[:, a], minlength=nn_tot)
+        for item in (case.forces, case.cload):
+            if item is None:
+                continue
+            nidx, vec = item
+            Fn = F.reshape(-1, 6)
             for a in range(3):
-                np.add.at(F, 6 * nidx + a, vec[:, a])
-        if case.cload is not None:
-            nidx, vec = case.cload
-            for a in range(3):
-                np.add.at(F, 6 * nidx + a, vec[:, a])
+                Fn[:, a] += np.bincount(nidx, weights=vec[:, a], minlength=nn_tot)
         R = self.node_R
         if not np.allclose(R, np.tile([1, 0, 0, 0, 1, 0, 0, 0, 1], (self.n_nodes, 1))):
             Rm = R.reshape(-1, 3, 3, order="C").transpose(0, 2, 1)  # column-major -> matrix

@@ -25,6 +25,7 @@ boundary_conditions.jl:62-75).  Here:
 """
 from __future__ import annotations
 
+import hashlib
 import math
 import queue
 import threading
@@ -191,26 +192,58 @@ class Resident:
     lock: threading.Lock
     last_used: float = 0.0
     evicted: bool = False              # set under `lock` when the group is freed
+    mesh: Optional[bytes] = None       # mesh key of a single model (structure sharing)
+
+
+def mesh_key(model) -> Optional[bytes]:
+    """Key of a model's mesh for structure sharing: grid count and CQUAD4 /
+    CTETRA10 connectivity (CQUAD8 patterns depend on values: no key)."""
+    if len(getattr(model, "q8_nodes", ())):
+        return None
+    h = hashlib.blake2b(digest_size=16)
+    h.update(np.int64(model.n_nodes).tobytes())
+    h.update(np.ascontiguousarray(model.q4_nodes, np.int32).tobytes())
+    h.update(b"|")
+    h.update(np.ascontiguousarray(model.t10_nodes, np.int32).tobytes())
+    return h.digest()
 
 
 class SolveServer:
-    """Continuous-batching SOL101 server on one device (see module docstring)."""
+    """Continuous-batching SOL101 server on one device (see module docstring).
+
+    Memory: a new model's bytes are admitted once its symbolic analysis is
+    known and before its factor is allocated; least-recently-used idle
+    residents are freed to make room (a pack as a unit), and when every
+    resident is busy the admission waits up to ``wait_s`` for one to finish.
+    A re-solve or update of a model freed meanwhile re-admits it from its
+    host description.  New models of a resident mesh take over its pattern
+    and symbolic analysis (``share_meshes``).
+    """
 
     def __init__(self, device: int = 0, slots: int = 4, hbm_budget_bytes: float = 150e9,
                  precision: int = lib.PREC_FP64, tol: float = 1e-10, small_dof: int = 60000,
-                 pack_dof: int = 400000, pack_models: int = 64):
+                 pack_dof: int = 400000, pack_models: int = 64, share_meshes: bool = True,
+                 wait_s: float = 300.0):
         self.device, self.precision, self.tol = device, precision, tol
         self.small_dof, self.pack_dof, self.pack_models = small_dof, pack_dof, pack_models
+        self.share_meshes, self.wait_s = share_meshes, wait_s
         self.budget = float(hbm_budget_bytes)
         self.q: "queue.Queue[Request]" = queue.Queue()
         self.pending: List[Request] = []
         self.plock = threading.Condition()
         self.registry: Dict[str, Resident] = {}
         self.groups: Dict[int, List[str]] = {}      # pack id -> member keys (freed together)
+        self.meshes: Dict[bytes, str] = {}          # mesh key -> key of a resident single model of that mesh
+        self.evicted: Dict[str, object] = {}        # key -> host model of a freed model (re-admitted on demand)
         self.rlock = threading.Lock()
+        self.mem_cv = threading.Condition(self.rlock)
         self.resident_bytes = 0
+        self.reserved = 0.0                          # bytes admitted for models still being prepared
         self.latencies: List[float] = []
+        self.kinds: List[str] = []
         self.subcase_solves = 0
+        self.readmissions = 0
+        self.shared_structures = 0
         self._next_key = 0
         self._stop = False
         self.backends = []
@@ -258,7 +291,8 @@ class SolveServer:
             return {"requests": 0}
         return {"requests": int(lat.size), "p50_ms": float(np.percentile(lat, 50) * 1e3),
                 "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3),
-                "subcase_solves": int(self.subcase_solves), "resident_bytes": int(self.resident_bytes)}
+                "subcase_solves": int(self.subcase_solves), "resident_bytes": int(self.resident_bytes),
+                "readmissions": int(self.readmissions), "shared_structures": int(self.shared_structures)}
 
     # ---------------------------------------------------------------- scheduling
     def _take(self) -> Optional[List[Request]]:
@@ -294,9 +328,9 @@ class SolveServer:
                 if work[0].kind == "solve":
                     self._do_solve(be, work)
                 elif work[0].kind == "resolve":
-                    self._do_resolve(work[0])
+                    self._do_resolve(be, work[0])
                 else:
-                    self._do_update(work[0])
+                    self._do_update(be, work[0])
             except Exception as exc:   # report to every waiting client
                 for r in work:
                     if not r.future.done():
@@ -306,6 +340,7 @@ class SolveServer:
         dt = time.perf_counter() - req.t_submit
         with self.rlock:
             self.latencies.append(dt)
+            self.kinds.append(req.kind)
             self.subcase_solves += int(result["U"].shape[1])
         result["latency_s"] = dt
         req.future.set_result(result)
@@ -317,78 +352,161 @@ class SolveServer:
         _, nnz, ntrip = dm.sizes()
         return int(info["factor_bytes"] * 1.6 + 24 * nnz + 8 * ntrip + 200 * dm.ndof)
 
-    def _admit(self, need: int):
-        """Free least-recently-used residents until `need` more bytes fit.
+    def _evict_group(self, r: Resident, key: str):
+        """Free one group (caller holds rlock and r.lock)."""
+        gid = id(r.dm)
+        keys = self.groups.pop(gid, [key])
+        for k in keys:
+            member = self.registry.pop(k, None)
+            if member is not None:
+                member.evicted = True
+                self.evicted[k] = member.model
+                if member.mesh is not None and self.meshes.get(member.mesh) == k:
+                    del self.meshes[member.mesh]
+        r.evicted = True
+        self.resident_bytes -= r.nbytes
+        r.dm.close()
+        self.mem_cv.notify_all()
+
+    def _admit(self, need: float, wait: bool = False):
+        """Free least-recently-used residents until `need` more bytes fit, and
+        reserve them for the model being prepared (released by _register).
 
         A pack is freed as a unit.  A group whose lock is held (a re-solve or
         an update is running on it) is skipped, so in-flight work is never
-        freed under it; when every remaining group is busy the request is
-        admitted over budget rather than waiting.  The group's bytes are
-        released once, and its registry entries go only after its lock is held.
+        freed under it.  When every remaining group is busy the request waits
+        (``wait``) up to ``wait_s`` for memory to be released, then is
+        admitted over budget rather than blocking the server.  The group's
+        bytes are released once, and its registry entries go only after its
+        lock is held.
         """
         with self.rlock:
+            deadline = time.perf_counter() + self.wait_s
             busy = set()
-            while self.resident_bytes + need > self.budget:
+            while self.resident_bytes + self.reserved + need > self.budget:
                 cands = [k for k in self.registry if id(self.registry[k].dm) not in busy]
                 if not cands:
-                    break
+                    if not wait or time.perf_counter() >= deadline or (not self.registry and self.reserved <= 0):
+                        break
+                    busy.clear()
+                    self.mem_cv.wait(timeout=0.5)
+                    continue
                 key = min(cands, key=lambda k: self.registry[k].last_used)
                 r = self.registry[key]
-                gid = id(r.dm)
                 if not r.lock.acquire(blocking=False):
-                    busy.add(gid)
+                    busy.add(id(r.dm))
                     continue
                 try:
-                    keys = self.groups.pop(gid, [key])
-                    for k in keys:
-                        member = self.registry.pop(k, None)
-                        if member is not None:
-                            member.evicted = True
-                    r.evicted = True
-                    self.resident_bytes -= r.nbytes
-                    r.dm.close()
+                    self._evict_group(r, key)
                 finally:
                     r.lock.release()
+            self.reserved += need
 
-    def _register(self, dm, state, pack, models) -> List[str]:
+    def _release(self, reserved: float):
+        with self.rlock:
+            self.reserved -= reserved
+            self.mem_cv.notify_all()
+
+    def _register(self, dm, state, pack, models, reserved: float = 0.0, keys: Optional[List[str]] = None,
+                  mesh: Optional[bytes] = None) -> List[str]:
         nbytes = self._bytes_of(dm)
-        self._admit(0)
         lock = threading.Lock()
-        keys = []
+        out = []
         with self.rlock:
             for i, m in enumerate(models):
-                key = f"m{self._next_key}"
-                self._next_key += 1
-                self.registry[key] = Resident(dm, state, pack, i, m, nbytes, lock, time.perf_counter())
-                keys.append(key)
-            self.groups[id(dm)] = keys
+                if keys is not None:
+                    key = keys[i]
+                else:
+                    key = f"m{self._next_key}"
+                    self._next_key += 1
+                self.registry[key] = Resident(dm, state, pack, i, m, nbytes, lock, time.perf_counter(),
+                                              mesh=mesh if len(models) == 1 else None)
+                self.evicted.pop(key, None)
+                out.append(key)
+            self.groups[id(dm)] = out
             self.resident_bytes += nbytes
-        return keys
+            self.reserved -= reserved
+            if mesh is not None and len(models) == 1:
+                self.meshes[mesh] = out[0]
+            self.mem_cv.notify_all()
+        return out
 
     # ---------------------------------------------------------------- work
+    def _prepare(self, be, model, pack: Optional[PackedModel]):
+        """Upload (sharing a resident mesh's structure when there is one),
+        analyse, admit the exact bytes, factor.  Returns (state, reserved, mesh)."""
+        target = pack if pack is not None else model
+        mk = mesh_key(model) if (pack is None and self.share_meshes) else None
+        dm = lib.DeviceModel(be.ctx, target)
+        donor = None
+        if mk is not None:
+            with self.rlock:
+                dk = self.meshes.get(mk)
+                donor = self.registry.get(dk) if dk is not None else None
+        if donor is not None:
+            with donor.lock:
+                if not donor.evicted:
+                    dm.share_structure(donor.dm)
+                    with self.rlock:
+                        self.shared_structures += 1
+        admitted = [0.0]
+
+        def admit(d):
+            need = float(self._bytes_of(d))
+            self._admit(need, wait=True)
+            admitted[0] = need
+
+        try:
+            st = B.prepare(be, target, dm=dm, before_factor=admit)
+        except Exception:
+            dm.close()
+            if admitted[0]:
+                self._release(admitted[0])
+            raise
+        return st, admitted[0], mk
+
     def _do_solve(self, be, reqs: List[Request]):
         models = [r.model for r in reqs]
-        est = sum(24 * 6 * m.n_nodes * 60 for m in models)   # rough pre-analysis estimate
-        self._admit(est)
-        out = solve_pack(be, models, self.tol)
-        keys = self._register(out["state"]["dm"], out["state"], out["pack"], models)
+        pack = PackedModel(models)
+        st, reserved, mk = self._prepare(be, models[0], pack if len(models) > 1 else None)
+        try:
+            if len(models) > 1:
+                F, scales = pack.load_columns()
+                tol_c = 0.5 * self.tol / math.sqrt(len(models))
+                U, rep = st["dm"].solve(F, tol_c, max(be.max_ir, 30), raise_on_stall=False)
+                res = member_residuals(st["dm"], pack, U, F, st["free"], [len(sc) for sc in scales])
+                Us = pack.split(U, scales)
+            else:
+                F = models[0].load_matrix()
+                U, rep = st["dm"].solve(F, 0.5 * self.tol, max(be.max_ir, 30), raise_on_stall=False)
+                R = st["dm"].residual(U, F)
+                mask = np.zeros(models[0].ndof, bool)
+                mask[st["free"]] = True
+                res = [np.linalg.norm(R[mask], axis=0) / np.maximum(np.linalg.norm(F[mask], axis=0), 1e-300)]
+                Us = [U]
+        except Exception:
+            st["dm"].close()
+            self._release(reserved)
+            raise
+        keys = self._register(st["dm"], st, pack, models, reserved=reserved, mesh=mk)
         for k, r in enumerate(reqs):
-            self._finish(r, {"key": keys[k], "U": out["U"][k], "rel_residual": out["residuals"][k],
-                             "batch": len(reqs)})
+            self._finish(r, {"key": keys[k], "U": Us[k], "rel_residual": res[k], "batch": len(reqs),
+                             "report": rep})
 
     def _member_solve(self, res: Resident, loads: Optional[np.ndarray]):
         pack = res.pack
-        L = [None] * len(pack.members)
-        L[res.index] = res.model.load_matrix() if loads is None else loads
+        Lm = res.model.load_matrix() if loads is None else np.asarray(loads)
+        if Lm.ndim == 1:
+            Lm = Lm[:, None]
         # only this member carries load; the others' columns are zero
-        F = np.zeros((pack.ndof, L[res.index].shape[1]), order="F")
+        F = np.zeros((pack.ndof, Lm.shape[1]), order="F")
         sl = pack.dof_slice(res.index)
         sc = []
         for c in range(F.shape[1]):
-            nrm = float(np.linalg.norm(L[res.index][:, c]))
-            s = 1.0 / nrm if nrm > 0 else 1.0
-            F[sl, c] = L[res.index][:, c] * s
-            sc.append(s)
+            nrm = float(np.linalg.norm(Lm[:, c]))
+            s_ = 1.0 / nrm if nrm > 0 else 1.0
+            F[sl, c] = Lm[:, c] * s_
+            sc.append(s_)
         U, rep = res.dm.solve(F, 0.5 * self.tol, 30, raise_on_stall=False)
         R = res.dm.residual(U, F)
         free = res.state["free"]
@@ -397,7 +515,7 @@ class SolveServer:
         mk = mask[sl]
         rel = np.linalg.norm(R[sl][mk], axis=0) / np.maximum(np.linalg.norm(F[sl][mk], axis=0), 1e-300)
         Um = np.asfortranarray(U[sl] / np.asarray(sc)[None, :])
-        return {"U": Um, "rel_residual": rel}
+        return {"U": Um, "rel_residual": rel, "report": rep}
 
     def _lookup(self, key: str) -> Resident:
         with self.rlock:
@@ -407,6 +525,24 @@ class SolveServer:
             res.last_used = time.perf_counter()
             return res
 
+    def _lookup_or_readmit(self, be, key: str) -> Resident:
+        """The resident of `key`; a model freed meanwhile is prepared again
+        from its host description and registered under the same key."""
+        with self.rlock:
+            res = self.registry.get(key)
+            if res is not None:
+                res.last_used = time.perf_counter()
+                return res
+            model = self.evicted.get(key)
+        if model is None:
+            raise KeyError(f"model {key} is unknown")
+        st, reserved, mk = self._prepare(be, model, None)
+        pack = PackedModel([model])
+        self._register(st["dm"], st, pack, [model], reserved=reserved, keys=[key], mesh=mk)
+        with self.rlock:
+            self.readmissions += 1
+        return self._lookup(key)
+
     @staticmethod
     def _check_live(res: Resident, key: str):
         """Called with res.lock held: the group may have been evicted between
@@ -414,26 +550,38 @@ class SolveServer:
         if res.evicted:
             raise KeyError(f"model {key} is not resident (evicted or unknown)")
 
-    def _do_resolve(self, req: Request):
-        res = self._lookup(req.key)
-        with res.lock:
-            self._check_live(res, req.key)
-            out = self._member_solve(res, req.loads)
+    def _do_resolve(self, be, req: Request):
+        for _ in range(3):
+            res = self._lookup_or_readmit(be, req.key)
+            with res.lock:
+                if res.evicted:
+                    continue       # freed between lookup and lock: admit it again
+                out = self._member_solve(res, req.loads)
+            break
+        else:
+            raise KeyError(f"model {req.key} could not be kept resident")
         out["key"] = req.key
         self._finish(req, out)
 
-    def _do_update(self, req: Request):
+    def _do_update(self, be, req: Request):
         """Thickness (section) update of a resident model: element kernels,
         assembly and the numeric factor rerun on the resident pattern and
         symbolic analysis, then the solve."""
-        res = self._lookup(req.key)
-        with res.lock:
-            self._check_live(res, req.key)
-            off = res.pack.q4_off[res.index]
-            res.dm.update_q4_sections(np.asarray(req.elems, np.int32) + off, req.sections)
-            res.pack._q4s[np.asarray(req.elems) + off] = req.sections
-            res.dm.assemble()
-            res.dm.factor(self.precision)
-            out = self._member_solve(res, req.loads)
+        for _ in range(3):
+            res = self._lookup_or_readmit(be, req.key)
+            with res.lock:
+                if res.evicted:
+                    continue
+                off = res.pack.q4_off[res.index]
+                res.dm.update_q4_sections(np.asarray(req.elems, np.int32) + off, req.sections)
+                res.pack._q4s[np.asarray(req.elems) + off] = req.sections
+                # keep the host description current (a freed model is re-admitted from it)
+                res.model.q4_sect_override = res.pack._q4s[off:res.pack.q4_off[res.index + 1]].copy()
+                res.dm.assemble()
+                res.dm.factor(self.precision)
+                out = self._member_solve(res, req.loads)
+            break
+        else:
+            raise KeyError(f"model {req.key} could not be kept resident")
         out["key"] = req.key
         self._finish(req, out)

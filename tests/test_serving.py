@@ -83,15 +83,42 @@ def test_server_mix_resolve_update_and_latency(alone):
         srv.close()
 
 
-def test_server_evicts_under_budget():
+def test_server_evicts_under_budget_and_readmits(alone):
+    """With a budget too small for two models, the second evicts the first;
+    a later re-solve of the first re-admits it from its host description and
+    still gives the model's own result."""
     srv = S.SolveServer(slots=1, tol=RESID_TOL, hbm_budget_bytes=1.0, small_dof=0)
     try:
         a = srv.solve(M.stiffened_panel(SEEDS[0])).result(timeout=600)
         b = srv.solve(M.stiffened_panel(SEEDS[1])).result(timeout=600)
         assert a["key"] != b["key"]
+        assert a["key"] not in srv.registry
+        r = srv.resolve(a["key"]).result(timeout=600)
+        assert srv.stats()["readmissions"] == 1
+        assert _rel(r["U"], alone[SEEDS[0]]) <= DISP_RTOL
         with pytest.raises(KeyError):
-            srv.resolve(a["key"]).result(timeout=600)
-        srv.resolve(b["key"]).result(timeout=600)
+            srv.resolve("no-such-model").result(timeout=600)
+    finally:
+        srv.close()
+
+
+def test_server_shares_the_structure_of_a_resident_mesh():
+    """Two wing panels of one mesh (different thicknesses): the second takes
+    over the first's pattern and symbolic analysis and matches its own
+    stand-alone solve; a thickness update and re-solve keep working."""
+    a = M.wing_panel(nx=24, ny=36, n_blades=3, blade_nz=4, n_cases=2, seed=5)
+    b = M.wing_panel(nx=24, ny=36, n_blades=3, blade_nz=4, n_cases=2, seed=6)
+    be = B.JFEMGPUBackend(tol=RESID_TOL)
+    ref = B.solve_model(be, b)
+    Ub = np.stack([sc["raw_displacement"] for sc in ref["subcases"]], axis=1)
+    ref["state"]["dm"].close()
+    srv = S.SolveServer(slots=2, tol=RESID_TOL, small_dof=0)
+    try:
+        srv.solve(a).result(timeout=600)
+        rb = srv.solve(b).result(timeout=600)
+        assert srv.stats()["shared_structures"] == 1
+        assert _rel(rb["U"], Ub) <= DISP_RTOL
+        assert rb["rel_residual"].max() <= RESID_TOL
     finally:
         srv.close()
 
