@@ -209,11 +209,15 @@ jfg_status jfg_assemble_values_noalloc(jfg_model* model, double* nzval_dev);
 /* ---- instrumentation ----------------------------------------------------- */
 /* Number of kernels this library has launched since load.                   */
 int64_t jfg_launch_count(void);
-/* When on, the library brackets the launches of its main kernels with CUDA
- * events on its stream and accumulates, per kernel class, launches, device
- * milliseconds and algorithmic work (which: 0 = Schur-complement update,
- * flops; 1 = CQUAD4 element kernel, bytes; 2 = assembly gather, bytes;
- * 3 = triangular solves, bytes; 4 = CTETRA10 element kernel, bytes).        */
+/* When on (1), the library brackets the launches of its main kernels with
+ * CUDA events on its stream and accumulates, per kernel class, launches,
+ * device milliseconds and algorithmic work (which: 0 = Schur-complement
+ * update, flops; 1 = CQUAD4 element kernel, bytes; 2 = assembly gather,
+ * bytes; 3 = triangular solves, bytes; 4 = CTETRA10 element kernel, bytes).
+ * Level 2 also brackets every factor and solve kernel class (5 = extend-add,
+ * 6 = diagonal-block Cholesky and inverse, flops; 7 = panel triangular
+ * solve, flops; 8 = panel updates, flops; 9..13 = solve sweeps).  While on,
+ * the factor and solve loops run eagerly instead of as CUDA graphs.        */
 jfg_status jfg_set_profiling(int32_t on);
 jfg_status jfg_get_kernel_stats(int32_t which, double* out3);
 jfg_status jfg_reset_kernel_stats(void);

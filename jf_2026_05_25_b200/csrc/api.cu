@@ -11,12 +11,13 @@ namespace jfg {
 
 static std::atomic<int64_t> g_launches{0};
 static KernelStats g_stats;
-static bool g_prof = false;
+static int g_prof = 0;   // 0 off, 1 coarse kernel classes, 2 every class
 void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 int64_t launch_count() { return g_launches.load(); }
 KernelStats& kernel_stats() { return g_stats; }
-bool profiling_enabled() { return g_prof; }
-void set_profiling(bool on) { g_prof = on; }
+bool profiling_enabled() { return g_prof > 0; }
+int profiling_level() { return g_prof; }
+void set_profiling(int level) { g_prof = level < 0 ? 0 : (level > 2 ? 2 : level); }
 
 struct ProfSlot { cudaEvent_t a = nullptr, b = nullptr; int kind = 0; double units = 0; bool live = false; };
 static std::vector<ProfSlot> g_slots;
@@ -537,7 +538,7 @@ jfg_status jfg_get_timings(jfg_model* m, double* s4) {
 int64_t jfg_launch_count(void) { return launch_count(); }
 
 jfg_status jfg_set_profiling(int32_t on) {
-  set_profiling(on != 0);
+  set_profiling(on);
   return JFG_OK;
 }
 

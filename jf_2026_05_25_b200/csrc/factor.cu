@@ -105,11 +105,12 @@ struct NumericFactor {
 namespace jfg {
 namespace {
 
-// fine-grained per-kernel-class event brackets (JFG_FINE_PROFILE=1)
+// fine-grained per-kernel-class event brackets (profiling level 2, or
+// JFG_FINE_PROFILE=1 with profiling on)
 inline bool fine_prof() {
   static int v = -1;
   if (v < 0) v = std::getenv("JFG_FINE_PROFILE") ? 1 : 0;
-  return v == 1 && profiling_enabled();
+  return profiling_level() >= 2 || (v == 1 && profiling_enabled());
 }
 
 // Launch-bound sequences (the level loop of the factorisation, the level and
@@ -1258,6 +1259,37 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
                                                             F->parent, F->Lptr, F->Uptr, F->relptr, F->rel, Lf, Uf, 0);
         count_launch(); } prof_end(ps_, st, KS_F_EA, 0.0); }
     }
+    // algorithmic flops of the level's diagonal-block, trsm and panel-update
+    // launches (kernel-class statistics only): fronts i < n of the level,
+    // widths lv.cs[i], rows sn_m
+    const bool count_work = fine_prof();
+    auto front_m = [&](int i) -> double { return (double)S.sn_m[S.level_sn[lv.off + i]]; };
+    auto potrf_flops = [&](int n, int k0) {
+      double f = 0;
+      for (int i = 0; count_work && i < n; ++i) {
+        const double kn = std::min(NB, lv.cs[i] - k0);
+        f += (2.0 / 3.0) * kn * kn * kn;   // Cholesky and inverse of the block
+      }
+      return f;
+    };
+    auto trsm_flops = [&](int n, int k0) {
+      double f = 0;
+      for (int i = 0; count_work && i < n; ++i) {
+        const double kn = std::min(NB, lv.cs[i] - k0);
+        f += 2.0 * kn * kn * std::max(0.0, front_m(i) - k0 - kn);
+      }
+      return f;
+    };
+    // C -= A B^T on the lower trapezoid rows r0.., columns r0..ce of K columns
+    auto update_flops = [&](int n, int kb, int ke, int r0, int cend) {
+      double f = 0;
+      for (int i = 0; count_work && i < n; ++i) {
+        const double K = std::min(ke, lv.cs[i]) - kb;
+        const double rows = front_m(i) - r0, cols = std::min(cend, lv.cs[i]) - r0;
+        if (K > 0 && rows > 0 && cols > 0) f += 2.0 * K * (rows * cols - cols * (cols - 1.0) / 2.0);
+      }
+      return f;
+    };
     // blocked partial factorisation of every front of the level, in
     // super-panels of PW columns: inside a super-panel the 64-column steps
     // update only the super-panel's own later columns; the columns after it
@@ -1269,21 +1301,21 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
         const int na = lv.active(k0);   // fronts wider than k0: a prefix of the list
         { int ps_ = fine_prof() ? prof_start(st) : -1; { k_potrf_diag<T><<<na, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr,
                                                                                F->Dptr, Lf, Dvf, k0, F->err);
-          count_launch(); } prof_end(ps_, st, KS_F_POTRF, 0.0); }
+          count_launch(); } prof_end(ps_, st, KS_F_POTRF, potrf_flops(na, k0)); }
         int rows_max = lv.maxm(na) - k0 - 1;
         if (rows_max <= 0) continue;
         unsigned gx = (unsigned)((rows_max + 63) / 64);
         { int ps_ = fine_prof() ? prof_start(st) : -1; { k_trsm_panel<T><<<dim3(gx, na), 256, 2 * NB * (NB + 1) * sizeof(T), st>>>(list, F->first, F->mrows,
                                                                                         F->Lptr, F->Dptr, Lf, Dvf, k0,
                                                                                         tc ? F->Phi : nullptr, F->Plo, F->PKptr);
-          count_launch(); } prof_end(ps_, st, KS_F_TRSM, 0.0); }
+          count_launch(); } prof_end(ps_, st, KS_F_TRSM, trsm_flops(na, k0)); }
         const int nu = lv.active(k0 + NB);   // fronts with columns after this block
         int nrow = lv.maxm(nu) - k0 - NB, ncol = std::min(P1, lv.max_c) - k0 - NB;
         if (nu > 0 && nrow > 0 && ncol > 0) {
           int64_t tiles = (int64_t)((nrow + TILE - 1) / TILE) * ((ncol + TILE - 1) / TILE);
           { int ps_ = fine_prof() ? prof_start(st) : -1;
             update(0, k0, k0 + NB, P1, nrow, ncol, tiles, nu);
-            prof_end(ps_, st, KS_F_PANEL, 0.0); }
+            prof_end(ps_, st, KS_F_PANEL, update_flops(nu, k0, k0 + NB, k0 + NB, P1)); }
         }
       }
       const int nt = lv.active(P1);   // fronts with columns after the super-panel
@@ -1292,7 +1324,7 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
         int64_t tiles = (int64_t)((nrow + TILE - 1) / TILE) * ((ncol + TILE - 1) / TILE);
         { int ps_ = fine_prof() ? prof_start(st) : -1;
           update(0, P0, P1, INT_MAX, nrow, ncol, tiles, nt);
-          prof_end(ps_, st, KS_F_PANEL, 0.0); }
+          prof_end(ps_, st, KS_F_PANEL, update_flops(nt, P0, P1, P1, INT_MAX)); }
       }
     }
     if (lv.max_r > 0) {

@@ -27,7 +27,8 @@ struct KernelStats {
 };
 KernelStats& kernel_stats();
 bool profiling_enabled();
-void set_profiling(bool on);
+int profiling_level();
+void set_profiling(int level);
 // Event brackets around instrumented launches (no-ops when profiling is off).
 int prof_start(cudaStream_t st);
 void prof_end(int slot, cudaStream_t st, int kind, double units);

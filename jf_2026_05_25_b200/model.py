@@ -187,7 +187,7 @@ class Sol101Model:
             for a in range(3):
                 Fn[:, a] += np.bincount(nidx, weights=vec[:, a], minlength=nn_tot)
         R = self.node_R
-        if not np.allclose(R, np.tile([1, 0, 0, 0, 1, 0, 0, 0, 1], (self.n_nodes, 1))):
+        if not self._identity_frames():
             Rm = R.reshape(-1, 3, 3, order="C").transpose(0, 2, 1)  # column-major -> matrix
             Fn = F.reshape(-1, 6)
             Fn[:, 0:3] = np.einsum("nji,nj->ni", Rm, Fn[:, 0:3])
@@ -195,9 +195,23 @@ class Sol101Model:
             F = Fn.reshape(-1)
         return F
 
+    def _identity_frames(self) -> bool:
+        """True when every grid's displacement frame is the basic frame
+        (cached against the node_R array it was computed for)."""
+        R = self.node_R
+        c = getattr(self, "_ident_cache", None)
+        if c is None or c[0] is not R:
+            ident = bool((R[:, [0, 4, 8]] == 1.0).all() and (R[:, [1, 2, 3, 5, 6, 7]] == 0.0).all())
+            self._ident_cache = (R, ident)
+            return ident
+        return c[1]
+
     def load_matrix(self) -> np.ndarray:
         """ndof x nrhs column-major (Fortran order) matrix of all subcases."""
-        return np.asfortranarray(np.stack([self.load_vector(c) for c in self.load_cases], axis=1))
+        F = np.empty((self.ndof, len(self.load_cases)), order="F")
+        for k, c in enumerate(self.load_cases):
+            F[:, k] = self.load_vector(c)
+        return F
 
     def spc_dofs(self) -> np.ndarray:
         """SPC1 DOFs (boundary_conditions.jl:1499-1540)."""
@@ -419,6 +433,30 @@ def wing_panel(nx: int = 200, ny: int = 400, lx: float = 1.0, ly: float = 2.0,
         spc1=[("123456", clamp)], load_cases=cases, seed=seed)
 
 
+def wing_panel_variant(base: Sol101Model, seed: int, n_cases: int, t_skin=(1.5e-3, 4.0e-3),
+                       t_blade: float = 3e-3, pressure: float = 5e3, edge_sigma: float = 100.0) -> Sol101Model:
+    """A wing-box panel of the same mesh as ``base`` (a ``wing_panel``): new
+    per-row skin thicknesses U[t_skin] and ``n_cases`` subcases (PLOAD4
+    `pressure` on the skin plus seeded N(0, edge_sigma) forces on the free-edge
+    grids), drawn from ``seed``.  The mesh arrays are shared with ``base``."""
+    rng = _rng([seed, 77])
+    rows = sorted(p for p in base.pshells if p >= 100)
+    t_rows = rng.uniform(t_skin[0], t_skin[1], size=len(rows))
+    pshells = {p: PShell(T=float(t_rows[k]), MID1=1, MID2=1, MID3=1) for k, p in enumerate(rows)}
+    pshells[2] = PShell(T=t_blade, MID1=1, MID2=1, MID3=1)
+    skin = np.where(base.q4_pid >= 100)[0]
+    ly = base.xyz[:, 1].max()
+    tip = np.where(np.isclose(base.xyz[:, 1], ly))[0]
+    cases = []
+    for c in range(n_cases):
+        crng = _rng([seed, 1000 + c])
+        cases.append(LoadCase(sid=c + 1, pload4=(skin, np.full(len(skin), pressure)),
+                              forces=(tip, crng.normal(0.0, edge_sigma, size=(len(tip), 3)))))
+    return Sol101Model(name=f"{base.name}_v{seed}", grid_ids=base.grid_ids, xyz=base.xyz, node_R=base.node_R,
+                       q4_nodes=base.q4_nodes, q4_pid=base.q4_pid, q4_eid=base.q4_eid, pshells=pshells,
+                       mats=base.mats, k6rot=base.k6rot, spc1=base.spc1, load_cases=cases, seed=seed)
+
+
 _KUHN_PERMS = [(0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)]
 _T10_EDGES = ((0, 1), (1, 2), (0, 2), (0, 3), (1, 3), (2, 3))
 
@@ -492,7 +530,7 @@ def solid_block(n: int = 40, L: float = 0.3, E: float = 210e9, nu: float = 0.3,
         load_cases=cases, seed=seed)
 
 
-def stiffened_panel(seed: int) -> Sol101Model:
+def stiffened_panel(seed: int, n_cases: Optional[int] = None) -> Sol101Model:
     """One batched-serving panel: skin nx,ny ~ U{8..64} CQUAD4 (10 mm), 0-6
     blades of depth U{4..8} elements, t ~ U[1,6] mm, edges clamped or simply
     supported, 1-16 subcases of PLOAD4 U[1,20] kPa + N(0,50 N) nodal forces.
@@ -529,7 +567,8 @@ def stiffened_panel(seed: int) -> Sol101Model:
         c00 = np.where(edges[0] & edges[2])[0]
         c10 = np.where(edges[1] & edges[2])[0]
         spc.append(("12", c00[:1])); spc.append(("2", c10[:1]))
-    n_cases = int(rng.integers(1, 17))
+    drawn = int(rng.integers(1, 17))
+    n_cases = drawn if n_cases is None else int(n_cases)
     n_skin_el = nx * ny
     free_nodes = np.setdiff1d(np.arange(len(xyz)), np.concatenate([s[1] for s in spc]))
     cases = []

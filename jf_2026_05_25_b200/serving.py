@@ -40,6 +40,10 @@ from . import backend as B
 from . import lib
 
 
+def _is_tensor(x) -> bool:
+    return x is not None and type(x).__module__.startswith("torch")
+
+
 class PackedModel:
     """Block-diagonal union of independent models (the batch unit)."""
 
@@ -177,6 +181,10 @@ class Request:
     loads: Optional[np.ndarray] = None # ndof x nrhs for "resolve"/"update" (None: the model's own cases)
     elems: Optional[np.ndarray] = None # CQUAD4 indices for "update"
     sections: Optional[np.ndarray] = None
+    # device-resident input and output: `loads` is a CUDA tensor (nrhs x ndof,
+    # i.e. the ndof x nrhs column-major load matrix) and the result's "U" is
+    # one too; for "solve" it replaces the model's own load cases
+    device: bool = False
     t_submit: float = 0.0
     future: Future = field(default_factory=Future)
 
@@ -263,14 +271,17 @@ class SolveServer:
             self.plock.notify()
         return req.future
 
-    def solve(self, model) -> Future:
-        return self.submit(Request("solve", model=model))
+    def solve(self, model, device_loads=None) -> Future:
+        """New model; ``device_loads`` (CUDA tensor, nrhs x ndof) keeps the
+        loads and the displacements in device memory."""
+        return self.submit(Request("solve", model=model, loads=device_loads, device=device_loads is not None))
 
-    def resolve(self, key: str, loads: Optional[np.ndarray] = None) -> Future:
-        return self.submit(Request("resolve", key=key, loads=loads))
+    def resolve(self, key: str, loads=None) -> Future:
+        return self.submit(Request("resolve", key=key, loads=loads, device=_is_tensor(loads)))
 
-    def update(self, key: str, elems: np.ndarray, sections: np.ndarray, loads: Optional[np.ndarray] = None) -> Future:
-        return self.submit(Request("update", key=key, elems=elems, sections=sections, loads=loads))
+    def update(self, key: str, elems: np.ndarray, sections: np.ndarray, loads=None) -> Future:
+        return self.submit(Request("update", key=key, elems=elems, sections=sections, loads=loads,
+                                   device=_is_tensor(loads)))
 
     def close(self):
         with self.plock:
@@ -309,8 +320,8 @@ class SolveServer:
             batch, dof = [first], first.model.ndof
             rest = []
             for r in self.pending:
-                if (r.kind == "solve" and r.model.ndof <= self.small_dof and len(batch) < self.pack_models
-                        and dof + r.model.ndof <= self.pack_dof):
+                if (r.kind == "solve" and r.device == first.device and r.model.ndof <= self.small_dof
+                        and len(batch) < self.pack_models and dof + r.model.ndof <= self.pack_dof):
                     batch.append(r)
                     dof += r.model.ndof
                 else:
@@ -320,6 +331,7 @@ class SolveServer:
 
     def _worker(self, slot: int):
         be = self.backends[slot]
+        be._tstream = None      # this slot's torch stream for device-resident loads
         while True:
             work = self._take()
             if work is None:
@@ -341,7 +353,7 @@ class SolveServer:
         with self.rlock:
             self.latencies.append(dt)
             self.kinds.append(req.kind)
-            self.subcase_solves += int(result["U"].shape[1])
+            self.subcase_solves += int(result["U"].shape[0] if req.device else result["U"].shape[1])
         result["latency_s"] = dt
         req.future.set_result(result)
 
@@ -470,7 +482,9 @@ class SolveServer:
         pack = PackedModel(models)
         st, reserved, mk = self._prepare(be, models[0], pack if len(models) > 1 else None)
         try:
-            if len(models) > 1:
+            if reqs[0].device:
+                Us, res, rep = self._device_solve(be, st["dm"], pack, [r.loads for r in reqs], self.tol)
+            elif len(models) > 1:
                 F, scales = pack.load_columns()
                 tol_c = 0.5 * self.tol / math.sqrt(len(models))
                 U, rep = st["dm"].solve(F, tol_c, max(be.max_ir, 30), raise_on_stall=False)
@@ -493,7 +507,41 @@ class SolveServer:
             self._finish(r, {"key": keys[k], "U": Us[k], "rel_residual": res[k], "batch": len(reqs),
                              "report": rep})
 
-    def _member_solve(self, res: Resident, loads: Optional[np.ndarray]):
+    def _device_solve(self, be, dm, pack: PackedModel, loads: List, tol: float, only: Optional[int] = None):
+        """Solve with loads and displacements in device memory.  loads[k]
+        (CUDA tensor nrhs_k x ndof_k) belongs to member k (or to member
+        `only`).  Every member's columns are scaled to unit norm in the packed
+        load matrix and the tolerance divided by sqrt(members), so that the
+        reported relative residual bounds each member's own.
+        Returns (list of U tensors, list of residual arrays, report)."""
+        import torch
+        if be._tstream is None:
+            be._tstream = torch.cuda.Stream()
+        members = [only] if only is not None else list(range(len(loads)))
+        with torch.cuda.stream(be._tstream):
+            ncol = max(int(L.shape[0]) for L in loads)
+            F = torch.zeros((ncol, pack.ndof), dtype=torch.float64, device="cuda")
+            scales = []
+            for k, L in zip(members, loads):
+                sl = pack.dof_slice(k)
+                nrm = torch.linalg.vector_norm(L, dim=1)
+                sc = torch.where(nrm > 0, 1.0 / nrm, torch.ones_like(nrm))
+                F[:L.shape[0], sl] = L * sc[:, None]
+                scales.append(sc)
+            U = torch.zeros_like(F)
+        be._tstream.synchronize()
+        tol_c = tol / math.sqrt(max(1, len(members))) * (0.5 if len(members) > 1 else 1.0)
+        rep = dm.solve_device(F.data_ptr(), U.data_ptr(), ncol, tol_c, max(be.max_ir, 30), raise_on_stall=False)
+        with torch.cuda.stream(be._tstream):
+            Us = [U[:L.shape[0], pack.dof_slice(k)] / sc[:, None] for k, L, sc in zip(members, loads, scales)]
+        be._tstream.synchronize()
+        res = [np.full(int(L.shape[0]), rep["rel_residual"]) for L in loads]
+        return Us, res, rep
+
+    def _member_solve(self, res: Resident, loads, be=None, device: bool = False):
+        if device:
+            Us, rr, rep = self._device_solve(be, res.dm, res.pack, [loads], 0.5 * self.tol, only=res.index)
+            return {"U": Us[0], "rel_residual": rr[0], "report": rep}
         pack = res.pack
         Lm = res.model.load_matrix() if loads is None else np.asarray(loads)
         if Lm.ndim == 1:
@@ -556,7 +604,7 @@ class SolveServer:
             with res.lock:
                 if res.evicted:
                     continue       # freed between lookup and lock: admit it again
-                out = self._member_solve(res, req.loads)
+                out = self._member_solve(res, req.loads, be, req.device)
             break
         else:
             raise KeyError(f"model {req.key} could not be kept resident")
@@ -579,7 +627,7 @@ class SolveServer:
                 res.model.q4_sect_override = res.pack._q4s[off:res.pack.q4_off[res.index + 1]].copy()
                 res.dm.assemble()
                 res.dm.factor(self.precision)
-                out = self._member_solve(res, req.loads)
+                out = self._member_solve(res, req.loads, be, req.device)
             break
         else:
             raise KeyError(f"model {req.key} could not be kept resident")

@@ -143,3 +143,26 @@ def test_autotune_picks_a_candidate_and_keeps_results(alone):
             assert _rel(U, alone[SEEDS[0]]) <= DISP_RTOL
         finally:
             AT.apply({})
+
+
+def test_server_device_resident_loads_match_host(alone):
+    """Loads given as CUDA tensors (and displacements returned as CUDA
+    tensors) give the same result as host buffers, for a packed batch of new
+    models and for a re-solve."""
+    import torch
+    srv = S.SolveServer(slots=1, tol=RESID_TOL, small_dof=20000, pack_dof=40000)
+    try:
+        models = {s: M.stiffened_panel(s) for s in SEEDS[:3]}
+        futs = {s: srv.solve(m, device_loads=torch.from_numpy(np.ascontiguousarray(m.load_matrix().T)).cuda())
+                for s, m in models.items()}
+        res = {s: f.result(timeout=600) for s, f in futs.items()}
+        for s in models:
+            U = res[s]["U"].cpu().numpy().T
+            assert _rel(U, alone[s]) <= DISP_RTOL
+            assert res[s]["rel_residual"].max() <= RESID_TOL
+        s0 = SEEDS[0]
+        F2 = torch.from_numpy(np.ascontiguousarray((3.0 * models[s0].load_matrix()).T)).cuda()
+        r2 = srv.resolve(res[s0]["key"], F2).result(timeout=600)
+        assert _rel(r2["U"].cpu().numpy().T, 3.0 * alone[s0]) <= DISP_RTOL
+    finally:
+        srv.close()
