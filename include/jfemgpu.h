@@ -46,9 +46,7 @@ typedef enum {
   JFG_PREC_FP64 = 0,        /* plain FP64 supernodal Cholesky                      */
   JFG_PREC_MIXED = 1        /* FP32-storage factor, FP64 iterative refinement on
                                the FP64 CSR matrix; front updates on the tensor
-                               cores in 3xTF32 for solid-only models, SIMT FP32
-                               where shells are present (JFG_TENSOR_CORES=1/0
-                               forces either)                                   */
+                               cores in 3xTF32 (JFG_TENSOR_CORES=0: SIMT FP32) */
 } jfg_precision;
 
 typedef struct jfg_ctx jfg_ctx;

@@ -73,6 +73,7 @@ struct NumericFactor {
   float *Phi = nullptr, *Plo = nullptr, *tc_zero = nullptr;
   int64_t* PKptr = nullptr;
   int64_t pk_len = 0;
+  int tc_drain = 1;           // K-slices per tensor-memory accumulator use
   float* U32 = nullptr;
   double* scale = nullptr;    // n, symmetric diagonal scaling of the mixed factor
   // inverse diagonal blocks of the strip solve
@@ -1245,7 +1246,8 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
       if constexpr (sizeof(T) == 4) {
         if (tc && max_rows >= tc_min && max_cols >= tc_min / 2 &&
             tc::front_update_tf32x3(list, cnt, F->first, F->mrows, F->Lptr, F->Uptr, Lf, F->Phi, F->Plo,
-                                    F->PKptr, F->tc_zero, Uf, mode, kbeg, kend, cend, max_rows, max_cols, F->err, st))
+                                    F->PKptr, F->tc_zero, Uf, mode, kbeg, kend, cend, max_rows, max_cols,
+                                    F->tc_drain, F->err, st))
           return;
       }
       launch_front_update<T>((unsigned)tiles, cnt, F, Lf, Uf, mode, kbeg, kend, cend, st);
@@ -1711,14 +1713,17 @@ jfg_status numeric_factor(jfg_model* m, int precision) {
       { k_scatter_A<float><<<ga, 256, 0, st>>>(F->n_amap, F->amap_src, F->amap_dst, F->amap_pr, F->amap_pc,
                                              m->d_nzval, F->scale, F->L32); count_launch(); }
     F->have32 = false;
-    // tensor-core updates by default for solid-only models; shell models
-    // (drilling DOFs, thin-shell conditioning) keep the FP32 SIMT updates:
-    // the 3xTF32 tensor-core sums carry one-sided errors of about 1e-6 per
-    // K-slice (truncating accumulation in tensor memory, missing lo*lo), which
-    // on the 914k-DOF wing panel raise refinement from 8 to 13 iterations
-    // while on the CTETRA10 block the iteration count is unchanged
+    // tensor-core 3xTF32 updates for every model (JFG_TENSOR_CORES=0: FP32
+    // SIMT).  The tensor core's own sums carry one-sided errors (truncating
+    // accumulation in tensor memory, no lo*lo term), so their length is
+    // chosen by model: shell models (thin-shell and drilling stiffness)
+    // drain every 16-column K-slice into FP32 registers -- 9 refinement steps
+    // on the 914k-DOF wing panel against 8 with the SIMT updates and 13 with
+    // 64-column sums -- while solid-only models let the tensor core sum 64
+    // columns (4 steps on the CTETRA10 block either way)
     const int tcs = tc::setting();
-    const bool use_tc = tcs == 1 || (tcs < 0 && m->n_q4 + m->n_q8 == 0);
+    const bool use_tc = tcs != 0;
+    F->tc_drain = tc::drain_slices(m->n_q4 + m->n_q8 > 0 ? 1 : 4);
     if (use_tc && !F->Phi) {
       // packed operand images: ceil(c/16) x ceil(m/8) atoms of 128 floats per
       // front, offsets relative to the front's level region

@@ -376,10 +376,16 @@ int setting() {
 
 bool enabled() { return setting() != 0; }
 
+int drain_slices(int dflt) {
+  const char* de = std::getenv("JFG_TC_DRAIN");
+  int v = de ? std::atoi(de) : dflt;
+  return v < 1 ? 1 : (v > 16 ? 16 : v);
+}
+
 bool front_update_tf32x3(const int32_t* list, int count, const int32_t* first, const int32_t* mrows,
                          const int64_t* Lptr, const int64_t* Uptr, float* L, const float* Phi, const float* Plo,
                          const int64_t* PKptr, const float* zero, float* U, int mode, int kbeg, int kend, int cend,
-                         int max_rows, int max_cols, DevError* err, cudaStream_t st) {
+                         int max_rows, int max_cols, int drain, DevError* err, cudaStream_t st) {
   if (!enabled() || !Phi || !Plo || !PKptr || !zero || count <= 0 || max_rows <= 0 || max_cols <= 0) return false;
   static bool attr = false;
   if (!attr) {
@@ -389,14 +395,7 @@ bool front_update_tf32x3(const int32_t* list, int count, const int32_t* first, c
   }
   const char* te = std::getenv("JFG_TC_TERMS");   // 4: add lo*lo
   const int terms = (te && te[0] == '4') ? 4 : 3;
-  // K-slices of 16 columns the tensor core sums per accumulator use before
-  // the drain warps add them in FP32 registers (JFG_TC_DRAIN, 1..16)
-  static int udr = -1;
-  if (udr < 0) {
-    const char* de = std::getenv("JFG_TC_DRAIN");
-    udr = de ? std::atoi(de) : 1;
-    udr = udr < 1 ? 1 : (udr > 16 ? 16 : udr);
-  }
+  const int udr = drain < 1 ? 1 : (drain > 16 ? 16 : drain);
   const int ext = mode == 1 ? 7 : 0;              // the mode-1 grid starts up to 7 rows early
   const int64_t tiles = (int64_t)((max_rows + ext + UM - 1) / UM) * ((max_cols + ext + UM - 1) / UM);
   k_update_tf32x3<<<dim3((unsigned)tiles, (unsigned)count), UTHREADS, USMEM, st>>>(

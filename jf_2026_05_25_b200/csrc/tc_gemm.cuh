@@ -24,11 +24,14 @@ namespace tc {
 bool front_update_tf32x3(const int32_t* list, int count, const int32_t* first, const int32_t* mrows,
                          const int64_t* Lptr, const int64_t* Uptr, float* L, const float* Phi, const float* Plo,
                          const int64_t* PKptr, const float* zero, float* U, int mode, int kbeg, int kend, int cend,
-                         int max_rows, int max_cols, DevError* err, cudaStream_t st);
+                         int max_rows, int max_cols, int drain, DevError* err, cudaStream_t st);
 
-// JFG_TENSOR_CORES, read at every call: 1 = on, 0 = off, -1 = not set (the
-// caller picks: on for solid-only models, off where shells are present).
+// JFG_TENSOR_CORES, read at every call: 1 = on, 0 = off, -1 = not set (on).
 int setting();
+
+// K-slices of 16 columns the tensor core sums per accumulator use before the
+// FP32 register drain: JFG_TC_DRAIN when set (1..16), else `dflt`.
+int drain_slices(int dflt);
 
 // Whether the tensor-core update may run at all (not switched off).
 bool enabled();
