@@ -3,7 +3,9 @@ Julia SOL101 path can be run on identical inputs elsewhere.
 
 ``write_bdf`` writes SOL 101 with one SUBCASE per load case: GRID (large
 field, full double precision), CQUAD4 / CQUAD8 / CTETRA (10 grids), PSHELL,
-PSOLID, MAT1, SPC1, PLOAD4, FORCE and PARAM,K6ROT.  ``read_bdf`` reads those
+PSOLID, MAT1, SPC1, PLOAD4, FORCE and PARAM,K6ROT.  The reference's bulk-data
+CTETRA reader keeps four grids, so CTETRA10 models go to the reference as
+Abaqus keyword input (``write_inp``: C3D10 and *CLOAD), which keeps all ten.  ``read_bdf`` reads those
 decks back (used by the round-trip tests; it understands exactly the cards
 written here).  ``write_reference_driver`` writes ``reproduce_reference.jl``,
 a driver for a machine with Julia and the reference package: it builds each
@@ -244,22 +246,155 @@ def read_bdf(path: str) -> "M.Sol101Model":
     return model
 
 
+# ----------------------------------------------------------------------------
+# Abaqus keyword input for CTETRA10 models
+# ----------------------------------------------------------------------------
+
+def write_inp(model, path: str, title: str = "") -> str:
+    """Abaqus keyword input of a CTETRA10 model: the reference's entry for
+    ten-node tetrahedra (its bulk-data CTETRA reader keeps only four grids,
+    src/parsing/extract_elements.jl:205-229; the Abaqus reader keeps all ten,
+    src/abaqus_input.jl:7-12).  *NODE (full double precision), *ELEMENT
+    TYPE=C3D10 (corners, then mid-edge nodes 1-2, 2-3, 3-1, 1-4, 2-4, 3-4, the
+    node order of the generated elements), one *MATERIAL / *ELASTIC and
+    *SOLID SECTION per solid property, the SPC1 translations as a model-level
+    *BOUNDARY on node sets, and one *STEP / *STATIC per subcase whose nodal
+    loads are a *CLOAD with OP=NEW (the reference turns step k into subcase k,
+    :455-545).  Shell elements have no Abaqus form here."""
+    if len(model.q4_nodes) or len(model.q8_nodes):
+        raise ValueError("write_inp writes CTETRA10 models only")
+    gid = np.asarray(model.grid_ids)
+    lines = ["*HEADING", title or model.name, "*NODE"]
+    for i in range(model.n_nodes):
+        x, y, z = model.xyz[i]
+        lines.append(f"{int(gid[i])}, {float(x)!r}, {float(y)!r}, {float(z)!r}")
+    pids = np.asarray(model.t10_pid)
+    eid0 = 1
+    for pid in np.unique(pids):
+        lines.append(f"*ELEMENT, TYPE=C3D10, ELSET=P{int(pid)}")
+        for e in np.where(pids == pid)[0]:
+            lines.append(", ".join([str(eid0 + int(e))] + [str(int(gid[n])) for n in model.t10_nodes[e]]))
+    for mid in sorted({model.psolids[int(p)] for p in np.unique(pids)}):
+        m = model.mats[mid]
+        lines += [f"*MATERIAL, NAME=M{mid}", "*ELASTIC", f"{float(m.E)!r}, {float(m.NU)!r}"]
+        if m.RHO:
+            lines += ["*DENSITY", f"{float(m.RHO)!r}"]
+    for pid in np.unique(pids):
+        lines.append(f"*SOLID SECTION, ELSET=P{int(pid)}, MATERIAL=M{model.psolids[int(pid)]}")
+    for k, (comps, nodes) in enumerate(model.spc1):
+        name = f"SPC{k + 1}"
+        lines.append(f"*NSET, NSET={name}")
+        ids = [str(int(gid[n])) for n in np.asarray(nodes)]
+        for a in range(0, len(ids), 16):
+            lines.append(", ".join(ids[a:a + 16]))
+        lines.append("*BOUNDARY")
+        for ch in comps:
+            if int(ch) > 3:
+                continue          # continuum grids carry translations only
+            lines.append(f"{name}, {int(ch)}, {int(ch)}")
+    for c in model.load_cases:
+        lines += [f"*STEP, NAME=SUBCASE{c.sid}", "*STATIC", "*CLOAD, OP=NEW"]
+        acc = {}
+        for item in (c.forces, c.cload):
+            if item is None:
+                continue
+            nidx, vec = item
+            for n, v in zip(np.asarray(nidx), np.asarray(vec, float)):
+                a = acc.setdefault(int(n), np.zeros(3))
+                a += v
+        if c.pload4 is not None:
+            raise ValueError("PLOAD4 has no CTETRA10 form; deliver face loads as nodal loads")
+        for n in sorted(acc):
+            for d in range(3):
+                if acc[n][d] != 0.0:
+                    lines.append(f"{int(gid[n])}, {d + 1}, {float(acc[n][d])!r}")
+        lines.append("*END STEP")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return path
+
+
+def read_inp(path: str) -> "M.Sol101Model":
+    """Read back a deck written by ``write_inp`` (exactly those keywords)."""
+    nodes, elems, mats, sections, nsets, bnd, steps = {}, {}, {}, {}, {}, [], []
+    key, opts, cur = None, {}, None
+    for raw in open(path):
+        line = raw.strip()
+        if not line or line.startswith("**"):
+            continue
+        if line.startswith("*"):
+            parts = [t.strip() for t in line[1:].split(",")]
+            key = parts[0].upper()
+            opts = dict((t.split("=", 1)[0].upper(), t.split("=", 1)[1] if "=" in t else "") for t in parts[1:])
+            if key == "STEP":
+                cur = {"name": opts.get("NAME", ""), "loads": []}
+                steps.append(cur)
+            elif key == "MATERIAL":
+                mats[opts["NAME"]] = {}
+            elif key == "SOLID SECTION":
+                sections[opts["ELSET"]] = opts["MATERIAL"]
+            elif key == "NSET":
+                nsets[opts["NSET"]] = []
+            continue
+        f = [t.strip() for t in line.split(",")]
+        if key == "NODE":
+            nodes[int(f[0])] = [float(v) for v in f[1:4]]
+        elif key == "ELEMENT":
+            elems[int(f[0])] = (opts["ELSET"], [int(v) for v in f[1:11]])
+        elif key == "ELASTIC":
+            mats[list(mats)[-1]]["E"], mats[list(mats)[-1]]["NU"] = float(f[0]), float(f[1])
+        elif key == "DENSITY":
+            mats[list(mats)[-1]]["RHO"] = float(f[0])
+        elif key == "NSET":
+            nsets[list(nsets)[-1]] += [int(v) for v in f if v]
+        elif key == "BOUNDARY":
+            bnd.append((f[0], int(f[1]), int(f[2])))
+        elif key == "CLOAD":
+            cur["loads"].append((int(f[0]), int(f[1]), float(f[2])))
+    gids = np.array(sorted(nodes), dtype=np.int64)
+    idx = {g: i for i, g in enumerate(gids)}
+    xyz = np.array([nodes[g] for g in gids])
+    eids = sorted(elems)
+    t10 = np.array([[idx[g] for g in elems[e][1]] for e in eids], np.int32)
+    set_pid = {name: int(name[1:]) for name in sections}
+    pid = np.array([set_pid[elems[e][0]] for e in eids], np.int64)
+    mid_of = {name: int(name[1:]) for name in mats}
+    psolids = {set_pid[s]: mid_of[m] for s, m in sections.items()}
+    mats_out = {mid_of[n]: M.Mat1(E=v["E"], NU=v["NU"], RHO=v.get("RHO", 0.0)) for n, v in mats.items()}
+    spc = {}
+    for name, a, b in bnd:
+        spc.setdefault(name, "")
+        spc[name] += "".join(str(c) for c in range(a, b + 1))
+    spc1 = [(comps, np.array([idx[g] for g in nsets[name]])) for name, comps in spc.items()]
+    cases = []
+    for k, st in enumerate(steps):
+        vec = {}
+        for g, d, v in st["loads"]:
+            vec.setdefault(idx[g], np.zeros(3))[d - 1] += v
+        ns = np.array(sorted(vec), np.int64)
+        cases.append(M.LoadCase(sid=k + 1, cload=(ns, np.array([vec[n] for n in ns]).reshape(-1, 3))))
+    return M.Sol101Model(name=os.path.basename(path), grid_ids=gids, xyz=xyz, t10_nodes=t10, t10_pid=pid,
+                         psolids=psolids, mats=mats_out, spc1=spc1, load_cases=cases)
+
+
 DRIVER = r'''# reproduce_reference.jl -- run the reference's own SOL101 on decks written by
-# jf_2026_05_25_b200.decks.write_bdf and store its results as JSON goldens.
+# jf_2026_05_25_b200.decks (write_bdf for shell models, write_inp for CTETRA10
+# models) and store its results as JSON goldens.
 #
-#   julia --project=<reference checkout> reproduce_reference.jl out_dir deck1.bdf [deck2.bdf ...]
+#   julia --project=<reference checkout> reproduce_reference.jl out_dir deck1.bdf [deck2.inp ...]
 #
-# For every deck: model = bdf_to_model(deck) (JFEMSolver.jl:69), results =
-# solve_model(model) (JFEMSolver.jl:2132, parity backend), then
-# <deck>.golden.json with, per subcase, raw_displacement (ndof, global DOF
-# order 6*(sorted GRID index) + component) and the SPC forces.
+# For every deck: model = input_to_model(deck) (JFEMSolver.jl:44-46: Abaqus
+# keyword input for .inp, bulk data otherwise), results = solve_model(model)
+# (JFEMSolver.jl:2132, parity backend), then <deck>.golden.json with, per
+# subcase, raw_displacement (ndof, global DOF order 6*(sorted GRID index) +
+# component) and the SPC forces.
 using OpenJFEM
 using JSON
 
 out_dir = ARGS[1]
 mkpath(out_dir)
 for deck in ARGS[2:end]
-    model = OpenJFEM.bdf_to_model(deck)
+    model = OpenJFEM.input_to_model(deck)
     results = OpenJFEM.solve_model(model)
     gold = Dict{String,Any}("deck" => basename(deck), "ndof" => results["ndof"], "subcases" => Any[])
     for sc in results["subcases"]

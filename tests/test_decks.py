@@ -50,4 +50,18 @@ def test_round_trip_plate_wing_q8_solid(tmp_path):
 def test_reference_driver_is_written(tmp_path):
     p = D.write_reference_driver(os.path.join(tmp_path, "reproduce_reference.jl"))
     txt = open(p).read()
-    assert "bdf_to_model" in txt and "solve_model" in txt
+    assert "input_to_model" in txt and "solve_model" in txt
+
+
+def test_solid_block_abaqus_round_trip(tmp_path):
+    """CTETRA10 models go to the reference as Abaqus C3D10 input (its bulk-
+    data CTETRA keeps only four grids): all ten nodes per element, the base
+    translations as *BOUNDARY, one step with *CLOAD OP=NEW per subcase."""
+    m = M.solid_block(n=2, n_cases=3)
+    path = D.write_inp(m, os.path.join(tmp_path, "block.inp"))
+    txt = open(path).read()
+    assert "*ELEMENT, TYPE=C3D10" in txt and txt.count("*STEP") == 3 and txt.count("*CLOAD, OP=NEW") == 3
+    r = D.read_inp(path)
+    _same(m, r, exact=True)
+    r2 = D.read_inp(D.write_inp(r, os.path.join(tmp_path, "block2.inp")))
+    _same(r, r2, exact=True)
