@@ -48,6 +48,7 @@ struct NumericFactor {
     int32_t ea_max_r;
     double schur_flops;   // sum over fronts of r(r+1) c (lower SYRK, 2 flops per FMA)
     int64_t pk_len = 0;   // floats of the packed tensor-core operand images of the level's fronts
+    int64_t nnz = 0;      // factor entries of the level's fronts (sum of m c)
     // the level's fronts are listed by decreasing width: cs[i] is the width
     // of the i-th, pm[i] the largest row count among the first i + 1
     std::vector<int32_t> cs, pm;
@@ -160,7 +161,18 @@ void drop_solve_graphs(NumericFactor* F) {
 
 constexpr int NB = 64;       // panel block width
 constexpr int TILE = 64;     // Schur-update tile
-constexpr int PW = 256;      // super-panel width of the blocked front factorisation
+// super-panel width of the blocked front factorisation (multiple of NB):
+// JFG_PANEL_WIDTH, default 256
+inline int panel_width() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = std::getenv("JFG_PANEL_WIDTH");
+    int w = e ? std::atoi(e) : 256;
+    w = std::max(64, std::min(2048, (w / 64) * 64));
+    v = w;
+  }
+  return v;
+}
 
 __device__ inline void rec_err(DevError* e, int32_t code, int64_t idx) {
   if (atomicCAS(&e->code, 0, code) == 0) e->index = idx;
@@ -1297,6 +1309,7 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
     // update only the super-panel's own later columns; the columns after it
     // take one update with K = PW, so the trailing part of a wide front is
     // read and written once per PW columns instead of once per 64
+    const int PW = panel_width();
     for (int P0 = 0; P0 < lv.max_c; P0 += PW) {
       const int P1 = P0 + PW;
       for (int k0 = P0; k0 < std::min(P1, lv.max_c); k0 += NB) {
@@ -1380,6 +1393,7 @@ void solve_inner(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int n
   for (size_t li = 0; li < F->levels.size(); ++li) {
     const auto& lv = F->levels[li];
     const int32_t* list = F->level_sn + lv.off;
+    const int pl = (fine_prof() && li < (size_t)KS_MAX_LEVELS) ? prof_start(st) : -1;
     { int ps_ = fine_prof() ? prof_start(st) : -1; { k_zero_V<<<lv.count, 256, 0, st>>>(list, F->first, F->mrows, F->relptr, nr, F->V); count_launch(); } prof_end(ps_, st, KS_S_VEC, 0.0); }
     for (const auto& seg : lv.ea)
       if (seg.second > 0)
@@ -1397,12 +1411,14 @@ void solve_inner(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int n
                                                               nr, n, F->tt, F->xp, F->V); count_launch(); } prof_end(ps_, st, KS_S_FUPD, 0.0); }
       }
     }
+    prof_end(pl, st, KS_LEVEL_FWD + (int)li, (double)sizeof(T) * (double)lv.nnz);
   }
   // backward, root first
   for (size_t li = F->levels.size(); li-- > 0;) {
     const auto& lv = F->levels[li];
     const int32_t* list = F->level_sn + lv.off;
     const int64_t* poff = F->part_off + lv.off;
+    const int pl = (fine_prof() && li < (size_t)KS_MAX_LEVELS) ? prof_start(st) : -1;
     int nstrip = (lv.max_c + SW - 1) / SW;
     for (int kb = nstrip - 1; kb >= 0; --kb) {
       const int na = lv.active(kb * SW);
@@ -1415,6 +1431,7 @@ void solve_inner(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int n
       { int ps_ = fine_prof() ? prof_start(st) : -1; { k_bwd_sdiag<T><<<dim3(SW / 32, na), 256, 0, st>>>(list, F->first, F->mrows, F->Sptr, poff, Sv, kb, nr, n,
                                                  F->part, F->tt, F->xp); count_launch(); } prof_end(ps_, st, KS_S_BDIAG, 0.0); }
     }
+    prof_end(pl, st, KS_LEVEL_BWD + (int)li, (double)sizeof(T) * (double)lv.nnz);
   }
   // algorithmic bytes: the factor read twice (forward and backward) plus the
   // permuted vectors read and written in each sweep
@@ -1542,6 +1559,7 @@ jfg_status numeric_create(jfg_model* m) {
     lv.max_c = lv.max_m = lv.max_r = 0;
     lv.cs.clear();
     lv.pm.clear();
+    lv.nnz = 0;
     for (int32_t q = lv.off; q < lv.off + lv.count; ++q) {
       int32_t s = S.level_sn[q];
       int32_t cc = S.sn_first[s + 1] - S.sn_first[s];
@@ -1550,6 +1568,7 @@ jfg_status numeric_create(jfg_model* m) {
       if (S.sn_parent[s] >= 0) lv.max_r = std::max(lv.max_r, S.sn_m[s] - cc);
       lv.cs.push_back(cc);
       lv.pm.push_back(lv.max_m);
+      lv.nnz += (int64_t)S.sn_m[s] * cc;
     }
     lv.schur_flops = 0;
     for (int32_t q = lv.off; q < lv.off + lv.count; ++q) {

@@ -19,7 +19,11 @@ int64_t launch_count();
 
 enum KernelStat : int { KS_SCHUR = 0, KS_Q4 = 1, KS_ASSEMBLY = 2, KS_SOLVE = 3, KS_T10 = 4,
                         KS_F_EA = 5, KS_F_POTRF = 6, KS_F_TRSM = 7, KS_F_PANEL = 8, KS_S_VEC = 9,
-                        KS_S_FDIAG = 10, KS_S_FUPD = 11, KS_S_BPART = 12, KS_S_BDIAG = 13, KS_COUNT = 14 };
+                        KS_S_FDIAG = 10, KS_S_FUPD = 11, KS_S_BPART = 12, KS_S_BDIAG = 13,
+                        // per elimination-tree level of a solve sweep (profiling level 2):
+                        // forward level l at KS_LEVEL_FWD + l, backward at KS_LEVEL_BWD + l
+                        KS_LEVEL_FWD = 14, KS_LEVEL_BWD = 14 + 48, KS_COUNT = 14 + 96 };
+constexpr int KS_MAX_LEVELS = 48;
 struct KernelStats {
   int64_t launches[KS_COUNT] = {0};
   double ms[KS_COUNT] = {0};
