@@ -185,6 +185,26 @@ jfg_status jfg_recover_stresses(jfg_model* model, int32_t kind, int32_t nrhs,
 jfg_status jfg_solve_device(jfg_model* model, int32_t nrhs, const double* F_dev,
                             double* U_dev, double tol, int32_t max_ir,
                             jfg_solve_report* report);
+/* ---- asynchronous calls ---------------------------------------------------- */
+/* The reference's calls block (cholesky(Symmetric(K_ff)) and F \ b at
+ * boundary_conditions.jl:1660, 1714); these variants only enqueue, so that a
+ * caller overlaps the factorisation and its applications with its own work
+ * on `stream` (a cudaStream_t; the library's stream waits for the work the
+ * caller has already put there, and the caller's stream waits for the
+ * library's).  jfg_factor_async enqueues the numeric factorisation (its first
+ * call for a precision allocates and so synchronises); its device error
+ * record -- a non-positive pivot, an expired tensor-core wait -- is read by
+ * jfg_wait, which every synchronous call on the model also makes first.
+ * jfg_apply_factor_async enqueues U = K_ff^{-1} F by one application of the
+ * last enqueued (or, without one, the current) factor: forward and backward
+ * sweeps with no refinement, F and U DEVICE arrays (ndof x nrhs, column-
+ * major, U zero at fixed DOFs); a new right-hand-side count may allocate its
+ * workspace.  jfg_wait blocks until the model's enqueued work is done.      */
+jfg_status jfg_factor_async(jfg_model* model, int32_t precision, void* stream);
+jfg_status jfg_apply_factor_async(jfg_model* model, int32_t nrhs, const double* F_dev,
+                                  double* U_dev, void* stream);
+jfg_status jfg_wait(jfg_model* model);
+
 /* Device time of the last element, assembly, factor and solve calls (s). */
 jfg_status jfg_get_timings(jfg_model* model, double* seconds4);
 

@@ -227,6 +227,9 @@ jfg_status jfg_model_upload(jfg_ctx* c, int64_t n_nodes, const double* xyz, cons
 jfg_status jfg_model_free(jfg_model* m) {
   if (!m) return JFG_OK;
   jfg_ctx* c = m->ctx;
+  if (m->aev_out) cudaEventSynchronize(m->aev_out);
+  if (m->aev_in) cudaEventDestroy(m->aev_in);
+  if (m->aev_out) cudaEventDestroy(m->aev_out);
   numeric_destroy(m);
   dev_free(c, m->d_xyz, 8 * m->h_xyz.size()); dev_free(c, m->d_R, 8 * m->h_R.size());
   dev_free(c, m->d_q4n, 4 * m->h_q4n.size()); dev_free(c, m->d_q4s, 8 * m->h_q4s.size());
@@ -446,17 +449,75 @@ jfg_status jfg_get_perm(jfg_model* m, int32_t* perm) {
 
 jfg_status jfg_factor(jfg_model* m, int32_t precision) {
   JFG_TRY(check_model(m));
+  if (m->async_factor >= 0) JFG_TRY(jfg_wait(m));
+  m->async_prec = -1;
   return numeric_factor(m, precision);
+}
+
+namespace {
+// the model's stream waits for the work the caller has already put on `user`
+jfg_status async_begin(jfg_model* m, cudaStream_t user) {
+  if (!m->aev_in) {
+    JFG_CUDA(cudaEventCreateWithFlags(&m->aev_in, cudaEventDisableTiming));
+    JFG_CUDA(cudaEventCreateWithFlags(&m->aev_out, cudaEventDisableTiming));
+  }
+  JFG_CUDA(cudaEventRecord(m->aev_in, user));
+  JFG_CUDA(cudaStreamWaitEvent(m->ctx->stream, m->aev_in, 0));
+  return JFG_OK;
+}
+// `user` waits for the work just put on the model's stream
+jfg_status async_end(jfg_model* m, cudaStream_t user) {
+  JFG_CUDA(cudaEventRecord(m->aev_out, m->ctx->stream));
+  JFG_CUDA(cudaStreamWaitEvent(user, m->aev_out, 0));
+  return JFG_OK;
+}
+}  // namespace
+
+jfg_status jfg_factor_async(jfg_model* m, int32_t precision, void* stream) {
+  JFG_TRY(check_model(m));
+  if (precision != JFG_PREC_FP64 && precision != JFG_PREC_MIXED) { set_error("unknown precision"); return JFG_BAD_INPUT; }
+  if (m->async_factor >= 0) JFG_TRY(jfg_wait(m));     // one unchecked factorisation at a time
+  cudaStream_t user = static_cast<cudaStream_t>(stream);
+  JFG_TRY(async_begin(m, user));
+  JFG_TRY(numeric_factor_enqueue(m, precision));
+  m->async_factor = precision;
+  m->async_prec = precision;
+  return async_end(m, user);
+}
+
+jfg_status jfg_apply_factor_async(jfg_model* m, int32_t nrhs, const double* F_dev, double* U_dev, void* stream) {
+  JFG_TRY(check_model(m));
+  if (!F_dev || !U_dev) { set_error("null F/U"); return JFG_BAD_INPUT; }
+  const int prec = m->async_prec >= 0 ? m->async_prec : numeric_current_precision(m);
+  if (prec < 0) { set_error("apply before factorisation"); return JFG_NOT_READY; }
+  cudaStream_t user = static_cast<cudaStream_t>(stream);
+  JFG_TRY(async_begin(m, user));
+  JFG_TRY(numeric_apply(m, nrhs, F_dev, U_dev, prec));
+  return async_end(m, user);
+}
+
+jfg_status jfg_wait(jfg_model* m) {
+  JFG_TRY(check_model(m));
+  if (m->aev_out) JFG_CUDA(cudaEventSynchronize(m->aev_out));
+  JFG_CUDA(cudaStreamSynchronize(m->ctx->stream));
+  if (m->async_factor >= 0) {
+    const int p = m->async_factor;
+    m->async_factor = -1;
+    JFG_TRY(numeric_factor_finish(m, p));
+  }
+  return JFG_OK;
 }
 
 jfg_status jfg_get_factor_diag(jfg_model* m, double* Ldiag) {
   JFG_TRY(check_model(m));
+  if (m->async_factor >= 0) JFG_TRY(jfg_wait(m));
   return numeric_factor_diag(m, Ldiag);
 }
 
 jfg_status jfg_solve(jfg_model* m, int32_t nrhs, const double* F, double* U, double tol, int32_t max_ir,
                      jfg_solve_report* report) {
   JFG_TRY(check_model(m));
+  if (m->async_factor >= 0) JFG_TRY(jfg_wait(m));
   if (!F || !U) { set_error("null F/U"); return JFG_BAD_INPUT; }
   return numeric_solve(m, nrhs, F, U, tol, max_ir, report, false);
 }
@@ -464,6 +525,7 @@ jfg_status jfg_solve(jfg_model* m, int32_t nrhs, const double* F, double* U, dou
 jfg_status jfg_solve_device(jfg_model* m, int32_t nrhs, const double* F, double* U, double tol, int32_t max_ir,
                             jfg_solve_report* report) {
   JFG_TRY(check_model(m));
+  if (m->async_factor >= 0) JFG_TRY(jfg_wait(m));
   if (!F || !U) { set_error("null F/U"); return JFG_BAD_INPUT; }
   return numeric_solve(m, nrhs, F, U, tol, max_ir, report, true);
 }

@@ -1687,6 +1687,13 @@ void numeric_destroy(jfg_model* m) {
 }
 
 jfg_status numeric_factor(jfg_model* m, int precision) {
+  JFG_TRY(numeric_factor_enqueue(m, precision));
+  return numeric_factor_finish(m, precision);
+}
+
+// Everything of the factorisation that goes on the model's stream; the
+// first factorisation of a precision also allocates (and so synchronises).
+jfg_status numeric_factor_enqueue(jfg_model* m, int precision) {
   NumericFactor* F = m->num;
   if (!F || !m->sym_ready) { set_error("factor before symbolic analysis"); return JFG_NOT_READY; }
   if (!m->values_ready) { set_error("factor before assembly"); return JFG_NOT_READY; }
@@ -1783,6 +1790,21 @@ jfg_status numeric_factor(jfg_model* m, int precision) {
     return JFG_BAD_INPUT;
   }
   JFG_CUDA(cudaEventRecord(F->ev1, st));
+  return JFG_OK;
+}
+
+// Precision of the factor a solve would use (-1: none).
+int numeric_current_precision(jfg_model* m) {
+  NumericFactor* F = m->num;
+  if (!F) return -1;
+  if (F->have32 && (!F->have64 || F->prefer_mixed)) return JFG_PREC_MIXED;
+  return F->have64 ? JFG_PREC_FP64 : -1;
+}
+
+// Waits for the enqueued factorisation and reads its device error record.
+jfg_status numeric_factor_finish(jfg_model* m, int precision) {
+  NumericFactor* F = m->num;
+  if (!F) { set_error("no factor"); return JFG_NOT_READY; }
   JFG_CUDA(cudaEventSynchronize(F->ev1));
   float ms = 0;
   cudaEventElapsedTime(&ms, F->ev0, F->ev1);
@@ -1791,6 +1813,39 @@ jfg_status numeric_factor(jfg_model* m, int precision) {
   JFG_TRY(check_err(F, "factorisation"));
   if (precision == JFG_PREC_FP64) F->have64 = true; else F->have32 = true;
   F->prefer_mixed = precision == JFG_PREC_MIXED;
+  return JFG_OK;
+}
+
+// U = K_ff^{-1} F by one application of the factor (forward and backward
+// sweeps, no refinement), F and U in device memory (ndof x nrhs, column-
+// major, global DOF space; U is zero at fixed DOFs).  Enqueued on the
+// model's stream; `precision` names the factor to use.
+jfg_status numeric_apply(jfg_model* m, int nrhs, const double* Fd, double* Ud, int precision) {
+  NumericFactor* F = m->num;
+  if (!F) { set_error("apply before symbolic analysis"); return JFG_NOT_READY; }
+  if (nrhs <= 0) { set_error("nrhs must be positive"); return JFG_BAD_INPUT; }
+  const bool use32 = precision == JFG_PREC_MIXED;
+  if ((use32 && !F->L32) || (!use32 && !F->L64)) { set_error("apply before factorisation"); return JFG_NOT_READY; }
+  const Symbolic& S = m->sym;
+  cudaStream_t st = m->ctx->stream;
+  const int64_t n = S.n, ndof = m->ndof;
+  const unsigned gn = (unsigned)((n + 255) / 256);
+  for (int done = 0; done < nrhs;) {
+    const int nr = std::min(8, nrhs - done);
+    JFG_TRY(ensure_workspace(m, F, nr));
+    const double* sc = use32 ? F->scale : nullptr;
+    { k_gather_perm<<<gn, 256, 0, st>>>(n, nr, F->perm_dof, sc, Fd + ndof * done, ndof, F->xp, 1.0); count_launch(); }
+    auto body = [&]() -> jfg_status {
+      if (use32) solve_inner<float>(m, F, F->L32, F->Sinv32, nr, st);
+      else solve_inner<double>(m, F, F->L64, F->Sinv64, nr, st);
+      return JFG_OK;
+    };
+    if (graphs_enabled()) JFG_TRY(run_graph(F->solve_graph[use32][nr], F->solve_graph_nodes[use32][nr], st, body));
+    else JFG_TRY(body());
+    JFG_CUDA(cudaMemsetAsync(Ud + ndof * done, 0, sizeof(double) * ndof * nr, st));
+    { k_scatter_add_perm<<<gn, 256, 0, st>>>(n, nr, F->perm_dof, sc, F->xp, Ud + ndof * done, ndof); count_launch(); }
+    done += nr;
+  }
   return JFG_OK;
 }
 

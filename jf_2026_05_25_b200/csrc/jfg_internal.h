@@ -139,6 +139,11 @@ struct jfg_model {
   jfg::Symbolic sym_cache;
   bool has_sym_cache = false;
   NumericFactor* num = nullptr;
+  // asynchronous calls (jfg_*_async): the caller's stream waits on aev_out;
+  // async_factor is the precision of a factorisation not yet checked (-1 none)
+  cudaEvent_t aev_in = nullptr, aev_out = nullptr;
+  int async_factor = -1;
+  int async_prec = -1;              // precision of the last factorisation enqueued
   // timings of the last calls (seconds, device events)
   double t_elements = 0, t_assembly = 0, t_factor = 0, t_solve = 0;
 };
@@ -159,6 +164,10 @@ void residual_dd(const jfg_model* m, int nrhs, const double* x, const double* f,
 jfg_status numeric_create(jfg_model* m);
 void numeric_destroy(jfg_model* m);
 jfg_status numeric_factor(jfg_model* m, int precision);
+jfg_status numeric_factor_enqueue(jfg_model* m, int precision);
+jfg_status numeric_factor_finish(jfg_model* m, int precision);
+jfg_status numeric_apply(jfg_model* m, int nrhs, const double* Fd, double* Ud, int precision);
+int numeric_current_precision(jfg_model* m);
 jfg_status numeric_solve(jfg_model* m, int nrhs, const double* hF, double* hU, double tol,
                          int max_ir, jfg_solve_report* rep, bool device_io);
 jfg_status numeric_factor_diag(jfg_model* m, double* out);

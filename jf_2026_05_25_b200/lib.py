@@ -94,6 +94,9 @@ def load():
         "jfg_assemble_values_noalloc": [P, P],
         "jfg_recover_stresses": [P, I32, I32, P, P],
         "jfg_model_share_structure": [P, P],
+        "jfg_factor_async": [P, I32, P],
+        "jfg_apply_factor_async": [P, I32, P, P, P],
+        "jfg_wait": [P],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -261,6 +264,17 @@ class DeviceModel:
 
     def factor(self, precision: int = PREC_FP64):
         _check(load().jfg_factor(self.h, precision))
+
+    def factor_async(self, precision: int, stream_ptr: int):
+        """Enqueue the factorisation on a CUDA stream (cudaStream_t as int)."""
+        _check(load().jfg_factor_async(self.h, precision, P(stream_ptr)))
+
+    def apply_factor_async(self, F_ptr: int, U_ptr: int, nrhs: int, stream_ptr: int):
+        """Enqueue U = K_ff^-1 F (one factor application, device arrays)."""
+        _check(load().jfg_apply_factor_async(self.h, nrhs, P(F_ptr), P(U_ptr), P(stream_ptr)))
+
+    def wait(self):
+        _check(load().jfg_wait(self.h))
 
     def factor_diag(self) -> np.ndarray:
         d = np.empty(self.n_free)

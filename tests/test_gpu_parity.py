@@ -457,3 +457,41 @@ def test_share_structure_gives_the_same_solution(ctx):
     assert e.value.status_name == "BAD_INPUT"
     for x in (dm, other, st_a["dm"], alone["state"]["dm"]):
         x.close()
+
+
+def test_async_factor_and_apply_on_a_caller_stream(ctx):
+    """jfg_factor_async / jfg_apply_factor_async enqueue on the caller's
+    stream and return; after jfg_wait the single factor application equals
+    the refined solve within the parity bar, and a deferred pivot failure is
+    reported by jfg_wait."""
+    import torch
+    m = M.flat_plate()
+    be = B.JFEMGPUBackend(tol=RESID_TOL)
+    be._ctx = ctx
+    st = B.prepare(be, m)
+    dm = st["dm"]
+    F = m.load_matrix()
+    U_ref, _ = dm.solve(F)
+    s = torch.cuda.Stream()
+    Fd = torch.from_numpy(np.ascontiguousarray(F.T)).cuda()
+    Ud = torch.full_like(Fd, float("nan"))
+    torch.cuda.synchronize()
+    for prec in (lib.PREC_FP64, lib.PREC_MIXED):
+        dm.assemble()
+        dm.factor_async(prec, s.cuda_stream)
+        dm.apply_factor_async(Fd.data_ptr(), Ud.data_ptr(), F.shape[1], s.cuda_stream)
+        dm.wait()
+        s.synchronize()
+        U = Ud.cpu().numpy().T
+        assert _rel(U, U_ref) <= (DISP_RTOL if prec == lib.PREC_FP64 else 1e-4)
+    bad = M.flat_plate(nx=4, ny=4)
+    bad.spc1 = []
+    dmb = lib.DeviceModel(ctx, bad)
+    dmb.assemble()
+    dmb.set_free_dofs(np.arange(bad.ndof, dtype=np.int32))
+    dmb.factor_async(lib.PREC_FP64, s.cuda_stream)
+    with pytest.raises(lib.JfgError) as e:
+        dmb.wait()
+    assert e.value.status_name == "NOT_SPD"
+    for x in (dm, dmb):
+        x.close()
