@@ -483,7 +483,13 @@ def test_async_factor_and_apply_on_a_caller_stream(ctx):
         dm.wait()
         s.synchronize()
         U = Ud.cpu().numpy().T
-        assert _rel(U, U_ref) <= (DISP_RTOL if prec == lib.PREC_FP64 else 1e-4)
+        if prec == lib.PREC_FP64:
+            assert _rel(U, U_ref) <= DISP_RTOL
+        else:
+            # one application of the FP32 factor: a preconditioner, not a solve
+            free = st["free"]
+            R = dm.residual(np.asfortranarray(U), F)[free]
+            assert np.linalg.norm(R) <= 1e-2 * np.linalg.norm(F[free])
     bad = M.flat_plate(nx=4, ny=4)
     bad.spc1 = []
     dmb = lib.DeviceModel(ctx, bad)
