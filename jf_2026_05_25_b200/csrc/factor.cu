@@ -34,12 +34,12 @@ struct NumericFactor {
   int64_t n_amap = 0;
   const int32_t* level_sn_cur = nullptr;   // the level the factor loop is on
   // CUDA graphs of the factorisation (per precision) and of one preconditioner
-  // application (per precision and right-hand-side count 1..8)
+  // application (per precision and right-hand-side count 1..32)
   cudaGraphExec_t factor_graph[2] = {nullptr, nullptr};
   int64_t factor_graph_nodes[2] = {0, 0};
   int factor_calls[2] = {0, 0};
-  cudaGraphExec_t solve_graph[2][9] = {};
-  int64_t solve_graph_nodes[2][9] = {};
+  cudaGraphExec_t solve_graph[2][33] = {};
+  int64_t solve_graph_nodes[2][33] = {};
   // host launch metadata
   struct Level {
     int32_t off, count;
@@ -160,6 +160,7 @@ void drop_solve_graphs(NumericFactor* F) {
 }
 
 constexpr int NB = 64;       // panel block width
+constexpr int MAXR = 32;     // right-hand sides per solve sweep (one read of the factor serves all)
 constexpr int TILE = 64;     // Schur-update tile
 // super-panel width of the blocked front factorisation (multiple of NB):
 // JFG_PANEL_WIDTH, default 256
@@ -761,6 +762,7 @@ __global__ void k_zero_V(const int32_t* __restrict__ list, const int32_t* __rest
   for (int64_t q = threadIdx.x; q < r * nr; q += blockDim.x) v[q] = 0.0;
 }
 
+template <int NRC>
 __global__ void k_vec_extend_add(const int32_t* __restrict__ child, const int32_t* __restrict__ first,
                                  const int32_t* __restrict__ mrows, const int32_t* __restrict__ parent,
                                  const int64_t* __restrict__ relptr, const int32_t* __restrict__ rel, int nr,
@@ -780,13 +782,13 @@ __global__ void k_vec_extend_add(const int32_t* __restrict__ child, const int32_
   int ra = rl[a];
   double* dst = (ra < cp) ? xp + first[p] + ra : vp + (ra - cp);
   const int64_t ld = (ra < cp) ? n : (int64_t)rp;
-  double v[8], d[8];
+  double v[NRC], d[NRC];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) v[k] = k < nr ? src[a + (int64_t)rc * k] : 0.0;
+  for (int k = 0; k < NRC; ++k) v[k] = k < nr ? src[a + (int64_t)rc * k] : 0.0;
 #pragma unroll
-  for (int k = 0; k < 8; ++k) d[k] = k < nr ? dst[ld * k] : 0.0;
+  for (int k = 0; k < NRC; ++k) d[k] = k < nr ? dst[ld * k] : 0.0;
 #pragma unroll
-  for (int k = 0; k < 8; ++k)
+  for (int k = 0; k < NRC; ++k)
     if (k < nr) dst[ld * k] = d[k] + v[k];
 }
 
@@ -900,7 +902,10 @@ k_strip_inverse(const int32_t* __restrict__ it_sn, const int32_t* __restrict__ i
 // launch reads, and at the end of the backward sweep xp holds the solution.
 // forward (a): y = X b on the rows of strip kb; CTA (g, front) owns rows
 // [32g, 32g + 32) and its 8 warps split the columns j (stride 8)
-template <typename T>
+template <int NRC>
+constexpr int fwd_sdiag_smem() { return (SW * NRC + 8 * 32 * (NRC + 1)) * (int)sizeof(double); }
+
+template <typename T, int NRC>
 __global__ void __launch_bounds__(256)
 k_fwd_sdiag(const int32_t* __restrict__ list, const int32_t* __restrict__ first, const int64_t* __restrict__ Sptr,
             const T* __restrict__ Sinv, int kb, int nr, int64_t n, const double* __restrict__ xp,
@@ -914,29 +919,32 @@ k_fwd_sdiag(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
   if (r0 >= kw) return;
   const T* X = Sinv + Sptr[s] + (int64_t)kb * SW * SW;
   int rmax = min(kw, r0 + 32);          // columns j < rmax can touch the slab
-  __shared__ double bs[SW][8];
-  __shared__ double red[8][32][9];
-  for (int e = threadIdx.x; e < rmax * 8; e += blockDim.x) {
+  extern __shared__ double sdyn[];
+  double (*bs)[NRC] = reinterpret_cast<double (*)[NRC]>(sdyn);
+  double (*red)[32][NRC + 1] = reinterpret_cast<double (*)[32][NRC + 1]>(sdyn + SW * NRC);
+  for (int e = threadIdx.x; e < rmax * NRC; e += blockDim.x) {
     int l = e % rmax, k = e / rmax;
     bs[l][k] = k < nr ? xp[f + j0 + l + n * k] : 0.0;
   }
   __syncthreads();
   int lane = threadIdx.x & 31, cg = threadIdx.x >> 5;
   int r = r0 + lane;
-  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double acc[NRC];
+#pragma unroll
+  for (int k = 0; k < NRC; ++k) acc[k] = 0.0;
   if (r < kw) {
     const T* xr = X + r;
 #pragma unroll 4
     for (int j = cg; j <= r; j += 8) {
       double x = (double)xr[(int64_t)kw * j];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) acc[k] += x * bs[j][k];
+      for (int k = 0; k < NRC; ++k) acc[k] += x * bs[j][k];
     }
   }
 #pragma unroll
-  for (int k = 0; k < 8; ++k) red[cg][lane][k] = acc[k];
+  for (int k = 0; k < NRC; ++k) red[cg][lane][k] = acc[k];
   __syncthreads();
-  for (int e = threadIdx.x; e < 32 * 8; e += blockDim.x) {
+  for (int e = threadIdx.x; e < 32 * NRC; e += blockDim.x) {
     int l = e & 31, k = e >> 5;
     if (r0 + l < kw && k < nr) {
       double v = 0.0;
@@ -998,33 +1006,89 @@ k_fwd_supdate(const int32_t* __restrict__ list, const int32_t* __restrict__ firs
   }
 }
 
-// Sums each of v[0..7] over the 32 lanes of a warp with 9 exchanges instead
-// of 8 separate 5-step reductions: every step hands half of the remaining
-// components to the partner lane.  Lane L ends with the total of component
-// (L >> 2) & 7 (all four lanes of a quad hold the same value).
-__device__ __forceinline__ double warp_sum8(const double (&v)[8], int lane) {
+// forward (b), 16 or 32 right-hand sides: one thread per row below the
+// strip, 128 rows per CTA, the strip's columns in tiles of 64 (y staged in
+// shared memory); every factor entry is read once for all right-hand sides
+template <typename T, int NRC>
+__global__ void __launch_bounds__(128)
+k_fwd_supdate_wide(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
+                   const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
+                   const int64_t* __restrict__ relptr, const T* __restrict__ L, int kb, int nr, int64_t n,
+                   const double* __restrict__ tt, double* __restrict__ xp, double* __restrict__ V) {
+  int s = list[blockIdx.y];
+  int f = first[s], c = first[s + 1] - f, m = mrows[s], r = m - c;
+  int j0 = kb * SW;
+  if (j0 >= c) return;
+  int kw = min(SW, c - j0);
+  int row0 = j0 + kw + blockIdx.x * 128;
+  if (row0 >= m) return;
+  __shared__ double ys[64][NRC];
+  const int i = row0 + threadIdx.x;
+  double acc[NRC];
+#pragma unroll
+  for (int k = 0; k < NRC; ++k) acc[k] = 0.0;
+  const T* P = L + Lptr[s] + i;
+  for (int l0 = 0; l0 < kw; l0 += 64) {
+    const int lw = min(64, kw - l0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < lw * NRC; e += 128) {
+      int l = e % lw, k = e / lw;
+      ys[l][k] = k < nr ? tt[f + j0 + l0 + l + n * k] : 0.0;
+    }
+    __syncthreads();
+    if (i < m) {
+#pragma unroll 8
+      for (int l = 0; l < lw; ++l) {
+        const double lv = (double)P[(int64_t)m * (j0 + l0 + l)];
+#pragma unroll
+        for (int k = 0; k < NRC; ++k) acc[k] += lv * ys[l][k];
+      }
+    }
+  }
+  if (i < m) {
+#pragma unroll
+    for (int k = 0; k < NRC; ++k) {
+      if (k >= nr) break;
+      if (i < c) xp[f + i + n * k] -= acc[k];
+      else V[relptr[s] * nr + (i - c) + (int64_t)r * k] -= acc[k];
+    }
+  }
+}
+
+// Sums each of v[0..NRC-1] over the 32 lanes of a warp by halving: every
+// step hands half of the remaining components to the partner lane (log2 NRC
+// exchanges), the rest is a plain butterfly.  Lane L ends with the total of
+// component L >> (5 - log2 NRC) (the other lanes of its group hold the same).
+template <int NRC>
+__device__ __forceinline__ double warp_sum_scatter(const double (&v)[NRC], int lane) {
+  constexpr int H = NRC >= 32 ? 5 : NRC >= 16 ? 4 : 3;
   const unsigned full = 0xffffffffu;
-  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
-  double a[4], b[2];
+  double a[NRC];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    double keep = b4 ? v[k + 4] : v[k], send = b4 ? v[k] : v[k + 4];
-    a[k] = keep + __shfl_xor_sync(full, send, 16);
-  }
+  for (int k = 0; k < NRC; ++k) a[k] = v[k];
 #pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    double keep = b3 ? a[k + 2] : a[k], send = b3 ? a[k] : a[k + 2];
-    b[k] = keep + __shfl_xor_sync(full, send, 8);
+  for (int step = 0; step < H; ++step) {
+    const int off = 16 >> step;
+    const int half = NRC >> (step + 1);
+    const bool hi = lane & off;
+#pragma unroll
+    for (int k = 0; k < half; ++k) {
+      const double keep = hi ? a[k + half] : a[k], send = hi ? a[k] : a[k + half];
+      a[k] = keep + __shfl_xor_sync(full, send, off);
+    }
   }
-  double c = (b2 ? b[1] : b[0]) + __shfl_xor_sync(full, b2 ? b[0] : b[1], 4);
-  c += __shfl_xor_sync(full, c, 2);
-  c += __shfl_xor_sync(full, c, 1);
+  double c = a[0];
+#pragma unroll
+  for (int off = 16 >> H; off > 0; off >>= 1) c += __shfl_xor_sync(full, c, off);
   return c;
 }
 
 // backward (a): partial dots for the SW columns of strip kb over a tile of
 // 256 rows x 32 columns below the strip (8 warps x 4 columns)
-template <typename T>
+template <int NRC>
+constexpr int bwd_spartial_smem() { return NRC * 256 * (int)sizeof(double); }
+
+template <typename T, int NRC>
 __global__ void __launch_bounds__(256)
 k_bwd_spartial(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
                const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
@@ -1042,19 +1106,23 @@ k_bwd_spartial(const int32_t* __restrict__ list, const int32_t* __restrict__ fir
   int row0 = j0 + kw + rb * 256;
   // right-hand-side major, so that lanes reading consecutive rows hit
   // consecutive banks
-  __shared__ double xs[8][256];
+  extern __shared__ double sdyn[];
+  double (*xs)[256] = reinterpret_cast<double (*)[256]>(sdyn);
   const int32_t* R = rows + rows_ptr[s];
-  for (int e = threadIdx.x; e < 256 * 8; e += blockDim.x) {
+  for (int e = threadIdx.x; e < 256 * NRC; e += blockDim.x) {
     int ii = e & 255, k = e >> 8;
     int i = row0 + ii;
     xs[k][ii] = (i < m && k < nr) ? xp[(int64_t)R[i] + n * k] : 0.0;
   }
   __syncthreads();
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* out = part + part_off[blockIdx.y] + (int64_t)rb * SW * 8;
+  double* out = part + part_off[blockIdx.y] + (int64_t)rb * SW * MAXR;
+  constexpr int GRP = 32 / NRC;   // lanes sharing one reduced component
   for (int q = 0; q < 4; ++q) {
     int jj = cg * 32 + warp * 4 + q;
-    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double acc[NRC];
+#pragma unroll
+    for (int k = 0; k < NRC; ++k) acc[k] = 0.0;
     if (jj < kw) {
       const T* col = L + Lptr[s] + (int64_t)m * (j0 + jj);
       double lv[8];
@@ -1066,17 +1134,20 @@ k_bwd_spartial(const int32_t* __restrict__ list, const int32_t* __restrict__ fir
 #pragma unroll
       for (int u = 0; u < 8; ++u)
 #pragma unroll
-        for (int k = 0; k < 8; ++k) acc[k] += lv[u] * xs[k][lane + 32 * u];
+        for (int k = 0; k < NRC; ++k) acc[k] += lv[u] * xs[k][lane + 32 * u];
     }
-    double v = warp_sum8(acc, lane);
-    if ((lane & 3) == 0 && jj < SW) out[jj * 8 + (lane >> 2)] = v;
+    double v = warp_sum_scatter<NRC>(acc, lane);
+    if ((lane % GRP) == 0 && jj < SW) out[jj * MAXR + lane / GRP] = v;
   }
 }
 
 // backward (b): x = X^T (b - sum of the partial dots) on the rows of strip kb;
 // CTA (g, front) owns outputs [32g, 32g + 32), a warp per output with lanes
 // along column i of X
-template <typename T>
+template <int NRC>
+constexpr int bwd_sdiag_smem() { return NRC * SW * (int)sizeof(double); }
+
+template <typename T, int NRC>
 __global__ void __launch_bounds__(256)
 k_bwd_sdiag(const int32_t* __restrict__ list, const int32_t* __restrict__ first, const int32_t* __restrict__ mrows,
             const int64_t* __restrict__ Sptr, const int64_t* __restrict__ part_off, const T* __restrict__ Sinv,
@@ -1092,30 +1163,34 @@ k_bwd_sdiag(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
   int nrb = (m - (j0 + kw) + 255) / 256;
   const double* pp = part + part_off[blockIdx.y];
   const T* X = Sinv + Sptr[s] + (int64_t)kb * SW * SW;
-  __shared__ double bs[8][SW];   // right-hand-side major (conflict-free row reads)
-  for (int e = threadIdx.x; e < (kw - i0) * 8; e += blockDim.x) {
-    int l = i0 + (e >> 3), k = e & 7;
+  extern __shared__ double sdyn[];
+  double (*bs)[SW] = reinterpret_cast<double (*)[SW]>(sdyn);   // right-hand-side major
+  for (int e = threadIdx.x; e < (kw - i0) * NRC; e += blockDim.x) {
+    int l = i0 + e / NRC, k = e % NRC;
     double v = 0.0;
     if (k < nr) {
       // independent partial sums: four loads in flight per step
       double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-      const double* q = pp + l * 8 + k;
+      const double* q = pp + l * MAXR + k;
       int rb = 0;
       for (; rb + 4 <= nrb; rb += 4) {
-        a0 += q[(int64_t)rb * SW * 8];
-        a1 += q[(int64_t)(rb + 1) * SW * 8];
-        a2 += q[(int64_t)(rb + 2) * SW * 8];
-        a3 += q[(int64_t)(rb + 3) * SW * 8];
+        a0 += q[(int64_t)rb * SW * MAXR];
+        a1 += q[(int64_t)(rb + 1) * SW * MAXR];
+        a2 += q[(int64_t)(rb + 2) * SW * MAXR];
+        a3 += q[(int64_t)(rb + 3) * SW * MAXR];
       }
-      for (; rb < nrb; ++rb) a0 += q[(int64_t)rb * SW * 8];
+      for (; rb < nrb; ++rb) a0 += q[(int64_t)rb * SW * MAXR];
       v = tt[f + j0 + l + n * k] - ((a0 + a1) + (a2 + a3));
     }
     bs[k][l] = v;
   }
   __syncthreads();
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int GRP = 32 / NRC;
   for (int i = i0 + warp; i < min(kw, i0 + 32); i += 8) {
-    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double acc[NRC];
+#pragma unroll
+    for (int k = 0; k < NRC; ++k) acc[k] = 0.0;
     const T* col = X + (int64_t)kw * i;
     double x[SW / 32];
 #pragma unroll
@@ -1128,12 +1203,12 @@ k_bwd_sdiag(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
       int j = i + lane + 32 * u;   // bs holds columns [i0, kw) only
       if (j < kw) {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) acc[k] += x[u] * bs[k][j];
+        for (int k = 0; k < NRC; ++k) acc[k] += x[u] * bs[k][j];
       }
     }
-    double v = warp_sum8(acc, lane);
-    int k = lane >> 2;
-    if ((lane & 3) == 0 && k < nr) xp[f + j0 + i + n * k] = v;
+    double v = warp_sum_scatter<NRC>(acc, lane);
+    int k = lane / GRP;
+    if ((lane % GRP) == 0 && k < nr) xp[f + j0 + i + n * k] = v;
   }
 }
 
@@ -1167,14 +1242,14 @@ __global__ void k_colnorm2_final(int nb, int nr, const double* __restrict__ part
   out[q] = s;
 }
 
-struct Coef8 { double v[8]; };
+struct CoefR { double v[MAXR]; };
 
-__global__ void k_axpy_cols(int64_t len, int nr, Coef8 a, const double* __restrict__ x, double* __restrict__ y) {
+__global__ void k_axpy_cols(int64_t len, int nr, CoefR a, const double* __restrict__ x, double* __restrict__ y) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= len) return;
   for (int k = 0; k < nr; ++k) y[i + len * k] += a.v[k] * x[i + len * k];
 }
-__global__ void k_xpby_cols(int64_t len, int nr, Coef8 b, const double* __restrict__ z, double* __restrict__ p) {
+__global__ void k_xpby_cols(int64_t len, int nr, CoefR b, const double* __restrict__ z, double* __restrict__ p) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= len) return;
   for (int k = 0; k < nr; ++k) p[i + len * k] = z[i + len * k] + b.v[k] * p[i + len * k];
@@ -1384,8 +1459,8 @@ jfg_status strip_inverses(NumericFactor* F, const T* Lf, const T* Dvf, T* Svf, c
   return JFG_OK;
 }
 
-template <typename T>
-void solve_inner(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int nr, cudaStream_t st) {
+template <typename T, int NRC>
+void solve_inner_n(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int nr, cudaStream_t st) {
   const Symbolic& S = m->sym;
   int64_t n = S.n;
   int ps = prof_start(st);
@@ -1397,18 +1472,27 @@ void solve_inner(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int n
     { int ps_ = fine_prof() ? prof_start(st) : -1; { k_zero_V<<<lv.count, 256, 0, st>>>(list, F->first, F->mrows, F->relptr, nr, F->V); count_launch(); } prof_end(ps_, st, KS_S_VEC, 0.0); }
     for (const auto& seg : lv.ea)
       if (seg.second > 0)
-        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_vec_extend_add<<<dim3(seg.second, std::max(1, (lv.ea_max_r + 255) / 256)), 256, 0, st>>>(F->ea_child + seg.first, F->first, F->mrows, F->parent,
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_vec_extend_add<NRC><<<dim3(seg.second, std::max(1, (lv.ea_max_r + 255) / 256)), 256, 0, st>>>(F->ea_child + seg.first, F->first, F->mrows, F->parent,
                                                      F->relptr, F->rel, nr, n, F->xp, F->V); count_launch(); } prof_end(ps_, st, KS_S_VEC, 0.0); }
     int nstrip = (lv.max_c + SW - 1) / SW;
     for (int kb = 0; kb < nstrip; ++kb) {
       const int na = lv.active(kb * SW);   // fronts that have strip kb: a prefix of the list
-      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_fwd_sdiag<T><<<dim3(SW / 32, na), 256, 0, st>>>(list, F->first, F->Sptr, Sv, kb, nr, n, F->xp, F->tt);
+      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_fwd_sdiag<T, NRC><<<dim3(SW / 32, na), 256, fwd_sdiag_smem<NRC>(), st>>>(list, F->first, F->Sptr, Sv, kb, nr, n, F->xp, F->tt);
         count_launch(); } prof_end(ps_, st, KS_S_FDIAG, 0.0); }
       int rows = lv.maxm(na) - kb * SW;
       if (rows > 0) {
-        unsigned gx = (unsigned)((rows + 31) / 32);
-        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_fwd_supdate<T><<<dim3(gx, na), 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->relptr, Lf, kb,
-                                                              nr, n, F->tt, F->xp, F->V); count_launch(); } prof_end(ps_, st, KS_S_FUPD, 0.0); }
+        int ps_ = fine_prof() ? prof_start(st) : -1;
+        if constexpr (NRC == 8) {
+          unsigned gx = (unsigned)((rows + 31) / 32);
+          k_fwd_supdate<T><<<dim3(gx, na), 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->relptr, Lf, kb,
+                                                          nr, n, F->tt, F->xp, F->V);
+        } else {
+          unsigned gx = (unsigned)((rows + 127) / 128);
+          k_fwd_supdate_wide<T, NRC><<<dim3(gx, na), 128, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->relptr, Lf,
+                                                                    kb, nr, n, F->tt, F->xp, F->V);
+        }
+        count_launch();
+        prof_end(ps_, st, KS_S_FUPD, 0.0);
       }
     }
     prof_end(pl, st, KS_LEVEL_FWD + (int)li, (double)sizeof(T) * (double)lv.nnz);
@@ -1425,10 +1509,10 @@ void solve_inner(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int n
       int rows = lv.maxm(na) - kb * SW;
       if (rows > 0) {
         unsigned gx = (unsigned)(((rows + 255) / 256) * (SW / 32));
-        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_bwd_spartial<T><<<dim3(gx, na), 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->rows_ptr, F->rows,
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_bwd_spartial<T, NRC><<<dim3(gx, na), 256, bwd_spartial_smem<NRC>(), st>>>(list, F->first, F->mrows, F->Lptr, F->rows_ptr, F->rows,
                                                                poff, Lf, kb, nr, n, F->xp, F->part); count_launch(); } prof_end(ps_, st, KS_S_BPART, 0.0); }
       }
-      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_bwd_sdiag<T><<<dim3(SW / 32, na), 256, 0, st>>>(list, F->first, F->mrows, F->Sptr, poff, Sv, kb, nr, n,
+      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_bwd_sdiag<T, NRC><<<dim3(SW / 32, na), 256, bwd_sdiag_smem<NRC>(), st>>>(list, F->first, F->mrows, F->Sptr, poff, Sv, kb, nr, n,
                                                  F->part, F->tt, F->xp); count_launch(); } prof_end(ps_, st, KS_S_BDIAG, 0.0); }
     }
     prof_end(pl, st, KS_LEVEL_BWD + (int)li, (double)sizeof(T) * (double)lv.nnz);
@@ -1436,6 +1520,36 @@ void solve_inner(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int n
   // algorithmic bytes: the factor read twice (forward and backward) plus the
   // permuted vectors read and written in each sweep
   prof_end(ps, st, KS_SOLVE, 2.0 * sizeof(T) * (double)S.nnz_L + 4.0 * 8.0 * n * nr);
+}
+
+// One application of the factor for nr <= MAXR right-hand sides: the
+// kernels are instantiated for 8, 16 and 32 columns (the smallest that holds nr).
+template <typename T>
+void solve_inner(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int nr, cudaStream_t st) {
+  if (nr <= 8) solve_inner_n<T, 8>(m, F, Lf, Sv, nr, st);
+  else if (nr <= 16) solve_inner_n<T, 16>(m, F, Lf, Sv, nr, st);
+  else solve_inner_n<T, 32>(m, F, Lf, Sv, nr, st);
+}
+
+// Dynamic shared-memory limits of the solve kernels that need more than the
+// default 48 KB (set once, outside any stream capture).
+template <typename T, int NRC>
+jfg_status solve_attributes_n() {
+  JFG_CUDA(cudaFuncSetAttribute(k_fwd_sdiag<T, NRC>, cudaFuncAttributeMaxDynamicSharedMemorySize, fwd_sdiag_smem<NRC>()));
+  JFG_CUDA(cudaFuncSetAttribute(k_bwd_spartial<T, NRC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                bwd_spartial_smem<NRC>()));
+  JFG_CUDA(cudaFuncSetAttribute(k_bwd_sdiag<T, NRC>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_sdiag_smem<NRC>()));
+  return JFG_OK;
+}
+
+jfg_status solve_attributes() {
+  static bool done = false;
+  if (done) return JFG_OK;
+  JFG_TRY((solve_attributes_n<double, 8>())); JFG_TRY((solve_attributes_n<double, 16>()));
+  JFG_TRY((solve_attributes_n<double, 32>())); JFG_TRY((solve_attributes_n<float, 8>()));
+  JFG_TRY((solve_attributes_n<float, 16>())); JFG_TRY((solve_attributes_n<float, 32>()));
+  done = true;
+  return JFG_OK;
 }
 
 jfg_status ensure_workspace(jfg_model* m, NumericFactor* F, int nrhs) {
@@ -1498,6 +1612,7 @@ jfg_status coldot(NumericFactor* F, int64_t len, int nr, const double* a, const 
 
 jfg_status numeric_create(jfg_model* m) {
   numeric_destroy(m);
+  JFG_TRY(solve_attributes());
   NumericFactor* F = new NumericFactor();
   m->num = F;
   Symbolic& S = m->sym;
@@ -1616,7 +1731,7 @@ jfg_status numeric_create(jfg_model* m) {
         int64_t kw0 = std::min<int64_t>(256, cc);
         int64_t nrb0 = (S.sn_m[sn] - kw0 + 255) / 256;
         poff[q] = acc;
-        acc += nrb0 * 256 * 8;
+        acc += nrb0 * 256 * MAXR;
       }
       pmax = std::max(pmax, acc);
     }
@@ -1831,7 +1946,7 @@ jfg_status numeric_apply(jfg_model* m, int nrhs, const double* Fd, double* Ud, i
   const int64_t n = S.n, ndof = m->ndof;
   const unsigned gn = (unsigned)((n + 255) / 256);
   for (int done = 0; done < nrhs;) {
-    const int nr = std::min(8, nrhs - done);
+    const int nr = std::min(MAXR, nrhs - done);
     JFG_TRY(ensure_workspace(m, F, nr));
     const double* sc = use32 ? F->scale : nullptr;
     { k_gather_perm<<<gn, 256, 0, st>>>(n, nr, F->perm_dof, sc, Fd + ndof * done, ndof, F->xp, 1.0); count_launch(); }
@@ -1892,7 +2007,7 @@ jfg_status numeric_solve(jfg_model* m, int nrhs, const double* hF, double* hU, d
   const unsigned gn = (unsigned)((n + 255) / 256), gd = (unsigned)((ndof + 255) / 256);
   int done_rhs = 0;
   while (done_rhs < nrhs) {
-    int nr = std::min(8, nrhs - done_rhs);
+    int nr = std::min(MAXR, nrhs - done_rhs);
     JFG_TRY(ensure_workspace(m, F, nr));
     double *X = F->dU, *Rv = F->dR, *Z = F->dZ, *Pv = F->dP, *Q = F->dQ;
     const double* srcF = hF + ndof * done_rhs;
@@ -1920,7 +2035,7 @@ jfg_status numeric_solve(jfg_model* m, int nrhs, const double* hF, double* hU, d
     // b = F restricted to the free DOFs
     JFG_CUDA(cudaMemcpyAsync(Rv, F->dF, sizeof(double) * ndof * nr, cudaMemcpyDeviceToDevice, st));
     { k_mask_free<<<gd, 256, 0, st>>>(ndof, nr, F->free_mask, Rv); count_launch(); }
-    double bn[8], rz[8], pq[8], rr[8], rzn[8];
+    double bn[MAXR], rz[MAXR], pq[MAXR], rr[MAXR], rzn[MAXR];
     JFG_TRY(coldot(F, ndof, nr, Rv, Rv, bn, st));
     JFG_CUDA(cudaMemsetAsync(X, 0, sizeof(double) * ndof * nr, st));
     int it = 0, restarts = 0, stall = 0;
@@ -1936,7 +2051,7 @@ jfg_status numeric_solve(jfg_model* m, int nrhs, const double* hF, double* hU, d
       }
       matvec(Pv, Q);
       JFG_TRY(coldot(F, ndof, nr, Pv, Q, pq, st));
-      Coef8 al{}, nal{};
+      CoefR al{}, nal{};
       for (int k = 0; k < nr; ++k) {
         al.v[k] = (pq[k] > 0.0 && rz[k] > 0.0) ? rz[k] / pq[k] : 0.0;
         nal.v[k] = -al.v[k];
@@ -1979,7 +2094,7 @@ jfg_status numeric_solve(jfg_model* m, int nrhs, const double* hF, double* hU, d
       }
       JFG_TRY(precond(Rv, Z));
       JFG_TRY(coldot(F, ndof, nr, Rv, Z, rzn, st));
-      Coef8 be{};
+      CoefR be{};
       for (int k = 0; k < nr; ++k) be.v[k] = rz[k] > 0.0 ? rzn[k] / rz[k] : 0.0;
       { k_xpby_cols<<<gd, 256, 0, st>>>(ndof, nr, be, Z, Pv); count_launch(); }
       for (int k = 0; k < nr; ++k) rz[k] = rzn[k];

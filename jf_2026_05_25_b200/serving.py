@@ -362,7 +362,8 @@ class SolveServer:
     def _bytes_of(dm) -> int:
         info = dm.symbolic_info()
         _, nnz, ntrip = dm.sizes()
-        return int(info["factor_bytes"] * 1.6 + 24 * nnz + 8 * ntrip + 200 * dm.ndof)
+        # factor and its workspaces, K, and the solve vectors of up to 32 right-hand sides
+        return int(info["factor_bytes"] * 1.6 + 24 * nnz + 8 * ntrip + 2600 * dm.ndof)
 
     def _evict_group(self, r: Resident, key: str):
         """Free one group (caller holds rlock and r.lock)."""
