@@ -501,3 +501,23 @@ def test_async_factor_and_apply_on_a_caller_stream(ctx):
     assert e.value.status_name == "NOT_SPD"
     for x in (dm, dmb):
         x.close()
+
+
+@pytest.mark.parametrize("prec", [lib.PREC_FP64, lib.PREC_MIXED])
+def test_wide_right_hand_side_sweeps_match_narrow(ctx, oracle_mod, prec):
+    """24 load cases go through the 32-column solve kernels in one sweep; the
+    result equals three separate solves of 8 (8-column kernels) and the FP64
+    oracle within the parity bar."""
+    m = M.stiffened_panel(3, n_cases=24)
+    be = B.JFEMGPUBackend(precision=prec, tol=RESID_TOL)
+    be._ctx = ctx
+    st = B.prepare(be, m)
+    dm = st["dm"]
+    F = m.load_matrix()
+    U, rep = dm.solve(F, RESID_TOL, 40)
+    assert rep["rel_residual"] <= RESID_TOL
+    parts = [dm.solve(np.asfortranarray(F[:, k:k + 8]), RESID_TOL, 40)[0] for k in (0, 8, 16)]
+    assert _rel(U, np.hstack(parts)) <= DISP_RTOL
+    ref = oracle_mod.solve_reference(m)
+    assert _rel(U, ref["u"]) <= DISP_RTOL
+    dm.close()
