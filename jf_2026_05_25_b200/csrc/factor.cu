@@ -404,6 +404,124 @@ k_potrf_diag(const int32_t* __restrict__ list, const int32_t* __restrict__ first
   }
 }
 
+// Cholesky of the NB x NB diagonal block at column k0 of every front of the
+// level and the inverse of its factor, with the whole CTA on both serial
+// chains.  Each thread owns up to 9 entries of the 64 x 64 lower triangle.
+// Factor: right-looking on unscaled columns (a_ik -= a_ij a_kj / a_jj for
+// j < k <= i, the L D L^T form), one block barrier per column, and the
+// columns scaled by 1/sqrt(a_jj) at the end.  Inverse: X = L^{-1} by rows,
+// right-looking on the residual R (R_iq -= L_ij R_jq / L_jj for q <= j < i),
+// one barrier per row, X_iq = R_iq / L_ii at the end.  Pivots that are not
+// positive and finite are replaced by 1 and the smallest such column is
+// recorded; rows and columns past the front's width are the identity.
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_potrf_cta(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
+            const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
+            const int64_t* __restrict__ Dptr, T* __restrict__ L, T* __restrict__ Dinv, int k0, DevError* err) {
+  int s = list[blockIdx.x];
+  int c = first[s + 1] - first[s];
+  if (k0 >= c) return;
+  int m = mrows[s];
+  int kn = min(NB, c - k0);
+  extern __shared__ unsigned char smem_raw[];
+  T (*A)[NB + 1] = reinterpret_cast<T (*)[NB + 1]>(smem_raw);
+  T (*B)[NB + 1] = A + NB;
+  T* sv = reinterpret_cast<T*>(B + NB);   // 64 entries: sqrt of the pivots
+  __shared__ int bad_idx;
+  T* P = L + Lptr[s] + k0 + (int64_t)m * k0;
+  const int t = threadIdx.x;
+  if (t == 0) bad_idx = NB;
+#pragma unroll
+  for (int u = 0; u < NB * NB / 256; ++u) {
+    int e = t + 256 * u;
+    int i = e & (NB - 1), j = e >> 6;
+    A[i][j] = (i < kn && j < kn) ? (i >= j ? P[i + (int64_t)m * j] : (T)0) : (i == j ? (T)1 : (T)0);
+    B[i][j] = (i == j) ? (T)1 : (T)0;
+  }
+  // this thread's lower-triangle entries (row-major enumeration, 2080 in all)
+  constexpr int NE = 9;
+  int ei[NE], ek[NE];
+#pragma unroll
+  for (int u = 0; u < NE; ++u) {
+    int e = t + 256 * u;
+    if (e < NB * (NB + 1) / 2) {
+      int i = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+      while ((i + 1) * (i + 2) / 2 <= e) ++i;
+      while (i * (i + 1) / 2 > e) --i;
+      ei[u] = i;
+      ek[u] = e - i * (i + 1) / 2;
+    } else {   // no entry: every predicate below is false for (-1, -1)
+      ei[u] = -1;
+      ek[u] = -1;
+    }
+  }
+  // factor
+  for (int j = 0; j < NB; ++j) {
+    __syncthreads();
+    T d = A[j][j];
+    const bool bad = !(d > (T)0) || !isfinite((double)d);
+    if (bad) {
+      if (t == 0 && j < kn) atomicMin(&bad_idx, j);
+      d = (T)1;
+    }
+    const T rd = (T)1 / d;
+#pragma unroll
+    for (int u = 0; u < NE; ++u) {
+      const int i = ei[u], k = ek[u];
+      if (k > j) A[i][k] = fma(-A[i][j] * rd, A[k][j], A[i][k]);
+    }
+  }
+  __syncthreads();
+  if (t < NB) {
+    T d = A[t][t];
+    const bool bad = !(d > (T)0) || !isfinite((double)d);
+    sv[t] = bad ? (T)1 : sqrt(d);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < NE; ++u) {
+    const int i = ei[u], k = ek[u];
+    if (i >= 0) A[i][k] = (i == k) ? sv[k] : A[i][k] / sv[k];
+  }
+  // inverse of the factor
+  for (int j = 0; j < NB; ++j) {
+    __syncthreads();
+    const T rl = (T)1 / A[j][j];
+#pragma unroll
+    for (int u = 0; u < NE; ++u) {
+      const int i = ei[u], q = ek[u];
+      if (q <= j && i > j) B[i][q] = fma(-A[i][j] * rl, B[j][q], B[i][q]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < NE; ++u) {
+    const int i = ei[u], q = ek[u];
+    if (i >= 0) B[i][q] = B[i][q] / A[i][i];
+  }
+  __syncthreads();
+  if (t == 0 && bad_idx < kn) rec_err(err, EE_PIVOT, (int64_t)first[s] + k0 + bad_idx);
+  T* Dv = Dinv + Dptr[s] + (int64_t)(k0 / NB) * NB * NB;
+  for (int e = t; e < NB * NB; e += blockDim.x) {
+    int i = e & (NB - 1), j = e >> 6;
+    bool in = i < kn && j < kn && i >= j;
+    if (in) P[i + (int64_t)m * j] = A[i][j];
+    Dv[i + NB * j] = in ? B[i][j] : (T)0;
+  }
+}
+
+// JFG_POTRF=1 selects the earlier diagonal-block kernel (one warp per 32 x 32
+// tile); the default runs the CTA-wide chains above
+inline bool potrf_cta() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = std::getenv("JFG_POTRF");
+    v = (e && e[0] == '1') ? 0 : 1;
+  }
+  return v == 1;
+}
+
 // rows [k1, m) of panel columns [k0, k1):  X := X * L_D^{-T} = X * Dinv^T,
 // 64 rows per CTA, both operands staged in shared memory.
 template <typename T>
@@ -1313,6 +1431,7 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
   if (!attr_set) {
     int bytes = 2 * NB * (NB + 1) * (int)sizeof(T);
     JFG_CUDA(cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, potrf_smem<T>()));
+    JFG_CUDA(cudaFuncSetAttribute(k_potrf_cta<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, potrf_smem<T>()));
     JFG_CUDA(cudaFuncSetAttribute(k_trsm_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     attr_set = true;
   }
@@ -1389,8 +1508,12 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
       const int P1 = P0 + PW;
       for (int k0 = P0; k0 < std::min(P1, lv.max_c); k0 += NB) {
         const int na = lv.active(k0);   // fronts wider than k0: a prefix of the list
-        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_potrf_diag<T><<<na, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr,
-                                                                               F->Dptr, Lf, Dvf, k0, F->err);
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { if (potrf_cta())
+            k_potrf_cta<T><<<na, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr, F->Dptr, Lf, Dvf, k0,
+                                                              F->err);
+          else
+            k_potrf_diag<T><<<na, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr,
+                                                               F->Dptr, Lf, Dvf, k0, F->err);
           count_launch(); } prof_end(ps_, st, KS_F_POTRF, potrf_flops(na, k0)); }
         int rows_max = lv.maxm(na) - k0 - 1;
         if (rows_max <= 0) continue;
