@@ -670,7 +670,11 @@ def stream_pass(srv, specs, sm: StreamModels, device: bool, rate: float = 0.0, s
         if sp["kind"] in ("panel", "wing", "solid"):
             chain(i, srv.solve(sm.models[i], device_loads=dev_loads.get(i)))
             return
-        key = proxies[sp["target"]].result()["key"]
+        tf = proxies[sp["target"]]
+        if tf.exception() is not None:      # its model never became resident
+            proxies[i].set_exception(tf.exception())
+            return
+        key = tf.result()["key"]
         loads = dev_loads[i] if device else sm.loads[i]
         if sp["kind"] == "resolve":
             chain(i, srv.resolve(key, loads))
@@ -691,8 +695,7 @@ def stream_pass(srv, specs, sm: StreamModels, device: bool, rate: float = 0.0, s
         if sp["kind"] in ("resolve", "update"):
             tf = proxies[sp["target"]]
             if not tf.done():
-                tf.add_done_callback(lambda f, i=i: submit(i) if f.exception() is None else
-                                     proxies[i].set_exception(f.exception()))
+                tf.add_done_callback(lambda f, i=i: submit(i))
                 continue
         submit(i)
     results, failed = [], []
@@ -763,6 +766,7 @@ def run_serving(args, rank=0, world=1, local_rank=0):
             secs_e = slowest_rank(secs_e, world, "cuda")
             worst_e = max((float(np.max(r["rel_residual"])) for r in res_e), default=float("nan"))
             del res_e
+            torch.cuda.empty_cache()
             arms[arm] = {"value": world * solved / secs, "stream_s": secs, "e2e": world * solved_e / secs_e,
                          "failed_requests": nfail + nfail_e,
                          "e2e_stream_s": secs_e, "h2d_bytes": h2d, "d2h_bytes": d2h,

@@ -185,6 +185,14 @@ jfg_status jfg_recover_stresses(jfg_model* model, int32_t kind, int32_t nrhs,
 jfg_status jfg_solve_device(jfg_model* model, int32_t nrhs, const double* F_dev,
                             double* U_dev, double tol, int32_t max_ir,
                             jfg_solve_report* report);
+/* No counterpart in the reference (for admission control in a server):
+ * device bytes the model holds now, and the bytes it will hold once factored
+ * at `precision` (with any factor it already has) and solved with `nrhs`
+ * right-hand sides (work space of up to 32 at a time).  Needs the symbolic
+ * analysis for the numeric part; before it only the inputs and pattern count. */
+jfg_status jfg_get_memory(jfg_model* model, int32_t precision, int32_t nrhs, int64_t* now,
+                          int64_t* peak);
+
 /* ---- asynchronous calls ---------------------------------------------------- */
 /* The reference's calls block (cholesky(Symmetric(K_ff)) and F \ b at
  * boundary_conditions.jl:1660, 1714); these variants only enqueue, so that a

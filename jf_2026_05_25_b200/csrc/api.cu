@@ -189,6 +189,11 @@ jfg_status jfg_model_upload(jfg_ctx* c, int64_t n_nodes, const double* xyz, cons
   cudaSetDevice(c->device);
   jfg_model* m = new jfg_model();
   m->ctx = c;
+  if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete m;
+    set_error("cudaStreamCreate failed for the model's stream");
+    return JFG_CUDA_ERROR;
+  }
   m->n_nodes = n_nodes; m->n_q4 = n_q4; m->n_q8 = n_q8; m->n_t10 = n_t10;
   m->ndof = 6 * n_nodes;
   m->h_xyz.assign(xyz, xyz + 3 * n_nodes);
@@ -228,6 +233,7 @@ jfg_status jfg_model_free(jfg_model* m) {
   if (!m) return JFG_OK;
   jfg_ctx* c = m->ctx;
   if (m->aev_out) cudaEventSynchronize(m->aev_out);
+  if (m->stream) cudaStreamSynchronize(m->stream);
   if (m->aev_in) cudaEventDestroy(m->aev_in);
   if (m->aev_out) cudaEventDestroy(m->aev_out);
   numeric_destroy(m);
@@ -243,13 +249,30 @@ jfg_status jfg_model_free(jfg_model* m) {
     dev_free(c, m->d_tpos, 8 * m->nnz); dev_free(c, m->d_nzval, 8 * m->nnz);
     dev_free(c, m->d_diag_pos, 8 * m->ndof);
   }
+  if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
+  return JFG_OK;
+}
+
+jfg_status jfg_get_memory(jfg_model* m, int32_t precision, int32_t nrhs, int64_t* now, int64_t* peak) {
+  JFG_TRY(check_model(m));
+  if (precision != JFG_PREC_FP64 && precision != JFG_PREC_MIXED) { set_error("unknown precision"); return JFG_BAD_INPUT; }
+  // inputs, element values and the CQUAD4 prep records
+  int64_t own = 8 * (int64_t)(m->h_xyz.size() + m->h_R.size() + m->h_q4s.size() + m->h_q8s.size() + m->h_t10m.size()) +
+                4 * (int64_t)(m->h_q4n.size() + m->h_q8n.size() + m->h_t10n.size()) + 8 * std::max<int64_t>(m->n_ev, 1) +
+                8 * Q4_PREP_STRIDE * std::max<int64_t>(m->n_q4, 1) + (int64_t)sizeof(DevError);
+  if (m->pattern_built)
+    own += 8 * (m->ndof + 1) + 4 * m->nnz + 4 * (m->nnz + 1) + 4 * m->n_trip + 8 * m->nnz + 8 * m->nnz + 8 * m->ndof;
+  int64_t num_now = 0, num_peak = 0;
+  if (m->sym_ready) numeric_bytes(m, precision, nrhs, &num_now, &num_peak);
+  if (now) *now = own + num_now;
+  if (peak) *peak = own + num_peak;
   return JFG_OK;
 }
 
 jfg_status jfg_assemble(jfg_model* m) {
   JFG_TRY(check_model(m));
-  cudaStream_t st = m->ctx->stream;
+  cudaStream_t st = m->stream;
   cudaEvent_t e0, e1, e2;
   JFG_CUDA(cudaEventCreate(&e0)); JFG_CUDA(cudaEventCreate(&e1)); JFG_CUDA(cudaEventCreate(&e2));
   JFG_CUDA(cudaEventRecord(e0, st));
@@ -409,7 +432,7 @@ jfg_status jfg_model_share_structure(jfg_model* dst, const jfg_model* src) {
   JFG_TRY(dev_alloc(c, (void**)&dst->d_tpos, sizeof(int64_t) * nnz));
   JFG_TRY(dev_alloc(c, (void**)&dst->d_nzval, sizeof(double) * nnz));
   JFG_TRY(up(c, dst->diag_pos, &dst->d_diag_pos));
-  cudaStream_t st = c->stream;
+  cudaStream_t st = dst->stream;
   JFG_CUDA(cudaMemcpyAsync(dst->d_colptr, src->d_colptr, sizeof(int64_t) * (ndof + 1), cudaMemcpyDeviceToDevice, st));
   JFG_CUDA(cudaMemcpyAsync(dst->d_rowval, src->d_rowval, sizeof(int32_t) * nnz, cudaMemcpyDeviceToDevice, st));
   JFG_CUDA(cudaMemcpyAsync(dst->d_nzptr, src->d_nzptr, sizeof(int32_t) * (nnz + 1), cudaMemcpyDeviceToDevice, st));
@@ -462,12 +485,12 @@ jfg_status async_begin(jfg_model* m, cudaStream_t user) {
     JFG_CUDA(cudaEventCreateWithFlags(&m->aev_out, cudaEventDisableTiming));
   }
   JFG_CUDA(cudaEventRecord(m->aev_in, user));
-  JFG_CUDA(cudaStreamWaitEvent(m->ctx->stream, m->aev_in, 0));
+  JFG_CUDA(cudaStreamWaitEvent(m->stream, m->aev_in, 0));
   return JFG_OK;
 }
 // `user` waits for the work just put on the model's stream
 jfg_status async_end(jfg_model* m, cudaStream_t user) {
-  JFG_CUDA(cudaEventRecord(m->aev_out, m->ctx->stream));
+  JFG_CUDA(cudaEventRecord(m->aev_out, m->stream));
   JFG_CUDA(cudaStreamWaitEvent(user, m->aev_out, 0));
   return JFG_OK;
 }
@@ -499,7 +522,7 @@ jfg_status jfg_apply_factor_async(jfg_model* m, int32_t nrhs, const double* F_de
 jfg_status jfg_wait(jfg_model* m) {
   JFG_TRY(check_model(m));
   if (m->aev_out) JFG_CUDA(cudaEventSynchronize(m->aev_out));
-  JFG_CUDA(cudaStreamSynchronize(m->ctx->stream));
+  JFG_CUDA(cudaStreamSynchronize(m->stream));
   if (m->async_factor >= 0) {
     const int p = m->async_factor;
     m->async_factor = -1;
@@ -539,7 +562,7 @@ jfg_status jfg_residual(jfg_model* m, int32_t nrhs, const double* U, const doubl
   JFG_TRY(dev_alloc(m->ctx, (void**)&dU, 8 * len));
   jfg_status st = dev_alloc(m->ctx, (void**)&dR, 8 * len);
   if (st) { dev_free(m->ctx, dU, 8 * len); return st; }
-  cudaStream_t s = m->ctx->stream;
+  cudaStream_t s = m->stream;
   cudaMemcpyAsync(dU, U, 8 * len, cudaMemcpyHostToDevice, s);
   spmv_csc_sym(m, nrhs, dU, m->ndof, dR, m->ndof, s);
   cudaError_t e = cudaMemcpyAsync(R, dR, 8 * len, cudaMemcpyDeviceToHost, s);
@@ -562,7 +585,7 @@ jfg_status jfg_recover_stresses(jfg_model* m, int32_t kind, int32_t nrhs, const 
   JFG_TRY(dev_alloc(m->ctx, (void**)&dU, 8 * len));
   jfg_status st = dev_alloc(m->ctx, (void**)&dO, 8 * olen);
   if (st) { dev_free(m->ctx, dU, 8 * len); return st; }
-  cudaStream_t s = m->ctx->stream;
+  cudaStream_t s = m->stream;
   cudaError_t e = cudaMemcpyAsync(dU, U, 8 * len, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) st = recover_t10_stresses(m, nrhs, dU, dO, s);
   if (e == cudaSuccess && st == JFG_OK) e = cudaMemcpyAsync(out, dO, 8 * olen, cudaMemcpyDeviceToHost, s);
@@ -585,8 +608,8 @@ jfg_status jfg_update_q4_sections(jfg_model* m, int64_t n, const int32_t* elems,
     std::memcpy(m->h_q4s.data() + JFG_Q4_SECT_STRIDE * e, sect + JFG_Q4_SECT_STRIDE * k, 8 * JFG_Q4_SECT_STRIDE);
   }
   // one upload of the whole section table keeps this call simple and ordered
-  JFG_CUDA(cudaMemcpyAsync(m->d_q4s, m->h_q4s.data(), 8 * m->h_q4s.size(), cudaMemcpyHostToDevice, m->ctx->stream));
-  JFG_CUDA(cudaStreamSynchronize(m->ctx->stream));
+  JFG_CUDA(cudaMemcpyAsync(m->d_q4s, m->h_q4s.data(), 8 * m->h_q4s.size(), cudaMemcpyHostToDevice, m->stream));
+  JFG_CUDA(cudaStreamSynchronize(m->stream));
   m->values_ready = false;
   return JFG_OK;
 }

@@ -1937,7 +1937,7 @@ jfg_status numeric_factor_enqueue(jfg_model* m, int precision) {
   if (!m->values_ready) { set_error("factor before assembly"); return JFG_NOT_READY; }
   const Symbolic& S = m->sym;
   jfg_ctx* c = m->ctx;
-  cudaStream_t st = c->stream;
+  cudaStream_t st = m->stream;
   int64_t ublk = std::max<int64_t>(S.u_arena, 1);
   unsigned ga = (unsigned)((F->n_amap + 255) / 256);
   JFG_CUDA(cudaEventRecord(F->ev0, st));
@@ -2031,6 +2031,64 @@ jfg_status numeric_factor_enqueue(jfg_model* m, int precision) {
   return JFG_OK;
 }
 
+// Device bytes of the numeric part of a model: `now` as allocated, `peak`
+// once a factorisation at `precision` and a solve with `nrhs` right-hand
+// sides have run (each allocation mirrored from numeric_create,
+// numeric_factor_enqueue and ensure_workspace).
+void numeric_bytes(jfg_model* m, int precision, int nrhs, int64_t* now, int64_t* peak) {
+  const Symbolic& S = m->sym;
+  NumericFactor* F = m->num;
+  const int64_t ns = S.ns, n = S.n, ndof = m->ndof, na = (int64_t)S.amap_dst.size();
+  int64_t base = 4 * (ns + 1) + 4 * ns + 4 * ns + 4 * std::max<int64_t>((int64_t)S.ea_child.size(), 1) +
+                 4 * std::max<int64_t>((int64_t)S.rel.size(), 1) + 4 * (int64_t)S.rows.size() + 4 * ns + 4 * n +
+                 4 * na + 8 * (ns + 1) + 8 * ns + 8 * (ns + 1) + 8 * (ns + 1) + 8 * na + 8 * na + 3 * 8 * ns +
+                 8 * (256 * 64 + 64) + ndof + (int64_t)sizeof(DevError);
+  int64_t items = 0, dl = 0, sl = 0;
+  for (int64_t s = 0; s < ns; ++s) {
+    const int64_t cc = S.sn_first[s + 1] - S.sn_first[s];
+    dl += ((cc + 63) / 64) * 64 * 64;
+    for (int64_t kb = 0; kb * 256 < cc; ++kb) {
+      const int64_t kw = std::min<int64_t>(256, cc - 256 * kb);
+      sl += kw * kw;
+      items += (kw + 63) / 64;
+    }
+  }
+  base += 12 * std::max<int64_t>(items, 1);
+  const int64_t ublk = std::max<int64_t>(S.u_arena, 1);
+  int64_t part = F ? F->part_len : 0;
+  base += 8 * part;
+  auto fp64 = [&]() { return 8 * S.nnz_L + 8 * ublk + 8 * std::max<int64_t>(dl, 1) + 8 * std::max<int64_t>(sl, 1); };
+  auto mixed = [&]() {
+    int64_t pk = 0;
+    for (int64_t l = 0; l < S.n_levels; ++l) {
+      int64_t acc = 0;
+      for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
+        const int32_t s = S.level_sn[q];
+        acc += ((S.sn_first[s + 1] - S.sn_first[s] + 15) / 16) * ((S.sn_m[s] + 7) / 8) * 128;
+      }
+      pk = std::max(pk, acc);
+    }
+    return 4 * S.nnz_L + 4 * ublk + 8 * n + 4 * std::max<int64_t>(dl, 1) + 4 * std::max<int64_t>(sl, 1) +
+           2 * 4 * std::max<int64_t>(pk, 128) + 8 * (ns + 1) + 8192;
+  };
+  auto work = [&](int cap) {
+    const int64_t vt = std::max<int64_t>(S.sn_relptr.empty() ? 0 : S.sn_relptr[ns], 1);
+    return 8 * cap * (3 * n + vt + 6 * ndof);
+  };
+  int64_t cur = base;
+  if (F) {
+    if (F->L64) cur += fp64();
+    if (F->L32) cur += mixed();
+    if (F->nrhs_cap > 0) cur += work(F->nrhs_cap);
+  }
+  const int cap = std::max(std::min(std::max(nrhs, 1), MAXR), F ? std::max(F->nrhs_cap, 8) : 8);
+  int64_t pk = base + (precision == JFG_PREC_FP64 ? fp64() : mixed()) + work(cap);
+  if (F && precision == JFG_PREC_FP64 && F->L32) pk += mixed();
+  if (F && precision == JFG_PREC_MIXED && F->L64) pk += fp64();
+  *now = cur;
+  *peak = std::max(pk, cur);
+}
+
 // Precision of the factor a solve would use (-1: none).
 int numeric_current_precision(jfg_model* m) {
   NumericFactor* F = m->num;
@@ -2065,7 +2123,7 @@ jfg_status numeric_apply(jfg_model* m, int nrhs, const double* Fd, double* Ud, i
   const bool use32 = precision == JFG_PREC_MIXED;
   if ((use32 && !F->L32) || (!use32 && !F->L64)) { set_error("apply before factorisation"); return JFG_NOT_READY; }
   const Symbolic& S = m->sym;
-  cudaStream_t st = m->ctx->stream;
+  cudaStream_t st = m->stream;
   const int64_t n = S.n, ndof = m->ndof;
   const unsigned gn = (unsigned)((n + 255) / 256);
   for (int done = 0; done < nrhs;) {
@@ -2091,7 +2149,7 @@ jfg_status numeric_factor_diag(jfg_model* m, double* out) {
   NumericFactor* F = m->num;
   if (!F || !(F->have64 || F->have32)) { set_error("no factor"); return JFG_NOT_READY; }
   const Symbolic& S = m->sym;
-  cudaStream_t st = m->ctx->stream;
+  cudaStream_t st = m->stream;
   double* d = nullptr;
   JFG_TRY(dev_alloc(m->ctx, (void**)&d, sizeof(double) * std::max<int64_t>(S.n, 1)));
   if (F->have64)
@@ -2120,7 +2178,7 @@ jfg_status numeric_solve(jfg_model* m, int nrhs, const double* hF, double* hU, d
   if (max_ir < 0) max_ir = 30;
   const Symbolic& S = m->sym;
   jfg_ctx* c = m->ctx;
-  cudaStream_t st = c->stream;
+  cudaStream_t st = m->stream;
   const int64_t n = S.n, ndof = m->ndof;
   const bool trace = std::getenv("JFG_IR_TRACE") != nullptr;
   JFG_CUDA(cudaEventRecord(F->ev0, st));

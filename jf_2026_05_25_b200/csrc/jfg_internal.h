@@ -102,6 +102,9 @@ struct NumericFactor;   // defined in factor.cu
 
 struct jfg_model {
   jfg_ctx* ctx = nullptr;
+  // the model's own stream: models of one context may be driven from
+  // different host threads (and captured into graphs) independently
+  cudaStream_t stream = nullptr;
   int64_t n_nodes = 0, n_q4 = 0, n_q8 = 0, n_t10 = 0, ndof = 0;
   // host copies of the inputs (pattern build, element capture)
   std::vector<double> h_xyz, h_R, h_q4s, h_q8s, h_t10m;
@@ -168,6 +171,7 @@ jfg_status numeric_factor_enqueue(jfg_model* m, int precision);
 jfg_status numeric_factor_finish(jfg_model* m, int precision);
 jfg_status numeric_apply(jfg_model* m, int nrhs, const double* Fd, double* Ud, int precision);
 int numeric_current_precision(jfg_model* m);
+void numeric_bytes(jfg_model* m, int precision, int nrhs, int64_t* now, int64_t* peak);
 jfg_status numeric_solve(jfg_model* m, int nrhs, const double* hF, double* hU, double tol,
                          int max_ir, jfg_solve_report* rep, bool device_io);
 jfg_status numeric_factor_diag(jfg_model* m, double* out);

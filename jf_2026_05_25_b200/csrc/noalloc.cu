@@ -153,7 +153,7 @@ jfg_status jfg_assemble_values_noalloc(jfg_model* m, double* nzval_dev) {
   DevError* err = reinterpret_cast<DevError*>(base);
   double* ev = reinterpret_cast<double*>(base + kHeaderBytes);
   double* q4prep = reinterpret_cast<double*>(base + kHeaderBytes + ev_bytes);
-  cudaStream_t st = m->ctx->stream;
+  cudaStream_t st = m->stream;
   JFG_CUDA(cudaMemsetAsync(err, 0, sizeof(DevError), st));
   JFG_TRY(launch_elements_into(m, st, ev, q4prep, err));
   JFG_TRY(launch_gather_into(m, st, ev, nzval_dev));

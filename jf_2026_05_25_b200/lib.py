@@ -97,6 +97,7 @@ def load():
         "jfg_factor_async": [P, I32, P],
         "jfg_apply_factor_async": [P, I32, P, P, P],
         "jfg_wait": [P],
+        "jfg_get_memory": [P, I32, I32, P, P],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -272,6 +273,12 @@ class DeviceModel:
     def apply_factor_async(self, F_ptr: int, U_ptr: int, nrhs: int, stream_ptr: int):
         """Enqueue U = K_ff^-1 F (one factor application, device arrays)."""
         _check(load().jfg_apply_factor_async(self.h, nrhs, P(F_ptr), P(U_ptr), P(stream_ptr)))
+
+    def memory(self, precision: int, nrhs: int):
+        """(bytes held now, bytes after factoring at `precision` and solving nrhs columns)."""
+        a, b = I64(), I64()
+        _check(load().jfg_get_memory(self.h, precision, nrhs, _c.byref(a), _c.byref(b)))
+        return a.value, b.value
 
     def wait(self):
         _check(load().jfg_wait(self.h))

@@ -422,7 +422,8 @@ class SolveServer:
 
     def _register(self, dm, state, pack, models, reserved: float = 0.0, keys: Optional[List[str]] = None,
                   mesh: Optional[bytes] = None) -> List[str]:
-        nbytes = self._bytes_of(dm)
+        # resident bytes: what was admitted for it, or an estimate from its sizes
+        nbytes = reserved if reserved > 0 else self._bytes_of(dm)
         lock = threading.Lock()
         out = []
         with self.rlock:
@@ -445,12 +446,34 @@ class SolveServer:
         return out
 
     # ---------------------------------------------------------------- work
-    def _prepare(self, be, model, pack: Optional[PackedModel]):
+    @staticmethod
+    def _upload_estimate(target) -> float:
+        """Device bytes of a model before its analysis (inputs, element
+        values, CSC pattern), from its sizes: 9 node pairs of 36 entries per
+        shell grid, 30 pairs of 9 per solid grid."""
+        n_q4 = len(getattr(target, "q4_nodes", ()))
+        n_q8 = len(getattr(target, "q8_nodes", ()))
+        n_t10 = len(getattr(target, "t10_nodes", ()))
+        n_ev = 576 * n_q4 + 2304 * n_q8 + 900 * n_t10
+        nnz = (324 if n_t10 == 0 else 270) * target.n_nodes
+        return float(8 * n_ev + 8 * 210 * n_q4 + 4 * n_ev + 28 * nnz + 150 * target.n_nodes)
+
+    def _prepare(self, be, model, pack: Optional[PackedModel], nrhs: int = 8):
         """Upload (sharing a resident mesh's structure when there is one),
-        analyse, admit the exact bytes, factor.  Returns (state, reserved, mesh)."""
+        analyse, admit the exact bytes, factor.  Device bytes are admitted
+        twice: an estimate before the upload, and the library's own figure
+        (jfg_get_memory: factor, its work arrays and the solve work space for
+        `nrhs`) once the analysis exists.  Returns (state, reserved, mesh)."""
         target = pack if pack is not None else model
         mk = mesh_key(model) if (pack is None and self.share_meshes) else None
-        dm = lib.DeviceModel(be.ctx, target)
+        pre = self._upload_estimate(target)
+        self._admit(pre, wait=True)
+        admitted = [pre]
+        try:
+            dm = lib.DeviceModel(be.ctx, target)
+        except Exception:
+            self._release(pre)
+            raise
         donor = None
         if mk is not None:
             with self.rlock:
@@ -462,26 +485,26 @@ class SolveServer:
                     dm.share_structure(donor.dm)
                     with self.rlock:
                         self.shared_structures += 1
-        admitted = [0.0]
 
         def admit(d):
-            need = float(self._bytes_of(d))
-            self._admit(need, wait=True)
-            admitted[0] = need
+            need = float(d.memory(self.precision, nrhs)[1])
+            if need > admitted[0]:
+                self._admit(need - admitted[0], wait=True)
+                admitted[0] = need
 
         try:
             st = B.prepare(be, target, dm=dm, before_factor=admit)
         except Exception:
             dm.close()
-            if admitted[0]:
-                self._release(admitted[0])
+            self._release(admitted[0])
             raise
         return st, admitted[0], mk
 
     def _do_solve(self, be, reqs: List[Request]):
         models = [r.model for r in reqs]
         pack = PackedModel(models)
-        st, reserved, mk = self._prepare(be, models[0], pack if len(models) > 1 else None)
+        nrhs = max(16, max((r.loads.shape[0] if r.device else len(r.model.load_cases)) for r in reqs))
+        st, reserved, mk = self._prepare(be, models[0], pack if len(models) > 1 else None, nrhs)
         try:
             if reqs[0].device:
                 Us, res, rep = self._device_solve(be, st["dm"], pack, [r.loads for r in reqs], self.tol)
@@ -585,7 +608,7 @@ class SolveServer:
             model = self.evicted.get(key)
         if model is None:
             raise KeyError(f"model {key} is unknown")
-        st, reserved, mk = self._prepare(be, model, None)
+        st, reserved, mk = self._prepare(be, model, None, 32)
         pack = PackedModel([model])
         self._register(st["dm"], st, pack, [model], reserved=reserved, keys=[key], mesh=mk)
         with self.rlock:
