@@ -521,3 +521,29 @@ def test_wide_right_hand_side_sweeps_match_narrow(ctx, oracle_mod, prec):
     ref = oracle_mod.solve_reference(m)
     assert _rel(U, ref["u"]) <= DISP_RTOL
     dm.close()
+
+
+@pytest.mark.parametrize("prec", [lib.PREC_FP64, lib.PREC_MIXED])
+def test_memory_figure_predicts_the_allocations(ctx, prec):
+    """jfg_get_memory's figure for a factorisation and an 8-column solve,
+    taken right after the analysis, equals the bytes the model holds once
+    both have run; and the device's free memory fell by at least that much
+    (allocations round up)."""
+    import torch
+    m = M.wing_panel(nx=24, ny=36, n_blades=3, blade_nz=4, n_cases=8, seed=5)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    dm = lib.DeviceModel(ctx, m)
+    dm.assemble()
+    d, _ = dm.diag()
+    free, _, _ = B.compute_free_dofs(m, d, dm.node_blocks())
+    dm.set_free_dofs(free)
+    now0, peak = dm.memory(prec, 8)
+    assert peak > now0 > 0
+    dm.factor(prec)
+    dm.solve(m.load_matrix(), RESID_TOL, 40, raise_on_stall=False)
+    now1, _ = dm.memory(prec, 8)
+    assert now1 == peak
+    free1, _ = torch.cuda.mem_get_info()
+    assert free0 - free1 >= 0.95 * now1
+    dm.close()
