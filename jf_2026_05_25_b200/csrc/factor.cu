@@ -1101,7 +1101,10 @@ k_fwd_supdate(const int32_t* __restrict__ list, const int32_t* __restrict__ firs
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (i < m) {
     const T* P = L + Lptr[s] + i;
-    int l0 = g * (SW / 8), l1 = min(l0 + SW / 8, kw);
+    // the strip's kw columns split evenly over the 8 warps (narrow fronts
+    // would otherwise leave most warps without columns)
+    const int cw = (kw + 7) / 8;
+    int l0 = g * cw, l1 = min(l0 + cw, kw);
 #pragma unroll 8
     for (int l = l0; l < l1; ++l) {
       double lv = (double)P[(int64_t)m * (j0 + l)];
