@@ -773,7 +773,8 @@ def run_serving(args, rank=0, world=1, local_rank=0):
                          "throughput_pass_latency": {"p50_ms": st_v["p50_ms"], "p99_ms": st_v["p99_ms"]},
                          "max_rel_residual": max(worst, worst_e), "pcg_iters_mean": float(np.mean(iters)),
                          "pcg_iters_max": int(np.max(iters)), "fallbacks": int(fb),
-                         "readmissions": st_v["readmissions"], "shared_structures": st_v["shared_structures"]}
+                         "readmissions": st_v["readmissions"], "shared_structures": st_v["shared_structures"],
+                         "fp64_meshes": st_v["fp64_meshes"], "fp64_factorisations": st_v["fp64_factorisations"]}
             rate = args.rate if args.rate > 0 else None
             if rate is None:
                 rate = 0.5 * (n_req / arms["fp64"]["stream_s"]) if "fp64" in arms else 0.5 * n_req / secs
@@ -809,7 +810,9 @@ def run_serving(args, rank=0, world=1, local_rank=0):
                        "slots": args.slots, "hbm_budget_gb": 150, "parallelism": f"replicas{world}",
                        "arrivals": "value and e2e: saturated (all new models queued at once); latency: Poisson",
                        "l2": "inputs larger than L2 (wing factor 2.3 GB, block factor 40 GB)",
-                       "precision": "mixed 3xTF32 tensor-core factor + FP64 refinement; fp64 arm: plain FP64"},
+                       "precision": "mixed arm: 3xTF32 tensor-core factor + FP64 refinement, with the FP64 (DMMA) "
+                                    "factor for meshes whose refinement took more than 6 steps (thin-shell / "
+                                    "drilling conditioning); fp64 arm: plain FP64"},
             "e2e": {"value": mixed["e2e"], "unit": "solves/s", "h2d_bytes_per_step": int(mixed["h2d_bytes"] / args.steps),
                     "d2h_bytes_per_step": int(mixed["d2h_bytes"] / args.steps)},
             "mixed_over_fp64": mixed["value"] / fp64["value"], "mixed_over_fp64_e2e": mixed["e2e"] / fp64["e2e"],

@@ -154,7 +154,7 @@ def compute_free_dofs(model, diag: np.ndarray, node_blocks: np.ndarray, eps_zero
 # ----------------------------------------------------------------------------
 
 def prepare(backend: JFEMGPUBackend, model, donor: Optional["lib.DeviceModel"] = None,
-            before_factor=None, dm: Optional["lib.DeviceModel"] = None) -> Dict:
+            before_factor=None, dm: Optional["lib.DeviceModel"] = None, precision: Optional[int] = None) -> Dict:
     """Upload, assemble, partition, analyse and factor: the per-model state
     that the reference caches in LinearSolveCacheEntry (boundary_conditions.jl:62-75).
 
@@ -163,7 +163,9 @@ def prepare(backend: JFEMGPUBackend, model, donor: Optional["lib.DeviceModel"] =
     ``before_factor(dm)``: called once the symbolic analysis exists and before
     the factor is allocated (the serving loop admits the model's bytes there).
     ``dm``: the model already uploaded (and possibly given a donor's structure).
+    ``precision``: the factor's precision when it differs from the backend's.
     """
+    prec = backend.precision if precision is None else precision
     timings = {}
     t0 = time.perf_counter()
     if dm is None:
@@ -181,7 +183,7 @@ def prepare(backend: JFEMGPUBackend, model, donor: Optional["lib.DeviceModel"] =
     if before_factor is not None:
         before_factor(dm)
     t2 = time.perf_counter()
-    dm.factor(backend.precision)
+    dm.factor(prec)
     # post-factor pivot check L_ii^2 / K_ii < threshold (boundary_conditions.jl:1662-1710)
     Ld = np.abs(dm.factor_diag())
     perm = dm.perm()
@@ -195,9 +197,9 @@ def prepare(backend: JFEMGPUBackend, model, donor: Optional["lib.DeviceModel"] =
         dm.set_free_dofs(keep)
         free = keep
         fixed = np.union1d(fixed, extra)
-        dm.factor(backend.precision)
+        dm.factor(prec)
     timings["factorization"] = time.perf_counter() - t2
-    return dict(dm=dm, free=free, fixed=fixed, bc=bc, max_elem_stiff=max_elem, timings=timings)
+    return dict(dm=dm, free=free, fixed=fixed, bc=bc, max_elem_stiff=max_elem, timings=timings, precision=prec)
 
 
 def solve_model(backend: JFEMGPUBackend, model, state: Optional[Dict] = None) -> Dict:

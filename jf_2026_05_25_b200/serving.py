@@ -231,10 +231,16 @@ class SolveServer:
     def __init__(self, device: int = 0, slots: int = 4, hbm_budget_bytes: float = 150e9,
                  precision: int = lib.PREC_FP64, tol: float = 1e-10, small_dof: int = 60000,
                  pack_dof: int = 400000, pack_models: int = 64, share_meshes: bool = True,
-                 wait_s: float = 300.0):
+                 wait_s: float = 300.0, slow_refinement_steps: int = 6):
         self.device, self.precision, self.tol = device, precision, tol
         self.small_dof, self.pack_dof, self.pack_models = small_dof, pack_dof, pack_models
         self.share_meshes, self.wait_s = share_meshes, wait_s
+        # mixed precision: a mesh whose refinement needed more than this many
+        # steps (thin-shell / drilling conditioning) takes the FP64 factor
+        # for its later models, updates and re-admissions
+        self.slow_refinement_steps = slow_refinement_steps
+        self.fp64_meshes = set()
+        self.fp64_factorisations = 0
         self.budget = float(hbm_budget_bytes)
         self.q: "queue.Queue[Request]" = queue.Queue()
         self.pending: List[Request] = []
@@ -303,7 +309,8 @@ class SolveServer:
         return {"requests": int(lat.size), "p50_ms": float(np.percentile(lat, 50) * 1e3),
                 "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3),
                 "subcase_solves": int(self.subcase_solves), "resident_bytes": int(self.resident_bytes),
-                "readmissions": int(self.readmissions), "shared_structures": int(self.shared_structures)}
+                "readmissions": int(self.readmissions), "shared_structures": int(self.shared_structures),
+                "fp64_meshes": len(self.fp64_meshes), "fp64_factorisations": int(self.fp64_factorisations)}
 
     # ---------------------------------------------------------------- scheduling
     def _take(self) -> Optional[List[Request]]:
@@ -466,6 +473,11 @@ class SolveServer:
         `nrhs`) once the analysis exists.  Returns (state, reserved, mesh)."""
         target = pack if pack is not None else model
         mk = mesh_key(model) if (pack is None and self.share_meshes) else None
+        prec = self.precision
+        if prec == lib.PREC_MIXED and mk is not None and mk in self.fp64_meshes:
+            prec = lib.PREC_FP64
+            with self.rlock:
+                self.fp64_factorisations += 1
         pre = self._upload_estimate(target)
         self._admit(pre, wait=True)
         admitted = [pre]
@@ -487,13 +499,13 @@ class SolveServer:
                         self.shared_structures += 1
 
         def admit(d):
-            need = float(d.memory(self.precision, nrhs)[1])
+            need = float(d.memory(prec, nrhs)[1])
             if need > admitted[0]:
                 self._admit(need - admitted[0], wait=True)
                 admitted[0] = need
 
         try:
-            st = B.prepare(be, target, dm=dm, before_factor=admit)
+            st = B.prepare(be, target, dm=dm, before_factor=admit, precision=prec)
         except Exception:
             dm.close()
             self._release(admitted[0])
@@ -526,6 +538,10 @@ class SolveServer:
             st["dm"].close()
             self._release(reserved)
             raise
+        if (self.precision == lib.PREC_MIXED and mk is not None and st.get("precision") == lib.PREC_MIXED
+                and rep.get("ir_iters", 0) > self.slow_refinement_steps):
+            with self.rlock:
+                self.fp64_meshes.add(mk)
         keys = self._register(st["dm"], st, pack, models, reserved=reserved, mesh=mk)
         for k, r in enumerate(reqs):
             self._finish(r, {"key": keys[k], "U": Us[k], "rel_residual": res[k], "batch": len(reqs),
@@ -650,7 +666,7 @@ class SolveServer:
                 # keep the host description current (a freed model is re-admitted from it)
                 res.model.q4_sect_override = res.pack._q4s[off:res.pack.q4_off[res.index + 1]].copy()
                 res.dm.assemble()
-                res.dm.factor(self.precision)
+                res.dm.factor(res.state.get("precision", self.precision))
                 out = self._member_solve(res, req.loads, be, req.device)
             break
         else:
