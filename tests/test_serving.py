@@ -166,3 +166,26 @@ def test_server_device_resident_loads_match_host(alone):
         assert _rel(r2["U"].cpu().numpy().T, 3.0 * alone[s0]) <= DISP_RTOL
     finally:
         srv.close()
+
+
+def test_mixed_server_moves_slow_meshes_to_the_fp64_factor():
+    """In a mixed-precision server a mesh whose refinement needs more than
+    `slow_refinement_steps` steps takes the FP64 factor for its later models
+    (the threshold is 0 here, so the first model marks its mesh); both
+    results meet the bar and match the FP64 solve."""
+    a = M.wing_panel(nx=24, ny=36, n_blades=3, blade_nz=4, n_cases=2, seed=5)
+    b = M.wing_panel(nx=24, ny=36, n_blades=3, blade_nz=4, n_cases=2, seed=6)
+    ref = B.solve_model(B.JFEMGPUBackend(tol=RESID_TOL), b)
+    Ub = np.stack([sc["raw_displacement"] for sc in ref["subcases"]], axis=1)
+    ref["state"]["dm"].close()
+    srv = S.SolveServer(slots=1, tol=RESID_TOL, small_dof=0, precision=lib.PREC_MIXED, slow_refinement_steps=0)
+    try:
+        ra = srv.solve(a).result(timeout=600)
+        rb = srv.solve(b).result(timeout=600)
+        st = srv.stats()
+        assert st["fp64_meshes"] == 1 and st["fp64_factorisations"] == 1
+        assert ra["rel_residual"].max() <= RESID_TOL and rb["rel_residual"].max() <= RESID_TOL
+        assert rb["report"]["precision"] == lib.PREC_FP64
+        assert _rel(rb["U"], Ub) <= DISP_RTOL
+    finally:
+        srv.close()
