@@ -57,8 +57,16 @@ struct NumericFactor {
       return (int)(std::upper_bound(cs.begin(), cs.end(), kmin, std::greater<int32_t>()) - cs.begin());
     }
     int maxm(int na) const { return na > 0 ? pm[na - 1] : 0; }
+    // tile lists (offset, count into NumericFactor::tiles) of the level's launches
+    struct Span { int64_t off = 0; int32_t cnt = 0; };
+    std::vector<Span> ea_f, ea_s;     // factor / solve extend-add, per child-rank segment
+    std::vector<Span> trsm;           // panel trsm, per 64-column step
+    struct StripSpans { Span diag, upd32, upd128, bwd; };
+    std::vector<StripSpans> strips;   // solve sweeps, per 256-column strip
   };
   std::vector<Level> levels;
+  int2* tiles = nullptr;      // every level launch's work tiles (see tile_of)
+  int64_t n_tiles = 0;
   // factor storage
   double* L64 = nullptr;
   double* U64 = nullptr;
@@ -175,6 +183,22 @@ inline int panel_width() {
   return v;
 }
 
+// Work tiles of a level launch: with a tile list, CTA x takes tile tiles[x]
+// = (position of the front in the level's list, block of that front); the
+// list holds only blocks that have work, so a level of fronts of very
+// different sizes launches no empty CTAs.  Without one the grid is
+// (blocks, fronts).
+__device__ __forceinline__ void tile_of(const int2* __restrict__ tiles, int& q, int& b) {
+  if (tiles) {
+    const int2 t = tiles[blockIdx.x];
+    q = t.x;
+    b = t.y;
+  } else {
+    q = blockIdx.y;
+    b = blockIdx.x;
+  }
+}
+
 __device__ inline void rec_err(DevError* e, int32_t code, int64_t idx) {
   if (atomicCAS(&e->code, 0, code) == 0) e->index = idx;
 }
@@ -206,12 +230,14 @@ __global__ void k_extend_add(const int32_t* __restrict__ child, const int32_t* _
                              const int32_t* __restrict__ mrows, const int32_t* __restrict__ parent,
                              const int64_t* __restrict__ Lptr, const int64_t* __restrict__ Uptr,
                              const int64_t* __restrict__ relptr, const int32_t* __restrict__ rel,
-                             T* __restrict__ L, T* __restrict__ U, int pass) {
-  int ch = child[blockIdx.y];
+                             T* __restrict__ L, T* __restrict__ U, int pass, const int2* __restrict__ tiles) {
+  int tq, tb;
+  tile_of(tiles, tq, tb);
+  int ch = child[tq];
   int64_t uc = Uptr[ch];
   if (uc < 0) return;
   int rc = mrows[ch] - (first[ch + 1] - first[ch]);
-  int cb = blockIdx.x * 8 + (threadIdx.x >> 5);   // one warp per child column
+  int cb = tb * 8 + (threadIdx.x >> 5);   // one warp per child column
   if (cb >= rc) return;
   int lane = threadIdx.x & 31;
   int p = parent[ch];
@@ -529,13 +555,15 @@ __global__ void __launch_bounds__(256)
 k_trsm_panel(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
              const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr, const int64_t* __restrict__ Dptr,
              T* __restrict__ L, const T* __restrict__ Dinv, int k0, float* __restrict__ Phi,
-             float* __restrict__ Plo, const int64_t* __restrict__ PKptr) {
-  int s = list[blockIdx.y];
+             float* __restrict__ Plo, const int64_t* __restrict__ PKptr, const int2* __restrict__ tiles) {
+  int tq, tb;
+  tile_of(tiles, tq, tb);
+  int s = list[tq];
   int c = first[s + 1] - first[s];
   if (k0 >= c) return;
   int m = mrows[s];
   int k1 = min(k0 + NB, c), kn = k1 - k0;
-  int row0 = k1 + blockIdx.x * 64;
+  int row0 = k1 + tb * 64;
   if (row0 >= m) return;
   extern __shared__ unsigned char smem_raw[];
   T (*Di)[NB + 1] = reinterpret_cast<T (*)[NB + 1]>(smem_raw);
@@ -884,8 +912,10 @@ template <int NRC>
 __global__ void k_vec_extend_add(const int32_t* __restrict__ child, const int32_t* __restrict__ first,
                                  const int32_t* __restrict__ mrows, const int32_t* __restrict__ parent,
                                  const int64_t* __restrict__ relptr, const int32_t* __restrict__ rel, int nr,
-                                 int64_t n, double* __restrict__ xp, double* __restrict__ V) {
-  int ch = child[blockIdx.x];
+                                 int64_t n, double* __restrict__ xp, double* __restrict__ V, const int2* __restrict__ tiles) {
+  int tq, tb;
+  tile_of(tiles, tq, tb);
+  int ch = child[tq];
   int rc = mrows[ch] - (first[ch + 1] - first[ch]);
   int p = parent[ch];
   int cp = first[p + 1] - first[p];
@@ -893,9 +923,9 @@ __global__ void k_vec_extend_add(const int32_t* __restrict__ child, const int32_
   const int32_t* rl = rel + relptr[ch];
   const double* src = V + relptr[ch] * nr;
   double* vp = V + relptr[p] * nr;
-  // blockIdx.y takes a chunk of 256 update rows; children of one launch have
+  // the tile's block is a chunk of 256 update rows; children of one launch have
   // distinct parents, and distinct rows of a child map to distinct targets
-  int a = blockIdx.y * 256 + threadIdx.x;
+  int a = tb * 256 + threadIdx.x;
   if (a >= rc) return;
   int ra = rl[a];
   double* dst = (ra < cp) ? xp + first[p] + ra : vp + (ra - cp);
@@ -1027,13 +1057,15 @@ template <typename T, int NRC>
 __global__ void __launch_bounds__(256)
 k_fwd_sdiag(const int32_t* __restrict__ list, const int32_t* __restrict__ first, const int64_t* __restrict__ Sptr,
             const T* __restrict__ Sinv, int kb, int nr, int64_t n, const double* __restrict__ xp,
-            double* __restrict__ tt) {
-  int s = list[blockIdx.y];
+            double* __restrict__ tt, const int2* __restrict__ tiles) {
+  int tq, tb;
+  tile_of(tiles, tq, tb);
+  int s = list[tq];
   int f = first[s], c = first[s + 1] - f;
   int j0 = kb * SW;
   if (j0 >= c) return;
   int kw = min(SW, c - j0);
-  int g = blockIdx.x, r0 = 32 * g;
+  int g = tb, r0 = 32 * g;
   if (r0 >= kw) return;
   const T* X = Sinv + Sptr[s] + (int64_t)kb * SW * SW;
   int rmax = min(kw, r0 + 32);          // columns j < rmax can touch the slab
@@ -1079,13 +1111,15 @@ __global__ void __launch_bounds__(256)
 k_fwd_supdate(const int32_t* __restrict__ list, const int32_t* __restrict__ first, const int32_t* __restrict__ mrows,
               const int64_t* __restrict__ Lptr, const int64_t* __restrict__ relptr, const T* __restrict__ L, int kb,
               int nr, int64_t n, const double* __restrict__ tt, double* __restrict__ xp,
-              double* __restrict__ V) {
-  int s = list[blockIdx.y];
+              double* __restrict__ V, const int2* __restrict__ tiles) {
+  int tq, tb;
+  tile_of(tiles, tq, tb);
+  int s = list[tq];
   int f = first[s], c = first[s + 1] - f, m = mrows[s], r = m - c;
   int j0 = kb * SW;
   if (j0 >= c) return;
   int kw = min(SW, c - j0);
-  int row0 = j0 + kw + blockIdx.x * 32;
+  int row0 = j0 + kw + tb * 32;
   if (row0 >= m) return;
   __shared__ double ys[SW][8];
   __shared__ double red[8][32][9];
@@ -1135,13 +1169,15 @@ __global__ void __launch_bounds__(128)
 k_fwd_supdate_wide(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
                    const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
                    const int64_t* __restrict__ relptr, const T* __restrict__ L, int kb, int nr, int64_t n,
-                   const double* __restrict__ tt, double* __restrict__ xp, double* __restrict__ V) {
-  int s = list[blockIdx.y];
+                   const double* __restrict__ tt, double* __restrict__ xp, double* __restrict__ V, const int2* __restrict__ tiles) {
+  int tq, tb;
+  tile_of(tiles, tq, tb);
+  int s = list[tq];
   int f = first[s], c = first[s + 1] - f, m = mrows[s], r = m - c;
   int j0 = kb * SW;
   if (j0 >= c) return;
   int kw = min(SW, c - j0);
-  int row0 = j0 + kw + blockIdx.x * 128;
+  int row0 = j0 + kw + tb * 128;
   if (row0 >= m) return;
   __shared__ double ys[64][NRC];
   const int i = row0 + threadIdx.x;
@@ -1215,14 +1251,16 @@ k_bwd_spartial(const int32_t* __restrict__ list, const int32_t* __restrict__ fir
                const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
                const int64_t* __restrict__ rows_ptr, const int32_t* __restrict__ rows,
                const int64_t* __restrict__ part_off, const T* __restrict__ L, int kb, int nr, int64_t n,
-               const double* __restrict__ xp, double* __restrict__ part) {
-  int s = list[blockIdx.y];
+               const double* __restrict__ xp, double* __restrict__ part, const int2* __restrict__ tiles) {
+  int tq, tb;
+  tile_of(tiles, tq, tb);
+  int s = list[tq];
   int c = first[s + 1] - first[s], m = mrows[s];
   int j0 = kb * SW;
   if (j0 >= c) return;
   int kw = min(SW, c - j0);
   int nrb = (m - (j0 + kw) + 255) / 256;
-  int rb = blockIdx.x / (SW / 32), cg = blockIdx.x % (SW / 32);
+  int rb = tb / (SW / 32), cg = tb % (SW / 32);
   if (rb >= nrb || cg * 32 >= kw) return;
   int row0 = j0 + kw + rb * 256;
   // right-hand-side major, so that lanes reading consecutive rows hit
@@ -1237,7 +1275,7 @@ k_bwd_spartial(const int32_t* __restrict__ list, const int32_t* __restrict__ fir
   }
   __syncthreads();
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* out = part + part_off[blockIdx.y] + (int64_t)rb * SW * MAXR;
+  double* out = part + part_off[tq] + (int64_t)rb * SW * MAXR;
   constexpr int GRP = 32 / NRC;   // lanes sharing one reduced component
   for (int q = 0; q < 4; ++q) {
     int jj = cg * 32 + warp * 4 + q;
@@ -1273,16 +1311,18 @@ __global__ void __launch_bounds__(256)
 k_bwd_sdiag(const int32_t* __restrict__ list, const int32_t* __restrict__ first, const int32_t* __restrict__ mrows,
             const int64_t* __restrict__ Sptr, const int64_t* __restrict__ part_off, const T* __restrict__ Sinv,
             int kb, int nr, int64_t n, const double* __restrict__ part, const double* __restrict__ tt,
-            double* __restrict__ xp) {
-  int s = list[blockIdx.y];
+            double* __restrict__ xp, const int2* __restrict__ tiles) {
+  int tq, tb;
+  tile_of(tiles, tq, tb);
+  int s = list[tq];
   int f = first[s], c = first[s + 1] - f, m = mrows[s];
   int j0 = kb * SW;
   if (j0 >= c) return;
   int kw = min(SW, c - j0);
-  int g = blockIdx.x, i0 = 32 * g;
+  int g = tb, i0 = 32 * g;
   if (i0 >= kw) return;
   int nrb = (m - (j0 + kw) + 255) / 256;
-  const double* pp = part + part_off[blockIdx.y];
+  const double* pp = part + part_off[tq];
   const T* X = Sinv + Sptr[s] + (int64_t)kb * SW * SW;
   extern __shared__ double sdyn[];
   double (*bs)[SW] = reinterpret_cast<double (*)[SW]>(sdyn);   // right-hand-side major
@@ -1462,12 +1502,13 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
       launch_front_update<T>((unsigned)tiles, cnt, F, Lf, Uf, mode, kbeg, kend, cend, st);
     };
     // extend-add, pass 0: children columns that land in this level's panels
-    for (const auto& seg : lv.ea) {
-      if (seg.second == 0) continue;
-      unsigned gx = (unsigned)((lv.ea_max_r + 7) / 8);
-      if (gx == 0) continue;
-      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_extend_add<T><<<dim3(gx, seg.second), 256, 0, st>>>(F->ea_child + seg.first, F->first, F->mrows,
-                                                            F->parent, F->Lptr, F->Uptr, F->relptr, F->rel, Lf, Uf, 0);
+    for (size_t si = 0; si < lv.ea.size(); ++si) {
+      const auto& seg = lv.ea[si];
+      const auto& tsp = lv.ea_f[si];
+      if (seg.second == 0 || tsp.cnt == 0) continue;
+      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_extend_add<T><<<(unsigned)tsp.cnt, 256, 0, st>>>(F->ea_child + seg.first, F->first, F->mrows,
+                                                            F->parent, F->Lptr, F->Uptr, F->relptr, F->rel, Lf, Uf, 0,
+                                                            F->tiles + tsp.off);
         count_launch(); } prof_end(ps_, st, KS_F_EA, 0.0); }
     }
     // algorithmic flops of the level's diagonal-block, trsm and panel-update
@@ -1520,10 +1561,11 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
           count_launch(); } prof_end(ps_, st, KS_F_POTRF, potrf_flops(na, k0)); }
         int rows_max = lv.maxm(na) - k0 - 1;
         if (rows_max <= 0) continue;
-        unsigned gx = (unsigned)((rows_max + 63) / 64);
-        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_trsm_panel<T><<<dim3(gx, na), 256, 2 * NB * (NB + 1) * sizeof(T), st>>>(list, F->first, F->mrows,
+        const auto& tsp = lv.trsm[k0 / NB];
+        if (tsp.cnt > 0) { int ps_ = fine_prof() ? prof_start(st) : -1; { k_trsm_panel<T><<<(unsigned)tsp.cnt, 256, 2 * NB * (NB + 1) * sizeof(T), st>>>(list, F->first, F->mrows,
                                                                                         F->Lptr, F->Dptr, Lf, Dvf, k0,
-                                                                                        tc ? F->Phi : nullptr, F->Plo, F->PKptr);
+                                                                                        tc ? F->Phi : nullptr, F->Plo, F->PKptr,
+                                                                                        F->tiles + tsp.off);
           count_launch(); } prof_end(ps_, st, KS_F_TRSM, trsm_flops(na, k0)); }
         const int nu = lv.active(k0 + NB);   // fronts with columns after this block
         int nrow = lv.maxm(nu) - k0 - NB, ncol = std::min(P1, lv.max_c) - k0 - NB;
@@ -1551,12 +1593,13 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
       prof_end(ps, st, KS_SCHUR, lv.schur_flops);
     }
     // extend-add, pass 1: children columns that land in the U of this level
-    for (const auto& seg : lv.ea) {
-      if (seg.second == 0) continue;
-      unsigned gx = (unsigned)((lv.ea_max_r + 7) / 8);
-      if (gx == 0) continue;
-      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_extend_add<T><<<dim3(gx, seg.second), 256, 0, st>>>(F->ea_child + seg.first, F->first, F->mrows,
-                                                            F->parent, F->Lptr, F->Uptr, F->relptr, F->rel, Lf, Uf, 1);
+    for (size_t si = 0; si < lv.ea.size(); ++si) {
+      const auto& seg = lv.ea[si];
+      const auto& tsp = lv.ea_f[si];
+      if (seg.second == 0 || tsp.cnt == 0) continue;
+      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_extend_add<T><<<(unsigned)tsp.cnt, 256, 0, st>>>(F->ea_child + seg.first, F->first, F->mrows,
+                                                            F->parent, F->Lptr, F->Uptr, F->relptr, F->rel, Lf, Uf, 1,
+                                                            F->tiles + tsp.off);
         count_launch(); } prof_end(ps_, st, KS_F_EA, 0.0); }
     }
     JFG_CUDA(cudaGetLastError());
@@ -1596,26 +1639,28 @@ void solve_inner_n(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int
     const int32_t* list = F->level_sn + lv.off;
     const int pl = (fine_prof() && li < (size_t)KS_MAX_LEVELS) ? prof_start(st) : -1;
     { int ps_ = fine_prof() ? prof_start(st) : -1; { k_zero_V<<<lv.count, 256, 0, st>>>(list, F->first, F->mrows, F->relptr, nr, F->V); count_launch(); } prof_end(ps_, st, KS_S_VEC, 0.0); }
-    for (const auto& seg : lv.ea)
-      if (seg.second > 0)
-        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_vec_extend_add<NRC><<<dim3(seg.second, std::max(1, (lv.ea_max_r + 255) / 256)), 256, 0, st>>>(F->ea_child + seg.first, F->first, F->mrows, F->parent,
-                                                     F->relptr, F->rel, nr, n, F->xp, F->V); count_launch(); } prof_end(ps_, st, KS_S_VEC, 0.0); }
+    for (size_t si = 0; si < lv.ea.size(); ++si) {
+      const auto& seg = lv.ea[si];
+      const auto& tsp = lv.ea_s[si];
+      if (seg.second > 0 && tsp.cnt > 0)
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_vec_extend_add<NRC><<<(unsigned)tsp.cnt, 256, 0, st>>>(F->ea_child + seg.first, F->first, F->mrows, F->parent,
+                                                     F->relptr, F->rel, nr, n, F->xp, F->V, F->tiles + tsp.off); count_launch(); } prof_end(ps_, st, KS_S_VEC, 0.0); }
+    }
     int nstrip = (lv.max_c + SW - 1) / SW;
     for (int kb = 0; kb < nstrip; ++kb) {
-      const int na = lv.active(kb * SW);   // fronts that have strip kb: a prefix of the list
-      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_fwd_sdiag<T, NRC><<<dim3(SW / 32, na), 256, fwd_sdiag_smem<NRC>(), st>>>(list, F->first, F->Sptr, Sv, kb, nr, n, F->xp, F->tt);
+      const auto& ts = lv.strips[kb];
+      if (ts.diag.cnt > 0) { int ps_ = fine_prof() ? prof_start(st) : -1; { k_fwd_sdiag<T, NRC><<<(unsigned)ts.diag.cnt, 256, fwd_sdiag_smem<NRC>(), st>>>(list, F->first, F->Sptr, Sv, kb, nr, n, F->xp, F->tt, F->tiles + ts.diag.off);
         count_launch(); } prof_end(ps_, st, KS_S_FDIAG, 0.0); }
-      int rows = lv.maxm(na) - kb * SW;
-      if (rows > 0) {
+      const auto& tu = NRC == 8 ? ts.upd32 : ts.upd128;
+      if (tu.cnt > 0) {
         int ps_ = fine_prof() ? prof_start(st) : -1;
         if constexpr (NRC == 8) {
-          unsigned gx = (unsigned)((rows + 31) / 32);
-          k_fwd_supdate<T><<<dim3(gx, na), 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->relptr, Lf, kb,
-                                                          nr, n, F->tt, F->xp, F->V);
+          k_fwd_supdate<T><<<(unsigned)tu.cnt, 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->relptr, Lf, kb,
+                                                              nr, n, F->tt, F->xp, F->V, F->tiles + tu.off);
         } else {
-          unsigned gx = (unsigned)((rows + 127) / 128);
-          k_fwd_supdate_wide<T, NRC><<<dim3(gx, na), 128, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->relptr, Lf,
-                                                                    kb, nr, n, F->tt, F->xp, F->V);
+          k_fwd_supdate_wide<T, NRC><<<(unsigned)tu.cnt, 128, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->relptr, Lf,
+                                                                        kb, nr, n, F->tt, F->xp, F->V,
+                                                                        F->tiles + tu.off);
         }
         count_launch();
         prof_end(ps_, st, KS_S_FUPD, 0.0);
@@ -1631,15 +1676,13 @@ void solve_inner_n(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int
     const int pl = (fine_prof() && li < (size_t)KS_MAX_LEVELS) ? prof_start(st) : -1;
     int nstrip = (lv.max_c + SW - 1) / SW;
     for (int kb = nstrip - 1; kb >= 0; --kb) {
-      const int na = lv.active(kb * SW);
-      int rows = lv.maxm(na) - kb * SW;
-      if (rows > 0) {
-        unsigned gx = (unsigned)(((rows + 255) / 256) * (SW / 32));
-        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_bwd_spartial<T, NRC><<<dim3(gx, na), 256, bwd_spartial_smem<NRC>(), st>>>(list, F->first, F->mrows, F->Lptr, F->rows_ptr, F->rows,
-                                                               poff, Lf, kb, nr, n, F->xp, F->part); count_launch(); } prof_end(ps_, st, KS_S_BPART, 0.0); }
+      const auto& ts = lv.strips[kb];
+      if (ts.bwd.cnt > 0) {
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { k_bwd_spartial<T, NRC><<<(unsigned)ts.bwd.cnt, 256, bwd_spartial_smem<NRC>(), st>>>(list, F->first, F->mrows, F->Lptr, F->rows_ptr, F->rows,
+                                                               poff, Lf, kb, nr, n, F->xp, F->part, F->tiles + ts.bwd.off); count_launch(); } prof_end(ps_, st, KS_S_BPART, 0.0); }
       }
-      { int ps_ = fine_prof() ? prof_start(st) : -1; { k_bwd_sdiag<T, NRC><<<dim3(SW / 32, na), 256, bwd_sdiag_smem<NRC>(), st>>>(list, F->first, F->mrows, F->Sptr, poff, Sv, kb, nr, n,
-                                                 F->part, F->tt, F->xp); count_launch(); } prof_end(ps_, st, KS_S_BDIAG, 0.0); }
+      if (ts.diag.cnt > 0) { int ps_ = fine_prof() ? prof_start(st) : -1; { k_bwd_sdiag<T, NRC><<<(unsigned)ts.diag.cnt, 256, bwd_sdiag_smem<NRC>(), st>>>(list, F->first, F->mrows, F->Sptr, poff, Sv, kb, nr, n,
+                                                 F->part, F->tt, F->xp, F->tiles + ts.diag.off); count_launch(); } prof_end(ps_, st, KS_S_BDIAG, 0.0); }
     }
     prof_end(pl, st, KS_LEVEL_BWD + (int)li, (double)sizeof(T) * (double)lv.nnz);
   }
@@ -1828,6 +1871,76 @@ jfg_status numeric_create(jfg_model* m) {
       }
     }
   }
+  // work tiles of every level launch (only blocks with work)
+  {
+    std::vector<int2> tl;
+    using Span = NumericFactor::Level::Span;
+    auto span = [&](auto&& gen) {
+      Span sp;
+      sp.off = (int64_t)tl.size();
+      gen();
+      sp.cnt = (int32_t)((int64_t)tl.size() - sp.off);
+      return sp;
+    };
+    for (int64_t l = 0; l < S.n_levels; ++l) {
+      auto& lv = F->levels[l];
+      const int cnt = lv.count;
+      auto mq = [&](int q) { return (int64_t)S.sn_m[S.level_sn[lv.off + q]]; };
+      // extend-add segments: children of one rank
+      for (const auto& seg : lv.ea) {
+        auto rc_of = [&](int q) {
+          const int32_t ch = S.ea_child[seg.first + q];
+          return (int64_t)S.sn_m[ch] - (S.sn_first[ch + 1] - S.sn_first[ch]);
+        };
+        lv.ea_f.push_back(span([&] {
+          for (int q = 0; q < seg.second; ++q)
+            for (int64_t b = 0; b * 8 < rc_of(q); ++b) tl.push_back(make_int2(q, (int)b));
+        }));
+        lv.ea_s.push_back(span([&] {
+          for (int q = 0; q < seg.second; ++q)
+            for (int64_t b = 0; b * 256 < rc_of(q); ++b) tl.push_back(make_int2(q, (int)b));
+        }));
+      }
+      // panel trsm of every 64-column step
+      for (int k0 = 0; k0 < lv.max_c; k0 += NB) {
+        lv.trsm.push_back(span([&] {
+          for (int q = 0; q < cnt && lv.cs[q] > k0; ++q) {
+            const int64_t rows = mq(q) - std::min(k0 + NB, lv.cs[q]);
+            for (int64_t b = 0; b * 64 < rows; ++b) tl.push_back(make_int2(q, (int)b));
+          }
+        }));
+      }
+      // solve strips
+      for (int kb = 0; kb * SW < lv.max_c; ++kb) {
+        NumericFactor::Level::StripSpans ss;
+        auto kw_of = [&](int q) { return (int64_t)std::min(SW, lv.cs[q] - kb * SW); };
+        auto rows_of = [&](int q) { return mq(q) - kb * SW - kw_of(q); };
+        ss.diag = span([&] {
+          for (int q = 0; q < cnt && lv.cs[q] > kb * SW; ++q)
+            for (int64_t g = 0; g * 32 < kw_of(q); ++g) tl.push_back(make_int2(q, (int)g));
+        });
+        ss.upd32 = span([&] {
+          for (int q = 0; q < cnt && lv.cs[q] > kb * SW; ++q)
+            for (int64_t b = 0; b * 32 < rows_of(q); ++b) tl.push_back(make_int2(q, (int)b));
+        });
+        ss.upd128 = span([&] {
+          for (int q = 0; q < cnt && lv.cs[q] > kb * SW; ++q)
+            for (int64_t b = 0; b * 128 < rows_of(q); ++b) tl.push_back(make_int2(q, (int)b));
+        });
+        ss.bwd = span([&] {
+          for (int q = 0; q < cnt && lv.cs[q] > kb * SW; ++q) {
+            const int64_t nrb = (rows_of(q) + 255) / 256, ncg = (kw_of(q) + 31) / 32;
+            for (int64_t rb = 0; rb < nrb; ++rb)
+              for (int64_t cg = 0; cg < ncg; ++cg) tl.push_back(make_int2(q, (int)(rb * (SW / 32) + cg)));
+          }
+        });
+        lv.strips.push_back(ss);
+      }
+    }
+    F->n_tiles = (int64_t)tl.size();
+    upload(tl, &F->tiles, c, st);
+    if (st != JFG_OK) return st;
+  }
   // strip metadata: 64-block inverse offsets, 256-strip inverse offsets with
   // their work items (front, strip, block column), per-level partial offsets
   {
@@ -1912,6 +2025,7 @@ void numeric_destroy(jfg_model* m) {
   }
   fr(F->free_mask, m->ndof);
   fr(F->Dptr, 8 * S.ns); fr(F->Sptr, 8 * S.ns); fr(F->part_off, 8 * S.ns);
+  fr(F->tiles, sizeof(int2) * std::max<int64_t>(F->n_tiles, 1));
   int64_t ni = std::max<int64_t>(F->n_inv_items, 1);
   fr(F->inv_sn, 4 * ni); fr(F->inv_kb, 4 * ni); fr(F->inv_jb, 4 * ni);
   fr(F->Dinv64, 8 * F->dinv_len); fr(F->Dinv32, 4 * F->dinv_len); fr(F->part, 8 * F->part_len);
@@ -2059,7 +2173,7 @@ void numeric_bytes(jfg_model* m, int precision, int nrhs, int64_t* now, int64_t*
   base += 12 * std::max<int64_t>(items, 1);
   const int64_t ublk = std::max<int64_t>(S.u_arena, 1);
   int64_t part = F ? F->part_len : 0;
-  base += 8 * part;
+  base += 8 * part + 8 * std::max<int64_t>(F ? F->n_tiles : 0, 1);
   auto fp64 = [&]() { return 8 * S.nnz_L + 8 * ublk + 8 * std::max<int64_t>(dl, 1) + 8 * std::max<int64_t>(sl, 1); };
   auto mixed = [&]() {
     int64_t pk = 0;
