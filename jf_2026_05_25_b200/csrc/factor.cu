@@ -63,6 +63,12 @@ struct NumericFactor {
     std::vector<Span> trsm;           // panel trsm, per 64-column step
     struct StripSpans { Span diag, upd32, upd128, bwd; };
     std::vector<StripSpans> strips;   // solve sweeps, per 256-column strip
+    // front updates: lower output tiles of 64 (SIMT / DMMA) and of 128
+    // (tensor cores), as (position, ti * ntj + tj) of each front's grid
+    struct UpdSpans { Span t64, t128; };
+    std::vector<UpdSpans> upd_step;    // inside the super-panel, per 64-column step
+    std::vector<UpdSpans> upd_trail;   // after the super-panel, per super-panel
+    UpdSpans schur;                    // U = -L21 L21^T
   };
   std::vector<Level> levels;
   int2* tiles = nullptr;      // every level launch's work tiles (see tile_of)
@@ -183,21 +189,6 @@ inline int panel_width() {
   return v;
 }
 
-// Work tiles of a level launch: with a tile list, CTA x takes tile tiles[x]
-// = (position of the front in the level's list, block of that front); the
-// list holds only blocks that have work, so a level of fronts of very
-// different sizes launches no empty CTAs.  Without one the grid is
-// (blocks, fronts).
-__device__ __forceinline__ void tile_of(const int2* __restrict__ tiles, int& q, int& b) {
-  if (tiles) {
-    const int2 t = tiles[blockIdx.x];
-    q = t.x;
-    b = t.y;
-  } else {
-    q = blockIdx.y;
-    b = blockIdx.x;
-  }
-}
 
 __device__ inline void rec_err(DevError* e, int32_t code, int64_t idx) {
   if (atomicCAS(&e->code, 0, code) == 0) e->index = idx;
@@ -640,8 +631,10 @@ __global__ void __launch_bounds__(256)
 k_front_update(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
                const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
                const int64_t* __restrict__ Uptr, T* __restrict__ L, T* __restrict__ U, int mode, int kbeg,
-               int kend, int cend) {
-  int s = list[blockIdx.y];
+               int kend, int cend, const int2* __restrict__ tiles) {
+  int tq, tb;
+  tile_of(tiles, tq, tb);
+  int s = list[tq];
   int c = first[s + 1] - first[s];
   int m = mrows[s];
   const T* P = L + Lptr[s];
@@ -664,7 +657,7 @@ k_front_update(const int32_t* __restrict__ list, const int32_t* __restrict__ fir
     ldc = r;
   }
   int ntj = (ncol + TILE - 1) / TILE, nti = (nrow + TILE - 1) / TILE;
-  int t = blockIdx.x;
+  int t = tb;
   if (t >= nti * ntj) return;
   int ti = t / ntj, tj = t % ntj;
   if (ti * TILE + TILE - 1 + row0 < tj * TILE + col0) return;   // strictly upper tile
@@ -750,8 +743,10 @@ __global__ void __launch_bounds__(128)
 k_front_update_dmma(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
                     const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
                     const int64_t* __restrict__ Uptr, double* __restrict__ L, double* __restrict__ U, int mode,
-                    int kbeg, int kend, int cend) {
-  int s = list[blockIdx.y];
+                    int kbeg, int kend, int cend, const int2* __restrict__ tiles) {
+  int tq, tb;
+  tile_of(tiles, tq, tb);
+  int s = list[tq];
   int c = first[s + 1] - first[s];
   int m = mrows[s];
   const double* P = L + Lptr[s];
@@ -773,7 +768,7 @@ k_front_update_dmma(const int32_t* __restrict__ list, const int32_t* __restrict_
     ldc = r;
   }
   int ntj = (ncol + TILE - 1) / TILE, nti = (nrow + TILE - 1) / TILE;
-  int t = blockIdx.x;
+  int t = tb;
   if (t >= nti * ntj) return;
   int ti = t / ntj, tj = t % ntj;
   if (ti * TILE + TILE - 1 + row0 < tj * TILE + col0) return;   // strictly upper tile
@@ -880,18 +875,18 @@ inline bool dmma_enabled() {
 // one launch of the front update for a level: DMMA for the FP64 factor,
 // SIMT tiles otherwise (and for the FP64 factor with JFG_DMMA=0)
 template <typename T>
-void launch_front_update(unsigned tiles, int count, NumericFactor* F, T* Lf, T* Uf, int mode, int kbeg, int kend,
-                         int cend, cudaStream_t st) {
+void launch_front_update(const int2* tiles, int n_tiles, NumericFactor* F, T* Lf, T* Uf, int mode, int kbeg,
+                         int kend, int cend, cudaStream_t st) {
   if constexpr (sizeof(T) == 8) {
     if (dmma_enabled()) {
-      k_front_update_dmma<<<dim3(tiles, count), 128, 0, st>>>(F->level_sn_cur, F->first, F->mrows, F->Lptr, F->Uptr,
-                                                              Lf, Uf, mode, kbeg, kend, cend);
+      k_front_update_dmma<<<(unsigned)n_tiles, 128, 0, st>>>(F->level_sn_cur, F->first, F->mrows, F->Lptr, F->Uptr,
+                                                             Lf, Uf, mode, kbeg, kend, cend, tiles);
       count_launch();
       return;
     }
   }
-  k_front_update<T><<<dim3(tiles, count), 256, 0, st>>>(F->level_sn_cur, F->first, F->mrows, F->Lptr, F->Uptr, Lf, Uf,
-                                                        mode, kbeg, kend, cend);
+  k_front_update<T><<<(unsigned)n_tiles, 256, 0, st>>>(F->level_sn_cur, F->first, F->mrows, F->Lptr, F->Uptr, Lf, Uf,
+                                                       mode, kbeg, kend, cend, tiles);
   count_launch();
 }
 
@@ -1491,15 +1486,17 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
     // one front update of the level: the tensor-core 3xTF32 kernel for the
     // FP32 factor when its low parts exist and the level's output is large
     // enough for 128 x 128 tiles, else the SIMT / DMMA tiles
-    auto update = [&](int mode, int kbeg, int kend, int cend, int max_rows, int max_cols, int64_t tiles, int cnt) {
+    using UpdSpans = NumericFactor::Level::UpdSpans;
+    auto update = [&](int mode, int kbeg, int kend, int cend, int max_rows, int max_cols, const UpdSpans& u) {
       if constexpr (sizeof(T) == 4) {
         if (tc && max_rows >= tc_min && max_cols >= tc_min / 2 &&
-            tc::front_update_tf32x3(list, cnt, F->first, F->mrows, F->Lptr, F->Uptr, Lf, F->Phi, F->Plo,
-                                    F->PKptr, F->tc_zero, Uf, mode, kbeg, kend, cend, max_rows, max_cols,
+            tc::front_update_tf32x3(list, F->tiles + u.t128.off, u.t128.cnt, F->first, F->mrows, F->Lptr, F->Uptr,
+                                    Lf, F->Phi, F->Plo, F->PKptr, F->tc_zero, Uf, mode, kbeg, kend, cend,
                                     F->tc_drain, F->err, st))
           return;
       }
-      launch_front_update<T>((unsigned)tiles, cnt, F, Lf, Uf, mode, kbeg, kend, cend, st);
+      if (u.t64.cnt > 0)
+        launch_front_update<T>(F->tiles + u.t64.off, u.t64.cnt, F, Lf, Uf, mode, kbeg, kend, cend, st);
     };
     // extend-add, pass 0: children columns that land in this level's panels
     for (size_t si = 0; si < lv.ea.size(); ++si) {
@@ -1570,26 +1567,22 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
         const int nu = lv.active(k0 + NB);   // fronts with columns after this block
         int nrow = lv.maxm(nu) - k0 - NB, ncol = std::min(P1, lv.max_c) - k0 - NB;
         if (nu > 0 && nrow > 0 && ncol > 0) {
-          int64_t tiles = (int64_t)((nrow + TILE - 1) / TILE) * ((ncol + TILE - 1) / TILE);
           { int ps_ = fine_prof() ? prof_start(st) : -1;
-            update(0, k0, k0 + NB, P1, nrow, ncol, tiles, nu);
+            update(0, k0, k0 + NB, P1, nrow, ncol, lv.upd_step[k0 / NB]);
             prof_end(ps_, st, KS_F_PANEL, update_flops(nu, k0, k0 + NB, k0 + NB, P1)); }
         }
       }
       const int nt = lv.active(P1);   // fronts with columns after the super-panel
       int nrow = lv.maxm(nt) - P1, ncol = lv.max_c - P1;
       if (nt > 0 && nrow > 0 && ncol > 0) {
-        int64_t tiles = (int64_t)((nrow + TILE - 1) / TILE) * ((ncol + TILE - 1) / TILE);
         { int ps_ = fine_prof() ? prof_start(st) : -1;
-          update(0, P0, P1, INT_MAX, nrow, ncol, tiles, nt);
+          update(0, P0, P1, INT_MAX, nrow, ncol, lv.upd_trail[P0 / PW]);
           prof_end(ps_, st, KS_F_PANEL, update_flops(nt, P0, P1, P1, INT_MAX)); }
       }
     }
     if (lv.max_r > 0) {
-      int64_t nt = (lv.max_r + TILE - 1) / TILE;
-      int64_t tiles = nt * nt;
       int ps = prof_start(st);
-      update(1, 0, 0, 0, lv.max_r, lv.max_r, tiles, lv.count);
+      update(1, 0, 0, 0, lv.max_r, lv.max_r, lv.schur);
       prof_end(ps, st, KS_SCHUR, lv.schur_flops);
     }
     // extend-add, pass 1: children columns that land in the U of this level
@@ -1779,65 +1772,25 @@ jfg_status coldot(NumericFactor* F, int64_t len, int nr, const double* a, const 
 
 }  // namespace
 
-jfg_status numeric_create(jfg_model* m) {
-  numeric_destroy(m);
-  JFG_TRY(solve_attributes());
-  NumericFactor* F = new NumericFactor();
-  m->num = F;
-  Symbolic& S = m->sym;
-  jfg_ctx* c = m->ctx;
-  jfg_status st = JFG_OK;
-  upload(S.sn_first, &F->first, c, st);
-  upload(S.sn_m, &F->mrows, c, st);
-  // fronts of a level by decreasing width (then by index), so that the
-  // fronts still active at a column step are a prefix of the level's list
-  // and each step launches only them
-  for (int64_t l = 0; l < S.n_levels; ++l) {
-    auto b = S.level_sn.begin() + S.level_ptr[l], e = S.level_sn.begin() + S.level_ptr[l + 1];
-    std::sort(b, e, [&](int32_t x, int32_t y) {
+// Fronts of a level by decreasing width (then by index), so that the fronts
+// still active at a column step are a prefix of the level's list and each
+// step launches only them.
+static void sort_levels(const Symbolic& S, std::vector<int32_t>& level_sn) {
+  for (int64_t l = 0; l < S.n_levels; ++l)
+    std::sort(level_sn.begin() + S.level_ptr[l], level_sn.begin() + S.level_ptr[l + 1], [&](int32_t x, int32_t y) {
       const int32_t cx = S.sn_first[x + 1] - S.sn_first[x], cy = S.sn_first[y + 1] - S.sn_first[y];
       return cx != cy ? cx > cy : x < y;
     });
-  }
-  upload(S.level_sn, &F->level_sn, c, st);
-  upload(S.ea_child, &F->ea_child, c, st);
-  upload(S.rel, &F->rel, c, st);
-  upload(S.rows, &F->rows, c, st);
-  upload(S.sn_parent, &F->parent, c, st);
-  upload(S.perm_dof, &F->perm_dof, c, st);
-  upload(S.amap_src, &F->amap_src, c, st);
-  upload(S.sn_Lptr, &F->Lptr, c, st);
-  upload(S.sn_Uptr, &F->Uptr, c, st);
-  upload(S.sn_rows_ptr, &F->rows_ptr, c, st);
-  upload(S.sn_relptr, &F->relptr, c, st);
-  upload(S.amap_dst, &F->amap_dst, c, st);
-  // permuted (row, col) of every scattered entry, for the mixed scaling
-  {
-    std::vector<int32_t> pr(S.amap_dst.size()), pc(S.amap_dst.size());
-    std::vector<int32_t> col_of(S.n);
-    for (int64_t s = 0; s < S.ns; ++s)
-      for (int64_t k = S.sn_first[s]; k < S.sn_first[s + 1]; ++k) col_of[k] = (int32_t)s;
-    // decode dst -> (front row, front col) through the supernode that owns it
-    std::vector<int64_t> Lp = S.sn_Lptr;
-    for (size_t q = 0; q < S.amap_dst.size(); ++q) {
-      int64_t d = S.amap_dst[q];
-      int64_t s = std::upper_bound(Lp.begin(), Lp.end(), d) - Lp.begin() - 1;
-      int64_t mm = S.sn_m[s];
-      int64_t off = d - Lp[s];
-      int64_t ri = off % mm, cj = off / mm;
-      pr[q] = S.rows[S.sn_rows_ptr[s] + ri];
-      pc[q] = S.sn_first[s] + (int32_t)cj;
-    }
-    upload(pr, &F->amap_pr, c, st);
-    upload(pc, &F->amap_pc, c, st);
-  }
-  if (st != JFG_OK) return st;
-  F->n_amap = (int64_t)S.amap_dst.size();
-  F->v_total = S.sn_relptr[S.ns];
-  // levels
-  F->levels.resize(S.n_levels);
+}
+
+// Host launch metadata of every level and the tile lists of its launches
+// (only blocks with work).  level_sn holds the level lists, each sorted by
+// decreasing width.
+static void build_levels(const Symbolic& S, const std::vector<int32_t>& level_sn,
+                         std::vector<NumericFactor::Level>& levels, std::vector<int2>& tl) {
+  levels.assign(S.n_levels, NumericFactor::Level());
   for (int64_t l = 0; l < S.n_levels; ++l) {
-    auto& lv = F->levels[l];
+    auto& lv = levels[l];
     lv.off = S.level_ptr[l];
     lv.count = S.level_ptr[l + 1] - S.level_ptr[l];
     lv.max_c = lv.max_m = lv.max_r = 0;
@@ -1845,7 +1798,7 @@ jfg_status numeric_create(jfg_model* m) {
     lv.pm.clear();
     lv.nnz = 0;
     for (int32_t q = lv.off; q < lv.off + lv.count; ++q) {
-      int32_t s = S.level_sn[q];
+      int32_t s = level_sn[q];
       int32_t cc = S.sn_first[s + 1] - S.sn_first[s];
       lv.max_c = std::max(lv.max_c, cc);
       lv.max_m = std::max(lv.max_m, S.sn_m[s]);
@@ -1856,7 +1809,7 @@ jfg_status numeric_create(jfg_model* m) {
     }
     lv.schur_flops = 0;
     for (int32_t q = lv.off; q < lv.off + lv.count; ++q) {
-      int32_t s = S.level_sn[q];
+      int32_t s = level_sn[q];
       double cc = S.sn_first[s + 1] - S.sn_first[s];
       double rr = S.sn_parent[s] >= 0 ? S.sn_m[s] - cc : 0.0;
       lv.schur_flops += rr * (rr + 1) * cc;
@@ -1873,7 +1826,6 @@ jfg_status numeric_create(jfg_model* m) {
   }
   // work tiles of every level launch (only blocks with work)
   {
-    std::vector<int2> tl;
     using Span = NumericFactor::Level::Span;
     auto span = [&](auto&& gen) {
       Span sp;
@@ -1883,9 +1835,9 @@ jfg_status numeric_create(jfg_model* m) {
       return sp;
     };
     for (int64_t l = 0; l < S.n_levels; ++l) {
-      auto& lv = F->levels[l];
+      auto& lv = levels[l];
       const int cnt = lv.count;
-      auto mq = [&](int q) { return (int64_t)S.sn_m[S.level_sn[lv.off + q]]; };
+      auto mq = [&](int q) { return (int64_t)S.sn_m[level_sn[lv.off + q]]; };
       // extend-add segments: children of one rank
       for (const auto& seg : lv.ea) {
         auto rc_of = [&](int q) {
@@ -1936,7 +1888,96 @@ jfg_status numeric_create(jfg_model* m) {
         });
         lv.strips.push_back(ss);
       }
+      // front updates, with the kernels' own geometry: mode 0 writes columns
+      // [k1, min(cend, c)) and rows [k1, m) (k1 = min(kend, c)), mode 1 the
+      // r x r update matrix; the 128-tile grid starts at the output origin
+      // rounded down to a multiple of 8 rows
+      auto upd = [&](int mode, int kbeg, int kend, int cend) {
+        auto gen = [&](int tile, bool align8) {
+          for (int q = 0; q < cnt; ++q) {
+            const int32_t s = level_sn[lv.off + q];
+            const int c = S.sn_first[s + 1] - S.sn_first[s], m = S.sn_m[s];
+            int row0, nrow, ncol;
+            if (mode == 0) {
+              const int k1 = std::min(kend, c), ce = std::min(cend, c);
+              if (kbeg >= c || k1 >= ce) continue;
+              row0 = k1; nrow = m - k1; ncol = ce - k1;
+            } else {
+              if (m - c <= 0 || S.sn_Uptr[s] < 0) continue;
+              row0 = c; nrow = ncol = m - c;
+            }
+            if (align8) { nrow += row0 & 7; ncol += row0 & 7; }
+            const int ntj = (ncol + tile - 1) / tile, nti = (nrow + tile - 1) / tile;
+            for (int ti = 0; ti < nti; ++ti)
+              for (int tj = 0; tj <= ti && tj < ntj; ++tj) tl.push_back(make_int2(q, ti * ntj + tj));
+          }
+        };
+        NumericFactor::Level::UpdSpans u;
+        u.t64 = span([&] { gen(TILE, false); });
+        u.t128 = span([&] { gen(tc::TILE_M, true); });
+        return u;
+      };
+      const int PW = panel_width();
+      for (int k0 = 0; k0 < lv.max_c; k0 += NB) {
+        const int P1 = (k0 / PW) * PW + PW;
+        lv.upd_step.push_back(upd(0, k0, k0 + NB, P1));
+      }
+      for (int P0 = 0; P0 < lv.max_c; P0 += PW) lv.upd_trail.push_back(upd(0, P0, P0 + PW, INT_MAX));
+      lv.schur = upd(1, 0, 0, 0);
     }
+  }
+}
+
+jfg_status numeric_create(jfg_model* m) {
+  numeric_destroy(m);
+  JFG_TRY(solve_attributes());
+  NumericFactor* F = new NumericFactor();
+  m->num = F;
+  Symbolic& S = m->sym;
+  jfg_ctx* c = m->ctx;
+  jfg_status st = JFG_OK;
+  upload(S.sn_first, &F->first, c, st);
+  upload(S.sn_m, &F->mrows, c, st);
+  sort_levels(S, S.level_sn);
+  upload(S.level_sn, &F->level_sn, c, st);
+  upload(S.ea_child, &F->ea_child, c, st);
+  upload(S.rel, &F->rel, c, st);
+  upload(S.rows, &F->rows, c, st);
+  upload(S.sn_parent, &F->parent, c, st);
+  upload(S.perm_dof, &F->perm_dof, c, st);
+  upload(S.amap_src, &F->amap_src, c, st);
+  upload(S.sn_Lptr, &F->Lptr, c, st);
+  upload(S.sn_Uptr, &F->Uptr, c, st);
+  upload(S.sn_rows_ptr, &F->rows_ptr, c, st);
+  upload(S.sn_relptr, &F->relptr, c, st);
+  upload(S.amap_dst, &F->amap_dst, c, st);
+  // permuted (row, col) of every scattered entry, for the mixed scaling
+  {
+    std::vector<int32_t> pr(S.amap_dst.size()), pc(S.amap_dst.size());
+    std::vector<int32_t> col_of(S.n);
+    for (int64_t s = 0; s < S.ns; ++s)
+      for (int64_t k = S.sn_first[s]; k < S.sn_first[s + 1]; ++k) col_of[k] = (int32_t)s;
+    // decode dst -> (front row, front col) through the supernode that owns it
+    std::vector<int64_t> Lp = S.sn_Lptr;
+    for (size_t q = 0; q < S.amap_dst.size(); ++q) {
+      int64_t d = S.amap_dst[q];
+      int64_t s = std::upper_bound(Lp.begin(), Lp.end(), d) - Lp.begin() - 1;
+      int64_t mm = S.sn_m[s];
+      int64_t off = d - Lp[s];
+      int64_t ri = off % mm, cj = off / mm;
+      pr[q] = S.rows[S.sn_rows_ptr[s] + ri];
+      pc[q] = S.sn_first[s] + (int32_t)cj;
+    }
+    upload(pr, &F->amap_pr, c, st);
+    upload(pc, &F->amap_pc, c, st);
+  }
+  if (st != JFG_OK) return st;
+  F->n_amap = (int64_t)S.amap_dst.size();
+  F->v_total = S.sn_relptr[S.ns];
+  // levels and the tile lists of their launches
+  {
+    std::vector<int2> tl;
+    build_levels(S, S.level_sn, F->levels, tl);
     F->n_tiles = (int64_t)tl.size();
     upload(tl, &F->tiles, c, st);
     if (st != JFG_OK) return st;
@@ -2173,7 +2214,16 @@ void numeric_bytes(jfg_model* m, int precision, int nrhs, int64_t* now, int64_t*
   base += 12 * std::max<int64_t>(items, 1);
   const int64_t ublk = std::max<int64_t>(S.u_arena, 1);
   int64_t part = F ? F->part_len : 0;
-  base += 8 * part + 8 * std::max<int64_t>(F ? F->n_tiles : 0, 1);
+  int64_t n_tiles = F ? F->n_tiles : 0;
+  if (!F && S.ns > 0) {   // the tile lists numeric_create will build
+    std::vector<int32_t> lsn = S.level_sn;
+    sort_levels(S, lsn);
+    std::vector<NumericFactor::Level> lv;
+    std::vector<int2> tl;
+    build_levels(S, lsn, lv, tl);
+    n_tiles = (int64_t)tl.size();
+  }
+  base += 8 * part + 8 * std::max<int64_t>(n_tiles, 1);
   auto fp64 = [&]() { return 8 * S.nnz_L + 8 * ublk + 8 * std::max<int64_t>(dl, 1) + 8 * std::max<int64_t>(sl, 1); };
   auto mixed = [&]() {
     int64_t pk = 0;

@@ -60,6 +60,24 @@ struct DevMem {
   size_t bytes = 0;
 };
 
+#ifdef __CUDACC__
+// Work tiles of a level launch: with a tile list, CTA x takes tile tiles[x]
+// = (position of the front in the level's list, block of that front); the
+// list holds only blocks that have work, so a level of fronts of very
+// different sizes launches no empty CTAs.  Without one the grid is
+// (blocks, fronts).
+__device__ __forceinline__ void tile_of(const int2* __restrict__ tiles, int& q, int& b) {
+  if (tiles) {
+    const int2 t = tiles[blockIdx.x];
+    q = t.x;
+    b = t.y;
+  } else {
+    q = blockIdx.y;
+    b = blockIdx.x;
+  }
+}
+#endif
+
 // Error record written by device kernels (first failing element / pivot).
 // doubles per CQUAD4 of the scratch record passed from the thread-per-element
 // pass to the warp-per-element pass of the element kernel

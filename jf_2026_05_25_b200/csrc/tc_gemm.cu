@@ -78,7 +78,7 @@ __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::aft
 // Every wait is bounded (about two seconds of clock) and also gives up as
 // soon as another warp has given up; the CTA then records EE_TC_TIMEOUT,
 // waits (bounded) for its own copies and MMAs and frees its tensor memory.
-constexpr int UM = 128;
+constexpr int UM = TILE_M;
 constexpr int UK = 16;
 #ifndef JFG_TC_STAGES
 #define JFG_TC_STAGES 4
@@ -152,9 +152,12 @@ k_update_tf32x3(const int32_t* __restrict__ list, const int32_t* __restrict__ fi
                 const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
                 const int64_t* __restrict__ Uptr, float* __restrict__ L, const float* __restrict__ Phi,
                 const float* __restrict__ Plo, const int64_t* __restrict__ PKptr, const float* __restrict__ zero,
-                float* __restrict__ U, int mode, int kbeg, int kend, int cend, int terms, int udr, DevError* err) {
+                float* __restrict__ U, int mode, int kbeg, int kend, int cend, int terms, int udr, DevError* err,
+                const int2* __restrict__ tiles) {
   const int UDR = udr;   // K-slices of 16 summed by the tensor core per accumulator use
-  const int s = list[blockIdx.y];
+  int tq, tb;
+  tile_of(tiles, tq, tb);
+  const int s = list[tq];
   const int c = first[s + 1] - first[s];
   const int m = mrows[s];
   int row0, col0, nrow, ncol, kb, ke;
@@ -178,7 +181,7 @@ k_update_tf32x3(const int32_t* __restrict__ list, const int32_t* __restrict__ fi
   const int sh = row0 & 7;
   const int row0e = row0 - sh, col0e = col0 - sh, nrowe = nrow + sh, ncole = ncol + sh;
   const int ntj = (ncole + UM - 1) / UM, nti = (nrowe + UM - 1) / UM;
-  const int t = blockIdx.x;
+  const int t = tb;
   if (t >= nti * ntj) return;
   const int ti = t / ntj, tj = t % ntj;
   if (ti * UM + UM - 1 + row0e < tj * UM + col0e) return;   // strictly upper tile
@@ -382,11 +385,12 @@ int drain_slices(int dflt) {
   return v < 1 ? 1 : (v > 16 ? 16 : v);
 }
 
-bool front_update_tf32x3(const int32_t* list, int count, const int32_t* first, const int32_t* mrows,
-                         const int64_t* Lptr, const int64_t* Uptr, float* L, const float* Phi, const float* Plo,
-                         const int64_t* PKptr, const float* zero, float* U, int mode, int kbeg, int kend, int cend,
-                         int max_rows, int max_cols, int drain, DevError* err, cudaStream_t st) {
-  if (!enabled() || !Phi || !Plo || !PKptr || !zero || count <= 0 || max_rows <= 0 || max_cols <= 0) return false;
+bool front_update_tf32x3(const int32_t* list, const int2* tiles, int n_tiles, const int32_t* first,
+                         const int32_t* mrows, const int64_t* Lptr, const int64_t* Uptr, float* L, const float* Phi,
+                         const float* Plo, const int64_t* PKptr, const float* zero, float* U, int mode, int kbeg,
+                         int kend, int cend, int drain, DevError* err, cudaStream_t st) {
+  if (!enabled() || !Phi || !Plo || !PKptr || !zero || !tiles) return false;
+  if (n_tiles <= 0) return true;   // no front of the level has output here
   static bool attr = false;
   if (!attr) {
     if (cudaFuncSetAttribute(k_update_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, USMEM) != cudaSuccess)
@@ -396,10 +400,8 @@ bool front_update_tf32x3(const int32_t* list, int count, const int32_t* first, c
   const char* te = std::getenv("JFG_TC_TERMS");   // 4: add lo*lo
   const int terms = (te && te[0] == '4') ? 4 : 3;
   const int udr = drain < 1 ? 1 : (drain > 16 ? 16 : drain);
-  const int ext = mode == 1 ? 7 : 0;              // the mode-1 grid starts up to 7 rows early
-  const int64_t tiles = (int64_t)((max_rows + ext + UM - 1) / UM) * ((max_cols + ext + UM - 1) / UM);
-  k_update_tf32x3<<<dim3((unsigned)tiles, (unsigned)count), UTHREADS, USMEM, st>>>(
-      list, first, mrows, Lptr, Uptr, L, Phi, Plo, PKptr, zero, U, mode, kbeg, kend, cend, terms, udr, err);
+  k_update_tf32x3<<<(unsigned)n_tiles, UTHREADS, USMEM, st>>>(
+      list, first, mrows, Lptr, Uptr, L, Phi, Plo, PKptr, zero, U, mode, kbeg, kend, cend, terms, udr, err, tiles);
   count_launch();
   return cudaGetLastError() == cudaSuccess;
 }
