@@ -105,6 +105,15 @@ jfg_status jfg_model_upload(jfg_ctx* ctx, int64_t n_nodes, const double* xyz,
                             const double* q8_sect, int64_t n_t10,
                             const int32_t* t10_nodes, const double* t10_mat,
                             jfg_model** out);
+/* CTRIA3 shells of a model (src/solver/assembly.jl:3293-3480 section arrays,
+ * :5386-5510 the TRIA3 loop; also the six triangles that replace a CQUAD8
+ * without the native eight-node section, :3176-3196).  Called at most once,
+ * after jfg_model_upload and before the first jfg_assemble.  t3_nodes: n_t3*3
+ * (0-based node idx); t3_sect: n_t3 records of JFG_Q4_SECT_STRIDE doubles
+ * laid out as for CQUAD4 (Cm Cb Cs h Eref k6rot flags; flags is ignored).
+ * The triangles' triplets follow the CQUAD4 ones, as in the reference.      */
+jfg_status jfg_model_add_tria3(jfg_model* model, int64_t n_t3, const int32_t* t3_nodes,
+                               const double* t3_sect);
 jfg_status jfg_model_free(jfg_model* model);
 
 /* ---- assembly ------------------------------------------------------------ */
@@ -126,8 +135,8 @@ jfg_status jfg_get_diag(jfg_model* model, double* diag, double* max_elem_stiff);
  * (src/solver/boundary_conditions.jl:745-845).                            */
 jfg_status jfg_get_node_blocks(jfg_model* model, double* blocks);
 /* Element stiffness in the global frame, as captured by element_capture
- * (assembly.jl:5333, 5885, 5918).  kind: 0=Q4 (24x24), 1=Q8 (48x48),
- * 2=T10 (30x30).                                                          */
+ * (assembly.jl:5333, 5885, 5918, 5508).  kind: 0=Q4 (24x24), 1=Q8 (48x48),
+ * 2=T10 (30x30), 3=T3 (18x18).                                            */
 jfg_status jfg_get_element_matrix(jfg_model* model, int32_t kind, int64_t elem,
                                   double* Ke);
 

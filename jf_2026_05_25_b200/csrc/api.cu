@@ -121,6 +121,7 @@ jfg_status read_elem_error(jfg_model* m) {
     case EE_Q8_SHAPE: what = "CQUAD8 is not a flat parallelogram with mid-side nodes at the edge midpoints"; st = JFG_UNSUPPORTED; break;
     case EE_Q8_DREF: what = "CQUAD8 bending section needs a positive reference stiffness D11"; break;
     case EE_Q8_SINGULAR: what = "CQUAD8 transverse-shear flexibility is singular"; break;
+    case EE_T3_FLEX: what = "CTRIA3 residual normal bending flexibility is not positive"; break;
     default:
       if (h.code >= EE_SHEAR && h.code < EE_SHEAR + 10) what = "CQUAD4 MacNeal shear block is degenerate";
       else what = "element kernel error " + std::to_string(h.code);
@@ -229,6 +230,34 @@ jfg_status jfg_model_upload(jfg_ctx* c, int64_t n_nodes, const double* xyz, cons
   return JFG_OK;
 }
 
+jfg_status jfg_model_add_tria3(jfg_model* m, int64_t n_t3, const int32_t* t3_nodes, const double* t3_sect) {
+  JFG_TRY(check_model(m));
+  if (n_t3 < 0 || (n_t3 > 0 && (!t3_nodes || !t3_sect))) { set_error("bad CTRIA3 arrays"); return JFG_BAD_INPUT; }
+  if (m->pattern_built || m->n_t3 > 0) {
+    set_error("CTRIA3 elements are added once, before the first assembly");
+    return JFG_BAD_INPUT;
+  }
+  for (int64_t i = 0; i < 3 * n_t3; ++i)
+    if (t3_nodes[i] < 0 || t3_nodes[i] >= m->n_nodes) { set_error("CTRIA3 node index out of range", i / 3); return JFG_BAD_INPUT; }
+  if (n_t3 == 0) return JFG_OK;
+  jfg_ctx* c = m->ctx;
+  cudaSetDevice(c->device);
+  m->h_t3n.assign(t3_nodes, t3_nodes + 3 * n_t3);
+  m->h_t3s.assign(t3_sect, t3_sect + JFG_Q4_SECT_STRIDE * n_t3);
+  jfg_status st = JFG_OK;
+  if ((st = up(c, m->h_t3n, &m->d_t3n)) || (st = up(c, m->h_t3s, &m->d_t3s))) return st;
+  // the element values grow by 324 per triangle, after the others
+  double* ev = nullptr;
+  const int64_t n_ev = m->n_ev + 324 * n_t3;
+  if ((st = dev_alloc(c, (void**)&ev, sizeof(double) * n_ev))) return st;
+  dev_free(c, m->d_ev, 8 * std::max<int64_t>(m->n_ev, 1));
+  m->d_ev = ev;
+  m->ev_t3_off = m->n_ev;
+  m->n_ev = n_ev;
+  m->n_t3 = n_t3;
+  return JFG_OK;
+}
+
 jfg_status jfg_model_free(jfg_model* m) {
   if (!m) return JFG_OK;
   jfg_ctx* c = m->ctx;
@@ -241,6 +270,7 @@ jfg_status jfg_model_free(jfg_model* m) {
   dev_free(c, m->d_q4n, 4 * m->h_q4n.size()); dev_free(c, m->d_q4s, 8 * m->h_q4s.size());
   dev_free(c, m->d_q8n, 4 * m->h_q8n.size()); dev_free(c, m->d_q8s, 8 * m->h_q8s.size());
   dev_free(c, m->d_t10n, 4 * m->h_t10n.size()); dev_free(c, m->d_t10m, 8 * m->h_t10m.size());
+  dev_free(c, m->d_t3n, 4 * m->h_t3n.size()); dev_free(c, m->d_t3s, 8 * m->h_t3s.size());
   dev_free(c, m->d_ev, 8 * std::max<int64_t>(m->n_ev, 1)); dev_free(c, m->d_err, sizeof(DevError));
   dev_free(c, m->d_q4prep, 8 * Q4_PREP_STRIDE * std::max<int64_t>(m->n_q4, 1));
   if (m->pattern_built) {
@@ -258,8 +288,10 @@ jfg_status jfg_get_memory(jfg_model* m, int32_t precision, int32_t nrhs, int64_t
   JFG_TRY(check_model(m));
   if (precision != JFG_PREC_FP64 && precision != JFG_PREC_MIXED) { set_error("unknown precision"); return JFG_BAD_INPUT; }
   // inputs, element values and the CQUAD4 prep records
-  int64_t own = 8 * (int64_t)(m->h_xyz.size() + m->h_R.size() + m->h_q4s.size() + m->h_q8s.size() + m->h_t10m.size()) +
-                4 * (int64_t)(m->h_q4n.size() + m->h_q8n.size() + m->h_t10n.size()) + 8 * std::max<int64_t>(m->n_ev, 1) +
+  int64_t own = 8 * (int64_t)(m->h_xyz.size() + m->h_R.size() + m->h_q4s.size() + m->h_q8s.size() + m->h_t10m.size() +
+                             m->h_t3s.size()) +
+                4 * (int64_t)(m->h_q4n.size() + m->h_q8n.size() + m->h_t10n.size() + m->h_t3n.size()) +
+                8 * std::max<int64_t>(m->n_ev, 1) +
                 8 * Q4_PREP_STRIDE * std::max<int64_t>(m->n_q4, 1) + (int64_t)sizeof(DevError);
   if (m->pattern_built)
     own += 8 * (m->ndof + 1) + 4 * m->nnz + 4 * (m->nnz + 1) + 4 * m->n_trip + 8 * m->nnz + 8 * m->nnz + 8 * m->ndof;
@@ -375,6 +407,7 @@ jfg_status jfg_get_element_matrix(jfg_model* m, int32_t kind, int64_t elem, doub
   if (kind == 0 && elem >= 0 && elem < m->n_q4) { off = 576 * elem; len = 576; }
   else if (kind == 2 && elem >= 0 && elem < m->n_t10) { off = m->ev_t10_off + 900 * elem; len = 900; }
   else if (kind == 1 && elem >= 0 && elem < m->n_q8) { off = m->ev_q8_off + 2304 * elem; len = 2304; }
+  else if (kind == 3 && elem >= 0 && elem < m->n_t3) { off = m->ev_t3_off + 324 * elem; len = 324; }
   else { set_error("element kind/index out of range"); return JFG_BAD_INPUT; }
   JFG_CUDA(cudaMemcpy(Ke, m->d_ev + off, sizeof(double) * len, cudaMemcpyDeviceToHost));
   return JFG_OK;
@@ -413,7 +446,8 @@ jfg_status jfg_model_share_structure(jfg_model* dst, const jfg_model* src) {
     set_error("CQUAD8 patterns depend on the element values and are not shared");
     return JFG_UNSUPPORTED;
   }
-  if (dst->n_nodes != src->n_nodes || dst->h_q4n != src->h_q4n || dst->h_t10n != src->h_t10n) {
+  if (dst->n_nodes != src->n_nodes || dst->h_q4n != src->h_q4n || dst->h_t10n != src->h_t10n ||
+      dst->h_t3n != src->h_t3n) {
     set_error("models do not share a mesh (grid count or element connectivity differ)");
     return JFG_BAD_INPUT;
   }

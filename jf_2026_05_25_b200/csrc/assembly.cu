@@ -128,7 +128,7 @@ void residual_dd(const jfg_model* m, int nrhs, const double* x, const double* f,
 
 jfg_status build_pattern(jfg_model* m) {
   const int64_t nn = m->n_nodes, ndof = m->ndof;
-  const int64_t nq4 = m->n_q4, nt10 = m->n_t10, nq8 = m->n_q8;
+  const int64_t nq4 = m->n_q4, nt10 = m->n_t10, nq8 = m->n_q8, nt3 = m->n_t3;
   const uint64_t mt10 = mask_t10();
   // CQUAD8 emits only its nonzero entries (assembly.jl:5912-5916), so its
   // part of the pattern depends on the element values computed just before:
@@ -159,11 +159,16 @@ jfg_status build_pattern(jfg_model* m) {
     }
     for (int64_t e = 0; e < nq8; ++e) q8off[e + 1] = q8off[e] + q8pref[49 * e + 48];
   }
-  const int64_t g8 = nq4 + nt10;   // first global index of the CQUAD8 elements
+  // global element order = the reference's triplet order: CQUAD4, CTRIA3,
+  // CTETRA10, CQUAD8
+  const int64_t g3 = nq4, g10 = nq4 + nt3;
+  const int64_t g8 = g10 + nt10;   // first global index of the CQUAD8 elements
   // node -> incident elements (ascending global order)
   std::vector<int64_t> iptr(nn + 1, 0);
   for (int64_t e = 0; e < nq4; ++e)
     for (int k = 0; k < 4; ++k) iptr[m->h_q4n[4 * e + k] + 1]++;
+  for (int64_t e = 0; e < nt3; ++e)
+    for (int k = 0; k < 3; ++k) iptr[m->h_t3n[3 * e + k] + 1]++;
   for (int64_t e = 0; e < nt10; ++e)
     for (int k = 0; k < 10; ++k) iptr[m->h_t10n[10 * e + k] + 1]++;
   for (int64_t e = 0; e < nq8; ++e)
@@ -174,20 +179,23 @@ jfg_status build_pattern(jfg_model* m) {
     std::vector<int64_t> pos(iptr.begin(), iptr.end() - 1);
     for (int64_t e = 0; e < nq4; ++e)
       for (int k = 0; k < 4; ++k) inc[pos[m->h_q4n[4 * e + k]]++] = {e, (int8_t)k};
+    for (int64_t e = 0; e < nt3; ++e)
+      for (int k = 0; k < 3; ++k) inc[pos[m->h_t3n[3 * e + k]]++] = {g3 + e, (int8_t)k};
     for (int64_t e = 0; e < nt10; ++e)
-      for (int k = 0; k < 10; ++k) inc[pos[m->h_t10n[10 * e + k]]++] = {nq4 + e, (int8_t)k};
+      for (int k = 0; k < 10; ++k) inc[pos[m->h_t10n[10 * e + k]]++] = {g10 + e, (int8_t)k};
     for (int64_t e = 0; e < nq8; ++e)
       for (int k = 0; k < 8; ++k) inc[pos[m->h_q8n[8 * e + k]]++] = {g8 + e, (int8_t)k};
   }
   auto enodes = [&](int64_t ge, int& nnd) -> const int32_t* {
     if (ge < nq4) { nnd = 4; return m->h_q4n.data() + 4 * ge; }
-    if (ge < g8) { nnd = 10; return m->h_t10n.data() + 10 * (ge - nq4); }
+    if (ge < g10) { nnd = 3; return m->h_t3n.data() + 3 * (ge - g3); }
+    if (ge < g8) { nnd = 10; return m->h_t10n.data() + 10 * (ge - g10); }
     nnd = 8;
     return m->h_q8n.data() + 8 * (ge - g8);
   };
   // 6x6 component mask of the (row node la, column node lb) block of element ge
   auto pmask = [&](int64_t ge, int la, int lb) -> uint64_t {
-    if (ge < nq4) return MASK_Q4;
+    if (ge < g10) return MASK_Q4;   // CQUAD4 and CTRIA3: dense 6 x 6 blocks
     if (ge < g8) return mt10;
     return q8pair[64 * (ge - g8) + 8 * la + lb];
   };
@@ -229,7 +237,7 @@ jfg_status build_pattern(jfg_model* m) {
   m->nnz = nnz;
   m->rowval.resize(nnz);
   m->diag_pos.assign(ndof, -1);
-  m->n_trip = 576 * nq4 + 900 * nt10 + q8off[nq8];
+  m->n_trip = 576 * nq4 + 324 * nt3 + 900 * nt10 + q8off[nq8];
   if (m->n_trip >= (int64_t)INT32_MAX || m->n_ev >= (int64_t)INT32_MAX) {
     set_error("triplet count exceeds the 32-bit slot-map range");
     return JFG_UNSUPPORTED;
@@ -303,14 +311,20 @@ jfg_status build_pattern(jfg_model* m) {
               if (ge < nq4) {
                 int rr = 6 * la + i, cc = 6 * lb + j;
                 t = src = 576 * ge + rr + 24 * cc;
+              } else if (ge < g10) {
+                int rr = 6 * la + i, cc = 6 * lb + j;
+                t = 576 * nq4 + 324 * (ge - g3) + rr + 18 * cc;
+                src = m->ev_t3_off + 324 * (ge - g3) + rr + 18 * cc;
               } else if (ge < g8) {
                 int rr = 3 * la + i, cc = 3 * lb + j;
-                t = src = 576 * nq4 + 900 * (ge - nq4) + rr + 30 * cc;
+                t = 576 * nq4 + 324 * nt3 + 900 * (ge - g10) + rr + 30 * cc;
+                src = m->ev_t10_off + 900 * (ge - g10) + rr + 30 * cc;
               } else {
                 int64_t e8 = ge - g8;
                 int rr = 6 * la + i, cc = 6 * lb + j;
                 uint64_t below = q8col[48 * e8 + cc] & ((1ull << rr) - 1);
-                t = 576 * nq4 + 900 * nt10 + q8off[e8] + q8pref[49 * e8 + cc] + __builtin_popcountll(below);
+                t = 576 * nq4 + 324 * nt3 + 900 * nt10 + q8off[e8] + q8pref[49 * e8 + cc] +
+                    __builtin_popcountll(below);
                 src = m->ev_q8_off + 2304 * e8 + rr + 48 * cc;
               }
               trip[w++] = (int32_t)src;

@@ -9,6 +9,7 @@
 // CTETRA10: tetra10.jl:6-79 (four-point rule, Symmetric upper copy),
 //   node_R congruence assembly.jl:5858-5870.
 // CQUAD8: quad8_shell.jl:96-204, node_R congruence assembly.jl:5899-5911.
+// CTRIA3: tria3.cu.
 //
 // Each lane owns a strided subset of the output entries and accumulates them
 // in registers; small shared quantities (condensation blocks, the MacNeal
@@ -1208,6 +1209,11 @@ jfg_status launch_elements(jfg_model* m, cudaStream_t st) {
     prof_end(ps, st, KS_T10, (double)m->n_q8 * (32 + 8 * 22 + 8 * 2304) + 24.0 * m->n_nodes);
     JFG_CUDA(cudaGetLastError());
   }
+  if (m->n_t3 > 0) {
+    int ps = prof_start(st);
+    JFG_TRY(launch_t3(m, st, m->d_ev + m->ev_t3_off, m->d_err));
+    prof_end(ps, st, KS_Q4, (double)m->n_t3 * (12 + 8 * 26 + 8 * 324) + 24.0 * m->n_nodes);
+  }
   return JFG_OK;
 }
 
@@ -1241,6 +1247,7 @@ jfg_status launch_elements_into(const jfg_model* m, cudaStream_t st, double* ev,
                                                    ev + m->ev_q8_off, err); count_launch(); }
     JFG_CUDA(cudaGetLastError());
   }
+  JFG_TRY(launch_t3(m, st, ev + m->ev_t3_off, err));
   return JFG_OK;
 }
 

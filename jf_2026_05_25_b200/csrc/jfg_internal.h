@@ -102,6 +102,7 @@ enum ElemErr : int32_t {
   EE_Q8_SHAPE = 300,
   EE_Q8_DREF = 301,
   EE_Q8_SINGULAR = 302,
+  EE_T3_FLEX = 400,      // CTRIA3 residual bending flexibility not positive
   EE_PIVOT = 500,
   EE_TC_TIMEOUT = 600,   // a bounded tensor-core pipeline wait expired
 };
@@ -123,15 +124,15 @@ struct jfg_model {
   // the model's own stream: models of one context may be driven from
   // different host threads (and captured into graphs) independently
   cudaStream_t stream = nullptr;
-  int64_t n_nodes = 0, n_q4 = 0, n_q8 = 0, n_t10 = 0, ndof = 0;
+  int64_t n_nodes = 0, n_q4 = 0, n_q8 = 0, n_t10 = 0, n_t3 = 0, ndof = 0;
   // host copies of the inputs (pattern build, element capture)
-  std::vector<double> h_xyz, h_R, h_q4s, h_q8s, h_t10m;
-  std::vector<int32_t> h_q4n, h_q8n, h_t10n;
+  std::vector<double> h_xyz, h_R, h_q4s, h_q8s, h_t10m, h_t3s;
+  std::vector<int32_t> h_q4n, h_q8n, h_t10n, h_t3n;
   // device inputs
-  double *d_xyz = nullptr, *d_R = nullptr, *d_q4s = nullptr, *d_q8s = nullptr, *d_t10m = nullptr;
-  int32_t *d_q4n = nullptr, *d_q8n = nullptr, *d_t10n = nullptr;
+  double *d_xyz = nullptr, *d_R = nullptr, *d_q4s = nullptr, *d_q8s = nullptr, *d_t10m = nullptr, *d_t3s = nullptr;
+  int32_t *d_q4n = nullptr, *d_q8n = nullptr, *d_t10n = nullptr, *d_t3n = nullptr;
   // element values: Q4 576 / T10 900 / Q8 2304 doubles per element
-  int64_t ev_t10_off = 0, ev_q8_off = 0, n_ev = 0;
+  int64_t ev_t10_off = 0, ev_q8_off = 0, ev_t3_off = 0, n_ev = 0;
   double* d_ev = nullptr;
   double* d_q4prep = nullptr;   // n_q4 x Q4_PREP_STRIDE scratch between the two CQUAD4 passes
   jfg::DevError* d_err = nullptr;
@@ -174,6 +175,8 @@ namespace jfg {
 // elements.cu
 jfg_status launch_elements(jfg_model* m, cudaStream_t st);
 jfg_status launch_elements_into(const jfg_model* m, cudaStream_t st, double* ev, double* q4prep, DevError* err);
+// CTRIA3 element matrices (324 doubles each, column-major) into ev
+jfg_status launch_t3(const jfg_model* m, cudaStream_t st, double* ev, DevError* err);
 // assembly.cu
 jfg_status build_pattern(jfg_model* m);
 jfg_status launch_assembly(jfg_model* m, cudaStream_t st);

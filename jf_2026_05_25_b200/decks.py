@@ -107,6 +107,10 @@ def write_bdf(model, path: str, title: str = "") -> str:
         this = int(q4eid[e]) if q4eid is not None and len(q4eid) == len(model.q4_nodes) else eid
         lines += _card("CQUAD4", [this, int(model.q4_pid[e])] + [int(gid[n]) for n in nd])
         eid = max(eid, this) + 1
+    t3_first = eid
+    for e, nd in enumerate(getattr(model, "t3_nodes", ())):
+        lines += _card("CTRIA3", [eid, int(model.t3_pid[e])] + [int(gid[n]) for n in nd])
+        eid += 1
     for e, nd in enumerate(model.q8_nodes):
         lines += _card("CQUAD8", [eid, int(model.q8_pid[e])] + [int(gid[n]) for n in nd])
         eid += 1
@@ -125,6 +129,11 @@ def write_bdf(model, path: str, title: str = "") -> str:
             for k, e in enumerate(np.asarray(eidx)):
                 ee = int(q4e[e]) if q4e is not None else int(e) + 1
                 lines.append("PLOAD4*".ljust(8) + str(sid).rjust(16) + str(ee).rjust(16) + _f16(pres[k]))
+        if getattr(lc, "pload4_t3", None) is not None:
+            eidx, pres = lc.pload4_t3
+            for k, e in enumerate(np.asarray(eidx)):
+                lines.append("PLOAD4*".ljust(8) + str(sid).rjust(16) + str(t3_first + int(e)).rjust(16) +
+                             _f16(pres[k]))
         for part in (lc.forces, lc.cload):
             if part is None:
                 continue
@@ -192,7 +201,7 @@ def read_bdf(path: str) -> "M.Sol101Model":
         else:
             cards.append([ln])
     grids, mats, pshells, psolids = {}, {}, {}, {}
-    q4, q8, t10, spc, loads = [], [], [], [], {}
+    q4, q8, t3, t10, spc, loads = [], [], [], [], [], {}
     for c in cards:
         name, v = _fields(c)
         if name == "GRID":
@@ -208,6 +217,8 @@ def read_bdf(path: str) -> "M.Sol101Model":
             q4.append((int(v[0]), int(v[1]), [int(x) for x in v[2:6]]))
         elif name == "CQUAD8":
             q8.append((int(v[0]), int(v[1]), [int(x) for x in v[2:10]]))
+        elif name == "CTRIA3":
+            t3.append((int(v[0]), int(v[1]), [int(x) for x in v[2:5]]))
         elif name == "CTETRA":
             t10.append((int(v[0]), int(v[1]), [int(x) for x in v[2:12]]))
         elif name == "SPC1":
@@ -223,26 +234,33 @@ def read_bdf(path: str) -> "M.Sol101Model":
     xyz = np.array([grids[g] for g in gid], float)
     q4eid = np.array([e for e, _, _ in q4], np.int64)
     epos = {e: i for i, e in enumerate(q4eid)}
+    t3pos = {e: i for i, (e, _, _) in enumerate(t3)}
     model = M.Sol101Model(
         name=os.path.basename(path), grid_ids=gid, xyz=xyz,
         q4_nodes=np.array([[pos[g] for g in n] for _, _, n in q4], np.int32).reshape(-1, 4),
         q4_pid=np.array([p for _, p, _ in q4], np.int64), q4_eid=q4eid,
         q8_nodes=np.array([[pos[g] for g in n] for _, _, n in q8], np.int32).reshape(-1, 8),
         q8_pid=np.array([p for _, p, _ in q8], np.int64),
+        t3_nodes=np.array([[pos[g] for g in n] for _, _, n in t3], np.int32).reshape(-1, 3),
+        t3_pid=np.array([p for _, p, _ in t3], np.int64),
         t10_nodes=np.array([[pos[g] for g in n] for _, _, n in t10], np.int32).reshape(-1, 10),
         t10_pid=np.array([p for _, p, _ in t10], np.int64),
         pshells=pshells, psolids=psolids, mats=mats, k6rot=k6rot,
         spc1=[(comp, np.array([pos[g] for g in ids], np.int64)) for comp, ids in spc])
     for sid in sorted(loads):
         ld = loads[sid]
-        p4 = None
-        if ld["p4"]:
-            p4 = (np.array([epos[e] for e, _ in ld["p4"]]), np.array([p for _, p in ld["p4"]]))
+        p4 = p4t = None
+        on_q4 = [(e, p) for e, p in ld["p4"] if e in epos]
+        on_t3 = [(e, p) for e, p in ld["p4"] if e not in epos and e in t3pos]
+        if on_q4:
+            p4 = (np.array([epos[e] for e, _ in on_q4]), np.array([p for _, p in on_q4]))
+        if on_t3:
+            p4t = (np.array([t3pos[e] for e, _ in on_t3]), np.array([p for _, p in on_t3]))
         fr = None
         if ld["f"]:
             nodes = np.array([pos[g] for g, _ in ld["f"]])
             fr = (nodes, np.array([f for _, f in ld["f"]]))
-        model.load_cases.append(M.LoadCase(sid=sid - 100, pload4=p4, forces=fr))
+        model.load_cases.append(M.LoadCase(sid=sid - 100, pload4=p4, pload4_t3=p4t, forces=fr))
     return model
 
 

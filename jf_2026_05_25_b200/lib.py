@@ -71,6 +71,7 @@ def load():
         "jfg_create": [P, P],
         "jfg_destroy": [P],
         "jfg_model_upload": [P, I64, P, P, I64, P, P, I64, P, P, I64, P, P, P],
+        "jfg_model_add_tria3": [P, I64, P, P],
         "jfg_model_free": [P],
         "jfg_assemble": [P],
         "jfg_get_sizes": [P, P, P, P],
@@ -163,13 +164,19 @@ class DeviceModel:
         self.ctx = ctx
         self.model = model
         self.h = P()
+        # shells as assembled: native CQUAD8 only; the model's CTRIA3 plus
+        # the six triangles of every other CQUAD8
+        q8n, q8s = model.device_q8()
+        t3n, t3s = model.device_t3()
         self._keep = dict(
             xyz=np.ascontiguousarray(model.xyz, np.float64),
             R=np.ascontiguousarray(model.node_R, np.float64),
             q4n=np.ascontiguousarray(model.q4_nodes, np.int32),
             q4s=np.ascontiguousarray(model.q4_sections(), np.float64),
-            q8n=np.ascontiguousarray(model.q8_nodes, np.int32),
-            q8s=np.ascontiguousarray(model.q8_sections(), np.float64),
+            q8n=np.ascontiguousarray(q8n, np.int32),
+            q8s=np.ascontiguousarray(q8s, np.float64),
+            t3n=np.ascontiguousarray(t3n, np.int32),
+            t3s=np.ascontiguousarray(t3s, np.float64),
             t10n=np.ascontiguousarray(model.t10_nodes, np.int32),
             t10m=np.ascontiguousarray(model.t10_materials(), np.float64),
         )
@@ -177,6 +184,12 @@ class DeviceModel:
         _check(L.jfg_model_upload(ctx.h, model.n_nodes, _p(k["xyz"]), _p(k["R"]), len(k["q4n"]), _p(k["q4n"]),
                                   _p(k["q4s"]), len(k["q8n"]), _p(k["q8n"]), _p(k["q8s"]), len(k["t10n"]),
                                   _p(k["t10n"]), _p(k["t10m"]), _c.byref(self.h)))
+        if len(k["t3n"]):
+            st = L.jfg_model_add_tria3(self.h, len(k["t3n"]), _p(k["t3n"]), _p(k["t3s"]))
+            if st != 0:
+                L.jfg_model_free(self.h)
+                self.h = P()
+                _check(st)
         self.ndof = model.ndof
         self.n_free = None
 
@@ -236,7 +249,7 @@ class DeviceModel:
         return b
 
     def element_matrix(self, kind: int, elem: int) -> np.ndarray:
-        n = {0: 24, 1: 48, 2: 30}[kind]
+        n = {0: 24, 1: 48, 2: 30, 3: 18}[kind]
         K = np.empty((n, n), order="F")
         _check(load().jfg_get_element_matrix(self.h, kind, elem, _p(K)))
         return K

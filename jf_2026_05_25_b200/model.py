@@ -49,9 +49,11 @@ class LoadCase:
     ``forces``: (node index array, (n,3) force vectors, global frame).
     ``cload``:  (node index array, (n,3) translational forces) -- consistent
                 C3D10 face loads delivered as nodal loads (abaqus_input.jl:347-405).
+    ``pload4_t3``: (element index array into the CTRIA3 list, pressure array).
     """
     sid: int
     pload4: Optional[Tuple[np.ndarray, np.ndarray]] = None
+    pload4_t3: Optional[Tuple[np.ndarray, np.ndarray]] = None
     forces: Optional[Tuple[np.ndarray, np.ndarray]] = None
     cload: Optional[Tuple[np.ndarray, np.ndarray]] = None
 
@@ -67,6 +69,8 @@ class Sol101Model:
     q4_eid: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
     q8_nodes: np.ndarray = field(default_factory=lambda: np.zeros((0, 8), np.int32))
     q8_pid: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    t3_nodes: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.int32))
+    t3_pid: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
     t10_nodes: np.ndarray = field(default_factory=lambda: np.zeros((0, 10), np.int32))
     t10_pid: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
     pshells: Dict[int, PShell] = field(default_factory=dict)
@@ -146,6 +150,48 @@ class Sol101Model:
             out[self.q8_pid == pid] = rec
         return out
 
+    def t3_sections(self) -> np.ndarray:
+        """Per-element CTRIA3 section records (assembly.jl:3300-3440 with n = 3):
+        the CQUAD4 record's Cm, Cb, Cs, h and k6rot; Eref = the shear modulus
+        (:3389, unused by the triangle's lumped drilling); flags 0."""
+        return _t3_records(self, self.t3_pid)
+
+    # ------------------------------------------------------------------ shells as assembled
+    def q8_native_mask(self) -> np.ndarray:
+        """CQUAD8 that keep the native eight-node stiffness: flat parallelograms
+        with mid-side nodes at the edge midpoints (assembly.jl:2585-2628,
+        quad8_shell.jl:34-46, tolerance 1e-6 of the longer edge from G1)."""
+        if len(self.q8_nodes) == 0:
+            return np.zeros(0, bool)
+        P = np.asarray(self.xyz, float)[np.asarray(self.q8_nodes)]          # (n, 8, 3)
+        scale = np.maximum(np.linalg.norm(P[:, 1] - P[:, 0], axis=1), np.linalg.norm(P[:, 3] - P[:, 0], axis=1))
+        lim = 1e-6 * scale
+        ok = scale > 0
+        ok &= np.linalg.norm(P[:, 0] + P[:, 2] - P[:, 1] - P[:, 3], axis=1) <= lim
+        for m, a, b in ((4, 0, 1), (5, 1, 2), (6, 2, 3), (7, 3, 0)):
+            ok &= np.linalg.norm(P[:, m] - (P[:, a] + P[:, b]) / 2, axis=1) <= lim
+        nrm = np.linalg.norm(np.cross(P[:, 1] - P[:, 0], P[:, 3] - P[:, 0]), axis=1)
+        ok &= nrm > 1e-12 * scale * scale
+        return ok
+
+    def device_q8(self) -> Tuple[np.ndarray, np.ndarray]:
+        """(nodes, section records) of the CQUAD8 assembled natively."""
+        keep = self.q8_native_mask()
+        return (np.ascontiguousarray(np.asarray(self.q8_nodes, np.int32)[keep]).reshape(-1, 8),
+                np.ascontiguousarray(self.q8_sections()[keep]).reshape(-1, Q8_SECT_STRIDE))
+
+    def device_t3(self) -> Tuple[np.ndarray, np.ndarray]:
+        """(nodes, section records) of every CTRIA3 as assembled: the model's
+        own, then six per CQUAD8 without the native section, in element order
+        (assembly.jl:3176-3196: [1,5,8] [5,2,6] [6,3,7] [7,4,8] [5,6,8] [6,7,8])."""
+        keep = self.q8_native_mask()
+        split = np.asarray(self.q8_nodes, np.int32)[~keep] if len(keep) else np.zeros((0, 8), np.int32)
+        sub = np.asarray(split)[:, Q8_TRIANGLES].reshape(-1, 3)
+        spid = np.repeat(np.asarray(self.q8_pid)[~keep], 6) if len(keep) else np.zeros(0, np.int64)
+        nodes = np.vstack([np.asarray(self.t3_nodes, np.int32).reshape(-1, 3), sub.astype(np.int32)])
+        pids = np.concatenate([np.asarray(self.t3_pid, np.int64), spid.astype(np.int64)])
+        return np.ascontiguousarray(nodes), np.ascontiguousarray(_t3_records(self, pids))
+
     def t10_materials(self) -> np.ndarray:
         out = np.zeros((len(self.t10_pid), 2))
         for pid in np.unique(self.t10_pid):
@@ -177,6 +223,18 @@ class Sol101Model:
             fnode = ldir * (tf / 4.0)[:, None]
             Fn = F.reshape(-1, 6)
             for k in range(4):
+                for a in range(3):
+                    Fn[:, a] += np.bincount(nodes[:, k], weights=fnode[:, a], minlength=nn_tot)
+        if case.pload4_t3 is not None:
+            # CTRIA3: p A / 3 per node along (x2 - x1) x (x3 - x1) (loads.jl:546-585)
+            eidx, p = case.pload4_t3
+            nodes = np.asarray(self.t3_nodes)[eidx]
+            X = self.xyz
+            nv = np.cross(X[nodes[:, 1]] - X[nodes[:, 0]], X[nodes[:, 2]] - X[nodes[:, 0]])
+            nn = np.linalg.norm(nv, axis=1)
+            fnode = (nv / nn[:, None]) * (0.5 * nn * p / 3.0)[:, None]
+            Fn = F.reshape(-1, 6)
+            for k in range(3):
                 for a in range(3):
                     Fn[:, a] += np.bincount(nodes[:, k], weights=fnode[:, a], minlength=nn_tot)
         for item in (case.forces, case.cload):
@@ -223,6 +281,25 @@ class Sol101Model:
         if not out:
             return np.zeros(0, np.int64)
         return np.unique(np.concatenate(out))
+
+
+# the six CTRIA3 of a CQUAD8 without the native section (assembly.jl:3187-3188)
+Q8_TRIANGLES = np.array([[0, 4, 7], [4, 1, 5], [5, 2, 6], [6, 3, 7], [4, 5, 7], [5, 6, 7]])
+
+
+def _t3_records(model: Sol101Model, pids: np.ndarray) -> np.ndarray:
+    out = np.zeros((len(pids), Q4_SECT_STRIDE))
+    for pid in np.unique(pids):
+        rec = _q4_section_record(model, int(pid)).copy()
+        p = model.pshells[int(pid)]
+        sm = model.mats[p.MID3] if p.MID3 != 0 else model.mats[p.MID1]
+        G = float(sm.G)
+        if G <= 0.0:
+            G = float(sm.E) / (2 * (1 + float(sm.NU))) if float(sm.E) > 0.0 else 0.0
+        rec[23] = G
+        rec[25] = 0.0
+        out[pids == pid] = rec
+    return out
 
 
 def _q4_section_record(model: Sol101Model, pid: int) -> np.ndarray:
@@ -311,12 +388,16 @@ def flat_plate(nx: int = 20, ny: int = 20, a: float = 0.5, b: float = 0.5,
 
 def quad8_plate(nx: int = 8, ny: int = 6, a: float = 0.4, b: float = 0.3, t: float = 0.003,
                 E: float = 70e9, nu: float = 0.33, skew: float = 0.0, tilt_deg: float = 0.0,
-                n_cases: int = 1, force_sigma: float = 50.0, seed: int = 11) -> Sol101Model:
+                n_cases: int = 1, force_sigma: float = 50.0, seed: int = 11,
+                taper: float = 0.0) -> Sol101Model:
     """Cantilever plate of CQUAD8 (native shell path, quad8_shell.jl).
 
     Corner and mid-side nodes on the (2nx+1) x (2ny+1) lattice of the
     parallelogram spanned by (a, 0) and (skew * b, b); element centres are not
-    nodes.  ``tilt_deg`` rotates the whole plate about the x axis and then about
+    nodes.  ``taper`` narrows the half x > a/2 linearly (y scaled by
+    1 - taper (u - 1/2)), so its elements are trapezoids, which the reference
+    assembles as six CTRIA3 each (nx even keeps every element on one side).
+    ``tilt_deg`` rotates the whole plate about the x axis and then about
     z by half that angle, so the elements lie in a general plane.  PSHELL
     MID1 = MID2 = MID3 = 1 with MAT1 G given.  SPC1 123456 on the edge x = 0.
     Subcase k: seeded N(0, force_sigma) nodal forces on every free node.
@@ -329,7 +410,7 @@ def quad8_plate(nx: int = 8, ny: int = 6, a: float = 0.4, b: float = 0.3, t: flo
                 continue
             u, v = i / (2 * nx), j / (2 * ny)
             idx[(i, j)] = len(pts)
-            pts.append([u * a + skew * b * v, v * b, 0.0])
+            pts.append([u * a + skew * b * v, v * b * (1.0 - taper * max(0.0, u - 0.5)), 0.0])
     xyz = np.asarray(pts, float)
     if tilt_deg:
         th = math.radians(tilt_deg)
@@ -355,6 +436,59 @@ def quad8_plate(nx: int = 8, ny: int = 6, a: float = 0.4, b: float = 0.3, t: flo
         pshells={1: PShell(T=t, MID1=1, MID2=1, MID3=1)},
         mats={1: Mat1(E=E, NU=nu, G=E / (2 * (1 + nu)))},
         spc1=[("123456", clamp)], load_cases=cases, seed=seed)
+
+
+def tria_plate(nx: int = 12, ny: int = 10, a: float = 0.6, b: float = 0.5, t: float = 0.002,
+               E: float = 70e9, nu: float = 0.33, jitter: float = 0.2, tilt_deg: float = 25.0,
+               pressure: float = 5e3, n_cases: int = 2, force_sigma: float = 20.0,
+               seed: int = 5) -> Sol101Model:
+    """Cantilever plate of CQUAD4 (cells with x < a/2) and CTRIA3 (two per cell,
+    alternating diagonals, x > a/2).  Interior nodes move in-plane by up to
+    ``jitter`` of a cell (seeded), so the triangles are irregular; the plate is
+    tilted into a general plane as in ``quad8_plate``.  SPC1 123456 on x = 0.
+    Subcase 1: PLOAD4 on every CQUAD4 and CTRIA3; subcase k > 1 adds seeded
+    N(0, force_sigma) nodal forces on the free nodes."""
+    rng = _rng(seed)
+    hx, hy = a / nx, b / ny
+    pts = np.zeros(((nx + 1) * (ny + 1), 3))
+    nid = lambda i, j: j * (nx + 1) + i
+    for j in range(ny + 1):
+        for i in range(nx + 1):
+            x, y = i * hx, j * hy
+            if 0 < i < nx and 0 < j < ny:
+                x += jitter * hx * rng.uniform(-0.5, 0.5)
+                y += jitter * hy * rng.uniform(-0.5, 0.5)
+            pts[nid(i, j)] = (x, y, 0.0)
+    if tilt_deg:
+        th = math.radians(tilt_deg)
+        Rx = np.array([[1, 0, 0], [0, math.cos(th), -math.sin(th)], [0, math.sin(th), math.cos(th)]])
+        ph = th / 2
+        Rz = np.array([[math.cos(ph), -math.sin(ph), 0], [math.sin(ph), math.cos(ph), 0], [0, 0, 1]])
+        pts = pts @ (Rz @ Rx).T
+    q4, t3 = [], []
+    for j in range(ny):
+        for i in range(nx):
+            n1, n2, n3, n4 = nid(i, j), nid(i + 1, j), nid(i + 1, j + 1), nid(i, j + 1)
+            if 2 * i < nx:
+                q4.append([n1, n2, n3, n4])
+            elif (i + j) % 2 == 0:
+                t3 += [[n1, n2, n3], [n1, n3, n4]]
+            else:
+                t3 += [[n1, n2, n4], [n2, n3, n4]]
+    q4 = np.asarray(q4, np.int32).reshape(-1, 4)
+    t3 = np.asarray(t3, np.int32).reshape(-1, 3)
+    clamp = np.array([nid(0, j) for j in range(ny + 1)], np.int64)
+    free = np.setdiff1d(np.arange(len(pts)), clamp)
+    cases = [LoadCase(sid=1, pload4=(np.arange(len(q4)), np.full(len(q4), pressure)),
+                      pload4_t3=(np.arange(len(t3)), np.full(len(t3), pressure)))]
+    for k in range(1, n_cases):
+        cases.append(LoadCase(sid=k + 1, forces=(free, rng.normal(0.0, force_sigma, (len(free), 3)))))
+    return Sol101Model(
+        name=f"tria_plate_{nx}x{ny}", grid_ids=np.arange(1, len(pts) + 1, dtype=np.int64), xyz=pts,
+        q4_nodes=q4, q4_pid=np.ones(len(q4), np.int64), q4_eid=np.arange(1, len(q4) + 1),
+        t3_nodes=t3, t3_pid=np.ones(len(t3), np.int64),
+        pshells={1: PShell(T=t, MID1=1, MID2=1, MID3=1)},
+        mats={1: Mat1(E=E, NU=nu)}, spc1=[("123456", clamp)], load_cases=cases, seed=seed)
 
 
 def wing_panel(nx: int = 200, ny: int = 400, lx: float = 1.0, ly: float = 2.0,

@@ -50,6 +50,7 @@ class PackedModel:
     def __init__(self, models: Sequence, gap: float = 1.0):
         self.members = list(models)
         xyz, R, q4n, q4s, q8n, q8s, t10n, t10m, spc = [], [], [], [], [], [], [], [], []
+        t3n, t3s = [], []
         self.node_off, self.q4_off = [], []
         n_off = 0
         q4_off = 0
@@ -63,8 +64,12 @@ class PackedModel:
             R.append(np.asarray(m.node_R, float))
             q4n.append(np.asarray(m.q4_nodes, np.int32) + n_off)
             q4s.append(m.q4_sections())
-            q8n.append(np.asarray(m.q8_nodes, np.int32) + n_off)
-            q8s.append(m.q8_sections())
+            n8, s8 = m.device_q8()
+            q8n.append(np.asarray(n8, np.int32) + n_off)
+            q8s.append(s8)
+            n3, s3 = m.device_t3()
+            t3n.append(np.asarray(n3, np.int32) + n_off)
+            t3s.append(s3)
             t10n.append(np.asarray(m.t10_nodes, np.int32) + n_off)
             t10m.append(m.t10_materials())
             spc.append(np.asarray(m.spc_dofs(), np.int64) + 6 * n_off)
@@ -80,6 +85,8 @@ class PackedModel:
         self._q4s = np.vstack(q4s).reshape(-1, 26)
         self.q8_nodes = np.vstack(q8n).reshape(-1, 8)
         self._q8s = np.vstack(q8s).reshape(-1, 22)
+        self._t3n = np.vstack(t3n).reshape(-1, 3)
+        self._t3s = np.vstack(t3s).reshape(-1, 26)
         self.t10_nodes = np.vstack(t10n).reshape(-1, 10)
         self._t10m = np.vstack(t10m).reshape(-1, 2)
         self._spc = np.unique(np.concatenate(spc))
@@ -99,6 +106,12 @@ class PackedModel:
 
     def q8_sections(self):
         return self._q8s
+
+    def device_q8(self):
+        return self.q8_nodes, self._q8s
+
+    def device_t3(self):
+        return self._t3n, self._t3s
 
     def t10_materials(self):
         return self._t10m
@@ -205,12 +218,14 @@ class Resident:
 
 def mesh_key(model) -> Optional[bytes]:
     """Key of a model's mesh for structure sharing: grid count and CQUAD4 /
-    CTETRA10 connectivity (CQUAD8 patterns depend on values: no key)."""
+    CTRIA3 / CTETRA10 connectivity (CQUAD8 patterns depend on values: no key)."""
     if len(getattr(model, "q8_nodes", ())):
         return None
     h = hashlib.blake2b(digest_size=16)
     h.update(np.int64(model.n_nodes).tobytes())
     h.update(np.ascontiguousarray(model.q4_nodes, np.int32).tobytes())
+    h.update(b"|")
+    h.update(np.ascontiguousarray(getattr(model, "t3_nodes", np.zeros((0, 3))), np.int32).tobytes())
     h.update(b"|")
     h.update(np.ascontiguousarray(model.t10_nodes, np.int32).tobytes())
     return h.digest()
@@ -461,7 +476,8 @@ class SolveServer:
         n_q4 = len(getattr(target, "q4_nodes", ()))
         n_q8 = len(getattr(target, "q8_nodes", ()))
         n_t10 = len(getattr(target, "t10_nodes", ()))
-        n_ev = 576 * n_q4 + 2304 * n_q8 + 900 * n_t10
+        n_t3 = len(target.device_t3()[0]) if hasattr(target, "device_t3") else 0
+        n_ev = 576 * n_q4 + 2304 * n_q8 + 900 * n_t10 + 324 * n_t3
         nnz = (324 if n_t10 == 0 else 270) * target.n_nodes
         return float(8 * n_ev + 8 * 210 * n_q4 + 4 * n_ev + 28 * nnz + 150 * target.n_nodes)
 

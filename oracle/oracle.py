@@ -57,12 +57,18 @@ def lib():
         L.or_q8_element.argtypes = [P, P, P, P]
         L.or_q8_parallelogram.argtypes = [P]
         L.or_t10_element.argtypes = [P, P, d, d, P]
-        L.or_assemble_triplets.argtypes = [i64, P, P, i64, P, P, i64, P, P, i64, P, P, i64, P, P, P, P]
+        L.or_assemble_triplets.argtypes = [i64, P, P, i64, P, P, i64, P, P, i64, P, P, i64, P, P, i64, P, P,
+                                           P, P]
+        L.or_tria3_guard.argtypes = [P, d, d, d, d, d]
+        L.or_tria3_guard.restype = i32
+        L.or_tria3_local.argtypes = [P, P, P, P, d, P]
+        L.or_t3_element.argtypes = [P, P, P, P]
         L.or_assemble_triplets.restype = i64
         L.or_build_csc.argtypes = [i64, i64, P, P, P, P, P, P, P]
         L.or_build_csc.restype = i64
         L.or_csc_matvec.argtypes = [i64, P, P, P, i32, P, P]
-        for name in ("or_q4_local", "or_q4_element", "or_q8_element", "or_q8_parallelogram", "or_t10_element"):
+        for name in ("or_q4_local", "or_q4_element", "or_q8_element", "or_q8_parallelogram", "or_t10_element",
+                     "or_tria3_local", "or_t3_element"):
             getattr(L, name).restype = ctypes.c_int
         L.or_chol_factor_solve.argtypes = [i64, P, P, P, P, i32, P, P, i32, P]
         L.or_chol_factor_solve.restype = ctypes.c_int
@@ -125,6 +131,98 @@ def q8_element(xyz, sect, nodeR=None):
     return Ke
 
 
+def tria3_guard(Zb, La, Lb, c, s, Dnormal):
+    """FEMKernels.jl:9281-9313 on a copy of Zb: (changed, Zb).  Raises where
+    the reference raises (non-positive residual normal flexibility)."""
+    Z = np.asfortranarray(np.array(Zb, float))
+    st = lib().or_tria3_guard(_p(Z), float(La), float(Lb), float(c), float(s), float(Dnormal))
+    if st < 0:
+        raise ValueError("Triangle residual normal flexibility must be positive")
+    return bool(st), Z
+
+
+def tria3_local(coords, Dm, Db, Ds, k6rot=100.0):
+    """18 x 18 local CTRIA3 stiffness (FEMKernels.jl:9375-9809, default path)."""
+    X = np.asfortranarray(np.asarray(coords, float).reshape(3, 2))
+    Ke = np.zeros((18, 18), order="F")
+    st = lib().or_tria3_local(_p(X), _p(np.asfortranarray(Dm, float)), _p(np.asfortranarray(Db, float)),
+                              _p(np.asfortranarray(Ds, float)), float(k6rot), _p(Ke))
+    if st:
+        raise ValueError(f"or_tria3_local status {st}")
+    return Ke
+
+
+def t3_element(xyz, sect, nodeR=None):
+    xyz = np.ascontiguousarray(xyz, float)
+    R = np.ascontiguousarray(_ident_R(3) if nodeR is None else nodeR, float)
+    Ke = np.zeros((18, 18), order="F")
+    st = lib().or_t3_element(_p(xyz), _p(R), _p(np.ascontiguousarray(sect, float)), _p(Ke))
+    if st:
+        raise ValueError(f"or_t3_element status {st}")
+    return Ke
+
+
+# the six CTRIA3 that replace a CQUAD8 without the native eight-node section
+# (assembly.jl:3176-3196): [1,5,8] [5,2,6] [6,3,7] [7,4,8] [5,6,8] [6,7,8]
+_Q8_SPLIT = ((0, 4, 7), (4, 1, 5), (5, 2, 6), (6, 3, 7), (4, 5, 7), (5, 6, 7))
+
+
+def shells_as_assembled(model):
+    """(native CQUAD8 nodes, their sections, CTRIA3 nodes, their sections): a
+    CQUAD8 keeps the native stiffness when quad8_shell_parallelogram holds
+    (quad8_shell.jl:34-46, or_q8_parallelogram), else it becomes six CTRIA3
+    with its PSHELL section, appended after the model's own triangles."""
+    L = lib()
+    X = np.asarray(model.xyz, float)
+    q8n = np.asarray(model.q8_nodes, np.int32).reshape(-1, 8)
+    q8s = np.asarray(model.q8_sections(), float).reshape(-1, 22)
+    keep = np.array([L.or_q8_parallelogram(_p(np.ascontiguousarray(X[nd]))) != 0 for nd in q8n], bool)
+    split = np.where(~keep)[0]
+    nodes = [np.asarray(getattr(model, "t3_nodes", np.zeros((0, 3))), np.int32).reshape(-1, 3)]
+    pids = [np.asarray(getattr(model, "t3_pid", np.zeros(0)), np.int64)]
+    if len(split):
+        nodes.append(np.array([[q8n[e][k] for k in tri] for e in split for tri in _Q8_SPLIT], np.int32))
+        pids.append(np.repeat(np.asarray(model.q8_pid, np.int64)[split], 6))
+    pid = np.concatenate(pids)
+    recs = np.zeros((len(pid), 26))
+    for q in np.unique(pid):
+        recs[pid == q] = _t3_record(model, int(q))
+    return (np.ascontiguousarray(q8n[keep]), np.ascontiguousarray(q8s[keep]),
+            np.ascontiguousarray(np.vstack(nodes)), recs)
+
+
+def _t3_record(model, pid: int) -> np.ndarray:
+    """CTRIA3 section record of an isotropic PSHELL (assembly.jl:3375-3461 with
+    n = 3): Cm = E h / (1 - nu^2) [1 nu 0; nu 1 0; 0 0 (1-nu)/2] of MID1; Cb
+    the same law of MID2 (MID1 when blank) times 12I/T^3 h^3 / 12; Cs =
+    TS/T h G I2 of MID3 (MID1 when blank), G derived as E / 2(1 + nu) when
+    blank; Cb = Cs = 0 and K6ROT 0 for a membrane-only shell (12I/T^3 <= 1e-12);
+    Eref = that G; flags 0."""
+    p = model.pshells[pid]
+    h, br, tst = float(p.T), float(p.BEND_RATIO), float(p.TS_T)
+
+    def law(mat):
+        E, nu = float(mat.E), float(mat.NU)
+        return E / (1 - nu * nu) * np.array([[1.0, nu, 0.0], [nu, 1.0, 0.0], [0.0, 0.0, (1 - nu) / 2]])
+    m1 = model.mats[p.MID1]
+    Cm = h * law(m1)
+    Cb = np.zeros((3, 3))
+    Cs = np.zeros((2, 2))
+    sm = model.mats[p.MID3] if p.MID3 != 0 else m1
+    G = float(sm.G) if float(sm.G) > 0 else (float(sm.E) / (2 * (1 + float(sm.NU))) if float(sm.E) > 0 else 0.0)
+    if br > 1e-12:
+        Cb = (br * h ** 3 / 12.0) * law(model.mats[p.MID2] if p.MID2 != 0 else m1)
+        Cs = tst * h * G * np.eye(2)
+    rec = np.zeros(26)
+    rec[0:9] = Cm.ravel(order="F")
+    rec[9:18] = Cb.ravel(order="F")
+    rec[18:22] = Cs.ravel(order="F")
+    rec[22] = h
+    rec[23] = G
+    rec[24] = 0.0 if br <= 1e-12 else float(model.k6rot)
+    return rec
+
+
 def t10_element(xyz, E, nu, nodeR=None):
     xyz = np.ascontiguousarray(xyz, float)
     R = np.ascontiguousarray(_ident_R(10) if nodeR is None else nodeR, float)
@@ -168,14 +266,14 @@ def assemble(model):
     R = np.ascontiguousarray(model.node_R, float)
     q4n = np.ascontiguousarray(model.q4_nodes, np.int32)
     q4s = np.ascontiguousarray(model.q4_sections())
-    q8n = np.ascontiguousarray(model.q8_nodes, np.int32)
-    q8s = np.ascontiguousarray(model.q8_sections())
+    q8n, q8s, t3n, t3s = shells_as_assembled(model)
     t10n = np.ascontiguousarray(model.t10_nodes, np.int32)
     t10m = np.ascontiguousarray(model.t10_materials())
-    cap = 576 * len(q4n) + 900 * len(t10n) + 2304 * len(q8n)
+    cap = 576 * len(q4n) + 324 * len(t3n) + 900 * len(t10n) + 2304 * len(q8n)
     I = np.empty(cap, np.int64); J = np.empty(cap, np.int64); V = np.empty(cap)
     err = np.full(1, -1, np.int32)
     nt = L.or_assemble_triplets(model.n_nodes, _p(xyz), _p(R), len(q4n), _p(q4n), _p(q4s),
+                                len(t3n), _p(t3n), _p(t3s),
                                 len(q8n), _p(q8n), _p(q8s), len(t10n), _p(t10n), _p(t10m),
                                 cap, _p(I), _p(J), _p(V), _p(err))
     if nt < 0:
@@ -376,7 +474,8 @@ def load_vector(model, case) -> np.ndarray:
 
     PLOAD4 on a 4-node shell (loads.jl:546-585): the face normal is
     (x3 - x1) x (x4 - x2), area = |normal| / 2, and each of the 4 nodes gets
-    area * p / 4 along the unit normal (no nodal moments).  FORCE and the
+    area * p / 4 along the unit normal (no nodal moments); on a 3-node shell
+    the normal is (x2 - x1) x (x3 - x1) and each node gets area * p / 3.  FORCE and the
     consistent C3D10 face loads (delivered as nodal forces, abaqus_input.jl:
     347-405) add their vectors to the translational DOFs.  The accumulated
     global vector is then expressed in each node's displacement frame,
@@ -401,6 +500,20 @@ def load_vector(model, case) -> np.ndarray:
         for k in range(4):
             for c in range(3):
                 acc[:, c] += np.bincount(q4[:, k], weights=fnode[:, c], minlength=n_nodes)
+    if getattr(case, "pload4_t3", None) is not None:
+        # PLOAD4 on a 3-node shell: normal (x2 - x1) x (x3 - x1), p A / 3 per node
+        eidx, pres = case.pload4_t3
+        t3 = np.asarray(model.t3_nodes)[np.asarray(eidx)]
+        a = X[t3[:, 1]] - X[t3[:, 0]]
+        b = X[t3[:, 2]] - X[t3[:, 0]]
+        nv = np.stack([a[:, 1] * b[:, 2] - a[:, 2] * b[:, 1], a[:, 2] * b[:, 0] - a[:, 0] * b[:, 2],
+                       a[:, 0] * b[:, 1] - a[:, 1] * b[:, 0]], axis=1)
+        nrm = np.sqrt((nv * nv).sum(axis=1))
+        share = np.where(0.5 * nrm > 1e-30, 0.5 * nrm * np.asarray(pres, float) / 3.0, 0.0)
+        fnode = nv / np.where(nrm > 0, nrm, 1.0)[:, None] * share[:, None]
+        for k in range(3):
+            for c in range(3):
+                acc[:, c] += np.bincount(t3[:, k], weights=fnode[:, c], minlength=n_nodes)
     for item in (case.forces, case.cload):
         if item is None:
             continue

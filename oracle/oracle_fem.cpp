@@ -819,13 +819,259 @@ int or_t10_element(const double* xyz, const double* nodeR, double E, double nu,
 }
 
 // ---------------------------------------------------------------------------
+// CTRIA3 (FEMKernels.jl:9375-9809 stiffness_tria3_matrices_generic on the
+// default SOL101 settings: plate kernel "mitc3", the recovered tying rigidity
+// (JFEM_TRIA3_MITC3_SHEAR_REF), the residual bending flexibility with
+// directional pairing (JFEM_TRIA3_MITC3_ZB, JFEM_TRIA3_ZB_DIRECTIONAL), the
+// lumped drilling penalty (JFEM_TRIA3_DRILL_LUMPED), no Bmb coupling, no
+// residual-bending shear relaxation (JFEM_TRIA3_RBF_C = 0)).
+
+// FEMKernels.jl:9281-9313 tria3_guard_bending_flexibility!: Zb 3x3 col-major,
+// modified in place; returns 1 when a bound changed it, 0 when not, -1 when
+// the residual normal flexibility is not positive (the reference throws).
+int or_tria3_guard(double* Zb, double La, double Lb, double c, double s, double Dnormal) {
+  const double scale = 6 * (La / Lb) * s * Dnormal;
+  if (!(scale > 0.0 && Zb[8] > 0.0)) return 0;
+  const double z11 = Zb[0], z12 = Zb[3], z13 = Zb[6], z22 = Zb[4], z23 = Zb[7], z33 = Zb[8];
+  const double h11 = scale * (z11 - z13 * z13 / z33) / (La * La);
+  const double h22 = scale * (z22 - z23 * z23 / z33) / (Lb * Lb);
+  const double h12 = scale * (z12 - z13 * z23 / z33) / (La * Lb);
+  const double p11 = h11, p12 = (h12 - c * h11) / s, p22 = (h22 - 2 * c * h12 + c * c * h11) / (s * s);
+  if (!(std::isfinite(p22) && p22 > 0.0)) return -1;
+  const double a = std::max(p11, 1.0 / 10000);
+  const double q = std::max(p22, a / 10000);
+  const double limit = std::sqrt((85.0 / 100) * a * q);
+  const double b = std::min(std::max(p12, -limit), limit);
+  if (a == p11 && b == p12 && q == p22) return 0;
+  const double n11 = a, n12 = c * a + s * b, n22 = c * c * a + 2 * c * s * b + s * s * q;
+  Zb[0] += (n11 - h11) * La * La / scale;
+  Zb[3] += (n12 - h12) * La * Lb / scale;
+  Zb[1] = Zb[3];
+  Zb[4] += (n22 - h22) * Lb * Lb / scale;
+  return 1;
+}
+
+// 18x18 local CTRIA3 stiffness (col-major), DOFs (u v w rx ry rz) per node.
+// coords: 3x2 local coordinates (col-major); Dm, Db: 3x3; Ds: 2x2.  Returns 0,
+// or 111 when the residual flexibility guard fails (the reference throws).
+int or_tria3_local(const double* coords, const double* Dm, const double* Db, const double* Ds,
+                   double k6rot, double* Ke) {
+  std::memset(Ke, 0, sizeof(double) * 324);
+  const double x[3] = {coords[0], coords[1], coords[2]}, y[3] = {coords[3], coords[4], coords[5]};
+  const double A2 = x[0] * (y[1] - y[2]) + x[1] * (y[2] - y[0]) + x[2] * (y[0] - y[1]);
+  const double A = 0.5 * std::fabs(A2);
+  if (A < 1e-12) return 0;   // :9380
+  // membrane CST (:9389-9396)
+  const double bv[3] = {(y[1] - y[2]) / (2 * A), (y[2] - y[0]) / (2 * A), (y[0] - y[1]) / (2 * A)};
+  const double cv[3] = {(x[2] - x[1]) / (2 * A), (x[0] - x[2]) / (2 * A), (x[1] - x[0]) / (2 * A)};
+  double Bm[18] = {0};   // 3 x 6
+  for (int i = 0; i < 3; ++i) {
+    at(Bm, 3, 0, 2 * i) = bv[i];
+    at(Bm, 3, 1, 2 * i + 1) = cv[i];
+    at(Bm, 3, 2, 2 * i) = cv[i];
+    at(Bm, 3, 2, 2 * i + 1) = bv[i];
+  }
+  double DB[18], Kmem[36] = {0};
+  mul(DB, 3, 6, Dm, 3, Bm);
+  mul_At_add(Kmem, 6, 6, Bm, 3, DB, A);
+  const int m_idx[6] = {0, 1, 6, 7, 12, 13};
+  for (int j = 0; j < 6; ++j)
+    for (int i = 0; i < 6; ++i) at(Ke, 18, m_idx[i], m_idx[j]) = at(Kmem, 6, i, j);
+  // constant-curvature bending (:9399-9408)
+  double Bb[27] = {0};   // 3 x 9
+  for (int i = 0; i < 3; ++i) {
+    const int crx = 3 * i + 1, cry = 3 * i + 2;
+    at(Bb, 3, 0, cry) = bv[i];
+    at(Bb, 3, 1, crx) = -cv[i];
+    at(Bb, 3, 2, crx) = -bv[i];
+    at(Bb, 3, 2, cry) = cv[i];
+  }
+  double DBb[27], Kb[81] = {0};
+  mul(DBb, 3, 9, Db, 3, Bb);
+  mul_At_add(Kb, 9, 9, Bb, 3, DBb, A);
+  // MITC3 covariant shear rows (:9482-9502)
+  const double x1 = x[0], y1 = y[0], x2 = x[1], y2 = y[1], x3 = x[2], y3 = y[2];
+  const double J[4] = {x2 - x1, x3 - x1, y2 - y1, y3 - y1};   // [x2-x1 y2-y1; x3-x1 y3-y1] col-major
+  double Ji[4];
+  inv_small(J, 2, Ji);
+  auto gcov = [&](double r, double s_, double* Br, double* Bs) {
+    const double N[3] = {1 - r - s_, r, s_};
+    const double dwdr[3] = {-1, 1, 0}, dwds[3] = {-1, 0, 1};
+    for (int i = 0; i < 3; ++i) {
+      const int cw = 3 * i, crx = 3 * i + 1, cry = 3 * i + 2;
+      Br[cw] = dwdr[i]; Bs[cw] = dwds[i];
+      Br[cry] = N[i] * at(J, 2, 0, 0); Bs[cry] = N[i] * at(J, 2, 1, 0);
+      Br[crx] = -N[i] * at(J, 2, 0, 1); Bs[crx] = -N[i] * at(J, 2, 1, 1);
+    }
+  };
+  double grA[9], gsA[9], grB[9], gsB[9], grC[9], gsC[9], cvec[9];
+  gcov(0.5, 0.0, grA, gsA);
+  gcov(0.0, 0.5, grB, gsB);
+  gcov(0.5, 0.5, grC, gsC);
+  for (int k = 0; k < 9; ++k) cvec[k] = (grC[k] - grA[k]) - (gsC[k] - gsB[k]);
+  // tying rigidity (:9507-9557)
+  const double La = std::hypot(x2 - x1, y2 - y1), Lb = std::hypot(x3 - x1, y3 - y1);
+  const double Lc = std::hypot(x3 - x2, y3 - y2), Pper = La + Lb + Lc;
+  const double cth = std::min(std::max(((x2 - x1) * (x3 - x1) + (y2 - y1) * (y3 - y1)) / std::max(La * Lb, 1e-30), -1.0), 1.0);
+  const double sth = std::sqrt(std::max(1.0 - cth * cth, 0.0));
+  double t2[4], G[4];
+  mul(t2, 2, 2, Ds, 2, Ji);   // Ds * Jinv
+  for (int j = 0; j < 2; ++j)
+    for (int i = 0; i < 2; ++i) at(G, 2, i, j) = at(Ji, 2, 0, i) * at(t2, 2, 0, j) + at(Ji, 2, 1, i) * at(t2, 2, 1, j);
+  const double uu = 3 * La / Pper, vv = 3 * Lb / Pper;
+  double W[9];
+  W[0] = at(G, 2, 0, 0) * A;
+  W[3] = at(G, 2, 0, 1) * A; W[1] = W[3];
+  W[4] = at(G, 2, 1, 1) * A;
+  W[6] = (A / 3) * (uu * at(G, 2, 0, 0) - vv * at(G, 2, 0, 1)); W[2] = W[6];
+  W[7] = (A / 3) * (uu * at(G, 2, 0, 1) - vv * at(G, 2, 1, 1)); W[5] = W[7];
+  W[8] = uu * uu * at(G, 2, 0, 0) * (A / 6) - 2 * uu * vv * at(G, 2, 0, 1) * (A * (2 - cth) / 18) +
+         vv * vv * at(G, 2, 1, 1) * (A / 6);
+  // residual bending flexibility with directional pairing (:9581-9756)
+  const double Dbend = std::fabs(Db[0]);
+  if (sth > 1e-9 && Dbend > 1e-30 && La > 1e-30 && Lb > 1e-30) {
+    const double Rr = (La - Lb) * (La - Lb) / (La * Lb);
+    const double Tt = (La * La - Lb * Lb) / (La * Lb);
+    const double sum_d = 2 * ((1 - cth + cth * cth) / (6 * sth) + 1.0 / 6) + Rr * (1 + cth * cth) / (6 * sth);
+    const double dif_d = Tt * sth / 6;
+    const double a11 = (sum_d + dif_d) / 2, a22 = (sum_d - dif_d) / 2;
+    const double a12 = (-1 + 4 * cth - cth * cth) / (12 * sth) - 1.0 / 6 + Rr * cth / (6 * sth);
+    const double S1 = La, S2 = Lb, S3 = Pper, s6 = 1.0 / 6;
+    const double D11e = Dbend, D22e = std::fabs(Db[4]);
+    const bool dir_pair = D11e > 1e-30 && D22e > 1e-30;
+    const double rho = La / Lb, Rr2 = rho + 1 / rho - 2, Tt2 = rho - 1 / rho;
+    const double fr = ((1 - cth) * (1 - cth) - (rho - cth)) / (6 * sth) + Rr2 * (1 + cth * cth) / (12 * sth) + Tt2 * sth / 12;
+    const double fri = ((1 - cth) * (1 - cth) - (1 / rho - cth)) / (6 * sth) + Rr2 * (1 + cth * cth) / (12 * sth) - Tt2 * sth / 12;
+    const double w12 = (1 / rho - cth) / (6 * sth), w13 = (rho - cth) / (6 * sth), w23 = cth / (6 * sth);
+    const double o12 = (Rr2 * cth - (1 - cth) * (1 - cth) - Tt2 * cth) / (12 * sth);
+    const double o13 = (Rr2 * cth - (1 - cth) * (1 - cth) + Tt2 * cth) / (12 * sth);
+    const double o23 = (1 + cth * cth) / (12 * sth);
+    auto ddir = [&](double vx, double vy) {
+      const double n = std::hypot(vx, vy);
+      if (n < 1e-30) return Dbend;
+      const double nx = -vy / n, ny = vx / n;
+      const double w[3] = {nx * nx, ny * ny, 2 * nx * ny};
+      double d = 0;
+      for (int ii = 0; ii < 3; ++ii)
+        for (int jj = 0; jj < 3; ++jj) d += w[ii] * Db[ii + 3 * jj] * w[jj];
+      return std::fabs(d) > 1e-30 ? d : Dbend;
+    };
+    const double Dn12 = dir_pair ? ddir(x2 - x1, y2 - y1) : Dbend;
+    const double Dn13 = dir_pair ? ddir(x3 - x1, y3 - y1) : Dbend;
+    const double Dn23 = dir_pair ? ddir(x3 - x2, y3 - y2) : Dbend;
+    const double Gd = dir_pair ? std::sqrt(D11e * D22e) : Dbend;
+    const double c11 = dir_pair ? s6 / Gd + fr / Dn12 + w13 / Dn13 + w23 / Dn23 : a11 / Dbend;
+    const double c22 = dir_pair ? s6 / Gd + w12 / Dn12 + fri / Dn13 + w23 / Dn23 : a22 / Dbend;
+    const double c12 = dir_pair ? -s6 / Gd + o12 / Dn12 + o13 / Dn13 + o23 / Dn23 : a12 / Dbend;
+    double Zb[9];
+    Zb[0] = c11 * S1 * S1; Zb[3] = c12 * S1 * S2;
+    Zb[1] = Zb[3]; Zb[4] = c22 * S2 * S2;
+    Zb[6] = -s6 / Gd * S1 * S3; Zb[2] = Zb[6];
+    Zb[7] = s6 / Gd * S2 * S3; Zb[5] = Zb[7];
+    Zb[8] = s6 / Gd * S3 * S3;
+    if (or_tria3_guard(Zb, La, Lb, cth, sth, dir_pair ? Dn12 : Dbend) < 0) return 111;
+    double Wi[9], Zt[9], Zs[9];
+    if (!inv_small(W, 3, Wi)) return 111;
+    for (int k = 0; k < 9; ++k) Zt[k] = Wi[k] + Zb[k];
+    for (int j = 0; j < 3; ++j)
+      for (int i = 0; i < 3; ++i) Zs[i + 3 * j] = 0.5 * (Zt[i + 3 * j] + Zt[j + 3 * i]);
+    if (!inv_small(Zs, 3, W)) return 111;
+  }
+  // Ks = D3' W D3, D3 = [grA; gsB; c] (:9758-9760)
+  double D3[27];
+  for (int k = 0; k < 9; ++k) { D3[3 * k] = grA[k]; D3[3 * k + 1] = gsB[k]; D3[3 * k + 2] = cvec[k]; }
+  double WD[27], Kp[81];
+  std::memcpy(Kp, Kb, sizeof Kp);
+  mul(WD, 3, 9, W, 3, D3);
+  mul_At_add(Kp, 9, 9, D3, 3, WD, 1.0);
+  const int b_idx[9] = {2, 3, 4, 8, 9, 10, 14, 15, 16};
+  for (int j = 0; j < 9; ++j)
+    for (int i = 0; i < 9; ++i) at(Ke, 18, b_idx[i], b_idx[j]) += at(Kp, 9, i, j);
+  // lumped drilling: alpha_L = K6ROT 1e-6 Dm[3,3] (2A) per node (:9800-9815)
+  const double alpha_L = (k6rot * 1e-6) * Dm[8] * (2 * A);
+  for (int i = 0; i < 3; ++i) {
+    double Bd[18] = {0};
+    for (int j = 0; j < 3; ++j) {
+      Bd[6 * j] = 0.5 * cv[j];
+      Bd[6 * j + 1] = -0.5 * bv[j];
+    }
+    Bd[6 * i + 5] = 1.0;
+    for (int c = 0; c < 18; ++c)
+      for (int r = 0; r < 18; ++r) at(Ke, 18, r, c) += alpha_L * (Bd[r] * Bd[c]);
+  }
+  return 0;
+}
+
+// Global-frame CTRIA3 stiffness (assembly.jl:5395-5503 without SNORM, offsets
+// or material rotation): frame helpers.jl:1487-1490 (v1 along G1G2, v3 the
+// normal of G1G2 x G1G3), local coordinates about the centroid (:5467-5470),
+// T = blockdiag(Rel node_R) (:5483-5493), Ke = T' Ke_loc T.  xyz: 3 rows x 3;
+// nodeR: 3 x 9; sect: the CQUAD4 section record (Cm Cb Cs h Eref k6rot flags).
+int or_t3_element(const double* xyz, const double* nodeR, const double* sect, double* Ke_global) {
+  double p[3][3];
+  for (int k = 0; k < 3; ++k)
+    for (int a = 0; a < 3; ++a) p[k][a] = xyz[3 * k + a];
+  double v1[3], e13[3], v3[3], v2[3];
+  for (int a = 0; a < 3; ++a) { v1[a] = p[1][a] - p[0][a]; e13[a] = p[2][a] - p[0][a]; }
+  double l1 = std::sqrt(v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2]);
+  for (int a = 0; a < 3; ++a) v1[a] /= l1;
+  v3[0] = v1[1] * e13[2] - v1[2] * e13[1];
+  v3[1] = v1[2] * e13[0] - v1[0] * e13[2];
+  v3[2] = v1[0] * e13[1] - v1[1] * e13[0];
+  double l3 = std::sqrt(v3[0] * v3[0] + v3[1] * v3[1] + v3[2] * v3[2]);
+  for (int a = 0; a < 3; ++a) v3[a] /= l3;
+  v2[0] = v3[1] * v1[2] - v3[2] * v1[1];
+  v2[1] = v3[2] * v1[0] - v3[0] * v1[2];
+  v2[2] = v3[0] * v1[1] - v3[1] * v1[0];
+  double c[3];
+  for (int a = 0; a < 3; ++a) c[a] = (p[0][a] + p[1][a] + p[2][a]) / 3.0;
+  double lc[6];
+  for (int k = 0; k < 3; ++k) {
+    double d[3] = {p[k][0] - c[0], p[k][1] - c[1], p[k][2] - c[2]};
+    lc[k] = d[0] * v1[0] + d[1] * v1[1] + d[2] * v1[2];
+    lc[k + 3] = d[0] * v2[0] + d[1] * v2[1] + d[2] * v2[2];
+  }
+  double Ke[324];
+  int st = or_tria3_local(lc, sect, sect + 9, sect + 18, sect[24], Ke);
+  if (st) return st;
+  double T[324] = {0};
+  const double Rel[3][3] = {{v1[0], v1[1], v1[2]}, {v2[0], v2[1], v2[2]}, {v3[0], v3[1], v3[2]}};
+  for (int k = 0; k < 3; ++k) {
+    const double* R = nodeR + 9 * k;
+    for (int rr = 0; rr < 3; ++rr)
+      for (int cc = 0; cc < 3; ++cc) {
+        double v = Rel[rr][0] * R[0 + 3 * cc] + Rel[rr][1] * R[1 + 3 * cc] + Rel[rr][2] * R[2 + 3 * cc];
+        T[(6 * k + rr) + 18 * (6 * k + cc)] = v;
+        T[(6 * k + 3 + rr) + 18 * (6 * k + 3 + cc)] = v;
+      }
+  }
+  double tmp[324] = {0};
+  for (int jj = 0; jj < 18; ++jj)
+    for (int ll = 0; ll < 18; ++ll) {
+      double v = T[ll + 18 * jj];
+      if (v != 0.0)
+        for (int ii = 0; ii < 18; ++ii) tmp[ii + 18 * jj] += Ke[ii + 18 * ll] * v;
+    }
+  std::memset(Ke_global, 0, sizeof(double) * 324);
+  for (int jj = 0; jj < 18; ++jj)
+    for (int ll = 0; ll < 18; ++ll) {
+      double v = tmp[ll + 18 * jj];
+      if (v != 0.0)
+        for (int ii = 0; ii < 18; ++ii) Ke_global[ii + 18 * jj] += T[ll + 18 * ii] * v;
+    }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
 // Triplet emission in the reference's order and Julia's sparse() semantics.
 //   Q4: positional slots (ei-1)*576, col-major (assembly.jl:3506-3508, :433-439)
+//   CTRIA3: 324 per element col-major (:5505-5507)
 //   solids: 900 per element col-major (:5882-5884)
 //   Q8: col-major, exact zeros skipped (:5912-5916)
 // Counts triplets first (n_q8 contribution depends on values).
 int64_t or_assemble_triplets(int64_t n_nodes, const double* xyz, const double* node_R,
                              int64_t n_q4, const int32_t* q4_nodes, const double* q4_sect,
+                             int64_t n_t3, const int32_t* t3_nodes, const double* t3_sect,
                              int64_t n_q8, const int32_t* q8_nodes, const double* q8_sect,
                              int64_t n_t10, const int32_t* t10_nodes, const double* t10_mat,
                              int64_t cap, int64_t* I, int64_t* J, double* V, int32_t* err_elem) {
@@ -867,6 +1113,25 @@ int64_t or_assemble_triplets(int64_t n_nodes, const double* xyz, const double* n
   }
   if (q4_err >= 0) { *err_elem = (int32_t)q4_err; return -q4_st; }
   cnt = 576 * n_q4;
+  // CTRIA3: all 324 entries, column-major, after the CQUAD4 (:5386-5510)
+  for (int64_t e = 0; e < n_t3; ++e) {
+    for (int k = 0; k < 3; ++k) {
+      int n = t3_nodes[3 * e + k];
+      for (int a = 0; a < 3; ++a) exyz[3 * k + a] = xyz[3 * n + a];
+      for (int a = 0; a < 9; ++a) eR[9 * k + a] = node_R[9 * n + a];
+    }
+    int st = or_t3_element(exyz, eR, t3_sect + 26 * e, Ke.data());
+    if (st) { *err_elem = (int32_t)(n_q4 + e); return -st; }
+    for (int cc = 0; cc < 18; ++cc)
+      for (int rr = 0; rr < 18; ++rr) {
+        if (cnt < cap) {
+          I[cnt] = 6 * (int64_t)t3_nodes[3 * e + rr / 6] + rr % 6;
+          J[cnt] = 6 * (int64_t)t3_nodes[3 * e + cc / 6] + cc % 6;
+          V[cnt] = Ke[rr + 18 * cc];
+        }
+        ++cnt;
+      }
+  }
   for (int64_t e = 0; e < n_t10; ++e) {
     for (int k = 0; k < 10; ++k) {
       int n = t10_nodes[10 * e + k];
@@ -874,7 +1139,7 @@ int64_t or_assemble_triplets(int64_t n_nodes, const double* xyz, const double* n
       for (int a = 0; a < 9; ++a) eR[9 * k + a] = node_R[9 * n + a];
     }
     int st = or_t10_element(exyz, eR, t10_mat[2 * e], t10_mat[2 * e + 1], Ke.data());
-    if (st) { *err_elem = (int32_t)(n_q4 + e); return -st; }
+    if (st) { *err_elem = (int32_t)(n_q4 + n_t3 + e); return -st; }
     for (int cc = 0; cc < 30; ++cc)
       for (int rr = 0; rr < 30; ++rr) {
         if (cnt < cap) {
@@ -893,7 +1158,7 @@ int64_t or_assemble_triplets(int64_t n_nodes, const double* xyz, const double* n
       for (int a = 0; a < 9; ++a) R8[9 * k + a] = node_R[9 * n + a];
     }
     int st = or_q8_element(x8.data(), R8.data(), q8_sect + 22 * e, Ke.data());
-    if (st) { *err_elem = (int32_t)(n_q4 + n_t10 + e); return -st; }
+    if (st) { *err_elem = (int32_t)(n_q4 + n_t3 + n_t10 + e); return -st; }
     for (int cc = 0; cc < 48; ++cc)
       for (int rr = 0; rr < 48; ++rr) {
         double v = Ke[rr + 48 * cc];

@@ -17,8 +17,10 @@ def _same(a, b, exact):
         return np.allclose(x, y, rtol=1e-12, atol=1e-12 * max(np.abs(x).max(initial=0.0), 1e-300))
     assert np.array_equal(a.grid_ids, b.grid_ids)
     assert eq(a.xyz, b.xyz)
-    for f in ("q4_nodes", "q8_nodes", "t10_nodes"):
+    for f in ("q4_nodes", "q8_nodes", "t3_nodes", "t10_nodes"):
         assert np.array_equal(getattr(a, f), getattr(b, f))
+    if len(a.t3_nodes):
+        assert eq(a.t3_sections(), b.t3_sections())
     if len(a.q4_nodes):
         assert eq(a.q4_sections(), b.q4_sections())
     if len(a.q8_nodes):
@@ -37,6 +39,7 @@ def test_round_trip_plate_wing_q8_solid(tmp_path):
     models = [M.flat_plate(nx=6, ny=5),
               M.wing_panel(nx=12, ny=10, n_blades=2, blade_nz=3, n_cases=3, seed=4),
               M.quad8_plate(4, 3, n_cases=2),
+              M.tria_plate(nx=6, ny=4, n_cases=2),
               M.solid_block(n=2, n_cases=1)]
     for k, m in enumerate(models):
         path = D.write_bdf(m, os.path.join(tmp_path, f"m{k}.bdf"))

@@ -113,15 +113,66 @@ def test_quad8_element_matrices(ctx, oracle_mod):
     assert worst <= ELEM_RTOL, worst
 
 
-def test_quad8_rejects_curved_element(ctx):
+def test_quad8_curved_element_becomes_triangles(ctx, oracle_mod):
+    # a CQUAD8 that is not a flat parallelogram is assembled as six CTRIA3,
+    # as the reference does (assembly.jl:3176-3196)
     m = M.quad8_plate(2, 2)
     m.xyz = m.xyz.copy()
     m.xyz[m.q8_nodes[0, 4], 2] += 0.01       # lift a mid-side node off the edge
+    assert m.q8_native_mask().tolist() == [False, True, True, True]
+    asm = oracle_mod.assemble(m)
+    dm = lib.DeviceModel(ctx, m)
+    dm.assemble()
+    assert np.array_equal(dm.slot_map(), asm["slot"])
+    assert np.abs(dm.values() - asm["nzval"]).max() <= ELEM_RTOL * np.abs(asm["nzval"]).max()
+
+
+def test_quad8_shape_check_still_guards_the_native_kernel(ctx):
+    # the C ABI refuses a non-parallelogram CQUAD8 handed to the native kernel
+    m = M.quad8_plate(2, 2)
+    m.xyz = m.xyz.copy()
+    m.xyz[m.q8_nodes[0, 4], 2] += 0.01
+    m.q8_native_mask = lambda: np.ones(len(m.q8_nodes), bool)
     dm = lib.DeviceModel(ctx, m)
     with pytest.raises(lib.JfgError) as e:
         dm.assemble()
     assert e.value.status_name == "UNSUPPORTED"
     assert e.value.detail == 0
+
+
+def test_tria3_element_matrices(ctx, oracle_mod):
+    rng = np.random.default_rng(17)
+    xyz, t3, nodeR = [], [], []
+    for k in range(96):
+        # triangles from slivers to obtuse, in random planes
+        a = rng.uniform(0.004, 0.05)
+        apex = np.array([rng.uniform(-0.5, 1.5) * a, rng.uniform(0.05, 1.5) * a])
+        P = np.c_[np.array([[0.0, 0.0], [a, 0.0], apex]), np.zeros(3)]
+        R = _rot(0, rng.uniform(0, 180)) @ _rot(1, rng.uniform(0, 180)) @ _rot(2, rng.uniform(0, 360))
+        xyz.append(P @ R.T + rng.uniform(-1, 1, 3))
+        t3.append(np.arange(3) + 3 * k)
+        for _ in range(3):
+            Rn = _rot(2, rng.uniform(0, 90)) @ _rot(0, rng.uniform(0, 90)) if k % 3 == 1 else np.eye(3)
+            nodeR.append(Rn.ravel(order="F"))
+    xyz = np.vstack(xyz)
+    t3 = np.asarray(t3, np.int32)
+    nodeR = np.asarray(nodeR)
+    pids = np.arange(len(t3)) % 3 + 1
+    m = M.Sol101Model(name="t3set", grid_ids=np.arange(1, len(xyz) + 1), xyz=xyz, node_R=nodeR, t3_nodes=t3,
+                      t3_pid=pids,
+                      pshells={1: M.PShell(T=0.003, MID1=1, MID2=1, MID3=1),
+                               2: M.PShell(T=0.006, MID1=1, MID2=2, MID3=0, BEND_RATIO=0.9, TS_T=0.8),
+                               3: M.PShell(T=0.002, MID1=2, BEND_RATIO=0.0)},
+                      mats={1: M.Mat1(E=70e9, NU=0.33), 2: M.Mat1(E=110e9, NU=0.3, G=40e9)})
+    dm = lib.DeviceModel(ctx, m)
+    dm.assemble()
+    sect = m.t3_sections()
+    worst = 0.0
+    for e in range(len(t3)):
+        Kd = dm.element_matrix(3, e)
+        Ko = oracle_mod.t3_element(xyz[t3[e]], sect[e], nodeR[t3[e]])
+        worst = max(worst, _rel(Kd, Ko))
+    assert worst <= ELEM_RTOL, worst
 
 
 def test_tetra10_element_matrices(ctx, oracle_mod):
@@ -144,6 +195,8 @@ MODELS = {
     "q8_tilted": lambda: M.quad8_plate(6, 5, skew=0.2, tilt_deg=30, n_cases=2),
     "wing_small": lambda: M.wing_panel(nx=24, ny=36, n_blades=3, blade_nz=4, n_cases=3, seed=5),
     "solid_small": lambda: M.solid_block(n=4, n_cases=2),
+    "tria_mixed": lambda: M.tria_plate(),
+    "q8_tapered": lambda: M.quad8_plate(8, 6, taper=0.6, tilt_deg=20, n_cases=2),
 }
 
 
