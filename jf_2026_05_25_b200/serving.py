@@ -216,6 +216,14 @@ class Resident:
     mesh: Optional[bytes] = None       # mesh key of a single model (structure sharing)
 
 
+def _model_class(model, pack) -> str:
+    """Class of a unit of work in the phase accounting: a pack of small
+    models, a solid model (CTETRA10) or a shell model."""
+    if pack is not None:
+        return "pack"
+    return "solid" if len(getattr(model, "t10_nodes", ())) else "shell"
+
+
 def mesh_key(model) -> Optional[bytes]:
     """Key of a model's mesh for structure sharing: grid count and CQUAD4 /
     CTRIA3 / CTETRA10 connectivity (CQUAD8 patterns depend on values: no key)."""
@@ -273,6 +281,7 @@ class SolveServer:
         self.subcase_solves = 0
         self.readmissions = 0
         self.shared_structures = 0
+        self.phase_s: Dict[str, Dict[str, float]] = {}   # class -> phase -> seconds (wall, summed over slots)
         self._next_key = 0
         self._stop = False
         self.backends = []
@@ -325,7 +334,8 @@ class SolveServer:
                 "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3),
                 "subcase_solves": int(self.subcase_solves), "resident_bytes": int(self.resident_bytes),
                 "readmissions": int(self.readmissions), "shared_structures": int(self.shared_structures),
-                "fp64_meshes": len(self.fp64_meshes), "fp64_factorisations": int(self.fp64_factorisations)}
+                "fp64_meshes": len(self.fp64_meshes), "fp64_factorisations": int(self.fp64_factorisations),
+                "phase_s": {c: {k: round(v, 4) for k, v in d.items()} for c, d in self.phase_s.items()}}
 
     # ---------------------------------------------------------------- scheduling
     def _take(self) -> Optional[List[Request]]:
@@ -497,6 +507,7 @@ class SolveServer:
         pre = self._upload_estimate(target)
         self._admit(pre, wait=True)
         admitted = [pre]
+        t_up = time.perf_counter()
         try:
             dm = lib.DeviceModel(be.ctx, target)
         except Exception:
@@ -520,19 +531,30 @@ class SolveServer:
                 self._admit(need - admitted[0], wait=True)
                 admitted[0] = need
 
+        t_prep = time.perf_counter()
         try:
             st = B.prepare(be, target, dm=dm, before_factor=admit, precision=prec)
         except Exception:
             dm.close()
             self._release(admitted[0])
             raise
+        tm = st.get("timings", {})
+        self._add_phases(_model_class(target, pack), upload=t_prep - t_up, assembly=tm.get("assembly", 0.0),
+                         analysis=tm.get("constraints", 0.0), factor=tm.get("factorization", 0.0))
         return st, admitted[0], mk
+
+    def _add_phases(self, cls: str, **secs):
+        with self.rlock:
+            d = self.phase_s.setdefault(cls, {})
+            for k, v in secs.items():
+                d[k] = d.get(k, 0.0) + float(v)
 
     def _do_solve(self, be, reqs: List[Request]):
         models = [r.model for r in reqs]
         pack = PackedModel(models)
         nrhs = max(16, max((r.loads.shape[0] if r.device else len(r.model.load_cases)) for r in reqs))
         st, reserved, mk = self._prepare(be, models[0], pack if len(models) > 1 else None, nrhs)
+        t_sol = time.perf_counter()
         try:
             if reqs[0].device:
                 Us, res, rep = self._device_solve(be, st["dm"], pack, [r.loads for r in reqs], self.tol)
@@ -554,6 +576,8 @@ class SolveServer:
             st["dm"].close()
             self._release(reserved)
             raise
+        self._add_phases(_model_class(models[0], pack if len(models) > 1 else None),
+                         solve=time.perf_counter() - t_sol)
         if (self.precision == lib.PREC_MIXED and mk is not None and st.get("precision") == lib.PREC_MIXED
                 and rep.get("ir_iters", 0) > self.slow_refinement_steps):
             with self.rlock:
