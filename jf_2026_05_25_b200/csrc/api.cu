@@ -226,6 +226,13 @@ jfg_status jfg_model_upload(jfg_ctx* c, int64_t n_nodes, const double* xyz, cons
     return st;
   }
   cudaMemset(m->d_err, 0, sizeof(DevError));
+  // pageable copies and memsets run on the legacy stream; the model's own
+  // stream does not wait for it, so they finish here
+  if (cudaStreamSynchronize(cudaStreamLegacy) != cudaSuccess) {
+    jfg_model_free(m);
+    set_error("uploading the model failed");
+    return JFG_CUDA_ERROR;
+  }
   *out = m;
   return JFG_OK;
 }
@@ -255,6 +262,7 @@ jfg_status jfg_model_add_tria3(jfg_model* m, int64_t n_t3, const int32_t* t3_nod
   m->ev_t3_off = m->n_ev;
   m->n_ev = n_ev;
   m->n_t3 = n_t3;
+  JFG_CUDA(cudaStreamSynchronize(cudaStreamLegacy));   // the pageable uploads above
   return JFG_OK;
 }
 
@@ -314,7 +322,8 @@ jfg_status jfg_assemble(jfg_model* m) {
     JFG_CUDA(cudaStreamSynchronize(st));
     JFG_TRY(read_elem_error(m));
     JFG_TRY(build_pattern(m));
-    JFG_TRY(up(m->ctx, m->diag_pos, &m->d_diag_pos));
+    JFG_TRY(up(m->ctx, m->pat->diag_pos, &m->d_diag_pos));
+    JFG_CUDA(cudaStreamSynchronize(cudaStreamLegacy));   // the pattern's pageable uploads
   }
   JFG_TRY(launch_assembly(m, st));
   JFG_CUDA(cudaEventRecord(e2, st));
@@ -342,8 +351,8 @@ jfg_status jfg_get_sizes(jfg_model* m, int64_t* ndof, int64_t* nnz, int64_t* n_t
 jfg_status jfg_get_pattern(jfg_model* m, int64_t* colptr, int32_t* rowval) {
   JFG_TRY(check_model(m));
   if (!m->pattern_built) { set_error("pattern not built: call jfg_assemble first"); return JFG_NOT_READY; }
-  if (colptr) std::memcpy(colptr, m->colptr.data(), sizeof(int64_t) * (m->ndof + 1));
-  if (rowval) std::memcpy(rowval, m->rowval.data(), sizeof(int32_t) * m->nnz);
+  if (colptr) std::memcpy(colptr, m->pat->colptr.data(), sizeof(int64_t) * (m->ndof + 1));
+  if (rowval) std::memcpy(rowval, m->pat->rowval.data(), sizeof(int32_t) * m->nnz);
   return JFG_OK;
 }
 
@@ -357,47 +366,22 @@ jfg_status jfg_get_values(jfg_model* m, double* nzval) {
 jfg_status jfg_get_slot_map(jfg_model* m, int64_t* slot) {
   JFG_TRY(check_model(m));
   if (!m->pattern_built) { set_error("pattern not built"); return JFG_NOT_READY; }
-  std::memcpy(slot, m->slot.data(), sizeof(int64_t) * m->n_trip);
+  std::memcpy(slot, m->pat->slot.data(), sizeof(int64_t) * m->n_trip);
   return JFG_OK;
 }
 
 jfg_status jfg_get_diag(jfg_model* m, double* diag, double* max_elem_stiff) {
   JFG_TRY(check_model(m));
   if (!m->values_ready) { set_error("values not assembled"); return JFG_NOT_READY; }
-  std::vector<double> v(m->nnz);
-  JFG_CUDA(cudaMemcpy(v.data(), m->d_nzval, sizeof(double) * m->nnz, cudaMemcpyDeviceToHost));
-  if (diag)
-    for (int64_t d = 0; d < m->ndof; ++d) diag[d] = m->diag_pos[d] >= 0 ? v[m->diag_pos[d]] : 0.0;
-  if (max_elem_stiff) {
-    std::vector<double> ev(m->n_ev);
-    JFG_CUDA(cudaMemcpy(ev.data(), m->d_ev, sizeof(double) * m->n_ev, cudaMemcpyDeviceToHost));
-    double mx = 0;
-    for (double x : ev) mx = std::max(mx, std::fabs(x));
-    *max_elem_stiff = mx;
-  }
-  return JFG_OK;
+  // gathered and reduced on the device: only ndof + 1 values cross to the host
+  return device_diag(m, diag, max_elem_stiff);
 }
 
 jfg_status jfg_get_node_blocks(jfg_model* m, double* blocks) {
   JFG_TRY(check_model(m));
   if (!m->values_ready) { set_error("values not assembled"); return JFG_NOT_READY; }
-  std::vector<double> v(m->nnz);
-  JFG_CUDA(cudaMemcpy(v.data(), m->d_nzval, sizeof(double) * m->nnz, cudaMemcpyDeviceToHost));
-  for (int64_t n = 0; n < m->n_nodes; ++n)
-    for (int off = 0; off < 2; ++off)
-      for (int b = 0; b < 3; ++b) {
-        int64_t col = 6 * n + 3 * off + b;
-        for (int a = 0; a < 3; ++a) {
-          int64_t row = 6 * n + 3 * off + a;
-          double val = 0.0;
-          const int32_t* beg = m->rowval.data() + m->colptr[col];
-          const int32_t* end = m->rowval.data() + m->colptr[col + 1];
-          const int32_t* f = std::lower_bound(beg, end, (int32_t)row);
-          if (f != end && *f == row) val = v[m->colptr[col] + (f - beg)];
-          blocks[18 * n + 9 * off + a + 3 * b] = val;
-        }
-      }
-  return JFG_OK;
+  if (!blocks) { set_error("null output"); return JFG_BAD_INPUT; }
+  return device_node_blocks(m, blocks);
 }
 
 jfg_status jfg_get_element_matrix(jfg_model* m, int32_t kind, int64_t elem, double* Ke) {
@@ -422,15 +406,18 @@ jfg_status jfg_set_free_dofs(jfg_model* m, int64_t n_free, const int32_t* free_d
   if (m->has_sym_cache && (int64_t)m->sym_cache_free.size() == n_free &&
       std::equal(m->sym_cache_free.begin(), m->sym_cache_free.end(), free_dofs)) {
     // the shared analysis of this mesh and free set
-    m->sym = std::move(m->sym_cache);
-    m->sym_cache = Symbolic();
+    m->symp = std::move(m->sym_cache);
+    m->sym_cache.reset();
     m->has_sym_cache = false;
     std::vector<int32_t>().swap(m->sym_cache_free);
   } else {
     SymbolicOptions opt = SymbolicOptions::from_env();
+    auto S = std::make_shared<Symbolic>();
     std::string e =
-        analyze(m->ndof, m->colptr.data(), m->rowval.data(), n_free, free_dofs, m->h_xyz.data(), opt, m->sym);
+        analyze(m->ndof, m->pat->colptr.data(), m->pat->rowval.data(), n_free, free_dofs, m->h_xyz.data(), opt, *S);
     if (!e.empty()) { set_error(e); return JFG_BAD_INPUT; }
+    sort_level_lists(*S);   // the analysis is read-only from here on
+    m->symp = std::move(S);
   }
   JFG_TRY(numeric_create(m));
   m->sym_ready = true;
@@ -455,17 +442,15 @@ jfg_status jfg_model_share_structure(jfg_model* dst, const jfg_model* src) {
   const int64_t ndof = dst->ndof, nnz = src->nnz;
   dst->nnz = nnz;
   dst->n_trip = src->n_trip;
-  dst->colptr = src->colptr;
-  dst->rowval = src->rowval;
-  dst->slot = src->slot;
-  dst->diag_pos = src->diag_pos;
+  dst->pat = src->pat;   // read-only once built: shared, not copied
   JFG_TRY(dev_alloc(c, (void**)&dst->d_colptr, sizeof(int64_t) * (ndof + 1)));
   JFG_TRY(dev_alloc(c, (void**)&dst->d_rowval, sizeof(int32_t) * nnz));
   JFG_TRY(dev_alloc(c, (void**)&dst->d_nzptr, sizeof(int32_t) * (nnz + 1)));
   JFG_TRY(dev_alloc(c, (void**)&dst->d_trip, sizeof(int32_t) * dst->n_trip));
   JFG_TRY(dev_alloc(c, (void**)&dst->d_tpos, sizeof(int64_t) * nnz));
   JFG_TRY(dev_alloc(c, (void**)&dst->d_nzval, sizeof(double) * nnz));
-  JFG_TRY(up(c, dst->diag_pos, &dst->d_diag_pos));
+  JFG_TRY(up(c, dst->pat->diag_pos, &dst->d_diag_pos));
+  JFG_CUDA(cudaStreamSynchronize(cudaStreamLegacy));   // the pageable upload above
   cudaStream_t st = dst->stream;
   JFG_CUDA(cudaMemcpyAsync(dst->d_colptr, src->d_colptr, sizeof(int64_t) * (ndof + 1), cudaMemcpyDeviceToDevice, st));
   JFG_CUDA(cudaMemcpyAsync(dst->d_rowval, src->d_rowval, sizeof(int32_t) * nnz, cudaMemcpyDeviceToDevice, st));
@@ -475,11 +460,11 @@ jfg_status jfg_model_share_structure(jfg_model* dst, const jfg_model* src) {
   JFG_CUDA(cudaStreamSynchronize(st));
   dst->pattern_built = true;
   if (src->sym_ready) {
-    dst->sym_cache = src->sym;
+    dst->sym_cache = src->symp;
     dst->sym_cache_free.clear();
-    dst->sym_cache_free.reserve(src->sym.n);
+    dst->sym_cache_free.reserve(src->sym().n);
     for (int64_t d = 0; d < ndof; ++d)
-      if (src->sym.gdof_to_perm[d] >= 0) dst->sym_cache_free.push_back((int32_t)d);
+      if (src->sym().gdof_to_perm[d] >= 0) dst->sym_cache_free.push_back((int32_t)d);
     dst->has_sym_cache = true;
   }
   return JFG_OK;
@@ -488,19 +473,19 @@ jfg_status jfg_model_share_structure(jfg_model* dst, const jfg_model* src) {
 jfg_status jfg_get_symbolic_info(jfg_model* m, jfg_symbolic_info* info) {
   JFG_TRY(check_model(m));
   if (!m->sym_ready) { set_error("no symbolic analysis"); return JFG_NOT_READY; }
-  info->n_supernodes = m->sym.ns;
-  info->n_levels = m->sym.n_levels;
-  info->nnz_L = m->sym.nnz_L;
-  info->flops = m->sym.flops;
-  info->factor_bytes = 8 * m->sym.nnz_L;
-  info->max_front = m->sym.max_front;
+  info->n_supernodes = m->sym().ns;
+  info->n_levels = m->sym().n_levels;
+  info->nnz_L = m->sym().nnz_L;
+  info->flops = m->sym().flops;
+  info->factor_bytes = 8 * m->sym().nnz_L;
+  info->max_front = m->sym().max_front;
   return JFG_OK;
 }
 
 jfg_status jfg_get_perm(jfg_model* m, int32_t* perm) {
   JFG_TRY(check_model(m));
   if (!m->sym_ready) { set_error("no symbolic analysis"); return JFG_NOT_READY; }
-  std::memcpy(perm, m->sym.perm_free.data(), sizeof(int32_t) * m->sym.n);
+  std::memcpy(perm, m->sym().perm_free.data(), sizeof(int32_t) * m->sym().n);
   return JFG_OK;
 }
 

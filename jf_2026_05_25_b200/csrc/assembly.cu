@@ -14,6 +14,8 @@
 
 #include <algorithm>
 
+#include <cstring>
+
 #include "jfg_internal.h"
 
 namespace jfg {
@@ -119,6 +121,96 @@ __global__ void k_residual_dd(int64_t n, const int64_t* __restrict__ colptr, con
 
 }  // namespace
 
+namespace {
+
+__global__ void k_gather_diag(int64_t ndof, const int64_t* __restrict__ diag_pos, const double* __restrict__ nzval,
+                              double* __restrict__ out) {
+  const int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (d < ndof) out[d] = diag_pos[d] >= 0 ? nzval[diag_pos[d]] : 0.0;
+}
+
+// max |v| over n values: per-thread maxima, a warp reduction, one atomic
+// per warp on the bit pattern (non-negative doubles order like their bits)
+__global__ void k_absmax(int64_t n, const double* __restrict__ v, unsigned long long* __restrict__ out) {
+  double mx = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    mx = fmax(mx, fabs(v[i]));
+  for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(mx));
+}
+
+// the 3 x 3 translational and rotational diagonal blocks of every grid:
+// thread (node, entry) finds its row in its column by bisection
+__global__ void k_node_blocks(int64_t n_nodes, const int64_t* __restrict__ colptr, const int32_t* __restrict__ rowval,
+                              const double* __restrict__ nzval, double* __restrict__ out) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 18 * n_nodes) return;
+  const int64_t n = t / 18;
+  const int k = (int)(t - 18 * n), off = k / 9, a = k % 3, b = (k % 9) / 3;
+  const int64_t col = 6 * n + 3 * off + b, row = 6 * n + 3 * off + a;
+  int64_t lo = colptr[col], hi = colptr[col + 1];
+  double val = 0.0;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    const int32_t r = rowval[mid];
+    if (r == row) { val = nzval[mid]; break; }
+    if (r < row) lo = mid + 1; else hi = mid;
+  }
+  out[t] = val;
+}
+
+}  // namespace
+
+jfg_status device_diag(jfg_model* m, double* diag, double* max_elem_stiff) {
+  cudaStream_t st = m->stream;
+  double* d = nullptr;
+  unsigned long long* mx = nullptr;
+  JFG_TRY(dev_alloc(m->ctx, (void**)&d, sizeof(double) * std::max<int64_t>(m->ndof, 1) + 64));
+  mx = reinterpret_cast<unsigned long long*>(d + std::max<int64_t>(m->ndof, 1));
+  jfg_status s = JFG_OK;
+  if (cudaMemsetAsync(mx, 0, sizeof(unsigned long long), st) != cudaSuccess) s = JFG_CUDA_ERROR;
+  if (s == JFG_OK && diag) {
+    k_gather_diag<<<(unsigned)((m->ndof + 255) / 256), 256, 0, st>>>(m->ndof, m->d_diag_pos, m->d_nzval, d);
+    count_launch();
+  }
+  if (s == JFG_OK && max_elem_stiff && m->n_ev > 0) {
+    const int64_t blocks = std::min<int64_t>((m->n_ev + 255) / 256, 148 * 16);
+    k_absmax<<<(unsigned)blocks, 256, 0, st>>>(m->n_ev, m->d_ev, mx);
+    count_launch();
+  }
+  unsigned long long bits = 0;
+  if (s == JFG_OK && (cudaGetLastError() != cudaSuccess ||
+                      (diag && cudaMemcpyAsync(diag, d, sizeof(double) * m->ndof, cudaMemcpyDeviceToHost, st) != cudaSuccess) ||
+                      cudaMemcpyAsync(&bits, mx, sizeof(bits), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                      cudaStreamSynchronize(st) != cudaSuccess))
+    s = JFG_CUDA_ERROR;
+  dev_free(m->ctx, d, sizeof(double) * std::max<int64_t>(m->ndof, 1) + 64);
+  if (s != JFG_OK) { set_error("device diagonal / element maximum failed"); return s; }
+  if (max_elem_stiff) {
+    double v;
+    std::memcpy(&v, &bits, sizeof v);
+    *max_elem_stiff = v;
+  }
+  return JFG_OK;
+}
+
+jfg_status device_node_blocks(jfg_model* m, double* blocks) {
+  cudaStream_t st = m->stream;
+  const int64_t len = 18 * m->n_nodes;
+  double* d = nullptr;
+  JFG_TRY(dev_alloc(m->ctx, (void**)&d, sizeof(double) * std::max<int64_t>(len, 1)));
+  k_node_blocks<<<(unsigned)((len + 255) / 256), 256, 0, st>>>(m->n_nodes, m->d_colptr, m->d_rowval, m->d_nzval, d);
+  count_launch();
+  jfg_status s = JFG_OK;
+  if (cudaGetLastError() != cudaSuccess ||
+      cudaMemcpyAsync(blocks, d, sizeof(double) * len, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    s = JFG_CUDA_ERROR;
+  dev_free(m->ctx, d, sizeof(double) * std::max<int64_t>(len, 1));
+  if (s != JFG_OK) set_error("device node blocks failed");
+  return s;
+}
+
 void residual_dd(const jfg_model* m, int nrhs, const double* x, const double* f, double* r, cudaStream_t st) {
   int64_t threads = m->ndof * 32;
   int64_t blocks = (threads + 255) / 256;
@@ -217,7 +309,7 @@ jfg_status build_pattern(jfg_model* m) {
     out.resize(w);
   };
   // pass 1: column counts
-  m->colptr.assign(ndof + 1, 0);
+  m->pat->colptr.assign(ndof + 1, 0);
 #pragma omp parallel
   {
     std::vector<Blk> blk;
@@ -228,15 +320,15 @@ jfg_status build_pattern(jfg_model* m) {
         int64_t cnt = 0;
         for (auto& x : blk)
           for (int i = 0; i < 6; ++i) cnt += (x.mask >> (i + 6 * j)) & 1;
-        m->colptr[6 * b + j + 1] = cnt;
+        m->pat->colptr[6 * b + j + 1] = cnt;
       }
     }
   }
-  for (int64_t j = 0; j < ndof; ++j) m->colptr[j + 1] += m->colptr[j];
-  const int64_t nnz = m->colptr[ndof];
+  for (int64_t j = 0; j < ndof; ++j) m->pat->colptr[j + 1] += m->pat->colptr[j];
+  const int64_t nnz = m->pat->colptr[ndof];
   m->nnz = nnz;
-  m->rowval.resize(nnz);
-  m->diag_pos.assign(ndof, -1);
+  m->pat->rowval.resize(nnz);
+  m->pat->diag_pos.assign(ndof, -1);
   m->n_trip = 576 * nq4 + 324 * nt3 + 900 * nt10 + q8off[nq8];
   if (m->n_trip >= (int64_t)INT32_MAX || m->n_ev >= (int64_t)INT32_MAX) {
     set_error("triplet count exceeds the 32-bit slot-map range");
@@ -251,12 +343,12 @@ jfg_status build_pattern(jfg_model* m) {
     for (int64_t b = 0; b < nn; ++b) {
       node_blocks(b, blk);
       for (int j = 0; j < 6; ++j) {
-        int64_t q = m->colptr[6 * b + j];
+        int64_t q = m->pat->colptr[6 * b + j];
         for (auto& x : blk)
           for (int i = 0; i < 6; ++i) {
             if (!((x.mask >> (i + 6 * j)) & 1)) continue;
-            m->rowval[q] = 6 * x.a + i;
-            if (x.a == b && i == j) m->diag_pos[6 * b + j] = q;
+            m->pat->rowval[q] = 6 * x.a + i;
+            if (x.a == b && i == j) m->pat->diag_pos[6 * b + j] = q;
             // contributions: incident elements of b that contain node a and
             // cover the (i, j) component pair
             int32_t c = 0;
@@ -281,7 +373,7 @@ jfg_status build_pattern(jfg_model* m) {
     return JFG_BAD_INPUT;
   }
   std::vector<int32_t> trip(m->n_trip);
-  m->slot.assign(m->n_trip, -1);
+  m->pat->slot.assign(m->n_trip, -1);
   // pass 3: contributions in triplet (element) order, and the slot map
 #pragma omp parallel
   {
@@ -290,7 +382,7 @@ jfg_status build_pattern(jfg_model* m) {
     for (int64_t b = 0; b < nn; ++b) {
       node_blocks(b, blk);
       for (int j = 0; j < 6; ++j) {
-        int64_t q = m->colptr[6 * b + j];
+        int64_t q = m->pat->colptr[6 * b + j];
         for (auto& x : blk)
           for (int i = 0; i < 6; ++i) {
             if (!((x.mask >> (i + 6 * j)) & 1)) continue;
@@ -328,7 +420,7 @@ jfg_status build_pattern(jfg_model* m) {
                 src = m->ev_q8_off + 2304 * e8 + rr + 48 * cc;
               }
               trip[w++] = (int32_t)src;
-              m->slot[t] = q;
+              m->pat->slot[t] = q;
             }
             ++q;
           }
@@ -339,12 +431,12 @@ jfg_status build_pattern(jfg_model* m) {
   std::vector<int64_t> tpos(nnz);
 #pragma omp parallel for schedule(dynamic, 4096)
   for (int64_t j = 0; j < ndof; ++j)
-    for (int64_t p = m->colptr[j]; p < m->colptr[j + 1]; ++p) {
-      int64_t i = m->rowval[p];
-      const int32_t* beg = m->rowval.data() + m->colptr[i];
-      const int32_t* end = m->rowval.data() + m->colptr[i + 1];
+    for (int64_t p = m->pat->colptr[j]; p < m->pat->colptr[j + 1]; ++p) {
+      int64_t i = m->pat->rowval[p];
+      const int32_t* beg = m->pat->rowval.data() + m->pat->colptr[i];
+      const int32_t* end = m->pat->rowval.data() + m->pat->colptr[i + 1];
       const int32_t* f = std::lower_bound(beg, end, (int32_t)j);
-      tpos[p] = (f != end && *f == j) ? m->colptr[i] + (f - beg) : -1;
+      tpos[p] = (f != end && *f == j) ? m->pat->colptr[i] + (f - beg) : -1;
     }
   for (int64_t p = 0; p < nnz; ++p)
     if (tpos[p] < 0) {
@@ -358,8 +450,8 @@ jfg_status build_pattern(jfg_model* m) {
   JFG_TRY(dev_alloc(c, (void**)&m->d_trip, sizeof(int32_t) * m->n_trip));
   JFG_TRY(dev_alloc(c, (void**)&m->d_tpos, sizeof(int64_t) * nnz));
   JFG_TRY(dev_alloc(c, (void**)&m->d_nzval, sizeof(double) * nnz));
-  JFG_CUDA(cudaMemcpy(m->d_colptr, m->colptr.data(), sizeof(int64_t) * (ndof + 1), cudaMemcpyHostToDevice));
-  JFG_CUDA(cudaMemcpy(m->d_rowval, m->rowval.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice));
+  JFG_CUDA(cudaMemcpy(m->d_colptr, m->pat->colptr.data(), sizeof(int64_t) * (ndof + 1), cudaMemcpyHostToDevice));
+  JFG_CUDA(cudaMemcpy(m->d_rowval, m->pat->rowval.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice));
   JFG_CUDA(cudaMemcpy(m->d_nzptr, cnt.data(), sizeof(int32_t) * (nnz + 1), cudaMemcpyHostToDevice));
   JFG_CUDA(cudaMemcpy(m->d_trip, trip.data(), sizeof(int32_t) * m->n_trip, cudaMemcpyHostToDevice));
   JFG_CUDA(cudaMemcpy(m->d_tpos, tpos.data(), sizeof(int64_t) * nnz, cudaMemcpyHostToDevice));

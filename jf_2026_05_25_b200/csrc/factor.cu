@@ -205,6 +205,27 @@ __global__ void k_scatter_A(int64_t na, const int32_t* __restrict__ src, const i
   L[dst[k]] = (T)v;
 }
 
+// (permuted row, permuted column) of each K_ff entry's front slot d: the
+// owning supernode s is the last with Lptr[s] <= d; the slot is row
+// (d - Lptr[s]) mod m_s, column (d - Lptr[s]) div m_s of its front
+__global__ void k_amap_rowcol(int64_t na, int64_t ns, const int64_t* __restrict__ dst, const int64_t* __restrict__ Lptr,
+                              const int32_t* __restrict__ mrows, const int64_t* __restrict__ rows_ptr,
+                              const int32_t* __restrict__ rows, const int32_t* __restrict__ first,
+                              int32_t* __restrict__ pr, int32_t* __restrict__ pc) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= na) return;
+  const int64_t d = dst[q];
+  int64_t lo = 0, hi = ns;   // upper_bound(Lptr[0..ns], d) - 1
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (Lptr[mid] <= d) lo = mid + 1; else hi = mid;
+  }
+  const int64_t s = lo - 1;
+  const int64_t mm = mrows[s], off = d - Lptr[s];
+  pr[q] = rows[rows_ptr[s] + off % mm];
+  pc[q] = first[s] + (int32_t)(off / mm);
+}
+
 __global__ void k_diag_scale(int64_t n, const int32_t* __restrict__ perm_dof, const int64_t* __restrict__ diag_pos,
                              const double* __restrict__ nzval, double* __restrict__ scale) {
   int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1449,7 +1470,7 @@ __global__ void k_diag_of_factor32(int64_t ns, const int32_t* first, const int32
 }
 
 template <typename T>
-void upload(std::vector<T>& h, T** d, jfg_ctx* c, jfg_status& st) {
+void upload(const std::vector<T>& h, T** d, jfg_ctx* c, jfg_status& st) {
   if (st != JFG_OK) return;
   size_t bytes = sizeof(T) * std::max<size_t>(h.size(), 1);
   st = dev_alloc(c, (void**)d, bytes);
@@ -1473,7 +1494,7 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
     JFG_CUDA(cudaFuncSetAttribute(k_trsm_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     attr_set = true;
   }
-  const Symbolic& S = m->sym;
+  const Symbolic& S = m->sym();
   const int tc_min = tc_min_dim();
   for (const auto& lv : F->levels) {
     const int32_t* list = F->level_sn + lv.off;
@@ -1623,7 +1644,7 @@ jfg_status strip_inverses(NumericFactor* F, const T* Lf, const T* Dvf, T* Svf, c
 
 template <typename T, int NRC>
 void solve_inner_n(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int nr, cudaStream_t st) {
-  const Symbolic& S = m->sym;
+  const Symbolic& S = m->sym();
   int64_t n = S.n;
   int ps = prof_start(st);
   // forward, leaves first
@@ -1721,7 +1742,7 @@ jfg_status ensure_workspace(jfg_model* m, NumericFactor* F, int nrhs) {
     if (p) dev_free(c, p, sizeof(double) * len);
     p = nullptr;
   };
-  int64_t n = m->sym.n, ndof = m->ndof;
+  int64_t n = m->sym().n, ndof = m->ndof;
   drop_solve_graphs(F);
   if (F->nrhs_cap > 0) {
     int oc = F->nrhs_cap;
@@ -1776,11 +1797,18 @@ jfg_status coldot(NumericFactor* F, int64_t len, int nr, const double* a, const 
 // still active at a column step are a prefix of the level's list and each
 // step launches only them.
 static void sort_levels(const Symbolic& S, std::vector<int32_t>& level_sn) {
+  if (S.n_levels == 0) return;
   for (int64_t l = 0; l < S.n_levels; ++l)
     std::sort(level_sn.begin() + S.level_ptr[l], level_sn.begin() + S.level_ptr[l + 1], [&](int32_t x, int32_t y) {
       const int32_t cx = S.sn_first[x + 1] - S.sn_first[x], cy = S.sn_first[y + 1] - S.sn_first[y];
       return cx != cy ? cx > cy : x < y;
     });
+}
+
+void sort_level_lists(Symbolic& S) {
+  std::vector<int32_t> lsn = S.level_sn;
+  sort_levels(S, lsn);
+  S.level_sn.swap(lsn);
 }
 
 // Host launch metadata of every level and the tile lists of its launches
@@ -1933,12 +1961,11 @@ jfg_status numeric_create(jfg_model* m) {
   JFG_TRY(solve_attributes());
   NumericFactor* F = new NumericFactor();
   m->num = F;
-  Symbolic& S = m->sym;
+  const Symbolic& S = m->sym();   // level lists sorted by sort_level_lists
   jfg_ctx* c = m->ctx;
   jfg_status st = JFG_OK;
   upload(S.sn_first, &F->first, c, st);
   upload(S.sn_m, &F->mrows, c, st);
-  sort_levels(S, S.level_sn);
   upload(S.level_sn, &F->level_sn, c, st);
   upload(S.ea_child, &F->ea_child, c, st);
   upload(S.rel, &F->rel, c, st);
@@ -1951,25 +1978,28 @@ jfg_status numeric_create(jfg_model* m) {
   upload(S.sn_rows_ptr, &F->rows_ptr, c, st);
   upload(S.sn_relptr, &F->relptr, c, st);
   upload(S.amap_dst, &F->amap_dst, c, st);
-  // permuted (row, col) of every scattered entry, for the mixed scaling
-  {
-    std::vector<int32_t> pr(S.amap_dst.size()), pc(S.amap_dst.size());
-    std::vector<int32_t> col_of(S.n);
-    for (int64_t s = 0; s < S.ns; ++s)
-      for (int64_t k = S.sn_first[s]; k < S.sn_first[s + 1]; ++k) col_of[k] = (int32_t)s;
-    // decode dst -> (front row, front col) through the supernode that owns it
-    std::vector<int64_t> Lp = S.sn_Lptr;
-    for (size_t q = 0; q < S.amap_dst.size(); ++q) {
-      int64_t d = S.amap_dst[q];
-      int64_t s = std::upper_bound(Lp.begin(), Lp.end(), d) - Lp.begin() - 1;
-      int64_t mm = S.sn_m[s];
-      int64_t off = d - Lp[s];
-      int64_t ri = off % mm, cj = off / mm;
-      pr[q] = S.rows[S.sn_rows_ptr[s] + ri];
-      pc[q] = S.sn_first[s] + (int32_t)cj;
+  // the pageable copies above run on the legacy stream and may still be in
+  // flight when cudaMemcpy returns: finish them before the model's own
+  // (non-blocking) stream reads the arrays
+  if (st == JFG_OK && cudaStreamSynchronize(cudaStreamLegacy) != cudaSuccess) {
+    set_error("uploading symbolic arrays failed");
+    st = JFG_CUDA_ERROR;
+  }
+  // permuted (row, col) of every scattered entry, for the mixed scaling:
+  // decoded on the device from the front slot through its supernode
+  if (st == JFG_OK) {
+    const int64_t na = (int64_t)S.amap_dst.size();
+    if ((st = dev_alloc(c, (void**)&F->amap_pr, sizeof(int32_t) * std::max<int64_t>(na, 1))) == JFG_OK &&
+        (st = dev_alloc(c, (void**)&F->amap_pc, sizeof(int32_t) * std::max<int64_t>(na, 1))) == JFG_OK && na > 0) {
+      k_amap_rowcol<<<(unsigned)((na + 255) / 256), 256, 0, m->stream>>>(na, S.ns, F->amap_dst, F->Lptr, F->mrows,
+                                                                       F->rows_ptr, F->rows, F->first, F->amap_pr,
+                                                                       F->amap_pc);
+      count_launch();
+      if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(m->stream) != cudaSuccess) {
+        set_error("decoding the scatter map failed");
+        st = JFG_CUDA_ERROR;
+      }
     }
-    upload(pr, &F->amap_pr, c, st);
-    upload(pc, &F->amap_pc, c, st);
   }
   if (st != JFG_OK) return st;
   F->n_amap = (int64_t)S.amap_dst.size();
@@ -2039,6 +2069,7 @@ jfg_status numeric_create(jfg_model* m) {
   JFG_TRY(dev_alloc(c, (void**)&F->norms, sizeof(double) * (256 * 64 + 64)));
   JFG_CUDA(cudaEventCreate(&F->ev0));
   JFG_CUDA(cudaEventCreate(&F->ev1));
+  JFG_CUDA(cudaStreamSynchronize(cudaStreamLegacy));   // the pageable uploads and memsets above
   return JFG_OK;
 }
 
@@ -2046,7 +2077,7 @@ void numeric_destroy(jfg_model* m) {
   NumericFactor* F = m->num;
   if (!F) return;
   jfg_ctx* c = m->ctx;
-  const Symbolic& S = m->sym;
+  const Symbolic& S = m->sym();
   auto fr = [&](void* p, size_t b) { if (p) dev_free(c, p, b); };
   fr(F->first, 4 * (S.ns + 1)); fr(F->mrows, 4 * S.ns); fr(F->level_sn, 4 * S.ns);
   fr(F->ea_child, 4 * std::max<size_t>(S.ea_child.size(), 1)); fr(F->rel, 4 * std::max<size_t>(S.rel.size(), 1));
@@ -2093,7 +2124,7 @@ jfg_status numeric_factor_enqueue(jfg_model* m, int precision) {
   NumericFactor* F = m->num;
   if (!F || !m->sym_ready) { set_error("factor before symbolic analysis"); return JFG_NOT_READY; }
   if (!m->values_ready) { set_error("factor before assembly"); return JFG_NOT_READY; }
-  const Symbolic& S = m->sym;
+  const Symbolic& S = m->sym();
   jfg_ctx* c = m->ctx;
   cudaStream_t st = m->stream;
   int64_t ublk = std::max<int64_t>(S.u_arena, 1);
@@ -2194,7 +2225,7 @@ jfg_status numeric_factor_enqueue(jfg_model* m, int precision) {
 // sides have run (each allocation mirrored from numeric_create,
 // numeric_factor_enqueue and ensure_workspace).
 void numeric_bytes(jfg_model* m, int precision, int nrhs, int64_t* now, int64_t* peak) {
-  const Symbolic& S = m->sym;
+  const Symbolic& S = m->sym();
   NumericFactor* F = m->num;
   const int64_t ns = S.ns, n = S.n, ndof = m->ndof, na = (int64_t)S.amap_dst.size();
   int64_t base = 4 * (ns + 1) + 4 * ns + 4 * ns + 4 * std::max<int64_t>((int64_t)S.ea_child.size(), 1) +
@@ -2289,7 +2320,7 @@ jfg_status numeric_apply(jfg_model* m, int nrhs, const double* Fd, double* Ud, i
   if (nrhs <= 0) { set_error("nrhs must be positive"); return JFG_BAD_INPUT; }
   const bool use32 = precision == JFG_PREC_MIXED;
   if ((use32 && !F->L32) || (!use32 && !F->L64)) { set_error("apply before factorisation"); return JFG_NOT_READY; }
-  const Symbolic& S = m->sym;
+  const Symbolic& S = m->sym();
   cudaStream_t st = m->stream;
   const int64_t n = S.n, ndof = m->ndof;
   const unsigned gn = (unsigned)((n + 255) / 256);
@@ -2315,7 +2346,7 @@ jfg_status numeric_apply(jfg_model* m, int nrhs, const double* Fd, double* Ud, i
 jfg_status numeric_factor_diag(jfg_model* m, double* out) {
   NumericFactor* F = m->num;
   if (!F || !(F->have64 || F->have32)) { set_error("no factor"); return JFG_NOT_READY; }
-  const Symbolic& S = m->sym;
+  const Symbolic& S = m->sym();
   cudaStream_t st = m->stream;
   double* d = nullptr;
   JFG_TRY(dev_alloc(m->ctx, (void**)&d, sizeof(double) * std::max<int64_t>(S.n, 1)));
@@ -2343,7 +2374,7 @@ jfg_status numeric_solve(jfg_model* m, int nrhs, const double* hF, double* hU, d
   if (nrhs <= 0) { set_error("nrhs must be positive"); return JFG_BAD_INPUT; }
   if (tol <= 0) tol = 1e-10;
   if (max_ir < 0) max_ir = 30;
-  const Symbolic& S = m->sym;
+  const Symbolic& S = m->sym();
   jfg_ctx* c = m->ctx;
   cudaStream_t st = m->stream;
   const int64_t n = S.n, ndof = m->ndof;

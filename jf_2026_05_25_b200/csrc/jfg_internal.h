@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -119,6 +120,16 @@ struct jfg_ctx {
 
 struct NumericFactor;   // defined in factor.cu
 
+namespace jfg {
+// CSC pattern and slot map on the host (built once per mesh)
+struct HostPattern {
+  std::vector<int64_t> colptr;
+  std::vector<int32_t> rowval;
+  std::vector<int64_t> slot;        // triplet -> nz position
+  std::vector<int64_t> diag_pos;    // ndof, -1 when structurally absent
+};
+}  // namespace jfg
+
 struct jfg_model {
   jfg_ctx* ctx = nullptr;
   // the model's own stream: models of one context may be driven from
@@ -139,10 +150,8 @@ struct jfg_model {
   // pattern + slot map (built once)
   bool pattern_built = false;
   int64_t nnz = 0, n_trip = 0;
-  std::vector<int64_t> colptr;
-  std::vector<int32_t> rowval;
-  std::vector<int64_t> slot;        // triplet -> nz position
-  std::vector<int64_t> diag_pos;    // ndof, -1 when structurally absent
+  // host pattern: shared (read-only once built) by the models of one mesh
+  std::shared_ptr<jfg::HostPattern> pat = std::make_shared<jfg::HostPattern>();
   int64_t* d_diag_pos = nullptr;
   int64_t* d_colptr = nullptr;
   int32_t* d_rowval = nullptr;
@@ -153,12 +162,15 @@ struct jfg_model {
   bool values_ready = false;
   // symbolic
   bool sym_ready = false;
-  jfg::Symbolic sym;
+  // the analysis (read-only once made; shared by the models of one mesh and
+  // free set)
+  std::shared_ptr<const jfg::Symbolic> symp = std::make_shared<jfg::Symbolic>();
+  const jfg::Symbolic& sym() const { return *symp; }
   // analysis of the same mesh taken over from another model
   // (jfg_model_share_structure): used by jfg_set_free_dofs when its free set
   // is the one this analysis was made for
   std::vector<int32_t> sym_cache_free;
-  jfg::Symbolic sym_cache;
+  std::shared_ptr<const jfg::Symbolic> sym_cache;
   bool has_sym_cache = false;
   NumericFactor* num = nullptr;
   // asynchronous calls (jfg_*_async): the caller's stream waits on aev_out;
@@ -174,6 +186,13 @@ namespace jfg {
 
 // elements.cu
 jfg_status launch_elements(jfg_model* m, cudaStream_t st);
+// assembly.cu: diag(K), max |element entry| and the grids' 3 x 3 diagonal
+// blocks, computed on the device (host outputs)
+jfg_status device_diag(jfg_model* m, double* diag, double* max_elem_stiff);
+jfg_status device_node_blocks(jfg_model* m, double* blocks);
+// factor.cu: fronts of each level listed by decreasing width (then index),
+// as the level launches expect; done once, right after the analysis
+void sort_level_lists(Symbolic& S);
 jfg_status launch_elements_into(const jfg_model* m, cudaStream_t st, double* ev, double* q4prep, DevError* err);
 // CTRIA3 element matrices (324 doubles each, column-major) into ev
 jfg_status launch_t3(const jfg_model* m, cudaStream_t st, double* ev, DevError* err);

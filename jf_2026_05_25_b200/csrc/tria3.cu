@@ -31,21 +31,36 @@ __device__ inline void t3_record_error(DevError* err, int32_t code, int64_t idx)
   if (atomicCAS(&err->code, 0, code) == 0) err->index = idx;
 }
 
-// inverse of a symmetric 3 x 3 (col-major) by cofactors; false if singular
-__device__ inline bool inv3(const double* M, double* X) {
-  const double c00 = M[4] * M[8] - M[7] * M[5], c01 = M[7] * M[2] - M[1] * M[8], c02 = M[1] * M[5] - M[4] * M[2];
-  const double det = M[0] * c00 + M[3] * c01 + M[6] * c02;
-  if (!(det != 0.0) || !isfinite(det)) return false;
-  const double id = 1.0 / det;
-  X[0] = c00 * id;
-  X[1] = c01 * id;
-  X[2] = c02 * id;
-  X[3] = (M[6] * M[5] - M[3] * M[8]) * id;
-  X[4] = (M[0] * M[8] - M[6] * M[2]) * id;
-  X[5] = (M[3] * M[2] - M[0] * M[5]) * id;
-  X[6] = (M[3] * M[7] - M[6] * M[4]) * id;
-  X[7] = (M[6] * M[1] - M[0] * M[7]) * id;
-  X[8] = (M[0] * M[4] - M[3] * M[1]) * id;
+// inverse of a 3 x 3 (col-major) by Gauss-Jordan elimination with partial
+// pivoting (the flexibilities inverted here are ill-conditioned on slivers;
+// elimination keeps the backward error at the level of one rounding);
+// false if singular
+__device__ inline bool inv3(const double* A, double* X) {
+  double M[9];
+  for (int q = 0; q < 9; ++q) { M[q] = A[q]; X[q] = (q % 4 == 0) ? 1.0 : 0.0; }
+  for (int k = 0; k < 3; ++k) {
+    int p = k;
+    double best = fabs(M[k + 3 * k]);
+    for (int i = k + 1; i < 3; ++i)
+      if (fabs(M[i + 3 * k]) > best) { best = fabs(M[i + 3 * k]); p = i; }
+    if (best == 0.0 || !isfinite(best)) return false;
+    if (p != k)
+      for (int j = 0; j < 3; ++j) {
+        double t = M[k + 3 * j]; M[k + 3 * j] = M[p + 3 * j]; M[p + 3 * j] = t;
+        t = X[k + 3 * j]; X[k + 3 * j] = X[p + 3 * j]; X[p + 3 * j] = t;
+      }
+    const double piv = M[k + 3 * k];
+    for (int j = 0; j < 3; ++j) { M[k + 3 * j] /= piv; X[k + 3 * j] /= piv; }
+    for (int i = 0; i < 3; ++i) {
+      if (i == k) continue;
+      const double f = M[i + 3 * k];
+      if (f == 0.0) continue;
+      for (int j = 0; j < 3; ++j) {
+        M[i + 3 * j] -= f * M[k + 3 * j];
+        X[i + 3 * j] -= f * X[k + 3 * j];
+      }
+    }
+  }
   return true;
 }
 
