@@ -1469,8 +1469,8 @@ __global__ void k_diag_of_factor32(int64_t ns, const int32_t* first, const int32
     out[f + j] = (double)L[Lptr[s] + j + (int64_t)m * j] / scale[f + j];
 }
 
-template <typename T>
-void upload(const std::vector<T>& h, T** d, jfg_ctx* c, jfg_status& st) {
+template <typename T, typename A>
+void upload(const std::vector<T, A>& h, T** d, jfg_ctx* c, jfg_status& st) {
   if (st != JFG_OK) return;
   size_t bytes = sizeof(T) * std::max<size_t>(h.size(), 1);
   st = dev_alloc(c, (void**)d, bytes);

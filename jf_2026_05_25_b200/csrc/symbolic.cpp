@@ -208,29 +208,35 @@ std::string analyze(int64_t ndof, const int64_t* colptr, const int32_t* rowval, 
   NodeGraph g;
   g.ptr.assign(n_nodes + 1, 0);
   {
-    std::vector<int64_t> mark(n_nodes, -1);
+    // two passes (count, fill) over the nodes; each node writes only its
+    // own count and adjacency segment, so nodes run in parallel with a
+    // thread-local mark array
     for (int pass = 0; pass < 2; ++pass) {
-      std::fill(mark.begin(), mark.end(), -1);
-      std::vector<int64_t> fill_pos;
       if (pass == 1) {
         for (int64_t b = 0; b < n_nodes; ++b) g.ptr[b + 1] += g.ptr[b];
         g.adj.resize(g.ptr[n_nodes]);
-        fill_pos.assign(g.ptr.begin(), g.ptr.end() - 1);
       }
-      for (int64_t b = 0; b < n_nodes; ++b) {
-        if (!nfree[b]) continue;
-        for (int c = 0; c < 6; ++c) {
-          int64_t j = 6 * b + c;
-          if (free_pos[j] < 0) continue;
-          for (int64_t p = colptr[j]; p < colptr[j + 1]; ++p) {
-            int64_t i = rowval[p];
-            if (free_pos[i] < 0) continue;
-            int64_t a = i / 6;
-            if (a == b || mark[a] == b) continue;
-            mark[a] = b;
-            if (pass == 0) g.ptr[b + 1]++;
-            else g.adj[fill_pos[b]++] = (int32_t)a;
+#pragma omp parallel
+      {
+        std::vector<int64_t> mark(n_nodes, -1);
+#pragma omp for schedule(dynamic, 1024)
+        for (int64_t b = 0; b < n_nodes; ++b) {
+          if (!nfree[b]) continue;
+          int64_t cnt = 0, at = pass == 1 ? g.ptr[b] : 0;
+          for (int c = 0; c < 6; ++c) {
+            int64_t j = 6 * b + c;
+            if (free_pos[j] < 0) continue;
+            for (int64_t p = colptr[j]; p < colptr[j + 1]; ++p) {
+              int64_t i = rowval[p];
+              if (free_pos[i] < 0) continue;
+              int64_t a = i / 6;
+              if (a == b || mark[a] == b) continue;
+              mark[a] = b;
+              if (pass == 0) ++cnt;
+              else g.adj[at++] = (int32_t)a;
+            }
           }
+          if (pass == 0) g.ptr[b + 1] = cnt;
         }
       }
     }
@@ -500,47 +506,52 @@ std::string analyze(int64_t ndof, const int64_t* colptr, const int32_t* rowval, 
   for (int64_t s = 0; s < ns; ++s)
     S.sn_relptr[s + 1] = S.sn_relptr[s] + (S.sn_m[s] - (S.sn_first[s + 1] - S.sn_first[s]));
   S.rel.assign(S.sn_relptr[ns], -1);
-  std::vector<int32_t> col2sn(n_free);
-  for (int64_t s = 0; s < ns; ++s)
-    for (int64_t k = S.sn_first[s]; k < S.sn_first[s + 1]; ++k) col2sn[k] = (int32_t)s;
-  // lower-permuted CSC of the upper triangle of K_ff, entries bucketed by their column
+  // lower-permuted CSC of K_ff: bucket c (permuted column c, global DOF
+  // perm_dof[c]) holds its entries of permuted row >= c, each with the
+  // position of its upper-triangle copy in K (row <= column); the pattern is
+  // structurally symmetric, so column perm_dof[c] lists them all.  Buckets
+  // are independent: both passes run in parallel over the columns.
+  const int32_t* g2p = S.gdof_to_perm.data();
   std::vector<int64_t> lp(n_free + 1, 0);
-  for (int64_t j = 0; j < ndof; ++j) {
-    int32_t pj = S.gdof_to_perm[j];
-    if (pj < 0) continue;
-    for (int64_t p = colptr[j]; p < colptr[j + 1]; ++p) {
-      int64_t i = rowval[p];
-      if (i > j) continue;
-      int32_t pi = S.gdof_to_perm[i];
-      if (pi < 0) continue;
-      lp[std::min(pi, pj) + 1]++;
-    }
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int64_t c = 0; c < n_free; ++c) {
+    const int64_t j = S.perm_dof[c];
+    int64_t cnt = 0;
+    for (int64_t p = colptr[j]; p < colptr[j + 1]; ++p)
+      if (g2p[rowval[p]] >= c) ++cnt;
+    lp[c + 1] = cnt;
   }
   for (int64_t k = 0; k < n_free; ++k) lp[k + 1] += lp[k];
-  std::vector<int32_t> lrow(lp[n_free]);
+  std::vector<int32_t, UninitAlloc<int32_t>> lrow(lp[n_free]);
   std::vector<int32_t> lsrc(lp[n_free]);
-  {
-    std::vector<int64_t> pos(lp.begin(), lp.end() - 1);
-    for (int64_t j = 0; j < ndof; ++j) {
-      int32_t pj = S.gdof_to_perm[j];
-      if (pj < 0) continue;
-      for (int64_t p = colptr[j]; p < colptr[j + 1]; ++p) {
-        int64_t i = rowval[p];
-        if (i > j) continue;
-        int32_t pi = S.gdof_to_perm[i];
-        if (pi < 0) continue;
-        int32_t c = std::min(pi, pj), r = std::max(pi, pj);
-        lrow[pos[c]] = r;
-        lsrc[pos[c]] = (int32_t)p;
-        pos[c]++;
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int64_t c = 0; c < n_free; ++c) {
+    const int64_t j = S.perm_dof[c];
+    int64_t q = lp[c];
+    for (int64_t p = colptr[j]; p < colptr[j + 1]; ++p) {
+      const int64_t i = rowval[p];
+      const int32_t pi = g2p[i];
+      if (pi < c) continue;
+      int64_t src = p;
+      if (i > j) {   // the upper-triangle copy is entry (j, i), in column i
+        const int32_t* b0 = rowval + colptr[i];
+        const int32_t* b1 = rowval + colptr[i + 1];
+        src = colptr[i] + (std::lower_bound(b0, b1, (int32_t)j) - b0);
       }
+      lrow[q] = pi;
+      lsrc[q] = (int32_t)src;
+      ++q;
     }
   }
-  S.amap_src.resize(lp[n_free]);
+  // scatter map (slot of every bucket entry in its supernode's front) and the
+  // child -> parent row maps, in parallel over supernodes; entry p of the
+  // buckets is entry p of the map, since supernodes own consecutive columns
   S.amap_dst.resize(lp[n_free]);
+  int bad = 0;
+#pragma omp parallel
   {
     std::vector<int32_t> rowidx(n_free, -1);
-    int64_t q = 0;
+#pragma omp for schedule(dynamic, 8) reduction(| : bad)
     for (int64_t s = 0; s < ns; ++s) {
       int64_t m = S.sn_m[s];
       const int32_t* R = S.rows.data() + S.sn_rows_ptr[s];
@@ -549,10 +560,8 @@ std::string analyze(int64_t ndof, const int64_t* colptr, const int32_t* rowval, 
       for (int64_t j = f; j < S.sn_first[s + 1]; ++j)
         for (int64_t p = lp[j]; p < lp[j + 1]; ++p) {
           int32_t ri = rowidx[lrow[p]];
-          if (ri < 0 || ri >= m || R[ri] != lrow[p]) return "internal: A entry outside its front";
-          S.amap_src[q] = lsrc[p];
-          S.amap_dst[q] = S.sn_Lptr[s] + ri + m * (j - f);
-          ++q;
+          if (ri < 0 || ri >= m || R[ri] != lrow[p]) { bad |= 1; continue; }
+          S.amap_dst[p] = S.sn_Lptr[s] + ri + m * (j - f);
         }
       for (int32_t ch : schildren[s]) {
         int64_t cc = S.sn_first[ch + 1] - S.sn_first[ch];
@@ -560,13 +569,16 @@ std::string analyze(int64_t ndof, const int64_t* colptr, const int32_t* rowval, 
         int64_t mc = S.sn_m[ch];
         for (int64_t k = cc; k < mc; ++k) {
           int32_t ri = rowidx[Rc[k]];
-          if (ri < 0 || ri >= m || R[ri] != Rc[k]) return "internal: child row outside its parent front";
+          if (ri < 0 || ri >= m || R[ri] != Rc[k]) { bad |= 2; continue; }
           S.rel[S.sn_relptr[ch] + (k - cc)] = ri;
         }
       }
       for (int64_t k = 0; k < m; ++k) rowidx[R[k]] = -1;
     }
   }
+  S.amap_src.swap(lsrc);   // entry p's source is bucket entry p's
+  if (bad & 1) return "internal: A entry outside its front";
+  if (bad & 2) return "internal: child row outside its parent front";
   // ---- levels
   S.sn_level.assign(ns, 0);
   for (int64_t s = 0; s < ns; ++s)

@@ -4,9 +4,27 @@
 #pragma once
 #include <cstdint>
 #include <string>
+#include <memory>
+#include <utility>
 #include <vector>
 
 namespace jfg {
+
+// Allocator whose value-initialising resize leaves the elements
+// uninitialised: for arrays that a parallel loop fills completely (the
+// zeroing pass of std::vector would run on one thread and touch every page)
+template <class T>
+struct UninitAlloc : std::allocator<T> {
+  template <class U>
+  struct rebind { using other = UninitAlloc<U>; };
+  UninitAlloc() = default;
+  template <class U>
+  UninitAlloc(const UninitAlloc<U>&) {}
+  template <class U>
+  void construct(U* p) { ::new ((void*)p) U; }
+  template <class U, class... Args>
+  void construct(U* p, Args&&... args) { ::new ((void*)p) U(std::forward<Args>(args)...); }
+};
 
 struct SymbolicOptions {
   int leaf_nodes = 24;          // nested-dissection leaf size (nodes)
@@ -48,7 +66,7 @@ struct Symbolic {
   std::vector<int32_t> ea_child;
   // A scatter: K CSC position -> factor offset (upper triangle of K_ff)
   std::vector<int32_t> amap_src;
-  std::vector<int64_t> amap_dst;
+  std::vector<int64_t, UninitAlloc<int64_t>> amap_dst;   // filled in parallel: no zeroing pass
   int64_t nnz_L = 0;                    // sum m*c
   int64_t u_arena = 0;                  // update arena size (entries)
   int64_t max_front = 0;
