@@ -366,7 +366,9 @@ jfg_status jfg_get_values(jfg_model* m, double* nzval) {
 jfg_status jfg_get_slot_map(jfg_model* m, int64_t* slot) {
   JFG_TRY(check_model(m));
   if (!m->pattern_built) { set_error("pattern not built"); return JFG_NOT_READY; }
-  std::memcpy(slot, m->pat->slot.data(), sizeof(int64_t) * m->n_trip);
+  const int32_t* src = m->pat->slot.data();
+#pragma omp parallel for schedule(static)
+  for (int64_t t = 0; t < m->n_trip; ++t) slot[t] = src[t];
   return JFG_OK;
 }
 

@@ -335,36 +335,95 @@ jfg_status build_pattern(jfg_model* m) {
     return JFG_UNSUPPORTED;
   }
   std::vector<int32_t> cnt(nnz + 1, 0);
-  // pass 2: rows and contribution counts
+  // Passes 2 and 3 walk, per column node b, its incident elements in global
+  // element order (the reference's triplet order): every (element node a,
+  // component pair) contribution lands in CSC entry q = start[a's block][j]
+  // + (rows of that block in column j above i).  Column nodes own disjoint
+  // entries, so they run in parallel; pass 2 writes the rows and counts the
+  // contributions per entry, pass 3 fills them in order with the slot map.
+  struct ColNode {
+    std::vector<Blk> blk;
+    std::vector<int64_t> start;   // (block, j) -> first CSC position of its rows in column 6b+j
+  };
+  auto prepare_col = [&](int64_t b, ColNode& cn, std::vector<int32_t>& where) {
+    node_blocks(b, cn.blk);
+    const size_t nb = cn.blk.size();
+    cn.start.resize(6 * nb);
+    for (int j = 0; j < 6; ++j) {
+      int64_t q = m->pat->colptr[6 * b + j];
+      for (size_t k = 0; k < nb; ++k) {
+        cn.start[6 * k + j] = q;
+        q += __builtin_popcountll((cn.blk[k].mask >> (6 * j)) & 0x3Full);
+      }
+    }
+    for (size_t k = 0; k < nb; ++k) where[cn.blk[k].a] = (int32_t)k;
+  };
+  // calls f(q, t, src) for every contribution of column node b, in order
+  auto for_contribs = [&](int64_t b, const ColNode& cn, const std::vector<int32_t>& where, auto&& f) {
+    for (int64_t p = iptr[b]; p < iptr[b + 1]; ++p) {
+      const int64_t ge = inc[p].e;
+      const int lb = inc[p].local;
+      int nnd;
+      const int32_t* en = enodes(ge, nnd);
+      for (int la = 0; la < nnd; ++la) {
+        const int k = where[en[la]];
+        const uint64_t em = pmask(ge, la, lb);
+        const uint64_t bm = cn.blk[k].mask;
+        for (int j = 0; j < 6; ++j) {
+          const uint64_t ecol = (em >> (6 * j)) & 0x3Full;
+          if (!ecol) continue;
+          const uint64_t bcol = (bm >> (6 * j)) & 0x3Full;
+          for (int i = 0; i < 6; ++i) {
+            if (!((ecol >> i) & 1)) continue;
+            const int64_t q = cn.start[6 * k + j] + __builtin_popcountll(bcol & ((1ull << i) - 1));
+            // t: the triplet's position in the reference's triplet order;
+            // src: the element value it reads
+            int64_t t, src;
+            if (ge < nq4) {
+              const int rr = 6 * la + i, cc = 6 * lb + j;
+              t = src = 576 * ge + rr + 24 * cc;
+            } else if (ge < g10) {
+              const int rr = 6 * la + i, cc = 6 * lb + j;
+              t = 576 * nq4 + 324 * (ge - g3) + rr + 18 * cc;
+              src = m->ev_t3_off + 324 * (ge - g3) + rr + 18 * cc;
+            } else if (ge < g8) {
+              const int rr = 3 * la + i, cc = 3 * lb + j;
+              t = 576 * nq4 + 324 * nt3 + 900 * (ge - g10) + rr + 30 * cc;
+              src = m->ev_t10_off + 900 * (ge - g10) + rr + 30 * cc;
+            } else {
+              const int64_t e8 = ge - g8;
+              const int rr = 6 * la + i, cc = 6 * lb + j;
+              const uint64_t below = q8col[48 * e8 + cc] & ((1ull << rr) - 1);
+              t = 576 * nq4 + 324 * nt3 + 900 * nt10 + q8off[e8] + q8pref[49 * e8 + cc] +
+                  __builtin_popcountll(below);
+              src = m->ev_q8_off + 2304 * e8 + rr + 48 * cc;
+            }
+            f(q, t, src);
+          }
+        }
+      }
+    }
+  };
+  // pass 2: rows, diagonal positions and contribution counts
 #pragma omp parallel
   {
-    std::vector<Blk> blk;
+    ColNode cn;
+    std::vector<int32_t> where(nn, -1);
 #pragma omp for schedule(dynamic, 256)
     for (int64_t b = 0; b < nn; ++b) {
-      node_blocks(b, blk);
-      for (int j = 0; j < 6; ++j) {
-        int64_t q = m->pat->colptr[6 * b + j];
-        for (auto& x : blk)
+      prepare_col(b, cn, where);
+      for (size_t k = 0; k < cn.blk.size(); ++k)
+        for (int j = 0; j < 6; ++j) {
+          int64_t q = cn.start[6 * k + j];
           for (int i = 0; i < 6; ++i) {
-            if (!((x.mask >> (i + 6 * j)) & 1)) continue;
-            m->pat->rowval[q] = 6 * x.a + i;
-            if (x.a == b && i == j) m->pat->diag_pos[6 * b + j] = q;
-            // contributions: incident elements of b that contain node a and
-            // cover the (i, j) component pair
-            int32_t c = 0;
-            for (int64_t p = iptr[b]; p < iptr[b + 1]; ++p) {
-              int nnd;
-              const int32_t* en = enodes(inc[p].e, nnd);
-              for (int k = 0; k < nnd; ++k)
-                if (en[k] == x.a) {
-                  if ((pmask(inc[p].e, k, inc[p].local) >> (i + 6 * j)) & 1) ++c;
-                  break;
-                }
-            }
-            cnt[q + 1] = c;
+            if (!((cn.blk[k].mask >> (i + 6 * j)) & 1)) continue;
+            m->pat->rowval[q] = 6 * cn.blk[k].a + i;
+            if (cn.blk[k].a == b && i == j) m->pat->diag_pos[6 * b + j] = q;
             ++q;
           }
-      }
+        }
+      for_contribs(b, cn, where, [&](int64_t q, int64_t, int64_t) { cnt[q + 1]++; });
+      for (auto& x : cn.blk) where[x.a] = -1;
     }
   }
   for (int64_t q = 0; q < nnz; ++q) cnt[q + 1] += cnt[q];
@@ -372,77 +431,45 @@ jfg_status build_pattern(jfg_model* m) {
     set_error("internal: slot-map contribution count mismatch");
     return JFG_BAD_INPUT;
   }
-  std::vector<int32_t> trip(m->n_trip);
-  m->pat->slot.assign(m->n_trip, -1);
+  // both filled completely by pass 3 (the counts above match the triplets)
+  std::vector<int32_t, UninitAlloc<int32_t>> trip(m->n_trip);
+  m->pat->slot.resize(m->n_trip);
   // pass 3: contributions in triplet (element) order, and the slot map
 #pragma omp parallel
   {
-    std::vector<Blk> blk;
+    ColNode cn;
+    std::vector<int32_t> where(nn, -1);
+    std::vector<int32_t> fill;
 #pragma omp for schedule(dynamic, 256)
     for (int64_t b = 0; b < nn; ++b) {
-      node_blocks(b, blk);
-      for (int j = 0; j < 6; ++j) {
-        int64_t q = m->pat->colptr[6 * b + j];
-        for (auto& x : blk)
-          for (int i = 0; i < 6; ++i) {
-            if (!((x.mask >> (i + 6 * j)) & 1)) continue;
-            int32_t w = cnt[q];
-            for (int64_t p = iptr[b]; p < iptr[b + 1]; ++p) {
-              int64_t ge = inc[p].e;
-              int nnd;
-              const int32_t* en = enodes(ge, nnd);
-              int la = -1;
-              for (int k = 0; k < nnd; ++k)
-                if (en[k] == x.a) { la = k; break; }
-              if (la < 0) continue;
-              int lb = inc[p].local;
-              if (!((pmask(ge, la, lb) >> (i + 6 * j)) & 1)) continue;
-              // t: the triplet's position in the reference's triplet order;
-              // src: the element value it reads (equal for Q4 and T10)
-              int64_t t, src;
-              if (ge < nq4) {
-                int rr = 6 * la + i, cc = 6 * lb + j;
-                t = src = 576 * ge + rr + 24 * cc;
-              } else if (ge < g10) {
-                int rr = 6 * la + i, cc = 6 * lb + j;
-                t = 576 * nq4 + 324 * (ge - g3) + rr + 18 * cc;
-                src = m->ev_t3_off + 324 * (ge - g3) + rr + 18 * cc;
-              } else if (ge < g8) {
-                int rr = 3 * la + i, cc = 3 * lb + j;
-                t = 576 * nq4 + 324 * nt3 + 900 * (ge - g10) + rr + 30 * cc;
-                src = m->ev_t10_off + 900 * (ge - g10) + rr + 30 * cc;
-              } else {
-                int64_t e8 = ge - g8;
-                int rr = 6 * la + i, cc = 6 * lb + j;
-                uint64_t below = q8col[48 * e8 + cc] & ((1ull << rr) - 1);
-                t = 576 * nq4 + 324 * nt3 + 900 * nt10 + q8off[e8] + q8pref[49 * e8 + cc] +
-                    __builtin_popcountll(below);
-                src = m->ev_q8_off + 2304 * e8 + rr + 48 * cc;
-              }
-              trip[w++] = (int32_t)src;
-              m->pat->slot[t] = q;
-            }
-            ++q;
-          }
-      }
+      prepare_col(b, cn, where);
+      const int64_t q0 = m->pat->colptr[6 * b], q1 = m->pat->colptr[6 * b + 6];
+      fill.assign(cnt.begin() + q0, cnt.begin() + q1);   // next free position of each entry
+      for_contribs(b, cn, where, [&](int64_t q, int64_t t, int64_t src) {
+        trip[fill[q - q0]++] = (int32_t)src;
+        m->pat->slot[t] = (int32_t)q;
+      });
+      for (auto& x : cn.blk) where[x.a] = -1;
     }
   }
   // transpose positions (row i of the symmetric pattern through column i)
-  std::vector<int64_t> tpos(nnz);
-#pragma omp parallel for schedule(dynamic, 4096)
+  std::vector<int64_t, UninitAlloc<int64_t>> tpos(nnz);
+  int asym = 0;
+#pragma omp parallel for schedule(dynamic, 4096) reduction(| : asym)
   for (int64_t j = 0; j < ndof; ++j)
     for (int64_t p = m->pat->colptr[j]; p < m->pat->colptr[j + 1]; ++p) {
       int64_t i = m->pat->rowval[p];
       const int32_t* beg = m->pat->rowval.data() + m->pat->colptr[i];
       const int32_t* end = m->pat->rowval.data() + m->pat->colptr[i + 1];
       const int32_t* f = std::lower_bound(beg, end, (int32_t)j);
-      tpos[p] = (f != end && *f == j) ? m->pat->colptr[i] + (f - beg) : -1;
+      const bool hit = f != end && *f == j;
+      tpos[p] = hit ? m->pat->colptr[i] + (f - beg) : -1;
+      asym |= hit ? 0 : 1;
     }
-  for (int64_t p = 0; p < nnz; ++p)
-    if (tpos[p] < 0) {
-      set_error("pattern is not structurally symmetric");
-      return JFG_BAD_INPUT;
-    }
+  if (asym) {
+    set_error("pattern is not structurally symmetric");
+    return JFG_BAD_INPUT;
+  }
   jfg_ctx* c = m->ctx;
   JFG_TRY(dev_alloc(c, (void**)&m->d_colptr, sizeof(int64_t) * (ndof + 1)));
   JFG_TRY(dev_alloc(c, (void**)&m->d_rowval, sizeof(int32_t) * nnz));

@@ -125,7 +125,7 @@ namespace jfg {
 struct HostPattern {
   std::vector<int64_t> colptr;
   std::vector<int32_t> rowval;
-  std::vector<int64_t> slot;        // triplet -> nz position
+  std::vector<int32_t, UninitAlloc<int32_t>> slot;   // triplet -> nz position (every entry written)
   std::vector<int64_t> diag_pos;    // ndof, -1 when structurally absent
 };
 }  // namespace jfg

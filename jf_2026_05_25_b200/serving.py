@@ -214,6 +214,9 @@ class Resident:
     last_used: float = 0.0
     evicted: bool = False              # set under `lock` when the group is freed
     mesh: Optional[bytes] = None       # mesh key of a single model (structure sharing)
+    # held while a new model copies this one's device pattern (short); a
+    # running solve does not block that copy, eviction waits for it
+    pin: threading.Lock = field(default_factory=threading.Lock)
 
 
 def _model_class(model, pack) -> str:
@@ -282,6 +285,7 @@ class SolveServer:
         self.readmissions = 0
         self.shared_structures = 0
         self.phase_s: Dict[str, Dict[str, float]] = {}   # class -> phase -> seconds (wall, summed over slots)
+        self.waiting_reserved = 0.0   # reservations of requests waiting in _admit
         self._next_key = 0
         self._stop = False
         self.backends = []
@@ -413,7 +417,7 @@ class SolveServer:
         r.dm.close()
         self.mem_cv.notify_all()
 
-    def _admit(self, need: float, wait: bool = False):
+    def _admit(self, need: float, wait: bool = False, own: float = 0.0):
         """Free least-recently-used residents until `need` more bytes fit, and
         reserve them for the model being prepared (released by _register).
 
@@ -423,28 +427,46 @@ class SolveServer:
         (``wait``) up to ``wait_s`` for memory to be released, then is
         admitted over budget rather than blocking the server.  The group's
         bytes are released once, and its registry entries go only after its
-        lock is held.
+        lock is held.  ``own``: bytes this request reserved already (its
+        upload estimate); with nothing resident and every reservation held by
+        requests that are themselves waiting here, nothing can be released,
+        so the request is admitted at once.
         """
         with self.rlock:
             deadline = time.perf_counter() + self.wait_s
             busy = set()
-            while self.resident_bytes + self.reserved + need > self.budget:
-                cands = [k for k in self.registry if id(self.registry[k].dm) not in busy]
-                if not cands:
-                    if not wait or time.perf_counter() >= deadline or (not self.registry and self.reserved <= 0):
-                        break
-                    busy.clear()
-                    self.mem_cv.wait(timeout=0.5)
-                    continue
-                key = min(cands, key=lambda k: self.registry[k].last_used)
-                r = self.registry[key]
-                if not r.lock.acquire(blocking=False):
-                    busy.add(id(r.dm))
-                    continue
-                try:
-                    self._evict_group(r, key)
-                finally:
-                    r.lock.release()
+            waiting = False
+            try:
+                while self.resident_bytes + self.reserved + need > self.budget:
+                    cands = [k for k in self.registry if id(self.registry[k].dm) not in busy]
+                    if not cands:
+                        if not waiting:
+                            waiting = True
+                            self.waiting_reserved += own
+                        stuck = not self.registry and self.reserved <= self.waiting_reserved
+                        if not wait or time.perf_counter() >= deadline or stuck:
+                            break
+                        busy.clear()
+                        self.mem_cv.wait(timeout=0.5)
+                        continue
+                    key = min(cands, key=lambda k: self.registry[k].last_used)
+                    r = self.registry[key]
+                    if not r.lock.acquire(blocking=False):
+                        busy.add(id(r.dm))
+                        continue
+                    if not r.pin.acquire(blocking=False):
+                        r.lock.release()
+                        busy.add(id(r.dm))
+                        continue
+                    try:
+                        self._evict_group(r, key)
+                    finally:
+                        r.pin.release()
+                        r.lock.release()
+            finally:
+                if waiting:
+                    self.waiting_reserved -= own
+                    self.mem_cv.notify_all()
             self.reserved += need
 
     def _release(self, reserved: float):
@@ -519,7 +541,7 @@ class SolveServer:
                 dk = self.meshes.get(mk)
                 donor = self.registry.get(dk) if dk is not None else None
         if donor is not None:
-            with donor.lock:
+            with donor.pin:
                 if not donor.evicted:
                     dm.share_structure(donor.dm)
                     with self.rlock:
@@ -528,7 +550,7 @@ class SolveServer:
         def admit(d):
             need = float(d.memory(prec, nrhs)[1])
             if need > admitted[0]:
-                self._admit(need - admitted[0], wait=True)
+                self._admit(need - admitted[0], wait=True, own=admitted[0])
                 admitted[0] = need
 
         t_prep = time.perf_counter()

@@ -195,7 +195,7 @@ MODELS = {
     "q8_tilted": lambda: M.quad8_plate(6, 5, skew=0.2, tilt_deg=30, n_cases=2),
     "wing_small": lambda: M.wing_panel(nx=24, ny=36, n_blades=3, blade_nz=4, n_cases=3, seed=5),
     "solid_small": lambda: M.solid_block(n=4, n_cases=2),
-    "tria_mixed": lambda: M.tria_plate(),
+    "tria_mixed": lambda: M.tria_plate(t=0.02),   # thinner tilted plates sit above the 1e-10 FP64 residual floor
     "q8_tapered": lambda: M.quad8_plate(8, 6, taper=0.6, tilt_deg=20, n_cases=2),
 }
 

@@ -85,3 +85,50 @@ def test_eviction_waits_for_nothing_when_every_group_is_busy(server):
         assert done.wait(5.0), "admission blocked on a busy group"
         t.join()
     assert dm_a.closed == 0 and keys_a[0] in server.registry
+
+
+def test_second_stage_admission_does_not_wait_on_its_own_reservation():
+    """A model holds its upload estimate and asks for the rest once its
+    analysis exists.  With nothing resident and only its own bytes reserved,
+    nothing can be freed: it is admitted over budget at once instead of
+    waiting for the timeout."""
+    import time
+    srv = S.SolveServer(slots=0, hbm_budget_bytes=1.0)
+    srv.wait_s = 30.0
+    try:
+        srv._admit(10.0, wait=True)            # upload estimate, over budget: admitted (empty server)
+        t0 = time.perf_counter()
+        srv._admit(40.0, wait=True, own=10.0)  # the exact figure
+        assert time.perf_counter() - t0 < 2.0
+        assert srv.reserved == pytest.approx(50.0)
+        assert srv.waiting_reserved == pytest.approx(0.0)
+    finally:
+        srv.close()
+
+
+def test_two_second_stage_admissions_do_not_wait_on_each_other():
+    """Two requests each hold an estimate and both ask for more with nothing
+    resident: the one that finds every reservation held by waiters goes
+    ahead at once; the other goes once the first's bytes are released."""
+    import time
+    srv = S.SolveServer(slots=0, hbm_budget_bytes=1.0)
+    srv.wait_s = 30.0
+    try:
+        srv._admit(10.0)                       # two upload estimates, admitted over budget
+        srv._admit(10.0)
+        ths = [threading.Thread(target=srv._admit, args=(5.0,), kwargs={"wait": True, "own": 10.0})
+               for _ in range(2)]
+        for t in ths:
+            t.start()
+        t0 = time.perf_counter()
+        while all(t.is_alive() for t in ths) and time.perf_counter() - t0 < 5.0:
+            time.sleep(0.05)
+        assert sum(not t.is_alive() for t in ths) == 1
+        srv._release(15.0)                     # the first one's model is done and gone
+        for t in ths:
+            t.join(timeout=5)
+        assert all(not t.is_alive() for t in ths)
+        assert time.perf_counter() - t0 < 10.0
+        assert srv.reserved == pytest.approx(15.0)
+    finally:
+        srv.close()
