@@ -549,15 +549,143 @@ k_potrf_cta(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
   }
 }
 
-// JFG_POTRF=1 selects the earlier diagonal-block kernel (one warp per 32 x 32
-// tile); the default runs the CTA-wide chains above
-inline bool potrf_cta() {
+// Blocked Cholesky and inverse of the NB x NB diagonal block, in four
+// 16-column blocks, so that the serial chains run inside one warp and the
+// CTA synchronises a dozen times instead of once per column:
+//   factor, for each block k: warp 0 factors the 16 x 16 diagonal block
+//     (warp-synchronous, one column per step), one thread per row below it
+//     solves X L_kk^T = A_ik, and the CTA applies the rank-16 update to the
+//     trailing lower triangle;
+//   inverse X = L^-1: four warps invert the four diagonal blocks at once,
+//     then X_ij = -X_ii (sum_{j <= k < i} L_ik X_kj) by block distance 1..3.
+// A non-positive or non-finite pivot is recorded (the first one) and
+// replaced by 1 so the block stays usable.  Padding (columns >= kn) is the
+// identity, as in the kernels above.
+constexpr int PB = 16;
+template <typename T>
+constexpr int potrf_blk_smem() { return (2 * NB * (NB + 1) + 3 * PB * (PB + 1)) * (int)sizeof(T); }
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_potrf_blk(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
+            const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
+            const int64_t* __restrict__ Dptr, T* __restrict__ L, T* __restrict__ Dinv, int k0, DevError* err) {
+  int s = list[blockIdx.x];
+  int c = first[s + 1] - first[s];
+  if (k0 >= c) return;
+  int m = mrows[s];
+  int kn = min(NB, c - k0);
+  extern __shared__ unsigned char smem_raw[];
+  T (*A)[NB + 1] = reinterpret_cast<T (*)[NB + 1]>(smem_raw);
+  T (*B)[NB + 1] = A + NB;
+  T (*W)[PB][PB + 1] = reinterpret_cast<T (*)[PB][PB + 1]>(B + NB);
+  __shared__ int bad_idx;
+  T* P = L + Lptr[s] + k0 + (int64_t)m * k0;
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  if (t == 0) bad_idx = NB;
+#pragma unroll
+  for (int u = 0; u < NB * NB / 256; ++u) {
+    int e = t + 256 * u;
+    int i = e & (NB - 1), j = e >> 6;
+    A[i][j] = (i < kn && j < kn) ? (i >= j ? P[i + (int64_t)m * j] : (T)0) : (i == j ? (T)1 : (T)0);
+    B[i][j] = (T)0;
+  }
+  __syncthreads();
+  for (int kb = 0; kb < NB / PB; ++kb) {
+    const int o = kb * PB;
+    if (warp == 0) {
+      for (int j = 0; j < PB; ++j) {
+        T d = A[o + j][o + j];
+        if (!(d > (T)0) || !isfinite((double)d)) {
+          if (lane == 0 && o + j < kn) atomicMin(&bad_idx, o + j);
+          d = (T)1;
+        }
+        const T r = sqrt(d);
+        __syncwarp();
+        if (lane == 0) A[o + j][o + j] = r;
+        if (lane > j && lane < PB) A[o + lane][o + j] /= r;
+        __syncwarp();
+        for (int e = lane; e < PB * PB; e += 32) {
+          const int i = e & (PB - 1), q = e >> 4;
+          if (q > j && i >= q) A[o + i][o + q] -= A[o + i][o + j] * A[o + q][o + j];
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    const int r0 = o + PB;
+    if (r0 < NB) {
+      for (int r = r0 + t; r < NB; r += blockDim.x) {   // X L_kk^T = A_rk, one row per thread
+        for (int j = 0; j < PB; ++j) {
+          T x = A[r][o + j];
+          for (int q = 0; q < j; ++q) x -= A[r][o + q] * A[o + j][o + q];
+          A[r][o + j] = x / A[o + j][o + j];
+        }
+      }
+      __syncthreads();
+      const int nt = NB - r0;
+      for (int e = t; e < nt * nt; e += blockDim.x) {   // trailing lower triangle, rank PB
+        const int i = r0 + e % nt, q = r0 + e / nt;
+        if (i < q) continue;
+        T acc = A[i][q];
+#pragma unroll
+        for (int p = 0; p < PB; ++p) acc -= A[i][o + p] * A[q][o + p];
+        A[i][q] = acc;
+      }
+      __syncthreads();
+    }
+  }
+  // inverse: diagonal blocks, one warp each; lane q solves column q
+  if (warp < NB / PB && lane < PB) {
+    const int o = warp * PB, q = lane;
+    for (int i = 0; i < PB; ++i) {
+      if (i < q) { B[o + i][o + q] = (T)0; continue; }
+      T x = (i == q) ? (T)1 : (T)0;
+      for (int p = q; p < i; ++p) x -= A[o + i][o + p] * B[o + p][o + q];
+      B[o + i][o + q] = x / A[o + i][o + i];
+    }
+  }
+  __syncthreads();
+  for (int dist = 1; dist < NB / PB; ++dist) {
+    const int nblk = NB / PB - dist;
+    for (int e = t; e < nblk * PB * PB; e += blockDim.x) {   // W_j = sum_{j <= k < i} L_ik X_kj
+      const int bj = e / (PB * PB), r = e % PB, cc = (e / PB) % PB, bi = bj + dist;
+      T acc = (T)0;
+      for (int k = bj; k < bi; ++k)
+#pragma unroll
+        for (int p = 0; p < PB; ++p) acc += A[bi * PB + r][k * PB + p] * B[k * PB + p][bj * PB + cc];
+      W[bj][r][cc] = acc;
+    }
+    __syncthreads();
+    for (int e = t; e < nblk * PB * PB; e += blockDim.x) {   // X_ij = -X_ii W_j
+      const int bj = e / (PB * PB), r = e % PB, cc = (e / PB) % PB, bi = bj + dist;
+      T acc = (T)0;
+#pragma unroll
+      for (int p = 0; p < PB; ++p) acc += B[bi * PB + r][bi * PB + p] * W[bj][p][cc];
+      B[bi * PB + r][bj * PB + cc] = -acc;
+    }
+    __syncthreads();
+  }
+  if (t == 0 && bad_idx < kn) rec_err(err, EE_PIVOT, (int64_t)first[s] + k0 + bad_idx);
+  T* Dv = Dinv + Dptr[s] + (int64_t)(k0 / NB) * NB * NB;
+  for (int e = t; e < NB * NB; e += blockDim.x) {
+    int i = e & (NB - 1), j = e >> 6;
+    bool in = i < kn && j < kn && i >= j;
+    if (in) P[i + (int64_t)m * j] = A[i][j];
+    Dv[i + NB * j] = in ? B[i][j] : (T)0;
+  }
+}
+
+// JFG_POTRF selects the diagonal-block kernel: 1 the warp-tile kernel
+// (one warp per 32 x 32 tile), 2 the CTA-wide column chains, otherwise (the
+// default) the blocked kernel above
+inline int potrf_kind() {
   static int v = -1;
   if (v < 0) {
     const char* e = std::getenv("JFG_POTRF");
-    v = (e && e[0] == '1') ? 0 : 1;
+    v = (e && e[0] == '1') ? 1 : (e && e[0] == '2') ? 2 : 0;
   }
-  return v == 1;
+  return v;
 }
 
 // rows [k1, m) of panel columns [k0, k1):  X := X * L_D^{-T} = X * Dinv^T,
@@ -1491,6 +1619,7 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
     int bytes = 2 * NB * (NB + 1) * (int)sizeof(T);
     JFG_CUDA(cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, potrf_smem<T>()));
     JFG_CUDA(cudaFuncSetAttribute(k_potrf_cta<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, potrf_smem<T>()));
+    JFG_CUDA(cudaFuncSetAttribute(k_potrf_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, potrf_blk_smem<T>()));
     JFG_CUDA(cudaFuncSetAttribute(k_trsm_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     attr_set = true;
   }
@@ -1570,7 +1699,10 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
       const int P1 = P0 + PW;
       for (int k0 = P0; k0 < std::min(P1, lv.max_c); k0 += NB) {
         const int na = lv.active(k0);   // fronts wider than k0: a prefix of the list
-        { int ps_ = fine_prof() ? prof_start(st) : -1; { if (potrf_cta())
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { if (potrf_kind() == 0)
+            k_potrf_blk<T><<<na, 256, potrf_blk_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr, F->Dptr, Lf, Dvf,
+                                                                  k0, F->err);
+          else if (potrf_kind() == 2)
             k_potrf_cta<T><<<na, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr, F->Dptr, Lf, Dvf, k0,
                                                               F->err);
           else
