@@ -464,8 +464,9 @@ struct Q4Slab {
   double P[Q4P];
   double Kab[96], Kabs[96], Kabb[96];
   double Pm[96], Pb[96];
-  double Ke[576];
+  double Ke[576];   // the element matrix, accumulated phase by phase (entry lane + 32 t owned by one lane)
   double T[36];
+  double W[368];    // Gauss-point derivatives and right columns of the B matrices
 };
 
 __global__ void __launch_bounds__(WARPS * 32)
@@ -487,101 +488,112 @@ k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ pr
   const double detJc = S.P[Q4P_DETJC];
   const double iJ11c = S.P[Q4P_IJC], iJ12c = S.P[Q4P_IJC + 1], iJ21c = S.P[Q4P_IJC + 2], iJ22c = S.P[Q4P_IJC + 3];
   const double k6rot = S.P[Q4P_K6];
-  double ke[18], kab[3], kabs[3], kabb[3];
-#pragma unroll
-  for (int t = 0; t < 18; ++t) ke[t] = 0.0;
-#pragma unroll
-  for (int t = 0; t < 3; ++t) { kab[t] = 0.0; kabs[t] = 0.0; kabb[t] = 0.0; }
-  const double pt = 0.57735026918962573;
-  const double gr[4] = {-pt, pt, pt, -pt}, gs[4] = {-pt, -pt, pt, pt};
-  for (int g = 0; g < 4; ++g) {
-    double r = gr[g], s = gs[g];
+  // ---- membrane, bending and the incompatible-mode couplings at the four
+  // Gauss points.  Lanes 0-3 prepare one point each: the shape derivatives
+  // (dx, dy per node) and, for every column of the B matrices, w = wgt * C b
+  // (membrane / bending columns of the 24 DOFs, the four incompatible modes);
+  // an entry is then u_i . w_j summed over the points, u_i the left B column
+  // (two nonzeros).
+  double* GD = S.W;               // [g][8]: dx[4], dy[4]
+  double* WM = S.W + 32;          // [g][8][3]: membrane column (node k, u/v) = 2k + c
+  double* WB = WM + 96;           // [g][8][3]: bending column (node k, rx/ry) = 2k + c
+  double* WI = WB + 96;           // [g][4][3]: Cm bi(q)
+  double* WIS = WI + 48;          // [g][4][3]: shp bib(q)
+  double* WIB = WIS + 48;         // [g][4][3]: Cb bib(q)
+  if (lane < 4) {
+    const double pt = 0.57735026918962573;
+    const int g = lane;
+    const double r = (g == 1 || g == 2) ? pt : -pt, s = (g >= 2) ? pt : -pt;
     double dNr[4], dNs[4];
     shape_d(r, s, dNr, dNs);
     double J11, J12, J21, J22;
     jac4(lc, dNr, dNs, J11, J12, J21, J22);
-    double detJ = J11 * J22 - J12 * J21;
-    double wgt = fabs(detJ), id = 1.0 / detJ;
-    double iJ11 = J22 * id, iJ12 = -J12 * id, iJ21 = -J21 * id, iJ22 = J11 * id;
+    const double detJ = J11 * J22 - J12 * J21;
+    const double wgt = fabs(detJ), id = 1.0 / detJ;
+    const double iJ11 = J22 * id, iJ12 = -J12 * id, iJ21 = -J21 * id, iJ22 = J11 * id;
     double dx[4], dy[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       dx[k] = iJ11 * dNr[k] + iJ12 * dNs[k];
       dy[k] = iJ21 * dNr[k] + iJ22 * dNs[k];
+      GD[8 * g + k] = dx[k];
+      GD[8 * g + 4 + k] = dy[k];
     }
-    double ratio = (iJ11 * iJ22 - iJ12 * iJ21) / (iJ11c * iJ22c - iJ12c * iJ21c);
-    double p1x = ratio * iJ11c * (-2 * r), p1y = ratio * iJ21c * (-2 * r);
-    double p2x = ratio * iJ12c * (-2 * s), p2y = ratio * iJ22c * (-2 * s);
-    double gq = detJc / detJ;
-    double b1x = (iJ11c * (-2 * r)) * gq, b1y = (iJ21c * (-2 * r)) * gq;
-    double b2x = (iJ12c * (-2 * s)) * gq, b2y = (iJ22c * (-2 * s)) * gq;
-    auto bm = [&](int i, double o[3]) {
-      int k = i / 6, cc = i % 6;
-      o[0] = o[1] = o[2] = 0.0;
-      if (cc == 0) { o[0] = dx[k]; o[2] = dy[k]; }
-      else if (cc == 1) { o[1] = dy[k]; o[2] = dx[k]; }
-    };
-    auto bb = [&](int i, double o[3]) {
-      int k = i / 6, cc = i % 6;
-      o[0] = o[1] = o[2] = 0.0;
-      if (cc == 4) { o[0] = dx[k]; o[2] = dy[k]; }
-      else if (cc == 3) { o[1] = -dy[k]; o[2] = -dx[k]; }
-    };
-    auto bi = [&](int q, double o[3]) {
-      if (q == 0) { o[0] = p1x; o[1] = 0; o[2] = p1y; }
-      else if (q == 1) { o[0] = 0; o[1] = p1y; o[2] = p1x; }
-      else if (q == 2) { o[0] = p2x; o[1] = 0; o[2] = p2y; }
-      else { o[0] = 0; o[1] = p2y; o[2] = p2x; }
-    };
-    auto bib = [&](int q, double o[3]) {
-      if (q == 0) { o[0] = 0; o[1] = -b1y; o[2] = -b1x; }
-      else if (q == 1) { o[0] = 0; o[1] = -b2y; o[2] = -b2x; }
-      else if (q == 2) { o[0] = b1x; o[1] = 0; o[2] = b1y; }
-      else { o[0] = b2x; o[1] = 0; o[2] = b2y; }
+    const double ratio = (iJ11 * iJ22 - iJ12 * iJ21) / (iJ11c * iJ22c - iJ12c * iJ21c);
+    const double p1x = ratio * iJ11c * (-2 * r), p1y = ratio * iJ21c * (-2 * r);
+    const double p2x = ratio * iJ12c * (-2 * s), p2y = ratio * iJ22c * (-2 * s);
+    const double gq = detJc / detJ;
+    const double b1x = (iJ11c * (-2 * r)) * gq, b1y = (iJ21c * (-2 * r)) * gq;
+    const double b2x = (iJ12c * (-2 * s)) * gq, b2y = (iJ22c * (-2 * s)) * gq;
+    // w = wgt * C v for a right column v
+    auto cv = [&](const double* C, double v0, double v1, double v2, double* w) {
+      w[0] = wgt * (C[0] * v0 + C[3] * v1 + C[6] * v2);
+      w[1] = wgt * (C[1] * v0 + C[4] * v1 + C[7] * v2);
+      w[2] = wgt * (C[2] * v0 + C[5] * v1 + C[8] * v2);
     };
 #pragma unroll
-    for (int t = 0; t < 18; ++t) {
-      int idx = lane + 32 * t;
-      int i = idx % 24, j = idx / 24;
-      int ci = i % 6, cj = j % 6;
-      double acc = 0.0;
-      if (ci < 2 && cj < 2) {
-        double u[3], v[3];
-        bm(i, u); bm(j, v);
-        acc += qf3(u, Cm, v);
-      }
-      if ((ci == 3 || ci == 4) && (cj == 3 || cj == 4)) {
-        double u[3], v[3];
-        bb(i, u); bb(j, v);
-        acc += qf3(u, Cb, v);
-      }
-      ke[t] += wgt * acc;
+    for (int k = 0; k < 4; ++k) {
+      cv(Cm, dx[k], 0.0, dy[k], WM + 24 * g + 3 * (2 * k));          // u
+      cv(Cm, 0.0, dy[k], dx[k], WM + 24 * g + 3 * (2 * k + 1));      // v
+      cv(Cb, 0.0, -dy[k], -dx[k], WB + 24 * g + 3 * (2 * k));        // rx
+      cv(Cb, dx[k], 0.0, dy[k], WB + 24 * g + 3 * (2 * k + 1));      // ry
     }
+    cv(Cm, p1x, 0.0, p1y, WI + 12 * g + 0);
+    cv(Cm, 0.0, p1y, p1x, WI + 12 * g + 3);
+    cv(Cm, p2x, 0.0, p2y, WI + 12 * g + 6);
+    cv(Cm, 0.0, p2y, p2x, WI + 12 * g + 9);
+    const double bib[4][3] = {{0.0, -b1y, -b1x}, {0.0, -b2y, -b2x}, {b1x, 0.0, b1y}, {b2x, 0.0, b2y}};
 #pragma unroll
-    for (int t = 0; t < 3; ++t) {
-      int idx = lane + 32 * t;
-      int i = idx % 24, q = idx / 24;
-      int ci = i % 6;
-      double u[3], v[3];
-      if (ci < 2) { bm(i, u); bi(q, v); kab[t] += wgt * qf3(u, Cm, v); }
-      if (ci == 3 || ci == 4) {
-        bb(i, u); bib(q, v);
-        kabs[t] += wgt * qf3(u, shp, v);
-        kabb[t] += wgt * qf3(u, Cb, v);
-      }
+    for (int q = 0; q < 4; ++q) {
+      cv(shp, bib[q][0], bib[q][1], bib[q][2], WIS + 12 * g + 3 * q);
+      cv(Cb, bib[q][0], bib[q][1], bib[q][2], WIB + 12 * g + 3 * q);
     }
+  }
+  __syncwarp();
+  // u_i . w over the four points; u_i of a membrane / bending row with two
+  // nonzeros: u (dx, 0, dy), v (0, dy, dx), rx (0, -dy, -dx), ry (dx, 0, dy)
+  auto udot = [&](int ci, int ki, const double* W, int stride) {
+    double acc = 0.0;
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+      const double dxk = GD[8 * g + ki], dyk = GD[8 * g + 4 + ki];
+      const double* w = W + stride * g;
+      if (ci == 0 || ci == 4) acc += dxk * w[0] + dyk * w[2];
+      else if (ci == 1) acc += dyk * w[1] + dxk * w[2];
+      else acc -= dyk * w[1] + dxk * w[2];   // ci == 3
+    }
+    return acc;
+  };
+#pragma unroll 2
+  for (int t = 0; t < 18; ++t) {
+    const int idx = lane + 32 * t;
+    const int i = idx % 24, j = idx / 24;
+    const int ci = i % 6, cj = j % 6, ki = i / 6, kj = j / 6;
+    double acc = 0.0;
+    if (ci < 2 && cj < 2) acc = udot(ci, ki, WM + 3 * (2 * kj + cj), 24);
+    else if ((ci == 3 || ci == 4) && (cj == 3 || cj == 4)) acc = udot(ci, ki, WB + 3 * (2 * kj + cj - 3), 24);
+    S.Ke[idx] = acc;
   }
 #pragma unroll
   for (int t = 0; t < 3; ++t) {
-    S.Kab[lane + 32 * t] = kab[t];
-    S.Kabs[lane + 32 * t] = kabs[t];
-    S.Kabb[lane + 32 * t] = kabb[t];
+    const int idx = lane + 32 * t;
+    const int i = idx % 24, q = idx / 24;
+    const int ci = i % 6, ki = i / 6;
+    double kab = 0.0, kabs = 0.0, kabb = 0.0;
+    if (ci < 2) kab = udot(ci, ki, WI + 3 * q, 12);
+    if (ci == 3 || ci == 4) {
+      kabs = udot(ci, ki, WIS + 3 * q, 12);
+      kabb = udot(ci, ki, WIB + 3 * q, 12);
+    }
+    S.Kab[idx] = kab;
+    S.Kabs[idx] = kabs;
+    S.Kabb[idx] = kabb;
   }
   // ---- MacNeal shear term
   if (S.P[Q4P_SHEAR] != 0.0) {
     const double* D = S.P + Q4P_D;
     const double* sol = S.P + Q4P_SOL;
-#pragma unroll
+#pragma unroll 2
     for (int t = 0; t < 18; ++t) {
       int idx = lane + 32 * t;
       int i = idx % 24, j = idx / 24;
@@ -594,7 +606,7 @@ k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ pr
           a += D[q + 4 * ii] * sol[q + 4 * jj];
           b += D[q + 4 * jj] * sol[q + 4 * ii];
         }
-        ke[t] += 0.5 * (a + b);
+        S.Ke[idx] += 0.5 * (a + b);
       }
     }
   }
@@ -618,12 +630,12 @@ k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ pr
         if (cc == 5 && k == corner) return 1.0;
         return 0.0;
       };
-#pragma unroll
+#pragma unroll 2
       for (int t = 0; t < 18; ++t) {
         int idx = lane + 32 * t;
         int i = idx % 24, j = idx / 24;
         double bi_ = bd(i);
-        if (bi_ != 0.0) ke[t] += wc * (bi_ * bd(j));
+        if (bi_ != 0.0) S.Ke[idx] += wc * (bi_ * bd(j));
       }
     }
   }
@@ -646,7 +658,7 @@ k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ pr
   __syncwarp();
   const double* Kbb = S.P + Q4P_KBB;
   const double* Kbbb = S.P + Q4P_KBBB;
-#pragma unroll
+#pragma unroll 1
   for (int t = 0; t < 18; ++t) {
     int idx = lane + 32 * t;
     int i = idx % 24, j = idx / 24;
@@ -660,11 +672,9 @@ k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ pr
         v += S.Pm[k + 4 * i] * Kbb[k + 4 * l] * S.Pm[l + 4 * j] +
              S.Pb[k + 4 * i] * Kbbb[k + 4 * l] * S.Pb[l + 4 * j];
     }
-    ke[t] += v;
+    S.Ke[idx] += v;
   }
   // ---- transform to the node DOF frames and emit
-#pragma unroll
-  for (int t = 0; t < 18; ++t) S.Ke[lane + 32 * t] = ke[t];
   if (lane < 4) {
     const double* R = nodeR + 9 * (int64_t)nodes[4 * e + lane];
     const double* V = S.P + Q4P_V;
