@@ -472,7 +472,8 @@ struct Q4Slab {
 __global__ void __launch_bounds__(WARPS * 32)
 k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ prep,
      const double* __restrict__ nodeR, double* __restrict__ ev) {
-  __shared__ Q4Slab slabs[WARPS];
+  extern __shared__ __align__(16) unsigned char q4smem[];   // WARPS slabs (above the 48 KB static limit)
+  Q4Slab* slabs = reinterpret_cast<Q4Slab*>(q4smem);
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t e = (int64_t)blockIdx.x * WARPS + w;
   if (e >= n) return;
@@ -707,6 +708,21 @@ k_q4(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ pr
     }
     out[idx] = sum;
   }
+}
+
+constexpr size_t Q4_SMEM = WARPS * sizeof(Q4Slab);
+
+// the warp pass's dynamic shared-memory limit, set once per device
+jfg_status q4_attributes() {
+  static bool done[64] = {};
+  int dev = 0;
+  JFG_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return JFG_OK;
+  if (!done[dev]) {
+    JFG_CUDA(cudaFuncSetAttribute(k_q4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Q4_SMEM));
+    done[dev] = true;
+  }
+  return JFG_OK;
 }
 
 struct T10Slab {
@@ -1188,11 +1204,12 @@ k_q8(int64_t n, const int32_t* __restrict__ q8n, const double* __restrict__ q8s,
 
 jfg_status launch_elements(jfg_model* m, cudaStream_t st) {
   if (m->n_q4 > 0) {
+    JFG_TRY(q4_attributes());
     int64_t blocks = (m->n_q4 + WARPS - 1) / WARPS;
     int ps = prof_start(st);
     { k_q4_prep<<<(unsigned)((m->n_q4 + 127) / 128), 128, 0, st>>>(m->n_q4, m->d_q4n, m->d_q4s, m->d_xyz,
                                                                  m->d_q4prep, m->d_err); count_launch(); }
-    { k_q4<<<(unsigned)blocks, WARPS * 32, 0, st>>>(m->n_q4, m->d_q4n, m->d_q4prep, m->d_R, m->d_ev);
+    { k_q4<<<(unsigned)blocks, WARPS * 32, Q4_SMEM, st>>>(m->n_q4, m->d_q4n, m->d_q4prep, m->d_R, m->d_ev);
       count_launch(); }
     // algorithmic bytes: connectivity + section in, matrix out, coordinates once
     prof_end(ps, st, KS_Q4, (double)m->n_q4 * (16 + 8 * 26 + 8 * 576) + 24.0 * m->n_nodes);
@@ -1233,10 +1250,11 @@ jfg_status launch_elements(jfg_model* m, cudaStream_t st) {
 // the model's own buffers; no profiling events.
 jfg_status launch_elements_into(const jfg_model* m, cudaStream_t st, double* ev, double* q4prep, DevError* err) {
   if (m->n_q4 > 0) {
+    JFG_TRY(q4_attributes());
     int64_t blocks = (m->n_q4 + WARPS - 1) / WARPS;
     { k_q4_prep<<<(unsigned)((m->n_q4 + 127) / 128), 128, 0, st>>>(m->n_q4, m->d_q4n, m->d_q4s, m->d_xyz, q4prep,
                                                                  err); count_launch(); }
-    { k_q4<<<(unsigned)blocks, WARPS * 32, 0, st>>>(m->n_q4, m->d_q4n, q4prep, m->d_R, ev); count_launch(); }
+    { k_q4<<<(unsigned)blocks, WARPS * 32, Q4_SMEM, st>>>(m->n_q4, m->d_q4n, q4prep, m->d_R, ev); count_launch(); }
     JFG_CUDA(cudaGetLastError());
   }
   if (m->n_t10 > 0) {
