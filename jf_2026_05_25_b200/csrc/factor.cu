@@ -549,143 +549,15 @@ k_potrf_cta(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
   }
 }
 
-// Blocked Cholesky and inverse of the NB x NB diagonal block, in four
-// 16-column blocks, so that the serial chains run inside one warp and the
-// CTA synchronises a dozen times instead of once per column:
-//   factor, for each block k: warp 0 factors the 16 x 16 diagonal block
-//     (warp-synchronous, one column per step), one thread per row below it
-//     solves X L_kk^T = A_ik, and the CTA applies the rank-16 update to the
-//     trailing lower triangle;
-//   inverse X = L^-1: four warps invert the four diagonal blocks at once,
-//     then X_ij = -X_ii (sum_{j <= k < i} L_ik X_kj) by block distance 1..3.
-// A non-positive or non-finite pivot is recorded (the first one) and
-// replaced by 1 so the block stays usable.  Padding (columns >= kn) is the
-// identity, as in the kernels above.
-constexpr int PB = 16;
-template <typename T>
-constexpr int potrf_blk_smem() { return (2 * NB * (NB + 1) + 3 * PB * (PB + 1)) * (int)sizeof(T); }
-
-template <typename T>
-__global__ void __launch_bounds__(256)
-k_potrf_blk(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
-            const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
-            const int64_t* __restrict__ Dptr, T* __restrict__ L, T* __restrict__ Dinv, int k0, DevError* err) {
-  int s = list[blockIdx.x];
-  int c = first[s + 1] - first[s];
-  if (k0 >= c) return;
-  int m = mrows[s];
-  int kn = min(NB, c - k0);
-  extern __shared__ unsigned char smem_raw[];
-  T (*A)[NB + 1] = reinterpret_cast<T (*)[NB + 1]>(smem_raw);
-  T (*B)[NB + 1] = A + NB;
-  T (*W)[PB][PB + 1] = reinterpret_cast<T (*)[PB][PB + 1]>(B + NB);
-  __shared__ int bad_idx;
-  T* P = L + Lptr[s] + k0 + (int64_t)m * k0;
-  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  if (t == 0) bad_idx = NB;
-#pragma unroll
-  for (int u = 0; u < NB * NB / 256; ++u) {
-    int e = t + 256 * u;
-    int i = e & (NB - 1), j = e >> 6;
-    A[i][j] = (i < kn && j < kn) ? (i >= j ? P[i + (int64_t)m * j] : (T)0) : (i == j ? (T)1 : (T)0);
-    B[i][j] = (T)0;
-  }
-  __syncthreads();
-  for (int kb = 0; kb < NB / PB; ++kb) {
-    const int o = kb * PB;
-    if (warp == 0) {
-      for (int j = 0; j < PB; ++j) {
-        T d = A[o + j][o + j];
-        if (!(d > (T)0) || !isfinite((double)d)) {
-          if (lane == 0 && o + j < kn) atomicMin(&bad_idx, o + j);
-          d = (T)1;
-        }
-        const T r = sqrt(d);
-        __syncwarp();
-        if (lane == 0) A[o + j][o + j] = r;
-        if (lane > j && lane < PB) A[o + lane][o + j] /= r;
-        __syncwarp();
-        for (int e = lane; e < PB * PB; e += 32) {
-          const int i = e & (PB - 1), q = e >> 4;
-          if (q > j && i >= q) A[o + i][o + q] -= A[o + i][o + j] * A[o + q][o + j];
-        }
-        __syncwarp();
-      }
-    }
-    __syncthreads();
-    const int r0 = o + PB;
-    if (r0 < NB) {
-      for (int r = r0 + t; r < NB; r += blockDim.x) {   // X L_kk^T = A_rk, one row per thread
-        for (int j = 0; j < PB; ++j) {
-          T x = A[r][o + j];
-          for (int q = 0; q < j; ++q) x -= A[r][o + q] * A[o + j][o + q];
-          A[r][o + j] = x / A[o + j][o + j];
-        }
-      }
-      __syncthreads();
-      const int nt = NB - r0;
-      for (int e = t; e < nt * nt; e += blockDim.x) {   // trailing lower triangle, rank PB
-        const int i = r0 + e % nt, q = r0 + e / nt;
-        if (i < q) continue;
-        T acc = A[i][q];
-#pragma unroll
-        for (int p = 0; p < PB; ++p) acc -= A[i][o + p] * A[q][o + p];
-        A[i][q] = acc;
-      }
-      __syncthreads();
-    }
-  }
-  // inverse: diagonal blocks, one warp each; lane q solves column q
-  if (warp < NB / PB && lane < PB) {
-    const int o = warp * PB, q = lane;
-    for (int i = 0; i < PB; ++i) {
-      if (i < q) { B[o + i][o + q] = (T)0; continue; }
-      T x = (i == q) ? (T)1 : (T)0;
-      for (int p = q; p < i; ++p) x -= A[o + i][o + p] * B[o + p][o + q];
-      B[o + i][o + q] = x / A[o + i][o + i];
-    }
-  }
-  __syncthreads();
-  for (int dist = 1; dist < NB / PB; ++dist) {
-    const int nblk = NB / PB - dist;
-    for (int e = t; e < nblk * PB * PB; e += blockDim.x) {   // W_j = sum_{j <= k < i} L_ik X_kj
-      const int bj = e / (PB * PB), r = e % PB, cc = (e / PB) % PB, bi = bj + dist;
-      T acc = (T)0;
-      for (int k = bj; k < bi; ++k)
-#pragma unroll
-        for (int p = 0; p < PB; ++p) acc += A[bi * PB + r][k * PB + p] * B[k * PB + p][bj * PB + cc];
-      W[bj][r][cc] = acc;
-    }
-    __syncthreads();
-    for (int e = t; e < nblk * PB * PB; e += blockDim.x) {   // X_ij = -X_ii W_j
-      const int bj = e / (PB * PB), r = e % PB, cc = (e / PB) % PB, bi = bj + dist;
-      T acc = (T)0;
-#pragma unroll
-      for (int p = 0; p < PB; ++p) acc += B[bi * PB + r][bi * PB + p] * W[bj][p][cc];
-      B[bi * PB + r][bj * PB + cc] = -acc;
-    }
-    __syncthreads();
-  }
-  if (t == 0 && bad_idx < kn) rec_err(err, EE_PIVOT, (int64_t)first[s] + k0 + bad_idx);
-  T* Dv = Dinv + Dptr[s] + (int64_t)(k0 / NB) * NB * NB;
-  for (int e = t; e < NB * NB; e += blockDim.x) {
-    int i = e & (NB - 1), j = e >> 6;
-    bool in = i < kn && j < kn && i >= j;
-    if (in) P[i + (int64_t)m * j] = A[i][j];
-    Dv[i + NB * j] = in ? B[i][j] : (T)0;
-  }
-}
-
-// JFG_POTRF selects the diagonal-block kernel: 1 the warp-tile kernel
-// (one warp per 32 x 32 tile), 2 the CTA-wide column chains, otherwise (the
-// default) the blocked kernel above
-inline int potrf_kind() {
+// JFG_POTRF=1 selects the earlier diagonal-block kernel (one warp per 32 x 32
+// tile); the default runs the CTA-wide chains above
+inline bool potrf_cta() {
   static int v = -1;
   if (v < 0) {
     const char* e = std::getenv("JFG_POTRF");
-    v = (e && e[0] == '1') ? 1 : (e && e[0] == '2') ? 2 : 0;
+    v = (e && e[0] == '1') ? 0 : 1;
   }
-  return v;
+  return v == 1;
 }
 
 // rows [k1, m) of panel columns [k0, k1):  X := X * L_D^{-T} = X * Dinv^T,
@@ -1517,183 +1389,6 @@ k_bwd_sdiag(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
   }
 }
 
-// ---------------------------------------------------------------- fused single-strip solves
-// JFG_FUSED_SOLVE=0 keeps every level on the strip kernels
-inline bool fused_solve() {
-  static int v = -1;
-  if (v < 0) {
-    const char* e = std::getenv("JFG_FUSED_SOLVE");
-    v = (e && e[0] == '0') ? 0 : 1;
-  }
-  return v == 1;
-}
-
-// Levels whose fronts are all at most SW columns wide (the leaves and the
-// levels above them, which hold most of the factor) run each sweep as one
-// launch with one CTA per front: the diagonal product and the update below
-// it (forward), or the dots below it and the diagonal product (backward),
-// with the front's right-hand sides kept in shared memory.  Same arithmetic
-// as the strip kernels, without the second launch and the round trip of
-// the strip's y through global memory between them.
-template <int NRC>
-constexpr int fwd_front_smem() { return (2 * SW * NRC + 8 * 32 * (NRC + 1)) * (int)sizeof(double); }
-
-template <typename T, int NRC>
-__global__ void __launch_bounds__(256)
-k_fwd_front(const int32_t* __restrict__ list, const int32_t* __restrict__ first, const int32_t* __restrict__ mrows,
-            const int64_t* __restrict__ Lptr, const int64_t* __restrict__ relptr, const int64_t* __restrict__ Sptr,
-            const T* __restrict__ L, const T* __restrict__ Sinv, int nr, int64_t n, const double* __restrict__ xp,
-            double* __restrict__ tt, double* __restrict__ V) {
-  const int s = list[blockIdx.x];
-  const int f = first[s], c = first[s + 1] - f, m = mrows[s], r = m - c;
-  extern __shared__ double sdyn[];
-  double (*bs)[NRC] = reinterpret_cast<double (*)[NRC]>(sdyn);
-  double (*ys)[NRC] = reinterpret_cast<double (*)[NRC]>(sdyn + SW * NRC);
-  double (*red)[32][NRC + 1] = reinterpret_cast<double (*)[32][NRC + 1]>(sdyn + 2 * SW * NRC);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int e = threadIdx.x; e < c * NRC; e += blockDim.x) {
-    const int l = e % c, k = e / c;
-    bs[l][k] = k < nr ? xp[f + l + n * k] : 0.0;
-  }
-  __syncthreads();
-  // y = X b (X = L_cc^-1, c x c column-major), 32 rows at a time
-  const T* X = Sinv + Sptr[s];
-  for (int r0 = 0; r0 < c; r0 += 32) {
-    const int row = r0 + lane;
-    double acc[NRC];
-#pragma unroll
-    for (int k = 0; k < NRC; ++k) acc[k] = 0.0;
-    if (row < c) {
-      const T* xr = X + row;
-#pragma unroll 4
-      for (int j = w; j <= row; j += 8) {
-        const double x = (double)xr[(int64_t)c * j];
-#pragma unroll
-        for (int k = 0; k < NRC; ++k) acc[k] += x * bs[j][k];
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < NRC; ++k) red[w][lane][k] = acc[k];
-    __syncthreads();
-    for (int e = threadIdx.x; e < 32 * NRC; e += blockDim.x) {
-      const int l = e & 31, k = e >> 5;
-      if (r0 + l < c) {
-        double v = 0.0;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) v += red[q][l][k];
-        ys[r0 + l][k] = v;
-        if (k < nr) tt[f + r0 + l + n * k] = v;
-      }
-    }
-    __syncthreads();
-  }
-  // V -= L21 y, 32 rows at a time, the c columns split evenly over the warps
-  const int cw = (c + 7) / 8, l0 = w * cw, l1 = min(l0 + cw, c);
-  const T* P = L + Lptr[s];
-  double* Vs = V + relptr[s] * nr;
-  for (int row0 = c; row0 < m; row0 += 32) {
-    const int i = row0 + lane;
-    double acc[NRC];
-#pragma unroll
-    for (int k = 0; k < NRC; ++k) acc[k] = 0.0;
-    if (i < m) {
-      const T* Pi = P + i;
-#pragma unroll 8
-      for (int l = l0; l < l1; ++l) {
-        const double lv = (double)Pi[(int64_t)m * l];
-#pragma unroll
-        for (int k = 0; k < NRC; ++k) acc[k] += lv * ys[l][k];
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < NRC; ++k) red[w][lane][k] = acc[k];
-    __syncthreads();
-    for (int e = threadIdx.x; e < 32 * NRC; e += blockDim.x) {
-      const int rr = e & 31, k = e >> 5, ii = row0 + rr;
-      if (ii < m && k < nr) {
-        double t = 0.0;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) t += red[q][rr][k];
-        Vs[(ii - c) + (int64_t)r * k] -= t;
-      }
-    }
-    __syncthreads();
-  }
-}
-
-
-// backward: z = y - L21^T x_below (the update rows' x gathered 256 rows at a
-// time, each warp dotting its columns), then x = X^T z (a warp per output)
-template <int NRC>
-constexpr int bwd_front_smem() { return (NRC * 256 + SW * NRC) * (int)sizeof(double); }
-
-template <typename T, int NRC>
-__global__ void __launch_bounds__(256)
-k_bwd_front(const int32_t* __restrict__ list, const int32_t* __restrict__ first, const int32_t* __restrict__ mrows,
-            const int64_t* __restrict__ Lptr, const int64_t* __restrict__ rows_ptr, const int32_t* __restrict__ rows,
-            const int64_t* __restrict__ Sptr, const T* __restrict__ L, const T* __restrict__ Sinv, int nr, int64_t n,
-            const double* __restrict__ tt, double* __restrict__ xp) {
-  const int s = list[blockIdx.x];
-  const int f = first[s], c = first[s + 1] - f, m = mrows[s];
-  extern __shared__ double sdyn[];
-  double (*xs)[256] = reinterpret_cast<double (*)[256]>(sdyn);           // right-hand-side major
-  double (*zs)[SW] = reinterpret_cast<double (*)[SW]>(sdyn + NRC * 256);  // right-hand-side major
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  constexpr int GRP = 32 / NRC;   // lanes sharing one reduced component
-  for (int e = threadIdx.x; e < c * NRC; e += blockDim.x) {
-    const int l = e % c, k = e / c;
-    zs[k][l] = k < nr ? tt[f + l + n * k] : 0.0;
-  }
-  const T* P = L + Lptr[s];
-  const int32_t* R = rows + rows_ptr[s];
-  for (int row0 = c; row0 < m; row0 += 256) {
-    __syncthreads();   // zs written / xs free
-    for (int e = threadIdx.x; e < 256 * NRC; e += blockDim.x) {
-      const int ii = e & 255, k = e >> 8, i = row0 + ii;
-      xs[k][ii] = (i < m && k < nr) ? xp[(int64_t)R[i] + n * k] : 0.0;
-    }
-    __syncthreads();
-    for (int j = w; j < c; j += 8) {   // column j: lanes along the rows
-      const T* col = P + (int64_t)m * j;
-      double lv[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int i = row0 + lane + 32 * u;
-        lv[u] = i < m ? (double)col[i] : 0.0;
-      }
-      double acc[NRC];
-#pragma unroll
-      for (int k = 0; k < NRC; ++k) acc[k] = 0.0;
-#pragma unroll
-      for (int u = 0; u < 8; ++u)
-#pragma unroll
-        for (int k = 0; k < NRC; ++k) acc[k] += lv[u] * xs[k][lane + 32 * u];
-      const double v = warp_sum_scatter<NRC>(acc, lane);
-      if ((lane % GRP) == 0) zs[lane / GRP][j] -= v;   // column j is this warp's alone
-    }
-  }
-  __syncthreads();
-  // x_i = sum_{j >= i} X[j][i] z_j
-  const T* X = Sinv + Sptr[s];
-  for (int i = w; i < c; i += 8) {
-    const T* col = X + (int64_t)c * i;
-    double acc[NRC];
-#pragma unroll
-    for (int k = 0; k < NRC; ++k) acc[k] = 0.0;
-    for (int j0 = i; j0 < c; j0 += 32) {
-      const int j = j0 + lane;
-      if (j < c) {
-        const double x = (double)col[j];
-#pragma unroll
-        for (int k = 0; k < NRC; ++k) acc[k] += x * zs[k][j];
-      }
-    }
-    const double v = warp_sum_scatter<NRC>(acc, lane);
-    const int k = lane / GRP;
-    if ((lane % GRP) == 0 && k < nr) xp[f + i + n * k] = v;
-  }
-}
-
 __global__ void k_gather_perm(int64_t n, int nr, const int32_t* __restrict__ perm_dof,
                               const double* __restrict__ scale, const double* __restrict__ src, int64_t ldsrc,
                               double* __restrict__ xp, double sign) {
@@ -1796,7 +1491,6 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
     int bytes = 2 * NB * (NB + 1) * (int)sizeof(T);
     JFG_CUDA(cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, potrf_smem<T>()));
     JFG_CUDA(cudaFuncSetAttribute(k_potrf_cta<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, potrf_smem<T>()));
-    JFG_CUDA(cudaFuncSetAttribute(k_potrf_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, potrf_blk_smem<T>()));
     JFG_CUDA(cudaFuncSetAttribute(k_trsm_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     attr_set = true;
   }
@@ -1876,10 +1570,7 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
       const int P1 = P0 + PW;
       for (int k0 = P0; k0 < std::min(P1, lv.max_c); k0 += NB) {
         const int na = lv.active(k0);   // fronts wider than k0: a prefix of the list
-        { int ps_ = fine_prof() ? prof_start(st) : -1; { if (potrf_kind() == 0)
-            k_potrf_blk<T><<<na, 256, potrf_blk_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr, F->Dptr, Lf, Dvf,
-                                                                  k0, F->err);
-          else if (potrf_kind() == 2)
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { if (potrf_cta())
             k_potrf_cta<T><<<na, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr, F->Dptr, Lf, Dvf, k0,
                                                               F->err);
           else
@@ -1969,16 +1660,6 @@ void solve_inner_n(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int
         { int ps_ = fine_prof() ? prof_start(st) : -1; { k_vec_extend_add<NRC><<<(unsigned)tsp.cnt, 256, 0, st>>>(F->ea_child + seg.first, F->first, F->mrows, F->parent,
                                                      F->relptr, F->rel, nr, n, F->xp, F->V, F->tiles + tsp.off); count_launch(); } prof_end(ps_, st, KS_S_VEC, 0.0); }
     }
-    if constexpr (NRC <= 16) {
-      if (lv.max_c <= SW && fused_solve()) {   // one launch for the whole level
-        { int ps_ = fine_prof() ? prof_start(st) : -1;
-          k_fwd_front<T, NRC><<<(unsigned)lv.count, 256, fwd_front_smem<NRC>(), st>>>(
-              list, F->first, F->mrows, F->Lptr, F->relptr, F->Sptr, Lf, Sv, nr, n, F->xp, F->tt, F->V);
-          count_launch(); prof_end(ps_, st, KS_S_FUPD, 0.0); }
-        prof_end(pl, st, KS_LEVEL_FWD + (int)li, (double)sizeof(T) * (double)lv.nnz);
-        continue;
-      }
-    }
     int nstrip = (lv.max_c + SW - 1) / SW;
     for (int kb = 0; kb < nstrip; ++kb) {
       const auto& ts = lv.strips[kb];
@@ -2007,16 +1688,6 @@ void solve_inner_n(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int
     const int32_t* list = F->level_sn + lv.off;
     const int64_t* poff = F->part_off + lv.off;
     const int pl = (fine_prof() && li < (size_t)KS_MAX_LEVELS) ? prof_start(st) : -1;
-    if constexpr (NRC <= 16) {
-      if (lv.max_c <= SW && fused_solve()) {
-        { int ps_ = fine_prof() ? prof_start(st) : -1;
-          k_bwd_front<T, NRC><<<(unsigned)lv.count, 256, bwd_front_smem<NRC>(), st>>>(
-              list, F->first, F->mrows, F->Lptr, F->rows_ptr, F->rows, F->Sptr, Lf, Sv, nr, n, F->tt, F->xp);
-          count_launch(); prof_end(ps_, st, KS_S_BDIAG, 0.0); }
-        prof_end(pl, st, KS_LEVEL_BWD + (int)li, (double)sizeof(T) * (double)lv.nnz);
-        continue;
-      }
-    }
     int nstrip = (lv.max_c + SW - 1) / SW;
     for (int kb = nstrip - 1; kb >= 0; --kb) {
       const auto& ts = lv.strips[kb];
@@ -2051,12 +1722,6 @@ jfg_status solve_attributes_n() {
   JFG_CUDA(cudaFuncSetAttribute(k_bwd_spartial<T, NRC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 bwd_spartial_smem<NRC>()));
   JFG_CUDA(cudaFuncSetAttribute(k_bwd_sdiag<T, NRC>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_sdiag_smem<NRC>()));
-  if constexpr (NRC <= 16) {
-    JFG_CUDA(cudaFuncSetAttribute(k_fwd_front<T, NRC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  fwd_front_smem<NRC>()));
-    JFG_CUDA(cudaFuncSetAttribute(k_bwd_front<T, NRC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  bwd_front_smem<NRC>()));
-  }
   return JFG_OK;
 }
 
