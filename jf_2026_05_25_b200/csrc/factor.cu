@@ -453,7 +453,7 @@ k_potrf_diag(const int32_t* __restrict__ list, const int32_t* __restrict__ first
 // positive and finite are replaced by 1 and the smallest such column is
 // recorded; rows and columns past the front's width are the identity.
 template <typename T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
 k_potrf_cta(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
             const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
             const int64_t* __restrict__ Dptr, T* __restrict__ L, T* __restrict__ Dinv, int k0, DevError* err) {
@@ -494,9 +494,16 @@ k_potrf_cta(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
       ek[u] = -1;
     }
   }
-  // factor
+  // factor.  Each thread keeps its entries in registers; an entry reaches
+  // shared memory when its column becomes the next pivot column (final after
+  // the update by the column before it), so a step reads only final values
+  // and all its loads are independent of its stores (they issue together).
+  T av[NE];
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < NE; ++u) av[u] = ei[u] >= 0 ? A[ei[u]][ek[u]] : (T)0;
   for (int j = 0; j < NB; ++j) {
-    __syncthreads();
+    __syncthreads();   // column j final in shared memory
     T d = A[j][j];
     const bool bad = !(d > (T)0) || !isfinite((double)d);
     if (bad) {
@@ -504,11 +511,16 @@ k_potrf_cta(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
       d = (T)1;
     }
     const T rd = (T)1 / d;
+    T lij[NE], lkj[NE];
 #pragma unroll
-    for (int u = 0; u < NE; ++u) {
-      const int i = ei[u], k = ek[u];
-      if (k > j) A[i][k] = fma(-A[i][j] * rd, A[k][j], A[i][k]);
-    }
+    for (int u = 0; u < NE; ++u)
+      if (ek[u] > j) { lij[u] = A[ei[u]][j]; lkj[u] = A[ek[u]][j]; }
+#pragma unroll
+    for (int u = 0; u < NE; ++u)
+      if (ek[u] > j) av[u] = fma(-lij[u] * rd, lkj[u], av[u]);
+#pragma unroll
+    for (int u = 0; u < NE; ++u)
+      if (ek[u] == j + 1) A[ei[u]][j + 1] = av[u];
   }
   __syncthreads();
   if (t < NB) {
@@ -522,15 +534,24 @@ k_potrf_cta(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
     const int i = ei[u], k = ek[u];
     if (i >= 0) A[i][k] = (i == k) ? sv[k] : A[i][k] / sv[k];
   }
-  // inverse of the factor
-  for (int j = 0; j < NB; ++j) {
-    __syncthreads();
-    const T rl = (T)1 / A[j][j];
+  // inverse of the factor, the same way: a row of B reaches shared memory
+  // when it becomes final (after the step of the row before it)
+  T bv[NE];
 #pragma unroll
-    for (int u = 0; u < NE; ++u) {
-      const int i = ei[u], q = ek[u];
-      if (q <= j && i > j) B[i][q] = fma(-A[i][j] * rl, B[j][q], B[i][q]);
-    }
+  for (int u = 0; u < NE; ++u) bv[u] = (ei[u] >= 0 && ei[u] == ek[u]) ? (T)1 : (T)0;
+  for (int j = 0; j < NB; ++j) {
+    __syncthreads();   // row j of B final; the scaled factor visible
+    const T rl = (T)1 / A[j][j];
+    T lij[NE], bjq[NE];
+#pragma unroll
+    for (int u = 0; u < NE; ++u)
+      if (ek[u] <= j && ei[u] > j) { lij[u] = A[ei[u]][j]; bjq[u] = B[j][ek[u]]; }
+#pragma unroll
+    for (int u = 0; u < NE; ++u)
+      if (ek[u] <= j && ei[u] > j) bv[u] = fma(-lij[u] * rl, bjq[u], bv[u]);
+#pragma unroll
+    for (int u = 0; u < NE; ++u)
+      if (ei[u] == j + 1 && ek[u] <= j + 1) B[j + 1][ek[u]] = bv[u];
   }
   __syncthreads();
 #pragma unroll
