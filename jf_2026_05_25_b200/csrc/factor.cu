@@ -1437,15 +1437,25 @@ inline bool subtree_solve() {
   return v == 1;
 }
 
+// fronts of the subtree levels: at most ST_C columns and ST_MC entries
+constexpr int ST_C = 64;
+constexpr int64_t ST_MC = 32768;
+constexpr int ST_WARPS = 4;
+template <int NRC>
+constexpr int fwd_subtree_smem() { return ST_WARPS * 2 * ST_C * NRC * (int)sizeof(double); }
+template <int NRC>
+constexpr int bwd_subtree_smem() { return ST_WARPS * ST_C * NRC * (int)sizeof(double); }
+
 // forward for one front by one warp: V_s = 0, the children's update vectors
-// added, y = X b written to tt, V_s -= L21 y
+// added, y = X b (b staged in shared memory) written to tt, V_s -= L21 y
 template <typename T, int NRC>
-__device__ void fwd_front_warp(int s, int lane, const int32_t* __restrict__ child_ptr,
-                               const int32_t* __restrict__ child_list, const int32_t* __restrict__ first,
-                               const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
-                               const int64_t* __restrict__ relptr, const int32_t* __restrict__ rel,
-                               const int64_t* __restrict__ Sptr, const T* __restrict__ L,
-                               const T* __restrict__ Sinv, int nr, int64_t n, double* xp, double* tt, double* V) {
+__device__ void fwd_front_warp(int s, int lane, double (*bs)[NRC], double (*ys)[NRC],
+                               const int32_t* __restrict__ child_ptr, const int32_t* __restrict__ child_list,
+                               const int32_t* __restrict__ first, const int32_t* __restrict__ mrows,
+                               const int64_t* __restrict__ Lptr, const int64_t* __restrict__ relptr,
+                               const int32_t* __restrict__ rel, const int64_t* __restrict__ Sptr,
+                               const T* __restrict__ L, const T* __restrict__ Sinv, int nr, int64_t n, double* xp,
+                               double* tt, double* V) {
   const int f = first[s], c = first[s + 1] - f, m = mrows[s], r = m - c;
   double* Vs = V + relptr[s] * nr;
   for (int64_t e = lane; e < (int64_t)r * nr; e += 32) Vs[e] = 0.0;
@@ -1463,25 +1473,30 @@ __device__ void fwd_front_warp(int s, int lane, const int32_t* __restrict__ chil
     }
     __syncwarp();
   }
+  for (int e = lane; e < c * NRC; e += 32) {
+    const int l = e % c, k = e / c;
+    bs[l][k] = k < nr ? xp[f + l + n * k] : 0.0;
+  }
+  __syncwarp();
   // y = X b (X = L_cc^-1, c x c column-major), a lane per row
   const T* X = Sinv + Sptr[s];
   for (int r0 = 0; r0 < c; r0 += 32) {
     const int row = r0 + lane;
-    double acc[NRC];
-#pragma unroll
-    for (int k = 0; k < NRC; ++k) acc[k] = 0.0;
     if (row < c) {
+      double acc[NRC];
+#pragma unroll
+      for (int k = 0; k < NRC; ++k) acc[k] = 0.0;
       const T* xr = X + row;
       for (int j = 0; j <= row; ++j) {
         const double x = (double)xr[(int64_t)c * j];
-        const double* b = xp + f + j;
 #pragma unroll
-        for (int k = 0; k < NRC; ++k)
-          if (k < nr) acc[k] += x * b[n * k];
+        for (int k = 0; k < NRC; ++k) acc[k] += x * bs[j][k];
       }
 #pragma unroll
-      for (int k = 0; k < NRC; ++k)
+      for (int k = 0; k < NRC; ++k) {
+        ys[row][k] = acc[k];
         if (k < nr) tt[f + row + n * k] = acc[k];
+      }
     }
   }
   __syncwarp();
@@ -1497,20 +1512,19 @@ __device__ void fwd_front_warp(int s, int lane, const int32_t* __restrict__ chil
 #pragma unroll 4
       for (int l = 0; l < c; ++l) {
         const double lv = (double)Pi[(int64_t)m * l];
-        const double* y = tt + f + l;
 #pragma unroll
-        for (int k = 0; k < NRC; ++k)
-          if (k < nr) acc[k] += lv * y[n * k];
+        for (int k = 0; k < NRC; ++k) acc[k] += lv * ys[l][k];
       }
 #pragma unroll
       for (int k = 0; k < NRC; ++k)
         if (k < nr) Vs[(i - c) + (int64_t)r * k] -= acc[k];
     }
   }
+  __syncwarp();   // bs / ys free for the warp's next front
 }
 
 template <typename T, int NRC>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(ST_WARPS * 32)
 k_fwd_subtree(const int32_t* __restrict__ sub_front, const int32_t* __restrict__ sub_lev, int nb,
               const int32_t* __restrict__ child_ptr, const int32_t* __restrict__ child_list,
               const int32_t* __restrict__ first, const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
@@ -1518,25 +1532,33 @@ k_fwd_subtree(const int32_t* __restrict__ sub_front, const int32_t* __restrict__
               const T* __restrict__ L, const T* __restrict__ Sinv, int nr, int64_t n, double* xp, double* tt,
               double* V) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  extern __shared__ double sdyn[];
+  double (*bs)[NRC] = reinterpret_cast<double (*)[NRC]>(sdyn + (int64_t)w * 2 * ST_C * NRC);
+  double (*ys)[NRC] = bs + ST_C;
   const int32_t* lev = sub_lev + (int64_t)blockIdx.x * (nb + 1);
   for (int l = 0; l < nb; ++l) {
-    for (int q = lev[l] + w; q < lev[l + 1]; q += 8)
-      fwd_front_warp<T, NRC>(sub_front[q], lane, child_ptr, child_list, first, mrows, Lptr, relptr, rel, Sptr, L,
-                             Sinv, nr, n, xp, tt, V);
+    for (int q = lev[l] + w; q < lev[l + 1]; q += ST_WARPS)
+      fwd_front_warp<T, NRC>(sub_front[q], lane, bs, ys, child_ptr, child_list, first, mrows, Lptr, relptr, rel,
+                             Sptr, L, Sinv, nr, n, xp, tt, V);
     __syncthreads();   // this level's V, xp and tt visible to the next
   }
 }
 
 // backward for one front by one warp: z = y - L21^T x_below (a lane per
-// update row, one warp reduction per column, z kept in tt), then x = X^T z
+// update row, one warp reduction per column, z in shared memory), x = X^T z
 template <typename T, int NRC>
-__device__ void bwd_front_warp(int s, int lane, const int32_t* __restrict__ first,
+__device__ void bwd_front_warp(int s, int lane, double (*zs)[NRC], const int32_t* __restrict__ first,
                                const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
                                const int64_t* __restrict__ rows_ptr, const int32_t* __restrict__ rows,
                                const int64_t* __restrict__ Sptr, const T* __restrict__ L,
-                               const T* __restrict__ Sinv, int nr, int64_t n, double* tt, double* xp) {
+                               const T* __restrict__ Sinv, int nr, int64_t n, const double* tt, double* xp) {
   const int f = first[s], c = first[s + 1] - f, m = mrows[s];
   constexpr int GRP = 32 / NRC;   // lanes sharing one reduced component
+  for (int e = lane; e < c * NRC; e += 32) {
+    const int l = e % c, k = e / c;
+    zs[l][k] = k < nr ? tt[f + l + n * k] : 0.0;
+  }
+  __syncwarp();
   const T* P = L + Lptr[s];
   const int32_t* R = rows + rows_ptr[s];
   for (int i0 = c; i0 < m; i0 += 32) {
@@ -1550,8 +1572,7 @@ __device__ void bwd_front_warp(int s, int lane, const int32_t* __restrict__ firs
 #pragma unroll
       for (int k = 0; k < NRC; ++k) acc[k] = lv * xb[k];
       const double v = warp_sum_scatter<NRC>(acc, lane);
-      const int k = lane / GRP;
-      if ((lane % GRP) == 0 && k < nr) tt[f + j + n * k] -= v;
+      if ((lane % GRP) == 0) zs[j][lane / GRP] -= v;
     }
   }
   __syncwarp();
@@ -1564,27 +1585,29 @@ __device__ void bwd_front_warp(int s, int lane, const int32_t* __restrict__ firs
     for (int j = i + lane; j < c; j += 32) {
       const double x = (double)col[j];
 #pragma unroll
-      for (int k = 0; k < NRC; ++k)
-        if (k < nr) acc[k] += x * tt[f + j + n * k];
+      for (int k = 0; k < NRC; ++k) acc[k] += x * zs[j][k];
     }
     const double v = warp_sum_scatter<NRC>(acc, lane);
     const int k = lane / GRP;
     if ((lane % GRP) == 0 && k < nr) xp[f + i + n * k] = v;
   }
+  __syncwarp();   // zs free for the warp's next front
 }
 
 template <typename T, int NRC>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(ST_WARPS * 32)
 k_bwd_subtree(const int32_t* __restrict__ sub_front, const int32_t* __restrict__ sub_lev, int nb,
               const int32_t* __restrict__ first, const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
               const int64_t* __restrict__ rows_ptr, const int32_t* __restrict__ rows,
               const int64_t* __restrict__ Sptr, const T* __restrict__ L, const T* __restrict__ Sinv, int nr,
-              int64_t n, double* tt, double* xp) {
+              int64_t n, const double* tt, double* xp) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  extern __shared__ double sdyn[];
+  double (*zs)[NRC] = reinterpret_cast<double (*)[NRC]>(sdyn + (int64_t)w * ST_C * NRC);
   const int32_t* lev = sub_lev + (int64_t)blockIdx.x * (nb + 1);
   for (int l = nb - 1; l >= 0; --l) {
-    for (int q = lev[l] + w; q < lev[l + 1]; q += 8)
-      bwd_front_warp<T, NRC>(sub_front[q], lane, first, mrows, Lptr, rows_ptr, rows, Sptr, L, Sinv, nr, n, tt, xp);
+    for (int q = lev[l] + w; q < lev[l + 1]; q += ST_WARPS)
+      bwd_front_warp<T, NRC>(sub_front[q], lane, zs, first, mrows, Lptr, rows_ptr, rows, Sptr, L, Sinv, nr, n, tt, xp);
     __syncthreads();   // this level's x visible to the level below
   }
 }
@@ -1848,10 +1871,10 @@ void solve_inner_n(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int
   int64_t n = S.n;
   int ps = prof_start(st);
   // forward, leaves first: the bottom levels by subtree, the rest by level
-  const size_t lb = (F->n_bottom > 0 && subtree_solve()) ? (size_t)F->n_bottom : 0;
+  const size_t lb = (NRC <= 16 && F->n_bottom > 0 && subtree_solve()) ? (size_t)F->n_bottom : 0;
   if (lb > 0) {
     int ps_ = fine_prof() ? prof_start(st) : -1;
-    k_fwd_subtree<T, NRC><<<(unsigned)F->n_sub, 256, 0, st>>>(F->sub_front, F->sub_lev, F->n_bottom, F->child_ptr,
+    k_fwd_subtree<T, NRC><<<(unsigned)F->n_sub, ST_WARPS * 32, fwd_subtree_smem<NRC>(), st>>>(F->sub_front, F->sub_lev, F->n_bottom, F->child_ptr,
                                                              F->child_list, F->first, F->mrows, F->Lptr, F->relptr,
                                                              F->rel, F->Sptr, Lf, Sv, nr, n, F->xp, F->tt, F->V);
     count_launch();
@@ -1911,7 +1934,7 @@ void solve_inner_n(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int
   }
   if (lb > 0) {
     int ps_ = fine_prof() ? prof_start(st) : -1;
-    k_bwd_subtree<T, NRC><<<(unsigned)F->n_sub, 256, 0, st>>>(F->sub_front, F->sub_lev, F->n_bottom, F->first,
+    k_bwd_subtree<T, NRC><<<(unsigned)F->n_sub, ST_WARPS * 32, bwd_subtree_smem<NRC>(), st>>>(F->sub_front, F->sub_lev, F->n_bottom, F->first,
                                                              F->mrows, F->Lptr, F->rows_ptr, F->rows, F->Sptr, Lf, Sv,
                                                              nr, n, F->tt, F->xp);
     count_launch();
@@ -1939,6 +1962,10 @@ jfg_status solve_attributes_n() {
   JFG_CUDA(cudaFuncSetAttribute(k_bwd_spartial<T, NRC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 bwd_spartial_smem<NRC>()));
   JFG_CUDA(cudaFuncSetAttribute(k_bwd_sdiag<T, NRC>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_sdiag_smem<NRC>()));
+  JFG_CUDA(cudaFuncSetAttribute(k_fwd_subtree<T, NRC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                fwd_subtree_smem<NRC>()));
+  JFG_CUDA(cudaFuncSetAttribute(k_bwd_subtree<T, NRC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                bwd_subtree_smem<NRC>()));
   return JFG_OK;
 }
 
@@ -2232,7 +2259,16 @@ jfg_status numeric_create(jfg_model* m) {
   // subtree schedule of the bottom levels
   {
     int nb = 0;
-    while (nb < (int)S.n_levels && F->levels[nb].max_c <= SW) ++nb;
+    // levels whose fronts are all small enough for one warp each
+    while (nb < (int)S.n_levels && F->levels[nb].max_c <= ST_C) {
+      int64_t mc = 0;
+      for (int32_t q = S.level_ptr[nb]; q < S.level_ptr[nb + 1]; ++q) {
+        const int32_t s2 = S.level_sn[q];
+        mc = std::max<int64_t>(mc, (int64_t)S.sn_m[s2] * (S.sn_first[s2 + 1] - S.sn_first[s2]));
+      }
+      if (mc > ST_MC) break;
+      ++nb;
+    }
     const int64_t ns = S.ns;
     std::vector<int32_t> cptr(ns + 1, 0), clist(std::max<int64_t>(ns, 1), 0);
     for (int64_t q = 0; q < ns; ++q)
