@@ -73,15 +73,6 @@ struct NumericFactor {
   std::vector<Level> levels;
   int2* tiles = nullptr;      // every level launch's work tiles (see tile_of)
   int64_t n_tiles = 0;
-  // subtree solves of the bottom levels [0, n_bottom): every front there is
-  // at most SW columns wide.  Subtree t (a front of those levels whose parent
-  // is above them, with its descendants) is one CTA's work: its fronts are
-  // sub_front[sub_ptr[t] ..), sorted by level, level l of it starting at
-  // sub_lev[t * (n_bottom + 1) + l].  child_ptr / child_list: children of
-  // every front.
-  int n_bottom = 0, n_sub = 0;
-  int32_t *sub_ptr = nullptr, *sub_front = nullptr, *sub_lev = nullptr;
-  int32_t *child_ptr = nullptr, *child_list = nullptr;
   // factor storage
   double* L64 = nullptr;
   double* U64 = nullptr;
@@ -1419,199 +1410,6 @@ k_bwd_sdiag(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
   }
 }
 
-// ---------------------------------------------------------------- subtree solves
-// The bottom levels (every front at most SW columns wide: the leaves and
-// the levels above them, which hold most of the factor) are swept per
-// subtree instead of per level: CTA t walks subtree t level by level, one
-// warp per front, with a CTA barrier between its levels, so the GPU runs
-// thousands of independent chains at once instead of two launches per level
-// over the whole tree.  xp, tt and V are written and read inside the kernel:
-// plain (coherent) loads only.
-// JFG_SUBTREE_SOLVE=0 keeps every level on the strip kernels.
-inline bool subtree_solve() {
-  static int v = -1;
-  if (v < 0) {
-    const char* e = std::getenv("JFG_SUBTREE_SOLVE");
-    v = (e && e[0] == '0') ? 0 : 1;
-  }
-  return v == 1;
-}
-
-// fronts of the subtree levels: at most ST_C columns and ST_MC entries
-constexpr int ST_C = 64;
-constexpr int64_t ST_MC = 32768;
-constexpr int ST_WARPS = 4;
-template <int NRC>
-constexpr int fwd_subtree_smem() { return ST_WARPS * 2 * ST_C * NRC * (int)sizeof(double); }
-template <int NRC>
-constexpr int bwd_subtree_smem() { return ST_WARPS * ST_C * NRC * (int)sizeof(double); }
-
-// forward for one front by one warp: V_s = 0, the children's update vectors
-// added, y = X b (b staged in shared memory) written to tt, V_s -= L21 y
-template <typename T, int NRC>
-__device__ void fwd_front_warp(int s, int lane, double (*bs)[NRC], double (*ys)[NRC],
-                               const int32_t* __restrict__ child_ptr, const int32_t* __restrict__ child_list,
-                               const int32_t* __restrict__ first, const int32_t* __restrict__ mrows,
-                               const int64_t* __restrict__ Lptr, const int64_t* __restrict__ relptr,
-                               const int32_t* __restrict__ rel, const int64_t* __restrict__ Sptr,
-                               const T* __restrict__ L, const T* __restrict__ Sinv, int nr, int64_t n, double* xp,
-                               double* tt, double* V) {
-  const int f = first[s], c = first[s + 1] - f, m = mrows[s], r = m - c;
-  double* Vs = V + relptr[s] * nr;
-  for (int64_t e = lane; e < (int64_t)r * nr; e += 32) Vs[e] = 0.0;
-  __syncwarp();
-  for (int q = child_ptr[s]; q < child_ptr[s + 1]; ++q) {
-    const int ch = child_list[q];
-    const int rc = mrows[ch] - (first[ch + 1] - first[ch]);
-    const int32_t* rl = rel + relptr[ch];
-    const double* src = V + relptr[ch] * nr;
-    for (int a = lane; a < rc; a += 32) {   // distinct rows of a child have distinct targets
-      const int ra = rl[a];
-      double* dst = ra < c ? xp + f + ra : Vs + (ra - c);
-      const int64_t ld = ra < c ? n : (int64_t)r;
-      for (int k = 0; k < nr; ++k) dst[ld * k] += src[a + (int64_t)rc * k];
-    }
-    __syncwarp();
-  }
-  for (int e = lane; e < c * NRC; e += 32) {
-    const int l = e % c, k = e / c;
-    bs[l][k] = k < nr ? xp[f + l + n * k] : 0.0;
-  }
-  __syncwarp();
-  // y = X b (X = L_cc^-1, c x c column-major), a lane per row
-  const T* X = Sinv + Sptr[s];
-  for (int r0 = 0; r0 < c; r0 += 32) {
-    const int row = r0 + lane;
-    if (row < c) {
-      double acc[NRC];
-#pragma unroll
-      for (int k = 0; k < NRC; ++k) acc[k] = 0.0;
-      const T* xr = X + row;
-      for (int j = 0; j <= row; ++j) {
-        const double x = (double)xr[(int64_t)c * j];
-#pragma unroll
-        for (int k = 0; k < NRC; ++k) acc[k] += x * bs[j][k];
-      }
-#pragma unroll
-      for (int k = 0; k < NRC; ++k) {
-        ys[row][k] = acc[k];
-        if (k < nr) tt[f + row + n * k] = acc[k];
-      }
-    }
-  }
-  __syncwarp();
-  // V_s -= L21 y, a lane per update row
-  const T* P = L + Lptr[s];
-  for (int i0 = c; i0 < m; i0 += 32) {
-    const int i = i0 + lane;
-    if (i < m) {
-      double acc[NRC];
-#pragma unroll
-      for (int k = 0; k < NRC; ++k) acc[k] = 0.0;
-      const T* Pi = P + i;
-#pragma unroll 4
-      for (int l = 0; l < c; ++l) {
-        const double lv = (double)Pi[(int64_t)m * l];
-#pragma unroll
-        for (int k = 0; k < NRC; ++k) acc[k] += lv * ys[l][k];
-      }
-#pragma unroll
-      for (int k = 0; k < NRC; ++k)
-        if (k < nr) Vs[(i - c) + (int64_t)r * k] -= acc[k];
-    }
-  }
-  __syncwarp();   // bs / ys free for the warp's next front
-}
-
-template <typename T, int NRC>
-__global__ void __launch_bounds__(ST_WARPS * 32)
-k_fwd_subtree(const int32_t* __restrict__ sub_front, const int32_t* __restrict__ sub_lev, int nb,
-              const int32_t* __restrict__ child_ptr, const int32_t* __restrict__ child_list,
-              const int32_t* __restrict__ first, const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
-              const int64_t* __restrict__ relptr, const int32_t* __restrict__ rel, const int64_t* __restrict__ Sptr,
-              const T* __restrict__ L, const T* __restrict__ Sinv, int nr, int64_t n, double* xp, double* tt,
-              double* V) {
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  extern __shared__ double sdyn[];
-  double (*bs)[NRC] = reinterpret_cast<double (*)[NRC]>(sdyn + (int64_t)w * 2 * ST_C * NRC);
-  double (*ys)[NRC] = bs + ST_C;
-  const int32_t* lev = sub_lev + (int64_t)blockIdx.x * (nb + 1);
-  for (int l = 0; l < nb; ++l) {
-    for (int q = lev[l] + w; q < lev[l + 1]; q += ST_WARPS)
-      fwd_front_warp<T, NRC>(sub_front[q], lane, bs, ys, child_ptr, child_list, first, mrows, Lptr, relptr, rel,
-                             Sptr, L, Sinv, nr, n, xp, tt, V);
-    __syncthreads();   // this level's V, xp and tt visible to the next
-  }
-}
-
-// backward for one front by one warp: z = y - L21^T x_below (a lane per
-// update row, one warp reduction per column, z in shared memory), x = X^T z
-template <typename T, int NRC>
-__device__ void bwd_front_warp(int s, int lane, double (*zs)[NRC], const int32_t* __restrict__ first,
-                               const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
-                               const int64_t* __restrict__ rows_ptr, const int32_t* __restrict__ rows,
-                               const int64_t* __restrict__ Sptr, const T* __restrict__ L,
-                               const T* __restrict__ Sinv, int nr, int64_t n, const double* tt, double* xp) {
-  const int f = first[s], c = first[s + 1] - f, m = mrows[s];
-  constexpr int GRP = 32 / NRC;   // lanes sharing one reduced component
-  for (int e = lane; e < c * NRC; e += 32) {
-    const int l = e % c, k = e / c;
-    zs[l][k] = k < nr ? tt[f + l + n * k] : 0.0;
-  }
-  __syncwarp();
-  const T* P = L + Lptr[s];
-  const int32_t* R = rows + rows_ptr[s];
-  for (int i0 = c; i0 < m; i0 += 32) {
-    const int i = i0 + lane;
-    double xb[NRC];
-#pragma unroll
-    for (int k = 0; k < NRC; ++k) xb[k] = (i < m && k < nr) ? xp[(int64_t)R[i] + n * k] : 0.0;
-    for (int j = 0; j < c; ++j) {   // warp-uniform: every lane takes part in the reduction
-      const double lv = i < m ? (double)P[i + (int64_t)m * j] : 0.0;
-      double acc[NRC];
-#pragma unroll
-      for (int k = 0; k < NRC; ++k) acc[k] = lv * xb[k];
-      const double v = warp_sum_scatter<NRC>(acc, lane);
-      if ((lane % GRP) == 0) zs[j][lane / GRP] -= v;
-    }
-  }
-  __syncwarp();
-  const T* X = Sinv + Sptr[s];
-  for (int i = 0; i < c; ++i) {   // x_i = sum_{j >= i} X[j][i] z_j, lanes along j
-    const T* col = X + (int64_t)c * i;
-    double acc[NRC];
-#pragma unroll
-    for (int k = 0; k < NRC; ++k) acc[k] = 0.0;
-    for (int j = i + lane; j < c; j += 32) {
-      const double x = (double)col[j];
-#pragma unroll
-      for (int k = 0; k < NRC; ++k) acc[k] += x * zs[j][k];
-    }
-    const double v = warp_sum_scatter<NRC>(acc, lane);
-    const int k = lane / GRP;
-    if ((lane % GRP) == 0 && k < nr) xp[f + i + n * k] = v;
-  }
-  __syncwarp();   // zs free for the warp's next front
-}
-
-template <typename T, int NRC>
-__global__ void __launch_bounds__(ST_WARPS * 32)
-k_bwd_subtree(const int32_t* __restrict__ sub_front, const int32_t* __restrict__ sub_lev, int nb,
-              const int32_t* __restrict__ first, const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
-              const int64_t* __restrict__ rows_ptr, const int32_t* __restrict__ rows,
-              const int64_t* __restrict__ Sptr, const T* __restrict__ L, const T* __restrict__ Sinv, int nr,
-              int64_t n, const double* tt, double* xp) {
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  extern __shared__ double sdyn[];
-  double (*zs)[NRC] = reinterpret_cast<double (*)[NRC]>(sdyn + (int64_t)w * ST_C * NRC);
-  const int32_t* lev = sub_lev + (int64_t)blockIdx.x * (nb + 1);
-  for (int l = nb - 1; l >= 0; --l) {
-    for (int q = lev[l] + w; q < lev[l + 1]; q += ST_WARPS)
-      bwd_front_warp<T, NRC>(sub_front[q], lane, zs, first, mrows, Lptr, rows_ptr, rows, Sptr, L, Sinv, nr, n, tt, xp);
-    __syncthreads();   // this level's x visible to the level below
-  }
-}
-
 __global__ void k_gather_perm(int64_t n, int nr, const int32_t* __restrict__ perm_dof,
                               const double* __restrict__ scale, const double* __restrict__ src, int64_t ldsrc,
                               double* __restrict__ xp, double sign) {
@@ -1870,17 +1668,8 @@ void solve_inner_n(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int
   const Symbolic& S = m->sym();
   int64_t n = S.n;
   int ps = prof_start(st);
-  // forward, leaves first: the bottom levels by subtree, the rest by level
-  const size_t lb = (NRC <= 16 && F->n_bottom > 0 && subtree_solve()) ? (size_t)F->n_bottom : 0;
-  if (lb > 0) {
-    int ps_ = fine_prof() ? prof_start(st) : -1;
-    k_fwd_subtree<T, NRC><<<(unsigned)F->n_sub, ST_WARPS * 32, fwd_subtree_smem<NRC>(), st>>>(F->sub_front, F->sub_lev, F->n_bottom, F->child_ptr,
-                                                             F->child_list, F->first, F->mrows, F->Lptr, F->relptr,
-                                                             F->rel, F->Sptr, Lf, Sv, nr, n, F->xp, F->tt, F->V);
-    count_launch();
-    prof_end(ps_, st, KS_S_FUPD, 0.0);
-  }
-  for (size_t li = lb; li < F->levels.size(); ++li) {
+  // forward, leaves first
+  for (size_t li = 0; li < F->levels.size(); ++li) {
     const auto& lv = F->levels[li];
     const int32_t* list = F->level_sn + lv.off;
     const int pl = (fine_prof() && li < (size_t)KS_MAX_LEVELS) ? prof_start(st) : -1;
@@ -1915,7 +1704,7 @@ void solve_inner_n(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int
     prof_end(pl, st, KS_LEVEL_FWD + (int)li, (double)sizeof(T) * (double)lv.nnz);
   }
   // backward, root first
-  for (size_t li = F->levels.size(); li-- > lb;) {
+  for (size_t li = F->levels.size(); li-- > 0;) {
     const auto& lv = F->levels[li];
     const int32_t* list = F->level_sn + lv.off;
     const int64_t* poff = F->part_off + lv.off;
@@ -1931,14 +1720,6 @@ void solve_inner_n(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int
                                                  F->part, F->tt, F->xp, F->tiles + ts.diag.off); count_launch(); } prof_end(ps_, st, KS_S_BDIAG, 0.0); }
     }
     prof_end(pl, st, KS_LEVEL_BWD + (int)li, (double)sizeof(T) * (double)lv.nnz);
-  }
-  if (lb > 0) {
-    int ps_ = fine_prof() ? prof_start(st) : -1;
-    k_bwd_subtree<T, NRC><<<(unsigned)F->n_sub, ST_WARPS * 32, bwd_subtree_smem<NRC>(), st>>>(F->sub_front, F->sub_lev, F->n_bottom, F->first,
-                                                             F->mrows, F->Lptr, F->rows_ptr, F->rows, F->Sptr, Lf, Sv,
-                                                             nr, n, F->tt, F->xp);
-    count_launch();
-    prof_end(ps_, st, KS_S_BDIAG, 0.0);
   }
   // algorithmic bytes: the factor read twice (forward and backward) plus the
   // permuted vectors read and written in each sweep
@@ -1962,10 +1743,6 @@ jfg_status solve_attributes_n() {
   JFG_CUDA(cudaFuncSetAttribute(k_bwd_spartial<T, NRC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 bwd_spartial_smem<NRC>()));
   JFG_CUDA(cudaFuncSetAttribute(k_bwd_sdiag<T, NRC>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_sdiag_smem<NRC>()));
-  JFG_CUDA(cudaFuncSetAttribute(k_fwd_subtree<T, NRC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                fwd_subtree_smem<NRC>()));
-  JFG_CUDA(cudaFuncSetAttribute(k_bwd_subtree<T, NRC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                bwd_subtree_smem<NRC>()));
   return JFG_OK;
 }
 
@@ -2256,69 +2033,6 @@ jfg_status numeric_create(jfg_model* m) {
     upload(tl, &F->tiles, c, st);
     if (st != JFG_OK) return st;
   }
-  // subtree schedule of the bottom levels
-  {
-    int nb = 0;
-    // levels whose fronts are all small enough for one warp each
-    while (nb < (int)S.n_levels && F->levels[nb].max_c <= ST_C) {
-      int64_t mc = 0;
-      for (int32_t q = S.level_ptr[nb]; q < S.level_ptr[nb + 1]; ++q) {
-        const int32_t s2 = S.level_sn[q];
-        mc = std::max<int64_t>(mc, (int64_t)S.sn_m[s2] * (S.sn_first[s2 + 1] - S.sn_first[s2]));
-      }
-      if (mc > ST_MC) break;
-      ++nb;
-    }
-    const int64_t ns = S.ns;
-    std::vector<int32_t> cptr(ns + 1, 0), clist(std::max<int64_t>(ns, 1), 0);
-    for (int64_t q = 0; q < ns; ++q)
-      if (S.sn_parent[q] >= 0) cptr[S.sn_parent[q] + 1]++;
-    for (int64_t q = 0; q < ns; ++q) cptr[q + 1] += cptr[q];
-    {
-      std::vector<int32_t> pos(cptr.begin(), cptr.end() - 1);
-      for (int64_t q = 0; q < ns; ++q)
-        if (S.sn_parent[q] >= 0) clist[pos[S.sn_parent[q]]++] = (int32_t)q;
-    }
-    // subtrees: bottom fronts whose parent is above the bottom levels, with
-    // their descendants (all bottom), fronts sorted by level; largest first
-    std::vector<std::vector<int32_t>> subs;
-    if (nb > 0) {
-      for (int64_t q = 0; q < ns; ++q) {
-        const int32_t p = S.sn_parent[q];
-        if (S.sn_level[q] >= nb || (p >= 0 && S.sn_level[p] < nb)) continue;
-        std::vector<int32_t> mem{(int32_t)q};
-        for (size_t h = 0; h < mem.size(); ++h)
-          for (int32_t k = cptr[mem[h]]; k < cptr[mem[h] + 1]; ++k) mem.push_back(clist[k]);
-        std::stable_sort(mem.begin(), mem.end(),
-                         [&](int32_t a, int32_t b) { return S.sn_level[a] < S.sn_level[b]; });
-        subs.push_back(std::move(mem));
-      }
-      std::stable_sort(subs.begin(), subs.end(),
-                       [](const std::vector<int32_t>& a, const std::vector<int32_t>& b) { return a.size() > b.size(); });
-    }
-    F->n_bottom = subs.empty() ? 0 : nb;
-    F->n_sub = (int)subs.size();
-    std::vector<int32_t> sptr(F->n_sub + 1, 0), sfront(std::max<int64_t>(ns, 1), 0),
-        slev(std::max<int64_t>((int64_t)F->n_sub * (F->n_bottom + 1), 1), 0);
-    for (int t = 0; t < F->n_sub; ++t) {
-      const auto& mem = subs[t];
-      const int32_t base = sptr[t];
-      for (size_t h = 0; h < mem.size(); ++h) sfront[base + h] = mem[h];
-      sptr[t + 1] = base + (int32_t)mem.size();
-      int32_t* lev = slev.data() + (int64_t)t * (F->n_bottom + 1);
-      size_t h = 0;
-      for (int l = 0; l <= F->n_bottom; ++l) {
-        while (h < mem.size() && S.sn_level[mem[h]] < l) ++h;
-        lev[l] = base + (int32_t)h;
-      }
-    }
-    upload(sptr, &F->sub_ptr, c, st);
-    upload(sfront, &F->sub_front, c, st);
-    upload(slev, &F->sub_lev, c, st);
-    upload(cptr, &F->child_ptr, c, st);
-    upload(clist, &F->child_list, c, st);
-    if (st != JFG_OK) return st;
-  }
   // strip metadata: 64-block inverse offsets, 256-strip inverse offsets with
   // their work items (front, strip, block column), per-level partial offsets
   {
@@ -2405,9 +2119,6 @@ void numeric_destroy(jfg_model* m) {
   fr(F->free_mask, m->ndof);
   fr(F->Dptr, 8 * S.ns); fr(F->Sptr, 8 * S.ns); fr(F->part_off, 8 * S.ns);
   fr(F->tiles, sizeof(int2) * std::max<int64_t>(F->n_tiles, 1));
-  fr(F->sub_ptr, 4 * (F->n_sub + 1)); fr(F->sub_front, 4 * std::max<int64_t>(S.ns, 1));
-  fr(F->sub_lev, 4 * std::max<int64_t>((int64_t)F->n_sub * (F->n_bottom + 1), 1));
-  fr(F->child_ptr, 4 * (S.ns + 1)); fr(F->child_list, 4 * std::max<int64_t>(S.ns, 1));
   int64_t ni = std::max<int64_t>(F->n_inv_items, 1);
   fr(F->inv_sn, 4 * ni); fr(F->inv_kb, 4 * ni); fr(F->inv_jb, 4 * ni);
   fr(F->Dinv64, 8 * F->dinv_len); fr(F->Dinv32, 4 * F->dinv_len); fr(F->part, 8 * F->part_len);
@@ -2565,8 +2276,6 @@ void numeric_bytes(jfg_model* m, int precision, int nrhs, int64_t* now, int64_t*
     n_tiles = (int64_t)tl.size();
   }
   base += 8 * part + 8 * std::max<int64_t>(n_tiles, 1);
-  // subtree schedule (bounded by every front starting a subtree)
-  base += 4 * (3 * (ns + 1) + (F ? (int64_t)F->n_sub * (F->n_bottom + 1) : ns * (S.n_levels + 1)) + 1);
   auto fp64 = [&]() { return 8 * S.nnz_L + 8 * ublk + 8 * std::max<int64_t>(dl, 1) + 8 * std::max<int64_t>(sl, 1); };
   auto mixed = [&]() {
     int64_t pk = 0;
