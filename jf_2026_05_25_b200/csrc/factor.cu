@@ -978,6 +978,18 @@ __global__ void k_vec_extend_add(const int32_t* __restrict__ child, const int32_
 }
 
 // ---------------------------------------------------------------- strip solves
+// JFG_FWD_ROWS128=1: the forward update of 8-column sweeps also runs the
+// 128-rows-per-CTA kernel (one thread per row) instead of 32 rows x 8
+// column groups
+inline bool fwd_rows128() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = std::getenv("JFG_FWD_ROWS128");
+    v = (e && e[0] == '1') ? 1 : 0;
+  }
+  return v == 1;
+}
+
 // The solve sweeps every front of a level in strips of SW = 256 columns.  The
 // inverse X of each strip's diagonal block (kw x kw, kw = min(256, width
 // left)) is formed once per factorisation (k_strip_inverse), so the diagonal
@@ -1686,10 +1698,11 @@ void solve_inner_n(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int
       const auto& ts = lv.strips[kb];
       if (ts.diag.cnt > 0) { int ps_ = fine_prof() ? prof_start(st) : -1; { k_fwd_sdiag<T, NRC><<<(unsigned)ts.diag.cnt, 256, fwd_sdiag_smem<NRC>(), st>>>(list, F->first, F->Sptr, Sv, kb, nr, n, F->xp, F->tt, F->tiles + ts.diag.off);
         count_launch(); } prof_end(ps_, st, KS_S_FDIAG, 0.0); }
-      const auto& tu = NRC == 8 ? ts.upd32 : ts.upd128;
+      const bool narrow = NRC == 8 && !fwd_rows128();
+      const auto& tu = narrow ? ts.upd32 : ts.upd128;
       if (tu.cnt > 0) {
         int ps_ = fine_prof() ? prof_start(st) : -1;
-        if constexpr (NRC == 8) {
+        if (narrow) {
           k_fwd_supdate<T><<<(unsigned)tu.cnt, 256, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->relptr, Lf, kb,
                                                               nr, n, F->tt, F->xp, F->V, F->tiles + tu.off);
         } else {
