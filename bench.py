@@ -288,6 +288,15 @@ def kernel_stats(L):
     return out
 
 
+# DRAM bytes per tensor-core flop of the mixed factor's 3xTF32 update kernel
+# (k_update_tf32x3), from one ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum over all 432 launches of four factorisations of the
+# 16^3 CTETRA10 block, 9.39 GB, divided by the updates' algorithmic flops,
+# 4 x 1.996e11).  Scaled to a launch of the full-size block by its flops: an
+# upper bound there, since larger fronts reuse their tiles more.
+TC_DRAM_BYTES_PER_FLOP = 0.01176
+
+
 def roofline_from_stats(stats, prec, note=""):
     """Roofline of the kernel class with the most device time among the
     classes whose algorithmic work is counted (the solve sweep is one class:
@@ -314,8 +323,15 @@ def roofline_from_stats(stats, prec, note=""):
         achieved = s["units"] / (s["ms"] / 1000.0) / 1e9
         peak, src = peaks["hbm_gbs"], peaks["src"] + " hbm_gbs"
         roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s"}
-    roof.update({"frac": achieved / peak, "traffic": None, "peak_source": src, "launches": s["launches"],
+    traffic = None
+    if kinds[name] == "flop" and prec == lib.PREC_MIXED and name in ("schur_update", "f_panel_update"):
+        traffic = TC_DRAM_BYTES_PER_FLOP * s["units"] / s["launches"]
+    roof.update({"frac": achieved / peak, "traffic": traffic, "peak_source": src, "launches": s["launches"],
                  "ms_total": s["ms"], "ms_per_launch": ms_launch, "units_per_launch": s["units"] / s["launches"],
+                 "traffic_source": (None if traffic is None else
+                                    "bytes per flop of the 3xTF32 update kernel from an ncu capture of the 16^3 "
+                                    "block (dram read + write of all its launches / their flops) x this launch's "
+                                    "flops; an upper bound at full size"),
                  "pass": "separate untimed pass with the library's event brackets (graphs off)" +
                          (": " + note if note else ""),
                  "all_classes": stats})
