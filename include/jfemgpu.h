@@ -182,6 +182,16 @@ jfg_status jfg_residual(jfg_model* model, int32_t nrhs, const double* U,
 /* Element stresses and strains from displacement fields U (ndof x nrhs,
  * column-major, the node-frame displacements jfg_solve returns), the step
  * after the solve in _build_results_from_state (solve_case.jl:182-303).
+ * kind 0 = CQUAD4, at the element centre in the element frame as
+ * recover_shell_stresses! on the default isotropic PSHELL path
+ * (src/solver/stress_recovery.jl:505-1237): out is nrhs x n_q4 records of
+ * 31 doubles (load case major): forces fx fy fxy mx my mxy qx qy; stresses
+ * at fibre -T/2 then +T/2, each sx sy txy von_mises major minor; membrane
+ * strain ex ey gxy major minor; curvature (-kappa, the reference's sign)
+ * kx ky kxy major minor; the major principal stress at -T/2.  The shear
+ * resultant is the area-mean MacNeal resultant.  Elements whose stiffness
+ * was refused get NaN records.  The bilinear corner forces are not
+ * returned.
  * kind 2 = CTETRA10, at the element centroid as recover_solid_stresses!
  * (src/solver/stress_recovery.jl:1823-1960): out is nrhs x n_t10 records of
  * 13 doubles (load case major): sxx syy szz txy tyz tzx, exx eyy ezz gxy gyz

@@ -599,8 +599,12 @@ jfg_status jfg_residual(jfg_model* m, int32_t nrhs, const double* U, const doubl
 jfg_status jfg_recover_stresses(jfg_model* m, int32_t kind, int32_t nrhs, const double* U, double* out) {
   JFG_TRY(check_model(m));
   if (nrhs <= 0 || !U || !out) { set_error("nrhs must be positive and U, out non-null"); return JFG_BAD_INPUT; }
-  if (kind != 2) { set_error("stress recovery is available for CTETRA10 (kind 2)"); return JFG_UNSUPPORTED; }
-  const int64_t len = m->ndof * (int64_t)nrhs, olen = 13 * m->n_t10 * (int64_t)nrhs;
+  if (kind != 0 && kind != 2) {
+    set_error("stress recovery is available for CQUAD4 (kind 0) and CTETRA10 (kind 2)");
+    return JFG_UNSUPPORTED;
+  }
+  const int64_t len = m->ndof * (int64_t)nrhs;
+  const int64_t olen = kind == 0 ? 31 * m->n_q4 * (int64_t)nrhs : 13 * m->n_t10 * (int64_t)nrhs;
   if (olen == 0) return JFG_OK;
   double *dU = nullptr, *dO = nullptr;
   JFG_TRY(dev_alloc(m->ctx, (void**)&dU, 8 * len));
@@ -608,7 +612,8 @@ jfg_status jfg_recover_stresses(jfg_model* m, int32_t kind, int32_t nrhs, const 
   if (st) { dev_free(m->ctx, dU, 8 * len); return st; }
   cudaStream_t s = m->stream;
   cudaError_t e = cudaMemcpyAsync(dU, U, 8 * len, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) st = recover_t10_stresses(m, nrhs, dU, dO, s);
+  if (e == cudaSuccess)
+    st = kind == 0 ? recover_q4_stresses(m, nrhs, dU, dO, s) : recover_t10_stresses(m, nrhs, dU, dO, s);
   if (e == cudaSuccess && st == JFG_OK) e = cudaMemcpyAsync(out, dO, 8 * olen, cudaMemcpyDeviceToHost, s);
   cudaError_t e2 = cudaStreamSynchronize(s);
   dev_free(m->ctx, dU, 8 * len);

@@ -215,11 +215,7 @@ __device__ int macneal_operator(const double lc[8], const double* Cb, const doub
 // membrane and bending, the shear term, lumped drilling, the
 // section-kinematic enrichment and the node-frame transform.  The prep record
 // per element is Q4P doubles of scratch.
-constexpr int Q4P_LC = 0, Q4P_V = 8, Q4P_CM = 17, Q4P_CB = 26, Q4P_CS = 35, Q4P_SHP = 39, Q4P_DETJC = 40,
-              Q4P_IJC = 41, Q4P_K6 = 45, Q4P_H = 46, Q4P_SHEAR = 47, Q4P_D = 48, Q4P_SOL = 96, Q4P_CI = 144,
-              Q4P_KBB = 176, Q4P_KBBB = 192, Q4P_STATUS = 208;
 constexpr int Q4P = Q4_PREP_STRIDE;
-static_assert(Q4P_STATUS < Q4P, "CQUAD4 prep record layout");
 
 __global__ void __launch_bounds__(128)
 k_q4_prep(int64_t n, const int32_t* __restrict__ nodes, const double* __restrict__ sect,
@@ -1201,6 +1197,15 @@ k_q8(int64_t n, const int32_t* __restrict__ q8n, const double* __restrict__ q8s,
 }
 
 }  // namespace
+
+jfg_status launch_q4_prep(const jfg_model* m, cudaStream_t st) {
+  if (m->n_q4 == 0) return JFG_OK;
+  k_q4_prep<<<(unsigned)((m->n_q4 + 127) / 128), 128, 0, st>>>(m->n_q4, m->d_q4n, m->d_q4s, m->d_xyz, m->d_q4prep,
+                                                                m->d_err);
+  count_launch();
+  JFG_CUDA(cudaGetLastError());
+  return JFG_OK;
+}
 
 jfg_status launch_elements(jfg_model* m, cudaStream_t st) {
   if (m->n_q4 > 0) {

@@ -443,16 +443,14 @@ k_potrf_diag(const int32_t* __restrict__ list, const int32_t* __restrict__ first
 }
 
 // Cholesky of the NB x NB diagonal block at column k0 of every front of the
-// level and the inverse of its factor, with the whole CTA on both serial
-// chains.  Each thread owns up to 9 entries of the 64 x 64 lower triangle.
-// Factor: right-looking on unscaled columns (a_ik -= a_ij a_kj / a_jj for
-// j < k <= i, the L D L^T form), one block barrier per column, and the
-// columns scaled by 1/sqrt(a_jj) at the end.  Inverse: X = L^{-1} by rows,
-// right-looking on the residual R (R_iq -= L_ij R_jq / L_jj for q <= j < i),
-// one barrier per row, X_iq = R_iq / L_ii at the end.  Pivots that are not
-// positive and finite are replaced by 1 and the smallest such column is
-// recorded; rows and columns past the front's width are the identity.
-template <typename T>
+// level and the inverse of its factor, with the whole CTA on the serial
+// chains: FUSED, one chain of one block barrier per column for both; else
+// the factor's chain and then the inverse's (twice the barriers, a third of
+// the entries busy per step instead of two thirds).  Each thread owns up to
+// 9 entries of the 64 x 64 lower triangle.  Pivots that are not positive
+// and finite are replaced by 1 and the smallest such column is recorded;
+// rows and columns past the front's width are the identity.
+template <typename T, bool FUSED>
 __global__ void __launch_bounds__(256, 2)
 k_potrf_cta(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
             const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
@@ -489,11 +487,77 @@ k_potrf_cta(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
       while (i * (i + 1) / 2 > e) --i;
       ei[u] = i;
       ek[u] = e - i * (i + 1) / 2;
-    } else {   // no entry: every predicate below is false for (-1, -1)
+    }
+    if (e >= NB * (NB + 1) / 2 || ei[u] >= kn) {
+      // no entry, or one of the identity rows past the block's width (they
+      // never change): every predicate below is false for (-1, -1)
       ei[u] = -1;
       ek[u] = -1;
     }
   }
+  if constexpr (FUSED) {
+  // One chain of kn steps computes the unscaled factor U (L = U D^-1/2,
+  // D = diag(U)) and the rows of R, where U^-1 = D^-1 R, together: step j
+  // applies pivot column j to the factor entries right of it (a_ik -=
+  // a_ij a_kj / a_jj, j < k <= i) and to the inverse entries left of it
+  // (r_iq -= a_ij r_jq / a_jj, q <= j < i).  An entry (i, k) is a factor
+  // entry until step k - 1, which makes it final; it is then published to
+  // shared memory as part of pivot column k and the same register restarts
+  // as r_ik (the identity), published as part of row i once step i - 1 has
+  // made it final.  Each step reads only published values, so all its loads
+  // issue together.  At the end L_ik = a_ik / sqrt(a_kk) and
+  // (L^-1)_iq = r_iq / sqrt(a_ii).
+  T v[NE];
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < NE; ++u)
+    v[u] = ei[u] < 0 ? (T)0 : ek[u] == 0 ? (ei[u] == 0 ? (T)1 : (T)0) : A[ei[u]][ek[u]];
+  // Rows and columns from kn on are the identity and stay so (their
+  // multipliers a_ij, j < kn <= i, are zero), so only kn steps do work.
+  for (int j = 0; j < kn; ++j) {
+    __syncthreads();   // pivot column j and row j of R final in shared memory
+    T d = A[j][j];
+    const bool bad = !(d > (T)0) || !isfinite((double)d);
+    if (bad) {
+      if (t == 0) atomicMin(&bad_idx, j);
+      d = (T)1;
+    }
+    const T rd = (T)1 / d;
+    T lij[NE], pj[NE];
+#pragma unroll
+    for (int u = 0; u < NE; ++u)
+      if (ei[u] > j) { lij[u] = A[ei[u]][j]; pj[u] = ek[u] > j ? A[ek[u]][j] : B[j][ek[u]]; }
+#pragma unroll
+    for (int u = 0; u < NE; ++u)
+      if (ei[u] > j) v[u] = fma(-lij[u] * rd, pj[u], v[u]);
+#pragma unroll
+    for (int u = 0; u < NE; ++u) {
+      if (ek[u] == j + 1) {   // factor entry final: publish, restart as r_ik
+        A[ei[u]][j + 1] = v[u];
+        v[u] = ei[u] == ek[u] ? (T)1 : (T)0;
+      } else if (ei[u] == j + 1 && ek[u] <= j) {
+        B[j + 1][ek[u]] = v[u];
+      }
+    }
+  }
+  __syncthreads();
+  if (t < NB) {
+    T d = A[t][t];
+    const bool bad = !(d > (T)0) || !isfinite((double)d);
+    sv[t] = bad ? (T)1 : sqrt(d);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < NE; ++u) {
+    const int i = ei[u], k = ek[u];
+    if (i >= 0) {
+      A[i][k] = (i == k) ? sv[k] : A[i][k] / sv[k];
+      B[i][k] = B[i][k] / sv[i];
+    }
+  }
+  __syncthreads();
+  } else {
+  // Two chains: the factor, then the inverse of the scaled factor.
   // factor.  Each thread keeps its entries in registers; an entry reaches
   // shared memory when its column becomes the next pivot column (final after
   // the update by the column before it), so a step reads only final values
@@ -502,12 +566,12 @@ k_potrf_cta(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
   __syncthreads();
 #pragma unroll
   for (int u = 0; u < NE; ++u) av[u] = ei[u] >= 0 ? A[ei[u]][ek[u]] : (T)0;
-  for (int j = 0; j < NB; ++j) {
+  for (int j = 0; j < kn; ++j) {
     __syncthreads();   // column j final in shared memory
     T d = A[j][j];
     const bool bad = !(d > (T)0) || !isfinite((double)d);
     if (bad) {
-      if (t == 0 && j < kn) atomicMin(&bad_idx, j);
+      if (t == 0) atomicMin(&bad_idx, j);
       d = (T)1;
     }
     const T rd = (T)1 / d;
@@ -539,7 +603,7 @@ k_potrf_cta(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
   T bv[NE];
 #pragma unroll
   for (int u = 0; u < NE; ++u) bv[u] = (ei[u] >= 0 && ei[u] == ek[u]) ? (T)1 : (T)0;
-  for (int j = 0; j < NB; ++j) {
+  for (int j = 0; j < kn; ++j) {
     __syncthreads();   // row j of B final; the scaled factor visible
     const T rl = (T)1 / A[j][j];
     T lij[NE], bjq[NE];
@@ -560,6 +624,7 @@ k_potrf_cta(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
     if (i >= 0) B[i][q] = B[i][q] / A[i][i];
   }
   __syncthreads();
+  }
   if (t == 0 && bad_idx < kn) rec_err(err, EE_PIVOT, (int64_t)first[s] + k0 + bad_idx);
   T* Dv = Dinv + Dptr[s] + (int64_t)(k0 / NB) * NB * NB;
   for (int e = t; e < NB * NB; e += blockDim.x) {
@@ -579,6 +644,20 @@ inline bool potrf_cta() {
     v = (e && e[0] == '1') ? 0 : 1;
   }
   return v == 1;
+}
+
+// which k_potrf_cta chain a launch of na CTAs runs: the fused chain where the
+// launch fills the GPU (about 2 x 148 CTAs and more: per-step issue, not the
+// chain's latency, sets the time), the two chains below that (a single CTA
+// runs its 64 x 64 block in 56 instead of 73 us).  JFG_POTRF_FUSED=0 / 1
+// forces either.
+inline bool potrf_fused(int na) {
+  static int v = -2;
+  if (v == -2) {
+    const char* e = std::getenv("JFG_POTRF_FUSED");
+    v = (e && e[0] == '0') ? 0 : (e && e[0] == '1') ? 1 : -1;
+  }
+  return v == 1 || (v == -1 && na >= 296);
 }
 
 // rows [k1, m) of panel columns [k0, k1):  X := X * L_D^{-T} = X * Dinv^T,
@@ -978,18 +1057,6 @@ __global__ void k_vec_extend_add(const int32_t* __restrict__ child, const int32_
 }
 
 // ---------------------------------------------------------------- strip solves
-// JFG_FWD_ROWS128=1: the forward update of 8-column sweeps also runs the
-// 128-rows-per-CTA kernel (one thread per row) instead of 32 rows x 8
-// column groups
-inline bool fwd_rows128() {
-  static int v = -1;
-  if (v < 0) {
-    const char* e = std::getenv("JFG_FWD_ROWS128");
-    v = (e && e[0] == '1') ? 1 : 0;
-  }
-  return v == 1;
-}
-
 // The solve sweeps every front of a level in strips of SW = 256 columns.  The
 // inverse X of each strip's diagonal block (kw x kw, kw = min(256, width
 // left)) is formed once per factorisation (k_strip_inverse), so the diagonal
@@ -1523,7 +1590,8 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
   if (!attr_set) {
     int bytes = 2 * NB * (NB + 1) * (int)sizeof(T);
     JFG_CUDA(cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, potrf_smem<T>()));
-    JFG_CUDA(cudaFuncSetAttribute(k_potrf_cta<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, potrf_smem<T>()));
+    JFG_CUDA(cudaFuncSetAttribute(k_potrf_cta<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, potrf_smem<T>()));
+    JFG_CUDA(cudaFuncSetAttribute(k_potrf_cta<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, potrf_smem<T>()));
     JFG_CUDA(cudaFuncSetAttribute(k_trsm_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     attr_set = true;
   }
@@ -1603,9 +1671,12 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
       const int P1 = P0 + PW;
       for (int k0 = P0; k0 < std::min(P1, lv.max_c); k0 += NB) {
         const int na = lv.active(k0);   // fronts wider than k0: a prefix of the list
-        { int ps_ = fine_prof() ? prof_start(st) : -1; { if (potrf_cta())
-            k_potrf_cta<T><<<na, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr, F->Dptr, Lf, Dvf, k0,
-                                                              F->err);
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { if (potrf_cta() && potrf_fused(na))
+            k_potrf_cta<T, true><<<na, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr, F->Dptr, Lf,
+                                                                    Dvf, k0, F->err);
+          else if (potrf_cta())
+            k_potrf_cta<T, false><<<na, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr, F->Dptr, Lf,
+                                                                     Dvf, k0, F->err);
           else
             k_potrf_diag<T><<<na, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr,
                                                                F->Dptr, Lf, Dvf, k0, F->err);
@@ -1698,7 +1769,7 @@ void solve_inner_n(jfg_model* m, NumericFactor* F, const T* Lf, const T* Sv, int
       const auto& ts = lv.strips[kb];
       if (ts.diag.cnt > 0) { int ps_ = fine_prof() ? prof_start(st) : -1; { k_fwd_sdiag<T, NRC><<<(unsigned)ts.diag.cnt, 256, fwd_sdiag_smem<NRC>(), st>>>(list, F->first, F->Sptr, Sv, kb, nr, n, F->xp, F->tt, F->tiles + ts.diag.off);
         count_launch(); } prof_end(ps_, st, KS_S_FDIAG, 0.0); }
-      const bool narrow = NRC == 8 && !fwd_rows128();
+      const bool narrow = NRC == 8;
       const auto& tu = narrow ? ts.upd32 : ts.upd128;
       if (tu.cnt > 0) {
         int ps_ = fine_prof() ? prof_start(st) : -1;

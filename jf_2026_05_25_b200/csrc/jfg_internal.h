@@ -83,6 +83,14 @@ __device__ __forceinline__ void tile_of(const int2* __restrict__ tiles, int& q, 
 // doubles per CQUAD4 of the scratch record passed from the thread-per-element
 // pass to the warp-per-element pass of the element kernel
 constexpr int Q4_PREP_STRIDE = 210;
+// CQUAD4 prep record (k_q4_prep, one per element): local corner coordinates,
+// element frame rows v1 v2 v3, rotated section Cm Cb Cs, the shape law,
+// centre Jacobian determinant and inverse, k6rot, h, the shear flag, the
+// MacNeal shear operator D (4 x 12) and Z^-1 D, internal-mode blocks, status.
+constexpr int Q4P_LC = 0, Q4P_V = 8, Q4P_CM = 17, Q4P_CB = 26, Q4P_CS = 35, Q4P_SHP = 39, Q4P_DETJC = 40,
+              Q4P_IJC = 41, Q4P_K6 = 45, Q4P_H = 46, Q4P_SHEAR = 47, Q4P_D = 48, Q4P_SOL = 96, Q4P_CI = 144,
+              Q4P_KBB = 176, Q4P_KBBB = 192, Q4P_STATUS = 208;
+static_assert(Q4P_STATUS < Q4_PREP_STRIDE, "CQUAD4 prep record layout");
 
 struct DevError {
   int32_t code;        // 0 = none
@@ -193,6 +201,7 @@ jfg_status device_node_blocks(jfg_model* m, double* blocks);
 // factor.cu: fronts of each level listed by decreasing width (then index),
 // as the level launches expect; done once, right after the analysis
 void sort_level_lists(Symbolic& S);
+jfg_status launch_q4_prep(const jfg_model* m, cudaStream_t st);
 jfg_status launch_elements_into(const jfg_model* m, cudaStream_t st, double* ev, double* q4prep, DevError* err);
 // CTRIA3 element matrices (324 doubles each, column-major) into ev
 jfg_status launch_t3(const jfg_model* m, cudaStream_t st, double* ev, DevError* err);
@@ -217,6 +226,7 @@ jfg_status numeric_solve(jfg_model* m, int nrhs, const double* hF, double* hU, d
 jfg_status numeric_factor_diag(jfg_model* m, double* out);
 // stress.cu
 jfg_status recover_t10_stresses(jfg_model* m, int nrhs, const double* U_dev, double* out_dev, cudaStream_t st);
+jfg_status recover_q4_stresses(jfg_model* m, int nrhs, const double* U_dev, double* out_dev, cudaStream_t st);
 // memory
 jfg_status dev_alloc(jfg_ctx* c, void** p, size_t bytes);
 void dev_free(jfg_ctx* c, void* p, size_t bytes);

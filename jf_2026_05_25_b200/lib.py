@@ -338,6 +338,20 @@ class DeviceModel:
         _check(load().jfg_recover_stresses(self.h, 2, U.shape[1], _p(U), _p(out)))
         return out
 
+    def q4_stresses(self, U: np.ndarray) -> np.ndarray:
+        """Centre forces, fibre stresses and strains of every CQUAD4 for every
+        column of U: array (nrhs, n_q4, 31) in the layout of jfg_recover_stresses
+        kind 0.  Elements whose PSHELL the reference leaves unrecovered (MID2 or
+        MID3 a different material law, _pshell_local_constitutive_gap,
+        stress_recovery.jl:193-215) are NaN, as the reference omits them."""
+        U = np.asfortranarray(U, np.float64)
+        if U.ndim == 1:
+            U = U[:, None]
+        out = np.empty((U.shape[1], len(self.model.q4_nodes), 31))
+        _check(load().jfg_recover_stresses(self.h, 0, U.shape[1], _p(U), _p(out)))
+        out[:, ~self.model.q4_recovery_mask()] = np.nan
+        return out
+
     def update_q4_sections(self, elems: np.ndarray, sect: np.ndarray):
         elems = np.ascontiguousarray(elems, np.int32)
         sect = np.ascontiguousarray(sect, np.float64)

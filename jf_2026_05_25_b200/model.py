@@ -115,6 +115,25 @@ class Sol101Model:
             out[self.q4_pid == pid] = rec
         return out
 
+    def q4_recovery_mask(self) -> np.ndarray:
+        """CQUAD4 whose stresses the reference recovers: the PSHELL's MID2 and
+        MID3 (when bending is active) are MID1 or a MAT1 with the same E, NU
+        and G (_pshell_local_constitutive_gap with equivalent materials,
+        stress_recovery.jl:176-215)."""
+        def same_law(a: int, b: int) -> bool:
+            if a == b:
+                return True
+            ma, mb = self.mats.get(a), self.mats.get(b)
+            return ma is not None and mb is not None and (ma.E, ma.NU, ma.G) == (mb.E, mb.NU, mb.G)
+
+        ok = {}
+        for pid in np.unique(self.q4_pid):
+            p = self.pshells[int(pid)]
+            bending = float(p.BEND_RATIO) > 1e-12
+            mids = [p.MID2, p.MID3] if bending else []
+            ok[int(pid)] = all(mid <= 0 or same_law(p.MID1, mid) for mid in mids)
+        return np.array([ok[int(pid)] for pid in self.q4_pid], dtype=bool)
+
     def q8_sections(self) -> np.ndarray:
         """CQUAD8 native section (assembly.jl:2585-2628 _quad8_native_section)."""
         out = np.zeros((len(self.q8_pid), Q8_SECT_STRIDE))

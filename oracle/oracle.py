@@ -80,6 +80,8 @@ def lib():
         L.or_chol_free.restype = None
         L.or_t10_stress.argtypes = [P, P, d, d, P, P]
         L.or_t10_stress.restype = ctypes.c_int
+        L.or_q4_stress.argtypes = [P, P, d, d, d, d, P, P, P]
+        L.or_q4_stress.restype = ctypes.c_int
         L.or_csc_residual_dd.argtypes = [i64, i64, P, P, P, i32, P, P, P]
         L.or_csc_residual_dd.restype = None
         L.or_chol_counts.argtypes = [i64, P, P, P, P]
@@ -255,6 +257,40 @@ def t10_stresses(model, U) -> np.ndarray:
                                  float(mat[e, 0]), float(mat[e, 1]), _p(np.ascontiguousarray(un[nd])), _p(rec))
             if st:
                 raise ValueError(f"element {e}: or_t10_stress status {st}")
+            out[k, e] = rec
+    return out
+
+
+Q4_STRESS_REC = 31
+
+
+def q4_stresses(model, U) -> np.ndarray:
+    """CQUAD4 centre forces, fibre stresses and strains of every element for
+    every column of U (ndof x nrhs): array (nrhs, n_q4, 31) in the layout of
+    or_q4_stress (recover_shell_stresses!, stress_recovery.jl:505-1237, the
+    default isotropic PSHELL path)."""
+    U = np.asarray(U, float)
+    if U.ndim == 1:
+        U = U[:, None]
+    L = lib()
+    nodes = np.asarray(model.q4_nodes)
+    sect = model.q4_sections()
+    R = np.asarray(model.node_R, float)
+    X = np.asarray(model.xyz, float)
+    out = np.zeros((U.shape[1], len(nodes), Q4_STRESS_REC))
+    rec = np.zeros(Q4_STRESS_REC)
+    for e in range(len(nodes)):
+        p = model.pshells[int(model.q4_pid[e])]
+        mat = model.mats[p.MID1]
+        nd = nodes[e]
+        Xe, Re = np.ascontiguousarray(X[nd]), np.ascontiguousarray(R[nd])
+        se = np.ascontiguousarray(sect[e])
+        for k in range(U.shape[1]):
+            ue = np.ascontiguousarray(U[:, k].reshape(-1, 6)[nd].ravel())
+            st = L.or_q4_stress(_p(Xe), _p(Re), float(mat.E), float(mat.NU), float(p.T), float(p.BEND_RATIO),
+                                _p(se), _p(ue), _p(rec))
+            if st:
+                raise ValueError(f"element {e}: or_q4_stress status {st}")
             out[k, e] = rec
     return out
 

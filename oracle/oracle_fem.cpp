@@ -102,7 +102,7 @@ inline bool jac_ok(double detj, double j11, double j12, double j21, double j22) 
 //   flexibility:   FEMKernels.jl:4223-4339 quad4_natural_shear_flexibility!
 //   K_plate:       FEMKernels.jl:6187-6200, added at plate dofs :6278-6285
 int macneal_shear(const double* lc, const double* Cb, const double* Cs, double h,
-                  double* Ke) {
+                  double* Ke, double* KP_out = nullptr) {
   double csmax = 0;
   for (int i = 0; i < 4; ++i) csmax = std::max(csmax, std::fabs(Cs[i]));
   if (h < 1e-30 || csmax < 1e-30) return 0;
@@ -208,11 +208,102 @@ int macneal_shear(const double* lc, const double* Cb, const double* Cs, double h
   mul(sol, 4, 12, Zi, 4, D);
   double KP[144] = {0};
   mul_At_add(KP, 12, 12, D, 4, sol, 1.0);
+  if (KP_out) std::memcpy(KP_out, KP, sizeof KP);
   const int pd[12] = {2, 3, 4, 8, 9, 10, 14, 15, 16, 20, 21, 22};
   for (int j = 0; j < 12; ++j)
     for (int i = 0; i < 12; ++i)
       Ke[pd[i] + 24 * pd[j]] += 0.5 * (KP[i + 12 * j] + KP[j + 12 * i]);
   return 0;
+}
+
+// CQUAD4 element frame (shell_element_frame_quad4, diagonal mode) and the
+// local in-plane coordinates of the corners about their centroid, as the
+// stiffness and the stress recovery both take them
+// (stress_recovery.jl:774-781, assembly.jl:5858-5870).  xyz: 4 x 3, node
+// major.  zmax / xmax: largest out-of-plane offset and in-plane coordinate.
+void q4_frame(const double* xyz, double v1[3], double v2[3], double v3[3], double lc[8],
+              double& zmax, double& xmax) {
+  double p[4][3];
+  for (int k = 0; k < 4; ++k)
+    for (int a = 0; a < 3; ++a) p[k][a] = xyz[3 * k + a];
+  auto sub = [](const double* a, const double* b, double* o) {
+    o[0] = a[0] - b[0]; o[1] = a[1] - b[1]; o[2] = a[2] - b[2];
+  };
+  auto dot = [](const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+  auto cross = [](const double* a, const double* b, double* o) {
+    o[0] = a[1] * b[2] - a[2] * b[1]; o[1] = a[2] * b[0] - a[0] * b[2]; o[2] = a[0] * b[1] - a[1] * b[0];
+  };
+  auto nrm = [&](double* a) {
+    double l = std::sqrt(dot(a, a));
+    a[0] /= l; a[1] /= l; a[2] /= l;
+  };
+  double gxi[3], geta[3];
+  for (int a = 0; a < 3; ++a) {
+    gxi[a] = 0.25 * (-p[0][a] + p[1][a] + p[2][a] - p[3][a]);
+    geta[a] = 0.25 * (-p[0][a] - p[1][a] + p[2][a] + p[3][a]);
+  }
+  cross(gxi, geta, v3);
+  double d13[3], d24[3];
+  sub(p[2], p[0], d13); sub(p[3], p[1], d24);
+  if (dot(v3, v3) <= 1e-24) cross(d13, d24, v3);
+  nrm(v3);
+  double d13n[3] = {d13[0], d13[1], d13[2]}, d24n[3] = {d24[0], d24[1], d24[2]};
+  nrm(d13n); nrm(d24n);
+  double xr[3];
+  for (int a = 0; a < 3; ++a) xr[a] = d13n[a] - d24n[a];
+  if (dot(xr, xr) < 1e-20)
+    for (int a = 0; a < 3; ++a) xr[a] = d13n[a] + d24n[a];
+  double xp[3];
+  double dv = dot(xr, v3);
+  for (int a = 0; a < 3; ++a) xp[a] = xr[a] - dv * v3[a];
+  if (dot(xp, xp) <= 1e-24) {
+    double ge = dot(geta, v3);
+    for (int a = 0; a < 3; ++a) xp[a] = geta[a] - ge * v3[a];
+    if (dot(xp, xp) <= 1e-24) {
+      double e12[3];
+      sub(p[1], p[0], e12);
+      double de = dot(e12, v3);
+      for (int a = 0; a < 3; ++a) xp[a] = e12[a] - de * v3[a];
+    }
+  }
+  for (int a = 0; a < 3; ++a) v1[a] = xp[a];
+  nrm(v1);
+  cross(v3, v1, v2);
+  double c[3];
+  for (int a = 0; a < 3; ++a) c[a] = (p[0][a] + p[1][a] + p[2][a] + p[3][a]) / 4.0;
+  zmax = 0;
+  xmax = 0;
+  for (int k = 0; k < 4; ++k) {
+    double d[3];
+    sub(p[k], c, d);
+    lc[k] = dot(d, v1);
+    lc[k + 4] = dot(d, v2);
+    zmax = std::max(zmax, std::fabs(dot(d, v3)));
+    xmax = std::max(xmax, std::fabs(lc[k]));
+  }
+}
+
+// Principal values of a 2-D symmetric tensor (xx, yy, xy) without
+// cancellation (_recovery_principal_2d, stress_recovery.jl:17-34).
+void principal_2d(double xx, double yy, double xy, double& major, double& minor) {
+  if (xy == 0.0) {
+    major = std::max(xx, yy);
+    minor = std::min(xx, yy);
+    return;
+  }
+  double scale = std::max(std::max(std::fabs(xx), std::fabs(yy)), std::fabs(xy));
+  double a = xx / scale, b = yy / scale, c = xy / scale;
+  double mean = (a + b) / 2, radius = std::hypot((a - b) / 2, c);
+  double large = (mean + std::copysign(radius, mean)) * scale;
+  if (!std::isfinite(large)) {
+    major = (mean + radius) * scale;
+    minor = (mean - radius) * scale;
+    return;
+  }
+  double hi = std::fabs(xx) >= std::fabs(yy) ? xx : yy, lo = std::fabs(xx) >= std::fabs(yy) ? yy : xx;
+  double small = (hi / large) * lo - (xy / large) * xy;
+  major = std::max(large, small);
+  minor = std::min(large, small);
 }
 
 }  // namespace
@@ -373,59 +464,8 @@ int or_q4_element(const double* xyz, const double* nodeR, const double* sect,
     o[0] = a[0] - b[0]; o[1] = a[1] - b[1]; o[2] = a[2] - b[2];
   };
   auto dot = [](const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
-  auto cross = [](const double* a, const double* b, double* o) {
-    o[0] = a[1] * b[2] - a[2] * b[1]; o[1] = a[2] * b[0] - a[0] * b[2]; o[2] = a[0] * b[1] - a[1] * b[0];
-  };
-  auto nrm = [&](double* a) {
-    double l = std::sqrt(dot(a, a));
-    a[0] /= l; a[1] /= l; a[2] /= l;
-  };
-  double gxi[3], geta[3];
-  for (int a = 0; a < 3; ++a) {
-    gxi[a] = 0.25 * (-p[0][a] + p[1][a] + p[2][a] - p[3][a]);
-    geta[a] = 0.25 * (-p[0][a] - p[1][a] + p[2][a] + p[3][a]);
-  }
-  double v3[3];
-  cross(gxi, geta, v3);
-  double d13[3], d24[3];
-  sub(p[2], p[0], d13); sub(p[3], p[1], d24);
-  if (dot(v3, v3) <= 1e-24) cross(d13, d24, v3);
-  nrm(v3);
-  double d13n[3] = {d13[0], d13[1], d13[2]}, d24n[3] = {d24[0], d24[1], d24[2]};
-  nrm(d13n); nrm(d24n);
-  double xr[3];
-  for (int a = 0; a < 3; ++a) xr[a] = d13n[a] - d24n[a];
-  if (dot(xr, xr) < 1e-20)
-    for (int a = 0; a < 3; ++a) xr[a] = d13n[a] + d24n[a];
-  double xp[3];
-  double dv = dot(xr, v3);
-  for (int a = 0; a < 3; ++a) xp[a] = xr[a] - dv * v3[a];
-  if (dot(xp, xp) <= 1e-24) {
-    double ge = dot(geta, v3);
-    for (int a = 0; a < 3; ++a) xp[a] = geta[a] - ge * v3[a];
-    if (dot(xp, xp) <= 1e-24) {
-      double e12[3];
-      sub(p[1], p[0], e12);
-      double de = dot(e12, v3);
-      for (int a = 0; a < 3; ++a) xp[a] = e12[a] - de * v3[a];
-    }
-  }
-  double v1[3] = {xp[0], xp[1], xp[2]};
-  nrm(v1);
-  double v2[3];
-  cross(v3, v1, v2);
-  double c[3];
-  for (int a = 0; a < 3; ++a) c[a] = (p[0][a] + p[1][a] + p[2][a] + p[3][a]) / 4.0;
-  double lc[8];
-  double zmax = 0, xmax = 0;
-  for (int k = 0; k < 4; ++k) {
-    double d[3];
-    sub(p[k], c, d);
-    lc[k] = dot(d, v1);
-    lc[k + 4] = dot(d, v2);
-    zmax = std::max(zmax, std::fabs(dot(d, v3)));
-    xmax = std::max(xmax, std::fabs(lc[k]));
-  }
+  double v1[3], v2[3], v3[3], lc[8], zmax, xmax;
+  q4_frame(xyz, v1, v2, v3, lc, zmax, xmax);
   // Only flat elements: the finite-warp multiplier is then skipped by the
   // reference itself (FEMKernels.jl:1100-1102).
   if (!(zmax <= 1e-12 * std::max(xmax, 1e-30))) return 100;
@@ -497,6 +537,189 @@ int or_q4_element(const double* xyz, const double* nodeR, const double* sect,
       if (v != 0.0)
         for (int ii = 0; ii < 24; ++ii) Ke_global[ii + 24 * jj] += T[ll + 24 * ii] * v;
     }
+  return 0;
+}
+
+// CQUAD4 stress recovery on the default isotropic PSHELL path
+// (recover_shell_stresses!, stress_recovery.jl:505-1237, n == 4: no offset,
+// no SNORM, no thermal load, flat so the warp map is the identity).
+//   element displacements: (Rel * node_R) u per node            (:774-781)
+//   centre fields: stress_strain_quad4's default branch, FEMKernels.jl:6794-6978
+//     (Wilson membrane modes condensed with Cm = h D, patch-consistent
+//     Jacobian :1847-1895; area-weighted Gauss-point means of eps and kappa)
+//   Q: the area-mean MacNeal shear resultant, FEMKernels.jl:6623-6646, which
+//     replaces the centre shear when _pshell_macneal_mean_shear_data applies
+//     (stress_recovery.jl:248-292, :917-927)
+//   fibres -T/2, +T/2; strains: membrane (tag 0) and -kappa (tag -1)
+//     (stress_recovery.jl:1118-1123, :1239-1255)
+// xyz: 4 x 3 node major; nodeR: 4 x 9; E, nu: MAT1 of MID1; h = T; br =
+// BEND_RATIO; sect: the element's 26-double section record (its Cs gives the
+// shear law); u: the 24 node-frame displacements.  out (31 doubles):
+//   0-7   fx fy fxy mx my mxy qx qy
+//   8-13  fibre z1: sx sy txy von_mises major minor;  14-19  fibre z2
+//   20-24 membrane strain ex ey gxy major minor;  25-29 -kappa, same layout
+//   30    major principal stress at z1 (compute_principal_2d, FEMKernels.jl:6509)
+int or_q4_stress(const double* xyz, const double* nodeR, double E, double nu, double h, double br,
+                 const double* sect, const double* u, double* out) {
+  double v1[3], v2[3], v3[3], lc[8], zmax, xmax;
+  q4_frame(xyz, v1, v2, v3, lc, zmax, xmax);
+  if (!(zmax <= 1e-12 * std::max(xmax, 1e-30))) return 100;
+  const double Rel[3][3] = {{v1[0], v1[1], v1[2]}, {v2[0], v2[1], v2[2]}, {v3[0], v3[1], v3[2]}};
+  double ue[24];
+  for (int k = 0; k < 4; ++k) {
+    const double* R = nodeR + 9 * k;
+    double Tn[3][3];
+    for (int rr = 0; rr < 3; ++rr)
+      for (int cc = 0; cc < 3; ++cc)
+        Tn[rr][cc] = Rel[rr][0] * R[0 + 3 * cc] + Rel[rr][1] * R[1 + 3 * cc] + Rel[rr][2] * R[2 + 3 * cc];
+    for (int rr = 0; rr < 3; ++rr) {
+      double a = 0, b = 0;
+      for (int cc = 0; cc < 3; ++cc) {
+        a += Tn[rr][cc] * u[6 * k + cc];
+        b += Tn[rr][cc] * u[6 * k + 3 + cc];
+      }
+      ue[6 * k + rr] = a;
+      ue[6 * k + 3 + rr] = b;
+    }
+  }
+  const double cmem = E / (1 - nu * nu);
+  const double D[9] = {cmem, cmem * nu, 0, cmem * nu, cmem, 0, 0, 0, cmem * (1 - nu) / 2};  // col-major
+  double Cm[9];
+  for (int i = 0; i < 9; ++i) Cm[i] = D[i] * h;
+  const double dNr_c[4] = {-0.25, 0.25, 0.25, -0.25};
+  const double dNs_c[4] = {-0.25, -0.25, 0.25, 0.25};
+  double J11c, J12c, J21c, J22c;
+  jac_quad(lc, dNr_c, dNs_c, J11c, J12c, J21c, J22c);
+  double detJc = J11c * J22c - J12c * J21c;
+  double idc = 1.0 / detJc;
+  double iJ11c = J22c * idc, iJ12c = -J12c * idc, iJ21c = -J21c * idc, iJ22c = J11c * idc;
+  const double pt = 1.0 / std::sqrt(3.0);
+  const double gr[4] = {-pt, pt, pt, -pt}, gs[4] = {-pt, -pt, pt, pt};
+  double Bm[4][72], Bb[4][72], Bi[4][12], wgt[4];
+  double K_ab[96] = {0}, K_bb[16] = {0};
+  for (int g = 0; g < 4; ++g) {
+    double r = gr[g], s = gs[g];
+    double dNr[4], dNs[4];
+    shape_derivs_quad(r, s, dNr, dNs);
+    double J11, J12, J21, J22;
+    jac_quad(lc, dNr, dNs, J11, J12, J21, J22);
+    double detJ = J11 * J22 - J12 * J21;
+    if (!jac_ok(detJ, J11, J12, J21, J22)) return 1;
+    wgt[g] = std::fabs(detJ);
+    double id = 1.0 / detJ;
+    double iJ11 = J22 * id, iJ12 = -J12 * id, iJ21 = -J21 * id, iJ22 = J11 * id;
+    std::memset(Bm[g], 0, sizeof Bm[g]);
+    std::memset(Bb[g], 0, sizeof Bb[g]);
+    for (int k = 0; k < 4; ++k) {
+      double dx = iJ11 * dNr[k] + iJ12 * dNs[k];
+      double dy = iJ21 * dNr[k] + iJ22 * dNs[k];
+      int c = 6 * k;
+      Bm[g][0 + 3 * (c + 0)] = dx; Bm[g][1 + 3 * (c + 1)] = dy;
+      Bm[g][2 + 3 * (c + 0)] = dy; Bm[g][2 + 3 * (c + 1)] = dx;
+      Bb[g][0 + 3 * (c + 4)] = dx; Bb[g][1 + 3 * (c + 3)] = -dy;
+      Bb[g][2 + 3 * (c + 4)] = dy; Bb[g][2 + 3 * (c + 3)] = -dx;
+    }
+    double ratio = (iJ11 * iJ22 - iJ12 * iJ21) / (iJ11c * iJ22c - iJ12c * iJ21c);
+    double m11 = ratio * iJ11c, m12 = ratio * iJ12c, m21 = ratio * iJ21c, m22 = ratio * iJ22c;
+    double p1x = m11 * (-2 * r), p1y = m21 * (-2 * r), p2x = m12 * (-2 * s), p2y = m22 * (-2 * s);
+    std::memset(Bi[g], 0, sizeof Bi[g]);
+    Bi[g][0 + 3 * 0] = p1x; Bi[g][2 + 3 * 0] = p1y; Bi[g][1 + 3 * 1] = p1y; Bi[g][2 + 3 * 1] = p1x;
+    Bi[g][0 + 3 * 2] = p2x; Bi[g][2 + 3 * 2] = p2y; Bi[g][1 + 3 * 3] = p2y; Bi[g][2 + 3 * 3] = p2x;
+    double t34[12];
+    mul(t34, 3, 4, Cm, 3, Bi[g]);
+    mul_At_add(K_ab, 24, 4, Bm[g], 3, t34, wgt[g]);
+    mul_At_add(K_bb, 4, 4, Bi[g], 3, t34, wgt[g]);
+  }
+  // alpha = -(K_bb \ (K_ab' u))
+  double rhs[4];
+  for (int j = 0; j < 4; ++j) {
+    double acc = 0;
+    for (int i = 0; i < 24; ++i) acc += K_ab[i + 24 * j] * ue[i];
+    rhs[j] = acc;
+  }
+  double Kbi[16];
+  if (!inv_small(K_bb, 4, Kbi)) return 2;
+  double alpha[4];
+  for (int i = 0; i < 4; ++i) {
+    double acc = 0;
+    for (int j = 0; j < 4; ++j) acc += Kbi[i + 4 * j] * rhs[j];
+    alpha[i] = -acc;
+  }
+  double eps[3] = {0, 0, 0}, kap[3] = {0, 0, 0}, area = 0;
+  for (int g = 0; g < 4; ++g) {
+    for (int a = 0; a < 3; ++a) {
+      double e = 0, k = 0;
+      for (int i = 0; i < 24; ++i) {
+        e += Bm[g][a + 3 * i] * ue[i];
+        k += Bb[g][a + 3 * i] * ue[i];
+      }
+      for (int j = 0; j < 4; ++j) e += Bi[g][a + 3 * j] * alpha[j];
+      eps[a] += e * wgt[g];
+      kap[a] += k * wgt[g];
+    }
+    area += wgt[g];
+  }
+  for (int a = 0; a < 3; ++a) { eps[a] /= area; kap[a] /= area; }
+  double N[3], M[3];
+  for (int a = 0; a < 3; ++a) {
+    double n = 0, m = 0;
+    for (int b = 0; b < 3; ++b) { n += Cm[a + 3 * b] * eps[b]; m += D[a + 3 * b] * kap[b]; }
+    N[a] = n;
+    M[a] = -br * m * (h * h * h / 12.0);
+  }
+  // area-mean MacNeal shear resultant from the plate operator K_plate
+  double q[2] = {0, 0};
+  if (br > 1e-12) {
+    double Cb[9];
+    for (int i = 0; i < 9; ++i) Cb[i] = br * (h * h * h) / 12 * D[i];
+    double Kscratch[576] = {0}, KP[144] = {0};
+    int st = macneal_shear(lc, Cb, sect + 18, h, Kscratch, KP);
+    if (st) return 10 + st;
+    double qx = 0, qy = 0;
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j)
+        for (int c = 0; c < 3; ++c) {
+          qx += KP[(3 * i + 2) + 12 * (3 * j + c)] * ue[6 * j + c + 2];
+          qy -= KP[(3 * i + 1) + 12 * (3 * j + c)] * ue[6 * j + c + 2];
+        }
+    double a4 = 4 * std::fabs(detJc);
+    q[0] = qx / a4;
+    q[1] = qy / a4;
+  }
+  double ez1[3], ez2[3], sz1[3], sz2[3];
+  for (int a = 0; a < 3; ++a) {
+    ez1[a] = eps[a] + (-h / 2.0) * kap[a];
+    ez2[a] = eps[a] + (h / 2.0) * kap[a];
+  }
+  for (int a = 0; a < 3; ++a) {
+    double x = 0, y = 0;
+    for (int b = 0; b < 3; ++b) { x += D[a + 3 * b] * ez1[b]; y += D[a + 3 * b] * ez2[b]; }
+    sz1[a] = x;
+    sz2[a] = y;
+  }
+  for (int a = 0; a < 3; ++a) { out[a] = N[a]; out[3 + a] = M[a]; }
+  out[6] = q[0];
+  out[7] = q[1];
+  auto stress_row = [&](const double* sg, double* o) {
+    o[0] = sg[0]; o[1] = sg[1]; o[2] = sg[2];
+    o[3] = std::sqrt(sg[0] * sg[0] - sg[0] * sg[1] + sg[1] * sg[1] + 3 * sg[2] * sg[2]);
+    principal_2d(sg[0], sg[1], sg[2], o[4], o[5]);
+  };
+  stress_row(sz1, out + 8);
+  stress_row(sz2, out + 14);
+  double em[3], kn[3];
+  for (int a = 0; a < 3; ++a) {
+    em[a] = (ez1[a] + ez2[a]) / 2.0;
+    kn[a] = (ez1[a] - ez2[a]) / h;
+  }
+  auto strain_row = [&](const double* e, double* o) {
+    o[0] = e[0]; o[1] = e[1]; o[2] = e[2];
+    principal_2d(e[0], e[1], e[2] / 2, o[3], o[4]);
+  };
+  strain_row(em, out + 20);
+  strain_row(kn, out + 25);
+  double savg = (sz1[0] + sz1[1]) / 2.0;
+  out[30] = savg + std::sqrt(((sz1[0] - sz1[1]) / 2.0) * ((sz1[0] - sz1[1]) / 2.0) + sz1[2] * sz1[2]);
   return 0;
 }
 

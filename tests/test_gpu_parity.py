@@ -476,9 +476,49 @@ def test_t10_stress_recovery_matches_oracle(ctx, oracle_mod):
     u1 = U[:, :1].copy(order="F")
     out = np.empty(13)
     with pytest.raises(lib.JfgError) as e:
-        lib._check(lib.load().jfg_recover_stresses(dm.h, 0, 1, lib._p(u1), lib._p(out)))
+        lib._check(lib.load().jfg_recover_stresses(dm.h, 1, 1, lib._p(u1), lib._p(out)))
     assert e.value.status_name == "UNSUPPORTED"
     dm.close()
+
+
+# the CQUAD4 record's field groups: forces N, M, Q; the two fibres' stresses;
+# membrane strain and curvature; the principal stress at -T/2
+Q4_STRESS_GROUPS = ((0, 3), (3, 6), (6, 8), (8, 14), (14, 20), (20, 25), (25, 30), (30, 31))
+
+
+def test_q4_stress_recovery_matches_oracle(ctx, oracle_mod):
+    """Device CQUAD4 centre forces, fibre stresses and strains
+    (recover_shell_stresses!, stress_recovery.jl:505-1237) against the
+    oracle on random displacement fields with rotated grid frames, and on a
+    solved stiffened panel: 1e-10 relative to each field group's maximum.
+    The device takes Q from the MacNeal operator of its prep record and the
+    Wilson-mode condensation in a different order than the oracle."""
+    m = M.stiffened_panel(3)
+    rng = np.random.default_rng(5)
+    R = np.zeros((m.n_nodes, 9))
+    for i in range(m.n_nodes):
+        Q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+        R[i] = Q.ravel(order="F")
+    m.node_R = R
+    U = rng.normal(scale=1e-4, size=(m.ndof, 3))
+    dm = lib.DeviceModel(ctx, m)
+    dm.assemble()
+    got = dm.q4_stresses(U)
+    ref = oracle_mod.q4_stresses(m, U)
+    assert got.shape == ref.shape == (3, len(m.q4_nodes), 31)
+    for a, b in Q4_STRESS_GROUPS:
+        assert _rel(got[..., a:b], ref[..., a:b]) <= 1e-10, (a, b)
+    dm.close()
+    # a solved model: pressure and forces on the stiffened panel
+    m = M.stiffened_panel(4)
+    st = B.prepare(B.JFEMGPUBackend(tol=1e-10), m)
+    U, _ = st["dm"].solve(m.load_matrix(), 1e-10, 30)
+    got = st["dm"].q4_stresses(U)
+    ref = oracle_mod.q4_stresses(m, U)
+    for a, b in Q4_STRESS_GROUPS:
+        assert _rel(got[..., a:b], ref[..., a:b]) <= 1e-10, (a, b)
+    assert np.abs(got[..., 3:6]).max() > 0 and np.abs(got[..., 6:8]).max() > 0
+    st["dm"].close()
 
 
 def test_share_structure_gives_the_same_solution(ctx):
