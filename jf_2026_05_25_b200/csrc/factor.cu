@@ -443,14 +443,17 @@ k_potrf_diag(const int32_t* __restrict__ list, const int32_t* __restrict__ first
 }
 
 // Cholesky of the NB x NB diagonal block at column k0 of every front of the
-// level and the inverse of its factor, with the whole CTA on the serial
-// chains: FUSED, one chain of one block barrier per column for both; else
-// the factor's chain and then the inverse's (twice the barriers, a third of
-// the entries busy per step instead of two thirds).  Each thread owns up to
-// 9 entries of the 64 x 64 lower triangle.  Pivots that are not positive
-// and finite are replaced by 1 and the smallest such column is recorded;
-// rows and columns past the front's width are the identity.
-template <typename T, bool FUSED>
+// level and the inverse of its factor, with the whole CTA on both serial
+// chains.  Each thread owns up to 9 entries of the 64 x 64 lower triangle.
+// Factor: right-looking on unscaled columns (a_ik -= a_ij a_kj / a_jj for
+// j < k <= i, the L D L^T form), one block barrier per column, and the
+// columns scaled by 1/sqrt(a_jj) at the end.  Inverse: X = L^{-1} by rows,
+// right-looking on the residual R (R_iq -= L_ij R_jq / L_jj for q <= j < i),
+// one barrier per row, X_iq = R_iq / L_ii at the end.  Both chains stop at
+// the block's width kn.  Pivots that are not positive and finite are
+// replaced by 1 and the smallest such column is recorded; rows and columns
+// past the front's width are the identity.
+template <typename T>
 __global__ void __launch_bounds__(256, 2)
 k_potrf_cta(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
             const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
@@ -495,69 +498,6 @@ k_potrf_cta(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
       ek[u] = -1;
     }
   }
-  if constexpr (FUSED) {
-  // One chain of kn steps computes the unscaled factor U (L = U D^-1/2,
-  // D = diag(U)) and the rows of R, where U^-1 = D^-1 R, together: step j
-  // applies pivot column j to the factor entries right of it (a_ik -=
-  // a_ij a_kj / a_jj, j < k <= i) and to the inverse entries left of it
-  // (r_iq -= a_ij r_jq / a_jj, q <= j < i).  An entry (i, k) is a factor
-  // entry until step k - 1, which makes it final; it is then published to
-  // shared memory as part of pivot column k and the same register restarts
-  // as r_ik (the identity), published as part of row i once step i - 1 has
-  // made it final.  Each step reads only published values, so all its loads
-  // issue together.  At the end L_ik = a_ik / sqrt(a_kk) and
-  // (L^-1)_iq = r_iq / sqrt(a_ii).
-  T v[NE];
-  __syncthreads();
-#pragma unroll
-  for (int u = 0; u < NE; ++u)
-    v[u] = ei[u] < 0 ? (T)0 : ek[u] == 0 ? (ei[u] == 0 ? (T)1 : (T)0) : A[ei[u]][ek[u]];
-  // Rows and columns from kn on are the identity and stay so (their
-  // multipliers a_ij, j < kn <= i, are zero), so only kn steps do work.
-  for (int j = 0; j < kn; ++j) {
-    __syncthreads();   // pivot column j and row j of R final in shared memory
-    T d = A[j][j];
-    const bool bad = !(d > (T)0) || !isfinite((double)d);
-    if (bad) {
-      if (t == 0) atomicMin(&bad_idx, j);
-      d = (T)1;
-    }
-    const T rd = (T)1 / d;
-    T lij[NE], pj[NE];
-#pragma unroll
-    for (int u = 0; u < NE; ++u)
-      if (ei[u] > j) { lij[u] = A[ei[u]][j]; pj[u] = ek[u] > j ? A[ek[u]][j] : B[j][ek[u]]; }
-#pragma unroll
-    for (int u = 0; u < NE; ++u)
-      if (ei[u] > j) v[u] = fma(-lij[u] * rd, pj[u], v[u]);
-#pragma unroll
-    for (int u = 0; u < NE; ++u) {
-      if (ek[u] == j + 1) {   // factor entry final: publish, restart as r_ik
-        A[ei[u]][j + 1] = v[u];
-        v[u] = ei[u] == ek[u] ? (T)1 : (T)0;
-      } else if (ei[u] == j + 1 && ek[u] <= j) {
-        B[j + 1][ek[u]] = v[u];
-      }
-    }
-  }
-  __syncthreads();
-  if (t < NB) {
-    T d = A[t][t];
-    const bool bad = !(d > (T)0) || !isfinite((double)d);
-    sv[t] = bad ? (T)1 : sqrt(d);
-  }
-  __syncthreads();
-#pragma unroll
-  for (int u = 0; u < NE; ++u) {
-    const int i = ei[u], k = ek[u];
-    if (i >= 0) {
-      A[i][k] = (i == k) ? sv[k] : A[i][k] / sv[k];
-      B[i][k] = B[i][k] / sv[i];
-    }
-  }
-  __syncthreads();
-  } else {
-  // Two chains: the factor, then the inverse of the scaled factor.
   // factor.  Each thread keeps its entries in registers; an entry reaches
   // shared memory when its column becomes the next pivot column (final after
   // the update by the column before it), so a step reads only final values
@@ -624,7 +564,6 @@ k_potrf_cta(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
     if (i >= 0) B[i][q] = B[i][q] / A[i][i];
   }
   __syncthreads();
-  }
   if (t == 0 && bad_idx < kn) rec_err(err, EE_PIVOT, (int64_t)first[s] + k0 + bad_idx);
   T* Dv = Dinv + Dptr[s] + (int64_t)(k0 / NB) * NB * NB;
   for (int e = t; e < NB * NB; e += blockDim.x) {
@@ -644,20 +583,6 @@ inline bool potrf_cta() {
     v = (e && e[0] == '1') ? 0 : 1;
   }
   return v == 1;
-}
-
-// which k_potrf_cta chain a launch of na CTAs runs: the fused chain where the
-// launch fills the GPU (about 2 x 148 CTAs and more: per-step issue, not the
-// chain's latency, sets the time), the two chains below that (a single CTA
-// runs its 64 x 64 block in 56 instead of 73 us).  JFG_POTRF_FUSED=0 / 1
-// forces either.
-inline bool potrf_fused(int na) {
-  static int v = -2;
-  if (v == -2) {
-    const char* e = std::getenv("JFG_POTRF_FUSED");
-    v = (e && e[0] == '0') ? 0 : (e && e[0] == '1') ? 1 : -1;
-  }
-  return v == 1 || (v == -1 && na >= 296);
 }
 
 // rows [k1, m) of panel columns [k0, k1):  X := X * L_D^{-T} = X * Dinv^T,
@@ -1590,8 +1515,7 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
   if (!attr_set) {
     int bytes = 2 * NB * (NB + 1) * (int)sizeof(T);
     JFG_CUDA(cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, potrf_smem<T>()));
-    JFG_CUDA(cudaFuncSetAttribute(k_potrf_cta<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, potrf_smem<T>()));
-    JFG_CUDA(cudaFuncSetAttribute(k_potrf_cta<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, potrf_smem<T>()));
+    JFG_CUDA(cudaFuncSetAttribute(k_potrf_cta<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, potrf_smem<T>()));
     JFG_CUDA(cudaFuncSetAttribute(k_trsm_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     attr_set = true;
   }
@@ -1671,12 +1595,9 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
       const int P1 = P0 + PW;
       for (int k0 = P0; k0 < std::min(P1, lv.max_c); k0 += NB) {
         const int na = lv.active(k0);   // fronts wider than k0: a prefix of the list
-        { int ps_ = fine_prof() ? prof_start(st) : -1; { if (potrf_cta() && potrf_fused(na))
-            k_potrf_cta<T, true><<<na, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr, F->Dptr, Lf,
-                                                                    Dvf, k0, F->err);
-          else if (potrf_cta())
-            k_potrf_cta<T, false><<<na, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr, F->Dptr, Lf,
-                                                                     Dvf, k0, F->err);
+        { int ps_ = fine_prof() ? prof_start(st) : -1; { if (potrf_cta())
+            k_potrf_cta<T><<<na, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr, F->Dptr, Lf, Dvf, k0,
+                                                              F->err);
           else
             k_potrf_diag<T><<<na, 256, potrf_smem<T>(), st>>>(list, F->first, F->mrows, F->Lptr,
                                                                F->Dptr, Lf, Dvf, k0, F->err);
