@@ -3,6 +3,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "jfg_internal.h"
@@ -63,6 +64,43 @@ void set_error(const std::string& msg, int64_t detail) {
   g_err_detail = detail;
 }
 
+// Device memory comes from one memory pool per device, owned by the
+// library, by stream-ordered allocation on the context's allocation stream
+// (an otherwise idle stream).  cudaFree synchronises the whole device: with
+// several models driven from several host threads, one model's free (a
+// temporary buffer, an evicted model) waited for every other model's kernels
+// -- a factorisation step of a large front runs for up to a second -- and
+// held the other threads' CUDA calls meanwhile.  A free ordered on the idle
+// allocation stream waits for nothing.  Every free site has first
+// synchronised the stream that used the memory (the model's stream), so the
+// memory is idle when it goes back to the pool.  The pool's release
+// threshold stays 0: freed memory returns to the device at the next
+// synchronisation, as after cudaFree, so the device's free-memory figure
+// keeps its meaning for other users of the GPU.
+namespace {
+constexpr int kMaxPoolDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[kMaxPoolDevices] = {};
+
+cudaError_t device_pool(int dev, cudaMemPool_t* out) {
+  if (dev < 0 || dev >= kMaxPoolDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    cudaError_t e = cudaMemPoolCreate(&pool, &props);
+    if (e != cudaSuccess) return e;
+    g_pools[dev] = pool;
+  }
+  *out = g_pools[dev];
+  return cudaSuccess;
+}
+}  // namespace
+
 jfg_status dev_alloc(jfg_ctx* c, void** p, size_t bytes) {
   if (bytes == 0) bytes = 8;
   if (c->budget > 0 && c->used + (int64_t)bytes > c->budget) {
@@ -70,19 +108,26 @@ jfg_status dev_alloc(jfg_ctx* c, void** p, size_t bytes) {
               std::to_string(c->budget) + " bytes)");
     return JFG_OOM_BUDGET;
   }
-  cudaError_t e = cudaMalloc(p, bytes);
+  cudaMemPool_t pool = nullptr;
+  cudaError_t e = device_pool(c->device, &pool);
+  if (e == cudaSuccess) e = cudaMallocFromPoolAsync(p, bytes, pool, c->astream);
+  // the allocation is ordered on the allocation stream: once that stream has
+  // reached it, any stream may use the memory
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->astream);
   if (e != cudaSuccess) {
-    set_error(std::string("cudaMalloc of ") + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+    set_error(std::string("device allocation of ") + std::to_string(bytes) + " bytes failed: " +
+              cudaGetErrorString(e));
     return JFG_OOM_BUDGET;
   }
   c->used += (int64_t)bytes;
   return JFG_OK;
 }
 
+// The caller has synchronised every stream that used p.
 void dev_free(jfg_ctx* c, void* p, size_t bytes) {
   if (!p) return;
   if (bytes == 0) bytes = 8;
-  cudaFree(p);
+  cudaFreeAsync(p, c->astream);
   c->used -= (int64_t)bytes;
 }
 
@@ -149,8 +194,10 @@ jfg_status jfg_create(jfg_ctx** out, const jfg_config* cfg) {
     return JFG_CUDA_ERROR;
   }
   e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->astream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     set_error(std::string("cudaStreamCreate failed: ") + cudaGetErrorString(e));
+    if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return JFG_CUDA_ERROR;
   }
@@ -160,6 +207,10 @@ jfg_status jfg_create(jfg_ctx** out, const jfg_config* cfg) {
 
 jfg_status jfg_destroy(jfg_ctx* c) {
   if (!c) return JFG_OK;
+  if (c->astream) {
+    cudaStreamSynchronize(c->astream);   // the frees ordered on it
+    cudaStreamDestroy(c->astream);
+  }
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return JFG_OK;
@@ -273,6 +324,7 @@ jfg_status jfg_model_free(jfg_model* m) {
   if (m->stream) cudaStreamSynchronize(m->stream);
   if (m->aev_in) cudaEventDestroy(m->aev_in);
   if (m->aev_out) cudaEventDestroy(m->aev_out);
+  m->aev_in = m->aev_out = nullptr;
   numeric_destroy(m);
   dev_free(c, m->d_xyz, 8 * m->h_xyz.size()); dev_free(c, m->d_R, 8 * m->h_R.size());
   dev_free(c, m->d_q4n, 4 * m->h_q4n.size()); dev_free(c, m->d_q4s, 8 * m->h_q4s.size());

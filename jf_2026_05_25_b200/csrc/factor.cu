@@ -1771,6 +1771,9 @@ jfg_status ensure_workspace(jfg_model* m, NumericFactor* F, int nrhs) {
   int64_t n = m->sym().n, ndof = m->ndof;
   drop_solve_graphs(F);
   if (F->nrhs_cap > 0) {
+    // the old work arrays go back to the pool: work enqueued on the model's
+    // stream (an asynchronous application) may still read them
+    JFG_CUDA(cudaStreamSynchronize(m->stream));
     int oc = F->nrhs_cap;
     fr(F->xp, n * oc); fr(F->tt, n * oc); fr(F->V, F->v_total * oc); fr(F->dF, ndof * oc); fr(F->dU, ndof * oc);
     fr(F->dR, ndof * oc); fr(F->dD, n * oc); fr(F->dZ, ndof * oc); fr(F->dP, ndof * oc); fr(F->dQ, ndof * oc);
@@ -2103,6 +2106,10 @@ void numeric_destroy(jfg_model* m) {
   NumericFactor* F = m->num;
   if (!F) return;
   jfg_ctx* c = m->ctx;
+  // the factor's arrays go back to the pool: nothing on the model's stream
+  // may still use them
+  if (m->aev_out) cudaEventSynchronize(m->aev_out);
+  cudaStreamSynchronize(m->stream);
   const Symbolic& S = m->sym();
   auto fr = [&](void* p, size_t b) { if (p) dev_free(c, p, b); };
   fr(F->first, 4 * (S.ns + 1)); fr(F->mrows, 4 * S.ns); fr(F->level_sn, 4 * S.ns);

@@ -122,6 +122,7 @@ enum ElemErr : int32_t {
 struct jfg_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t astream = nullptr;   // device allocations and frees (stream-ordered, otherwise idle)
   int64_t budget = 0;
   int64_t used = 0;
 };
