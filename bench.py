@@ -702,6 +702,8 @@ def stream_pass(srv, specs, sm: StreamModels, device: bool, rate: float = 0.0, s
     srv.kinds.clear()
     with srv.rlock:
         srv.phase_s.clear()
+        srv.trace.clear()
+        srv.deferred = 0
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     target = t0
@@ -793,7 +795,8 @@ def run_serving(args, rank=0, world=1, local_rank=0):
                          "pcg_iters_max": int(np.max(iters)), "fallbacks": int(fb),
                          "readmissions": st_v["readmissions"], "shared_structures": st_v["shared_structures"],
                          "fp64_meshes": st_v["fp64_meshes"], "fp64_factorisations": st_v["fp64_factorisations"],
-                         "phase_s": st_v["phase_s"]}
+                         "deferred_same_mesh": st_v["deferred_same_mesh"],
+                         "phase_s": st_v["phase_s"], "timeline": st_v["timeline"]}
             rate = args.rate if args.rate > 0 else None
             if rate is None:
                 rate = 0.5 * (n_req / arms["fp64"]["stream_s"]) if "fp64" in arms else 0.5 * n_req / secs

@@ -27,6 +27,7 @@ from __future__ import annotations
 
 import hashlib
 import math
+import os
 import queue
 import threading
 import time
@@ -199,6 +200,10 @@ class Request:
     # one too; for "solve" it replaces the model's own load cases
     device: bool = False
     t_submit: float = 0.0
+    t_start: float = 0.0               # when a slot took it
+    mesh: Optional[bytes] = None       # mesh key of a single new model (set by the dispatcher)
+    mesh_done: bool = False            # mesh key computed (it may be None: no key)
+    was_deferred: bool = False         # skipped at least once by the dispatcher
     future: Future = field(default_factory=Future)
 
 
@@ -285,6 +290,14 @@ class SolveServer:
         self.readmissions = 0
         self.shared_structures = 0
         self.phase_s: Dict[str, Dict[str, float]] = {}   # class -> phase -> seconds (wall, summed over slots)
+        # per finished request: (class, submitted, taken by a slot, finished), perf_counter seconds
+        self.trace: List[tuple] = []
+        # meshes whose first model is being prepared by a slot: a new model of
+        # the same mesh waits in the queue (other work goes first) and then
+        # takes over that model's pattern and analysis instead of repeating them
+        self.preparing: Dict[bytes, int] = {}
+        self.defer_same_mesh = share_meshes and os.environ.get("JFG_SERVE_DEFER", "1") != "0"
+        self.deferred = 0
         self.waiting_reserved = 0.0   # reservations of requests waiting in _admit
         self._next_key = 0
         self._stop = False
@@ -339,18 +352,83 @@ class SolveServer:
                 "subcase_solves": int(self.subcase_solves), "resident_bytes": int(self.resident_bytes),
                 "readmissions": int(self.readmissions), "shared_structures": int(self.shared_structures),
                 "fp64_meshes": len(self.fp64_meshes), "fp64_factorisations": int(self.fp64_factorisations),
-                "phase_s": {c: {k: round(v, 4) for k, v in d.items()} for c, d in self.phase_s.items()}}
+                "deferred_same_mesh": int(self.deferred),
+                "phase_s": {c: {k: round(v, 4) for k, v in d.items()} for c, d in self.phase_s.items()},
+                "timeline": self.timeline()}
+
+    def timeline(self) -> Dict:
+        """Per class of request: count, first taken and last finished (seconds
+        from the earliest submission), summed slot seconds, and the request
+        that finished last (the critical one of a saturated pass)."""
+        with self.rlock:
+            tr = list(self.trace)
+        if not tr:
+            return {}
+        t0 = min(t[1] for t in tr)
+        out: Dict[str, Dict] = {}
+        for cls, ts, tt, te in tr:
+            d = out.setdefault(cls, {"n": 0, "first_start_s": 1e30, "last_end_s": 0.0, "busy_s": 0.0,
+                                     "max_wait_s": 0.0})
+            d["n"] += 1
+            d["first_start_s"] = min(d["first_start_s"], tt - t0)
+            d["last_end_s"] = max(d["last_end_s"], te - t0)
+            d["busy_s"] += te - tt
+            d["max_wait_s"] = max(d["max_wait_s"], tt - ts)
+        for d in out.values():
+            for k in ("first_start_s", "last_end_s", "busy_s", "max_wait_s"):
+                d[k] = round(d[k], 3)
+        last = max(tr, key=lambda t: t[3])
+        out["last_request"] = {"class": last[0], "submitted_s": round(last[1] - t0, 3),
+                               "start_s": round(last[2] - t0, 3), "end_s": round(last[3] - t0, 3)}
+        return out
 
     # ---------------------------------------------------------------- scheduling
+    def _req_mesh(self, r: Request) -> Optional[bytes]:
+        """Mesh key of a single new model (computed once per request; packs
+        of small models have none)."""
+        if not r.mesh_done:
+            r.mesh = (mesh_key(r.model) if (self.share_meshes and r.kind == "solve"
+                                            and r.model.ndof > self.small_dof) else None)
+            r.mesh_done = True
+        return r.mesh
+
+    def _deferred(self, r: Request) -> bool:
+        """A new model whose mesh another slot is preparing right now, with
+        no resident model of that mesh yet: taking it now would repeat the
+        pattern build and the symbolic analysis that the other slot is about
+        to make resident, so it stays queued until that model is registered."""
+        mk = self._req_mesh(r)
+        if mk is None or not self.defer_same_mesh or mk not in self.preparing:
+            return False
+        with self.rlock:
+            return mk not in self.meshes
+
     def _take(self) -> Optional[List[Request]]:
-        """Next unit of work: one request, or every queued new small model up
-        to the pack limits (continuous batching: whatever arrived meanwhile)."""
+        """Next unit of work: the first queued request that is not deferred
+        (see _deferred), or every queued new small model up to the pack
+        limits (continuous batching: whatever arrived meanwhile)."""
         with self.plock:
-            while not self.pending and not self._stop:
+            while True:
+                while not self.pending and not self._stop:
+                    self.plock.wait(timeout=0.5)
+                if self._stop and not self.pending:
+                    return None
+                idx = None
+                for i, r in enumerate(self.pending):
+                    if not self._deferred(r):
+                        idx = i
+                        break
+                    if not r.was_deferred:
+                        r.was_deferred = True
+                        self.deferred += 1
+                if idx is not None:
+                    break
                 self.plock.wait(timeout=0.5)
-            if self._stop and not self.pending:
-                return None
-            first = self.pending.pop(0)
+            first = self.pending.pop(idx)
+            first.t_start = time.perf_counter()
+            mk = self._req_mesh(first)
+            if mk is not None:
+                self.preparing[mk] = self.preparing.get(mk, 0) + 1
             if first.kind != "solve" or first.model.ndof > self.small_dof:
                 return [first]
             batch, dof = [first], first.model.ndof
@@ -383,12 +461,24 @@ class SolveServer:
                 for r in work:
                     if not r.future.done():
                         r.future.set_exception(exc)
+            finally:
+                mk = work[0].mesh
+                if mk is not None:
+                    with self.plock:     # deferred models of this mesh may go now
+                        n = self.preparing.get(mk, 0) - 1
+                        if n > 0:
+                            self.preparing[mk] = n
+                        else:
+                            self.preparing.pop(mk, None)
+                        self.plock.notify_all()
 
-    def _finish(self, req: Request, result: Dict):
-        dt = time.perf_counter() - req.t_submit
+    def _finish(self, req: Request, result: Dict, cls: Optional[str] = None):
+        t_end = time.perf_counter()
+        dt = t_end - req.t_submit
         with self.rlock:
             self.latencies.append(dt)
             self.kinds.append(req.kind)
+            self.trace.append((cls or req.kind, req.t_submit, req.t_start or req.t_submit, t_end))
             self.subcase_solves += int(result["U"].shape[0] if req.device else result["U"].shape[1])
         result["latency_s"] = dt
         req.future.set_result(result)
@@ -513,14 +603,15 @@ class SolveServer:
         nnz = (324 if n_t10 == 0 else 270) * target.n_nodes
         return float(8 * n_ev + 8 * 210 * n_q4 + 4 * n_ev + 28 * nnz + 150 * target.n_nodes)
 
-    def _prepare(self, be, model, pack: Optional[PackedModel], nrhs: int = 8):
+    def _prepare(self, be, model, pack: Optional[PackedModel], nrhs: int = 8, mk: Optional[bytes] = None):
         """Upload (sharing a resident mesh's structure when there is one),
         analyse, admit the exact bytes, factor.  Device bytes are admitted
         twice: an estimate before the upload, and the library's own figure
         (jfg_get_memory: factor, its work arrays and the solve work space for
         `nrhs`) once the analysis exists.  Returns (state, reserved, mesh)."""
         target = pack if pack is not None else model
-        mk = mesh_key(model) if (pack is None and self.share_meshes) else None
+        if mk is None:
+            mk = mesh_key(model) if (pack is None and self.share_meshes) else None
         prec = self.precision
         if prec == lib.PREC_MIXED and mk is not None and mk in self.fp64_meshes:
             prec = lib.PREC_FP64
@@ -575,7 +666,8 @@ class SolveServer:
         models = [r.model for r in reqs]
         pack = PackedModel(models)
         nrhs = max(16, max((r.loads.shape[0] if r.device else len(r.model.load_cases)) for r in reqs))
-        st, reserved, mk = self._prepare(be, models[0], pack if len(models) > 1 else None, nrhs)
+        st, reserved, mk = self._prepare(be, models[0], pack if len(models) > 1 else None, nrhs,
+                                         mk=reqs[0].mesh if len(models) == 1 else None)
         t_sol = time.perf_counter()
         try:
             if reqs[0].device:
@@ -607,7 +699,7 @@ class SolveServer:
         keys = self._register(st["dm"], st, pack, models, reserved=reserved, mesh=mk)
         for k, r in enumerate(reqs):
             self._finish(r, {"key": keys[k], "U": Us[k], "rel_residual": res[k], "batch": len(reqs),
-                             "report": rep})
+                             "report": rep}, cls=_model_class(models[0], pack if len(models) > 1 else None))
 
     def _device_solve(self, be, dm, pack: PackedModel, loads: List, tol: float, only: Optional[int] = None):
         """Solve with loads and displacements in device memory.  loads[k]

@@ -132,3 +132,56 @@ def test_two_second_stage_admissions_do_not_wait_on_each_other():
         assert srv.reserved == pytest.approx(15.0)
     finally:
         srv.close()
+
+
+class _Mesh:
+    """Stand-in model: a mesh key from its connectivity, a size above the
+    pack limit (single-model requests)."""
+
+    def __init__(self, tag, ndof=100000):
+        import numpy as np
+        self.n_nodes = ndof // 6
+        self.ndof = ndof
+        self.q4_nodes = np.full((4, 4), tag, np.int32)
+        self.t10_nodes = np.zeros((0, 10), np.int32)
+
+
+def test_dispatch_defers_a_model_whose_mesh_is_being_prepared(server):
+    """Two new models of one mesh queued together: the second is not taken
+    while the first is being prepared (it would repeat the pattern build and
+    the analysis); other work goes first, and once the first is registered
+    as a resident of that mesh the second is taken."""
+    a1, a2, b = _Mesh(1), _Mesh(1), _Mesh(2)
+    server.submit(S.Request("solve", model=a1))
+    server.submit(S.Request("solve", model=a2))
+    server.submit(S.Request("solve", model=b))
+    w1 = server._take()
+    assert w1[0].model is a1
+    mk = w1[0].mesh
+    assert mk is not None and server.preparing == {mk: 1}
+    w2 = server._take()                       # a2 is deferred: b goes first
+    assert w2[0].model is b
+    assert server.deferred == 1
+    # a1 registered as the mesh's resident: a2 may go (and will share)
+    server.meshes[mk] = "k0"
+    w3 = server._take()
+    assert w3[0].model is a2 and w3[0].was_deferred
+
+
+def test_dispatch_waits_when_only_deferred_work_is_queued(server):
+    """With only a deferred model queued, a slot waits; the end of the
+    preparing slot's request releases it."""
+    a1, a2 = _Mesh(3), _Mesh(3)
+    server.submit(S.Request("solve", model=a1))
+    server.submit(S.Request("solve", model=a2))
+    w1 = server._take()
+    got = []
+    t = threading.Thread(target=lambda: got.append(server._take()))
+    t.start()
+    t.join(timeout=1.2)
+    assert t.is_alive() and not got          # still waiting on the deferred a2
+    with server.plock:                       # what _worker does when a1's request ends
+        server.preparing.pop(w1[0].mesh)
+        server.plock.notify_all()
+    t.join(timeout=5)
+    assert got and got[0][0].model is a2
