@@ -96,6 +96,18 @@ def compute_free_dofs(model, diag: np.ndarray, node_blocks: np.ndarray, eps_zero
         idx = np.where(full)[0]
         if len(idx):
             S = 0.5 * (B[idx, off] + B[idx, off].transpose(0, 2, 1))
+            # screen before the eigen-decomposition: with |l_1| >= |l_2| >=
+            # |l_3| and |l_1| <= ||S||_F, |l_3| / |l_1| >= |det S| / ||S||_F^3,
+            # so a block with |det S| > 10 eps ||S||_F^3 has no eigenvalue
+            # below eps |l_1| and fixes nothing; only the others are decomposed
+            a, b, c = S[:, 0, 0], S[:, 0, 1], S[:, 0, 2]
+            d, e, f = S[:, 1, 0], S[:, 1, 1], S[:, 1, 2]
+            g, h, k = S[:, 2, 0], S[:, 2, 1], S[:, 2, 2]
+            det = a * (e * k - f * h) - b * (d * k - f * g) + c * (d * h - e * g)
+            fro = np.sqrt(np.einsum("nij,nij->n", S, S))
+            keep = ~(np.abs(det) > 10.0 * eps_zero * fro ** 3)
+            idx, S = idx[keep], S[keep]
+        if len(idx):
             vals, vecs = np.linalg.eigh(S)
             lam = np.abs(vals).max(axis=1)
             ratio = np.abs(vals) / np.where(lam > 0, lam, 1.0)[:, None]

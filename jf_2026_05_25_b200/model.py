@@ -109,11 +109,13 @@ class Sol101Model:
         """
         if self.q4_sect_override is not None:
             return self.q4_sect_override
-        out = np.zeros((len(self.q4_pid), Q4_SECT_STRIDE))
-        for pid in np.unique(self.q4_pid):
-            rec = _q4_section_record(self, int(pid))
-            out[self.q4_pid == pid] = rec
-        return out
+        if len(self.q4_pid) == 0:
+            return np.zeros((0, Q4_SECT_STRIDE))
+        # one record per PSHELL, gathered per element (a mesh with a PSHELL per
+        # skin row has hundreds of them)
+        pids, inv = np.unique(self.q4_pid, return_inverse=True)
+        recs = np.stack([np.asarray(_q4_section_record(self, int(pid)), dtype=np.float64) for pid in pids])
+        return recs[inv.reshape(-1)]
 
     def q4_recovery_mask(self) -> np.ndarray:
         """CQUAD4 whose stresses the reference recovers: the PSHELL's MID2 and
@@ -219,7 +221,7 @@ class Sol101Model:
         return out
 
     # ------------------------------------------------------------------ loads
-    def load_vector(self, case: LoadCase) -> np.ndarray:
+    def load_vector(self, case: LoadCase, q4_pressure: bool = True) -> np.ndarray:
         """Global F (ndof) for one subcase (loads.jl:541-586, solve_case.jl:57-111).
 
         PLOAD4 on CQUAD4: area = |(x3-x1)x(x4-x2)|/2, force p*area/4 per node
@@ -228,7 +230,7 @@ class Sol101Model:
         """
         F = np.zeros(self.ndof)
         nn_tot = self.n_nodes
-        if case.pload4 is not None:
+        if case.pload4 is not None and q4_pressure:
             eidx, p = case.pload4
             nodes = self.q4_nodes[eidx]
             X = self.xyz
@@ -284,11 +286,53 @@ class Sol101Model:
         return c[1]
 
     def load_matrix(self) -> np.ndarray:
-        """ndof x nrhs column-major (Fortran order) matrix of all subcases."""
-        F = np.empty((self.ndof, len(self.load_cases)), order="F")
-        for k, c in enumerate(self.load_cases):
-            F[:, k] = self.load_vector(c)
+        """ndof x nrhs column-major (Fortran order) matrix of all subcases.
+
+        With basic-frame grids, the CQUAD4 PLOAD4 of all subcases that load
+        the same element list are applied at once: the per-element nodal force
+        per unit pressure (p A / 4 along the element normal, as in
+        load_vector) is a sparse (3 grids x elements) operator built once and
+        multiplied by the subcases' pressures."""
+        cases = self.load_cases
+        F = np.empty((self.ndof, len(cases)), order="F")
+        batch = len(cases) > 1 and self._identity_frames()
+        for k, c in enumerate(cases):
+            F[:, k] = self.load_vector(c, q4_pressure=not batch)
+        if batch:
+            groups: Dict[int, Tuple[np.ndarray, List[int]]] = {}
+            for k, c in enumerate(cases):
+                if c.pload4 is not None:
+                    groups.setdefault(id(c.pload4[0]), (c.pload4[0], []))[1].append(k)
+            for eidx, ks in groups.values():
+                A = self._pload4_operator(eidx)
+                P = np.empty((A.shape[1], len(ks)))
+                for j, k in enumerate(ks):
+                    P[:, j] = cases[k].pload4[1]
+                G = A @ P
+                for j, k in enumerate(ks):
+                    F[:, k].reshape(-1, 6)[:, 0:3] += G[:, j].reshape(-1, 3)
         return F
+
+    def _pload4_operator(self, eidx: np.ndarray):
+        """CSC (3 n_nodes x len(eidx)): nodal force of a unit PLOAD4 on each
+        listed CQUAD4 (cached for the element list and coordinates it was built
+        from)."""
+        import scipy.sparse as sp
+        c = getattr(self, "_p4_cache", None)
+        if c is not None and c[0] is eidx and c[1] is self.xyz:
+            return c[2]
+        nodes = self.q4_nodes[eidx]
+        X = self.xyz
+        nv = np.cross(X[nodes[:, 2]] - X[nodes[:, 0]], X[nodes[:, 3]] - X[nodes[:, 1]])
+        nn = np.linalg.norm(nv, axis=1)
+        fdir = (nv / nn[:, None]) * (0.5 * nn / 4.0)[:, None]
+        ne = len(eidx)
+        # column e holds the element's 12 entries (4 grids x 3 components)
+        rows = (3 * nodes[:, :, None] + np.arange(3)[None, None, :]).reshape(-1)
+        vals = np.broadcast_to(fdir[:, None, :], (ne, 4, 3)).reshape(-1)
+        A = sp.csc_matrix((vals, rows, np.arange(0, 12 * ne + 1, 12)), shape=(3 * self.n_nodes, ne))
+        self._p4_cache = (eidx, self.xyz, A)
+        return A
 
     def spc_dofs(self) -> np.ndarray:
         """SPC1 DOFs (boundary_conditions.jl:1499-1540)."""
