@@ -190,8 +190,10 @@ def prepare(backend: JFEMGPUBackend, model, donor: Optional["lib.DeviceModel"] =
     diag, max_elem = dm.diag()
     blocks = dm.node_blocks()
     free, fixed, bc = compute_free_dofs(model, diag, blocks, backend.eps_zero)
+    t_sym = time.perf_counter()
     dm.set_free_dofs(free)
     timings["constraints"] = time.perf_counter() - t1
+    timings["symbolic"] = time.perf_counter() - t_sym
     if before_factor is not None:
         before_factor(dm)
     t2 = time.perf_counter()
