@@ -613,6 +613,16 @@ def serving_specs(n_req: int, seed: int):
     return specs
 
 
+def _pinned(a: np.ndarray) -> np.ndarray:
+    """Column-major copy of a host load matrix in page-locked memory (the
+    client's input buffers of the host-buffer pass)."""
+    import torch
+    t = torch.empty((a.shape[1], a.shape[0]), dtype=torch.float64, pin_memory=True)
+    out = t.numpy().T
+    out[...] = a
+    return out
+
+
 class StreamModels:
     """Host models and load matrices of a request list (built before timing)."""
 
@@ -626,14 +636,14 @@ class StreamModels:
             if sp["kind"] in ("panel", "wing", "solid"):
                 m = self._model(sp)
                 self.models[i] = m
-                self.loads[i] = m.load_matrix()
+                self.loads[i] = _pinned(m.load_matrix())
         for i, sp in enumerate(specs):
             if sp["kind"] in ("resolve", "update"):
                 base = self.loads[sp["target"]]
                 rng = np.random.default_rng(sp["seed"])
                 cols = [base[:, c % base.shape[1]] * rng.uniform(0.5, 2.0) +
                         base[:, (c + 1) % base.shape[1]] * rng.uniform(-0.5, 0.5) for c in range(sp["nrhs"])]
-                self.loads[i] = np.asfortranarray(np.stack(cols, axis=1))
+                self.loads[i] = _pinned(np.stack(cols, axis=1))
                 if sp["kind"] == "update":
                     sect = self.models[sp["target"]].q4_sections().copy()
                     f = sp["scale"]          # thickness scale: Cm, Cs, h ~ t; Cb ~ t^3
@@ -684,7 +694,10 @@ def stream_pass(srv, specs, sm: StreamModels, device: bool, rate: float = 0.0, s
     def submit(i):
         sp = specs[i]
         if sp["kind"] in ("panel", "wing", "solid"):
-            chain(i, srv.solve(sm.models[i], device_loads=dev_loads.get(i)))
+            if device:
+                chain(i, srv.solve(sm.models[i], device_loads=dev_loads[i]))
+            else:
+                chain(i, srv.solve(sm.models[i], loads=sm.loads[i]))
             return
         tf = proxies[sp["target"]]
         if tf.exception() is not None:      # its model never became resident

@@ -189,3 +189,34 @@ def test_mixed_server_moves_slow_meshes_to_the_fp64_factor():
         assert _rel(rb["U"], Ub) <= DISP_RTOL
     finally:
         srv.close()
+
+
+@pytest.mark.parametrize("prec", [lib.PREC_FP64, lib.PREC_MIXED])
+def test_server_wing_boxes_and_solids_against_the_oracle(oracle_mod, prec):
+    """Two wing-box panels of one mesh and two CTETRA10 blocks of one mesh,
+    queued together on a four-slot server (single-model requests: the
+    second model of each mesh waits for the first and shares its pattern
+    and analysis), one of each with host load matrices passed in, and a
+    re-solve of a block: every result equals the FP64 oracle's within the
+    parity tolerance, on both precisions."""
+    base = M.wing_panel(nx=24, ny=36, n_blades=3, blade_nz=4, n_cases=1, seed=5)
+    wings = [M.wing_panel_variant(base, s, 3) for s in (1, 2)]
+    blocks = [M.solid_block(n=6, n_cases=2, seed=s) for s in (3, 4)]
+    srv = S.SolveServer(slots=4, precision=prec, tol=RESID_TOL, small_dof=1000, pack_dof=2000)
+    try:
+        futs = [srv.solve(wings[0]), srv.solve(wings[1], loads=wings[1].load_matrix()),
+                srv.solve(blocks[0]), srv.solve(blocks[1], loads=blocks[1].load_matrix())]
+        res = [f.result(timeout=900) for f in futs]
+        assert srv.shared_structures >= 2
+        for mdl, r in zip(wings + blocks, res):
+            ref = oracle_mod.solve_reference(mdl)
+            assert _rel(r["U"], ref["u"]) <= DISP_RTOL
+            assert r["rel_residual"].max() <= RESID_TOL
+        F2 = 3.0 * blocks[0].load_matrix()
+        r2 = srv.resolve(res[2]["key"], F2).result(timeout=900)
+        ref = oracle_mod.solve_reference(blocks[0])
+        assert _rel(r2["U"], 3.0 * ref["u"]) <= DISP_RTOL
+        tl = srv.stats()["timeline"]
+        assert tl["shell"]["n"] == 2 and tl["solid"]["n"] == 2
+    finally:
+        srv.close()
