@@ -907,6 +907,94 @@ k_front_update_dmma(const int32_t* __restrict__ list, const int32_t* __restrict_
   }
 }
 
+// FP64 panel triangular solve on the FP64 tensor cores: rows [k1 + 64 tb,
+// +64) of panel columns [k0, k1) become X Dinv^T, a 64 x kn x kn product
+// (Dinv is stored with zeros above its diagonal, so the dense product is
+// the triangular one).  Same tiles as k_trsm_panel; 4 warps, each 32 rows x
+// 32 columns of the 64 x 64 output, K in slices of 16 double-buffered in
+// shared memory (the layout of k_front_update_dmma: As[k][row],
+// Bs[k][col] with Bs[q][l] = Dinv[l][q]).  Every read of the CTA's rows
+// happens before the barrier that ends the K loop, so the result is
+// written in place.
+__global__ void __launch_bounds__(128)
+k_trsm_panel_dmma(const int32_t* __restrict__ list, const int32_t* __restrict__ first,
+                  const int32_t* __restrict__ mrows, const int64_t* __restrict__ Lptr,
+                  const int64_t* __restrict__ Dptr, double* __restrict__ L, const double* __restrict__ Dinv,
+                  int k0, const int2* __restrict__ tiles) {
+  int tq, tb;
+  tile_of(tiles, tq, tb);
+  const int s = list[tq];
+  const int c = first[s + 1] - first[s];
+  if (k0 >= c) return;
+  const int m = mrows[s];
+  const int k1 = min(k0 + NB, c), kn = k1 - k0;
+  const int row0 = k1 + tb * 64;
+  if (row0 >= m) return;
+  const int nrow = min(64, m - row0);
+  __shared__ double As[2][16][DM_LD];
+  __shared__ double Bs[2][16][DM_LD];
+  const double* Dv = Dinv + Dptr[s] + (int64_t)(k0 / NB) * NB * NB;
+  double* X = L + Lptr[s] + row0 + (int64_t)m * k0;   // X[r + m q], r < nrow, q < kn
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wr = warp >> 1, wc = warp & 1;
+  const int g = lane >> 2, q4 = lane & 3;
+  double ra[8], rb[8];
+  // loader: element e = tid + 128 j -> row / column e & 63, k (e >> 6) in [0, 16)
+  auto gload = [&](int k) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int e = tid + 128 * j, r = e & 63, kk = k + (e >> 6);
+      ra[j] = (kk < kn && r < nrow) ? X[r + (int64_t)m * kk] : 0.0;
+      rb[j] = (kk < kn && r < kn) ? Dv[r + NB * kk] : 0.0;
+    }
+  };
+  auto sstore = [&](int buf) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int e = tid + 128 * j, r = e & 63, kk = e >> 6;
+      As[buf][kk][r] = ra[j];
+      Bs[buf][kk][r] = rb[j];
+    }
+  };
+  double acc[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+  gload(0);
+  sstore(0);
+  __syncthreads();
+  int buf = 0;
+  for (int k = 0; k < kn; k += 16) {
+    const bool more = k + 16 < kn;
+    if (more) gload(k + 16);
+#pragma unroll
+    for (int k4 = 0; k4 < 16; k4 += 4) {
+      double af[4], bf[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) af[a] = As[buf][k4 + q4][wr * 32 + a * 8 + g];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) bf[b] = Bs[buf][k4 + q4][wc * 32 + b * 8 + g];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) dmma_884(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+    }
+    if (more) sstore(buf ^ 1);
+    __syncthreads();
+    buf ^= 1;
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int i = wr * 32 + a * 8 + g, j = wc * 32 + b * 8 + 2 * q4 + h;
+        if (i < nrow && j < kn) X[i + (int64_t)m * j] = acc[a][b][h];
+      }
+}
+
 // smallest level output (rows) handed to the tensor-core update kernel
 inline int tc_min_dim() {
   const char* e = std::getenv("JFG_TC_MIN");
@@ -916,6 +1004,17 @@ inline int tc_min_dim() {
 inline bool dmma_enabled() {
   const char* e = std::getenv("JFG_DMMA");
   return !(e && e[0] == '0');
+}
+
+// FP64 panel triangular solves on the FP64 tensor cores (JFG_DMMA_TRSM=0:
+// the SIMT kernel)
+inline bool dmma_trsm() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = std::getenv("JFG_DMMA_TRSM");
+    v = (e && e[0] == '0') ? 0 : (dmma_enabled() ? 1 : 0);
+  }
+  return v == 1;
 }
 
 // one launch of the front update for a level: DMMA for the FP64 factor,
@@ -1605,10 +1704,22 @@ jfg_status factor_levels(jfg_model* m, NumericFactor* F, T* Lf, T* Uf, T* Dvf, b
         int rows_max = lv.maxm(na) - k0 - 1;
         if (rows_max <= 0) continue;
         const auto& tsp = lv.trsm[k0 / NB];
-        if (tsp.cnt > 0) { int ps_ = fine_prof() ? prof_start(st) : -1; { k_trsm_panel<T><<<(unsigned)tsp.cnt, 256, 2 * NB * (NB + 1) * sizeof(T), st>>>(list, F->first, F->mrows,
-                                                                                        F->Lptr, F->Dptr, Lf, Dvf, k0,
-                                                                                        tc ? F->Phi : nullptr, F->Plo, F->PKptr,
-                                                                                        F->tiles + tsp.off);
+        if (tsp.cnt > 0) { int ps_ = fine_prof() ? prof_start(st) : -1; {
+          if constexpr (sizeof(T) == 8) {
+            if (dmma_trsm())
+              k_trsm_panel_dmma<<<(unsigned)tsp.cnt, 128, 0, st>>>(list, F->first, F->mrows, F->Lptr, F->Dptr,
+                                                                   reinterpret_cast<double*>(Lf),
+                                                                   reinterpret_cast<const double*>(Dvf), k0,
+                                                                   F->tiles + tsp.off);
+            else
+              k_trsm_panel<T><<<(unsigned)tsp.cnt, 256, 2 * NB * (NB + 1) * sizeof(T), st>>>(
+                  list, F->first, F->mrows, F->Lptr, F->Dptr, Lf, Dvf, k0, nullptr, F->Plo, F->PKptr,
+                  F->tiles + tsp.off);
+          } else {
+            k_trsm_panel<T><<<(unsigned)tsp.cnt, 256, 2 * NB * (NB + 1) * sizeof(T), st>>>(
+                list, F->first, F->mrows, F->Lptr, F->Dptr, Lf, Dvf, k0, tc ? F->Phi : nullptr, F->Plo, F->PKptr,
+                F->tiles + tsp.off);
+          }
           count_launch(); } prof_end(ps_, st, KS_F_TRSM, trsm_flops(na, k0)); }
         const int nu = lv.active(k0 + NB);   // fronts with columns after this block
         int nrow = lv.maxm(nu) - k0 - NB, ncol = std::min(P1, lv.max_c) - k0 - NB;
