@@ -510,7 +510,7 @@ class SolveServer:
         r.dm.close()
         self.mem_cv.notify_all()
 
-    def _admit(self, need: float, wait: bool = False, own: float = 0.0):
+    def _admit(self, need: float, wait: bool = False, own: float = 0.0, keep: Optional[int] = None):
         """Free least-recently-used residents until `need` more bytes fit, and
         reserve them for the model being prepared (released by _register).
 
@@ -523,7 +523,10 @@ class SolveServer:
         lock is held.  ``own``: bytes this request reserved already (its
         upload estimate); with nothing resident and every reservation held by
         requests that are themselves waiting here, nothing can be released,
-        so the request is admitted at once.
+        so the request is admitted at once.  ``keep``: id of a group's device
+        model that this request has pinned (its structure donor); it is not
+        freed, and when nothing but it is left the request is admitted over
+        budget instead of waiting.
         """
         with self.rlock:
             deadline = time.perf_counter() + self.wait_s
@@ -531,7 +534,10 @@ class SolveServer:
             waiting = False
             try:
                 while self.resident_bytes + self.reserved + need > self.budget:
-                    cands = [k for k in self.registry if id(self.registry[k].dm) not in busy]
+                    cands = [k for k in self.registry if id(self.registry[k].dm) not in busy
+                             and id(self.registry[k].dm) != keep]
+                    if not cands and keep is not None and not busy:
+                        break          # only the pinned donor is left
                     if not cands:
                         if not waiting:
                             waiting = True
@@ -620,26 +626,33 @@ class SolveServer:
             prec = lib.PREC_FP64
             with self.rlock:
                 self.fp64_factorisations += 1
-        pre = self._upload_estimate(target)
-        self._admit(pre, wait=True)
-        admitted = [pre]
-        t_up = time.perf_counter()
-        try:
-            dm = lib.DeviceModel(be.ctx, target)
-        except Exception:
-            self._release(pre)
-            raise
+        # the resident model of this mesh is pinned before the admission, so
+        # that making room for the new model never frees the structure it is
+        # about to take over (eviction skips pinned groups)
         donor = None
         if mk is not None:
             with self.rlock:
                 dk = self.meshes.get(mk)
                 donor = self.registry.get(dk) if dk is not None else None
-        if donor is not None:
-            with donor.pin:
-                if not donor.evicted:
-                    dm.share_structure(donor.dm)
-                    with self.rlock:
-                        self.shared_structures += 1
+            if donor is not None and not donor.pin.acquire(timeout=60.0):
+                donor = None
+        try:
+            pre = self._upload_estimate(target)
+            self._admit(pre, wait=True, keep=id(donor.dm) if donor is not None else None)
+            admitted = [pre]
+            t_up = time.perf_counter()
+            try:
+                dm = lib.DeviceModel(be.ctx, target)
+            except Exception:
+                self._release(pre)
+                raise
+            if donor is not None and not donor.evicted:
+                dm.share_structure(donor.dm)
+                with self.rlock:
+                    self.shared_structures += 1
+        finally:
+            if donor is not None:
+                donor.pin.release()
 
         def admit(d):
             need = float(d.memory(prec, nrhs)[1])

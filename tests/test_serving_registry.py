@@ -185,3 +185,24 @@ def test_dispatch_waits_when_only_deferred_work_is_queued(server):
         server.plock.notify_all()
     t.join(timeout=5)
     assert got and got[0][0].model is a2
+
+
+def test_admission_keeps_the_pinned_structure_donor(server):
+    """A new model pins the resident model whose structure it will take over
+    before its admission: room is made by freeing other groups, never the
+    donor, and with only the donor left the request is admitted over budget
+    at once instead of waiting for it."""
+    dm_a, keys_a = _group(server, 1, 50.0)     # the donor (least recently used)
+    dm_b, keys_b = _group(server, 1, 50.0)
+    server._lookup(keys_b[0])
+    donor = server.registry[keys_a[0]]
+    with donor.pin:
+        server._admit(50.0, wait=True, keep=id(dm_a))
+        assert dm_a.closed == 0 and dm_b.closed == 1
+        assert keys_a[0] in server.registry
+        import time as _t
+        t0 = _t.perf_counter()
+        server._admit(80.0, wait=True, keep=id(dm_a))   # nothing else to free
+        assert _t.perf_counter() - t0 < 1.0
+        assert dm_a.closed == 0
+    server._release(130.0)
