@@ -175,3 +175,33 @@ def test_autotune_candidates_cover_update_kernels():
     given = [{"JFG_ND_LEAF": "16"}]
     assert AT.candidate_list(lib.PREC_MIXED, given) == given
     assert "JFG_TENSOR_CORES" in AT.KNOBS
+
+
+@pytest.mark.parametrize("mk", [
+    lambda: M.wing_panel_variant(M.wing_panel(nx=24, ny=36, n_blades=3, blade_nz=4, n_cases=1), 7, 5),
+    lambda: M.stiffened_panel(11, n_cases=6),
+    lambda: M.flat_plate(),
+], ids=["wing_variant", "stiffened_panel", "plate"])
+def test_load_matrix_batches_pressures_like_per_case_vectors(oracle_mod, mk):
+    """load_matrix applies the CQUAD4 PLOAD4 of all subcases through one
+    sparse unit-pressure operator; every column equals load_vector of its
+    subcase and the oracle's independent restatement (loads.jl:546-585)."""
+    m = mk()
+    F = m.load_matrix()
+    ref = np.stack([m.load_vector(c) for c in m.load_cases], axis=1)
+    scale = max(np.abs(ref).max(), 1e-300)
+    assert np.abs(F - ref).max() <= 1e-14 * scale
+    assert np.abs(F - oracle_mod.load_matrix(m)).max() <= 1e-13 * scale
+    # a second call reuses the operator and gives the same matrix
+    assert np.array_equal(m.load_matrix(), F)
+
+
+def test_section_records_gathered_per_pshell():
+    """q4_sections gathers one record per PSHELL: every element carries its
+    own PSHELL's record."""
+    m = M.wing_panel_variant(M.wing_panel(nx=24, ny=36, n_blades=3, blade_nz=4, n_cases=1), 3, 1)
+    S = m.q4_sections()
+    assert S.shape == (len(m.q4_pid), M.Q4_SECT_STRIDE)
+    for pid in np.unique(m.q4_pid)[:20]:
+        rec = np.asarray(M._q4_section_record(m, int(pid)))
+        assert np.array_equal(S[m.q4_pid == pid], np.broadcast_to(rec, (int((m.q4_pid == pid).sum()), len(rec))))
